@@ -1,0 +1,446 @@
+// extern "C" entry points of libcuotf (declared in include/binsim_cuotf.h).
+#include "../../include/binsim_cuotf.h"
+#include "dav.h"
+#include "vqe.h"
+
+#include <cstdio>
+#include <mutex>
+
+using bsim::DevBasis;
+using bsim::DevNet;
+using bsim::i64;
+
+namespace {
+
+using Basis = DevBasis<unsigned>;
+using Net = DevNet<unsigned>;
+
+int check(void *b, void *n)
+{
+    if (!bsim::valid(static_cast<Basis *>(b))) { bsim::set_error("invalid basis handle"); return BSIM_ERR_ARG; }
+    if (n && !bsim::valid(static_cast<Net *>(n))) { bsim::set_error("invalid network handle"); return BSIM_ERR_ARG; }
+    return BSIM_OK;
+}
+
+Basis *B(void *p) { return static_cast<Basis *>(p); }
+Net *N(void *p) { return static_cast<Net *>(p); }
+
+// Legacy entry points report like the reference (stderr) but do not exit.
+void report(int st, const char *where)
+{
+    if (st != BSIM_OK) fprintf(stderr, "libcuotf %s: %s (status %d)\n", where, bsim::last_error(), st);
+}
+
+// A result slot for the synchronous legacy grad/backgrad: one device double per
+// basis handle, allocated on first use.
+double *result_slot(Basis *b)
+{
+    double *p = nullptr;
+    const size_t ns = (size_t)bsim::pair_grid(b);
+    // partials [ns] + ticket + result: reuse the workspace, keeping its layout
+    if (b->ws.partials(ns + 2, &p) != BSIM_OK) return nullptr;
+    return p + ns + 1;
+}
+
+std::mutex g_dav_mu;
+bsim::DavScratch &dav_scratch()
+{
+    static bsim::DavScratch S;
+    return S;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ============================== Part 1 ======================================
+void sync_device_cuda(void) { cudaDeviceSynchronize(); }
+
+void *build_basisdev_f64(void *host_basis)
+{
+    Basis *out = nullptr;
+    int st = bsim::basis_from_ref_handle(host_basis, &out);
+    report(st, "build_basisdev_f64");
+    return out;
+}
+
+void destroy_basisdev_f64(void *basis)
+{
+    if (basis && bsim::valid(B(basis))) delete B(basis);
+}
+
+void *build_networkdev_f64(void *host_net)
+{
+    Net *out = nullptr;
+    int st = bsim::network_from_ref_handle(host_net, &out);
+    report(st, "build_networkdev_f64");
+    return out;
+}
+
+void destroy_networkdev_f64(void *net)
+{
+    if (net && bsim::valid(N(net))) delete N(net);
+}
+
+void hvec_cuda(void *basis, void *net, const double *src, double *dst)
+{
+    report(bsim_hvec(basis, net, src, dst, nullptr), "hvec_cuda");
+}
+
+void get_diags_elements_cuda(void *basis, void *net, double *diags)
+{
+    report(bsim_diag(basis, net, diags, nullptr), "get_diags_elements_cuda");
+}
+
+void expm_cuda(void *basis, void *net, int64_t idx, double theta, double *vec)
+{
+    report(bsim_expm(basis, net, idx, theta, vec, nullptr), "expm_cuda");
+}
+
+static double legacy_scalar(void *basis, void *net, int64_t idx, double theta, double *l, double *r, bool back,
+                            const char *name)
+{
+    int st = check(basis, net);
+    double h = 0.0;
+    if (st == BSIM_OK) {
+        double *slot = result_slot(B(basis));
+        if (!slot) st = BSIM_ERR_ALLOC;
+        else {
+            st = back ? bsim::backgrad(B(basis), N(net), idx, theta, l, r, slot, false, nullptr)
+                      : bsim::grad(B(basis), N(net), idx, theta, l, r, slot, false, nullptr);
+            if (st == BSIM_OK) {
+                cudaError_t e = cudaMemcpy(&h, slot, sizeof(double), cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess) st = bsim::cuda_status(e, name);
+            }
+        }
+    }
+    report(st, name);
+    return h;
+}
+
+double grad_cuda(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r)
+{
+    return legacy_scalar(basis, net, idx, theta, const_cast<double *>(l), const_cast<double *>(r), false, "grad_cuda");
+}
+
+double backgrad_cuda(void *basis, void *net, int64_t idx, double theta, double *l, double *r)
+{
+    return legacy_scalar(basis, net, idx, theta, l, r, true, "backgrad_cuda");
+}
+
+void batchgrad_cuda(void *basis, void *net, const double *thetas, const double *l, const double *r, double *grads)
+{
+    report(bsim_batchgrad(basis, net, thetas, l, r, grads, nullptr), "batchgrad_cuda");
+}
+
+void expm_cuda_2d(void *basis, void *net, int64_t idx, double theta, double *vec)
+{
+    expm_cuda(basis, net, idx, theta, vec);
+}
+
+double grad_cuda_2d(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r)
+{
+    return grad_cuda(basis, net, idx, theta, l, r);
+}
+
+double backgrad_cuda_2d(void *basis, void *net, int64_t idx, double theta, double *l, double *r)
+{
+    return backgrad_cuda(basis, net, idx, theta, l, r);
+}
+
+// ============================== Part 2 ======================================
+const char *bsim_last_error(void) { return bsim::last_error(); }
+const char *bsim_version(void) { return "libcuotf sm_100a 0.1"; }
+
+int bsim_basis_create_u32(int64_t norb, int64_t na, int64_t nb, int64_t total_sym, const int64_t *orbsym,
+                          int64_t num_irreps, void **out)
+{
+    if (!out) { bsim::set_error("null out"); return BSIM_ERR_NULL; }
+    Basis *b = nullptr;
+    int st = bsim::make_basis<unsigned>(norb, na, nb, total_sym, (const i64 *)orbsym, num_irreps, &b);
+    *out = b;
+    return st;
+}
+
+int bsim_basis_from_host(void *host_basis, void **out)
+{
+    if (!out) { bsim::set_error("null out"); return BSIM_ERR_NULL; }
+    Basis *b = nullptr;
+    int st = bsim::basis_from_ref_handle(host_basis, &b);
+    *out = b;
+    return st;
+}
+
+int bsim_basis_destroy(void *basis)
+{
+    int st = check(basis, nullptr);
+    if (st == BSIM_OK) delete B(basis);
+    return st;
+}
+
+int64_t bsim_basis_dim(void *basis) { return check(basis, nullptr) == BSIM_OK ? B(basis)->dim : -1; }
+
+int64_t bsim_basis_find_det(void *basis, uint64_t astr, uint64_t bstr)
+{
+    return check(basis, nullptr) == BSIM_OK ? B(basis)->find_det(astr, bstr) : -1;
+}
+
+int bsim_network_create_u32(const int64_t *orbsym, int64_t norb, int64_t ngs, const uint32_t *axs,
+                            const uint32_t *bxs, const int64_t *ranks, const int64_t *num_zas,
+                            const int64_t *num_zbs, const uint32_t *flat_zas, const uint32_t *flat_zbs,
+                            const double *flat_wa, const double *flat_wb, void **out)
+{
+    if (!out) { bsim::set_error("null out"); return BSIM_ERR_NULL; }
+    Net *n = nullptr;
+    int st = bsim::make_network<unsigned>((const i64 *)orbsym, norb, ngs, axs, bxs, (const i64 *)ranks,
+                                          (const i64 *)num_zas, (const i64 *)num_zbs, flat_zas, flat_zbs, flat_wa,
+                                          flat_wb, &n);
+    *out = n;
+    return st;
+}
+
+int bsim_network_from_host(void *host_net, void **out)
+{
+    if (!out) { bsim::set_error("null out"); return BSIM_ERR_NULL; }
+    Net *n = nullptr;
+    int st = bsim::network_from_ref_handle(host_net, &n);
+    *out = n;
+    return st;
+}
+
+int bsim_network_destroy(void *net)
+{
+    if (!bsim::valid(N(net))) { bsim::set_error("invalid network handle"); return BSIM_ERR_ARG; }
+    delete N(net);
+    return BSIM_OK;
+}
+
+int64_t bsim_network_ngs(void *net) { return bsim::valid(N(net)) ? N(net)->ngs : -1; }
+
+#define CHECK2(b, n) do { int st__ = check(b, n); if (st__ != BSIM_OK) return st__; } while (0)
+#define NEED(p) do { if (!(p)) { bsim::set_error("null pointer argument: %s", #p); return BSIM_ERR_NULL; } } while (0)
+
+int bsim_hvec(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(src); NEED(dst);
+    return bsim::sigma(B(basis), N(net), src, nullptr, dst, false, stream);
+}
+
+int bsim_hvec_mixed(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(src); NEED(dst);
+    return bsim::sigma(B(basis), N(net), src, nullptr, dst, true, stream);
+}
+
+int bsim_hvec_f32in(void *basis, void *net, const float *src, double *dst, bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(src); NEED(dst);
+    return bsim::sigma(B(basis), N(net), nullptr, src, dst, true, stream);
+}
+
+int bsim_diag(void *basis, void *net, double *diags, bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(diags);
+    return bsim::diag_elements(B(basis), N(net), diags, stream);
+}
+
+int bsim_expm(void *basis, void *net, int64_t idx, double theta, double *vec, bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(vec);
+    return bsim::expm(B(basis), N(net), idx, theta, vec, stream);
+}
+
+int bsim_expm_seq(void *basis, void *net, int64_t n, const int64_t *idx, const double *theta, double *vec,
+                  bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(vec);
+    if (n > 0) { NEED(idx); NEED(theta); }
+    for (int64_t i = 0; i < n; ++i) {
+        int st = bsim::expm(B(basis), N(net), idx[i], theta[i], vec, stream);
+        if (st != BSIM_OK) return st;
+    }
+    return BSIM_OK;
+}
+
+int bsim_grad(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r,
+              double *out_dev, bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(l); NEED(r); NEED(out_dev);
+    return bsim::grad(B(basis), N(net), idx, theta, l, r, out_dev, false, stream);
+}
+
+int bsim_backgrad(void *basis, void *net, int64_t idx, double theta, double *l, double *r, double *out_dev,
+                  bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(l); NEED(r); NEED(out_dev);
+    return bsim::backgrad(B(basis), N(net), idx, theta, l, r, out_dev, false, stream);
+}
+
+int bsim_batchgrad(void *basis, void *net, const double *thetas, const double *l, const double *r, double *grads,
+                   bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(thetas); NEED(l); NEED(r); NEED(grads);
+    return bsim::batchgrad(B(basis), N(net), thetas, l, r, grads, stream);
+}
+
+int bsim_prepare_state(void *basis, void *pool, int64_t n_ops, const int64_t *op_idx, const int64_t *param_idx,
+                       const double *thetas, const int64_t *ref_idx, const double *ref_val, int64_t n_ref,
+                       double *vec, bsim_stream_t stream)
+{
+    CHECK2(basis, pool);
+    NEED(vec);
+    if (n_ops > 0) { NEED(op_idx); NEED(param_idx); NEED(thetas); }
+    if (n_ref > 0) { NEED(ref_idx); NEED(ref_val); }
+    for (int64_t i = 0; i < n_ops; ++i)
+        if (op_idx[i] < 0 || op_idx[i] >= N(pool)->ngs || param_idx[i] < 0) {
+            bsim::set_error("op_idx/param_idx[%lld] out of range", (long long)i);
+            return BSIM_ERR_ARG;
+        }
+    return bsim::prepare_state(B(basis), N(pool), n_ops, (const i64 *)op_idx, (const i64 *)param_idx, thetas,
+                               (const i64 *)ref_idx, ref_val, n_ref, vec, stream);
+}
+
+int bsim_vqe_energy_grad(void *basis, void *ham, void *pool, int64_t n_ops, const int64_t *op_idx,
+                         const int64_t *param_idx, int64_t n_params, const double *thetas, const int64_t *ref_idx,
+                         const double *ref_val, int64_t n_ref, int64_t ckpt_every, double *lv, double *rv,
+                         double *energy, double *variance, double *grad, bsim_stream_t stream)
+{
+    CHECK2(basis, ham);
+    CHECK2(basis, pool);
+    NEED(lv); NEED(rv);
+    if (n_ops > 0) { NEED(op_idx); NEED(param_idx); NEED(thetas); }
+    if (n_ref > 0) { NEED(ref_idx); NEED(ref_val); }
+    return bsim::vqe_energy_grad(B(basis), N(ham), N(pool), n_ops, (const i64 *)op_idx, (const i64 *)param_idx,
+                                 n_params, thetas, (const i64 *)ref_idx, ref_val, n_ref, ckpt_every, lv, rv, energy,
+                                 variance, grad, stream);
+}
+
+int bsim_davidson(void *basis, void *net, double *v0, const double *diags, double tol, int maxiter, int ncv,
+                  int maxspace, int mixed, double *x_out, double *energy, double *residual, int *iterations,
+                  int *sigma_fp64, int *sigma_fp32, int verbose, bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(v0); NEED(diags); NEED(x_out);
+    bsim::DavStats st{};
+    int rc = mixed ? bsim::davidson_mixed(B(basis), N(net), v0, diags, tol, maxiter, maxspace, x_out, &st, verbose,
+                                          stream)
+                   : bsim::davidson_fp64(B(basis), N(net), v0, diags, tol, maxiter, ncv, maxspace, x_out, &st,
+                                         verbose, stream);
+    if (rc == BSIM_OK) {
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) rc = bsim::cuda_status(e, "davidson");
+    }
+    if (energy) *energy = st.energy;
+    if (residual) *residual = st.residual;
+    if (iterations) *iterations = st.iterations;
+    if (sigma_fp64) *sigma_fp64 = st.sigma_fp64;
+    if (sigma_fp32) *sigma_fp32 = st.sigma_fp32;
+    return rc;
+}
+
+// ============================== Part 3 ======================================
+static double fetch1(const double *dev)
+{
+    double h = 0.0;
+    cudaError_t e = cudaMemcpy(&h, dev, sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) report(bsim::cuda_status(e, "davidson helper"), "davidson helper");
+    return h;
+}
+
+double build_ritz_and_residual_cuda(int64_t N, int dim, const double *coeffs, double min_e, const double **V,
+                                    const double **AV, double *axt)
+{
+    std::lock_guard<std::mutex> g(g_dav_mu);
+    auto &S = dav_scratch();
+    int st = S.ensure();
+    if (st == BSIM_OK) st = bsim::dav_ritz_residual<double>(S, N, dim, coeffs, min_e, V, AV, axt, S.res, nullptr);
+    report(st, "build_ritz_and_residual_cuda");
+    return st == BSIM_OK ? fetch1(S.res) : 0.0;
+}
+
+void build_ritz_vector_cuda(int64_t N, int dim, const double *coeffs, const double **V, double *xt)
+{
+    int st = bsim::dav_combine<double, double>(N, dim, coeffs, V, xt, nullptr);
+    if (st == BSIM_OK) cudaDeviceSynchronize();
+    report(st, "build_ritz_vector_cuda");
+}
+
+void apply_preconditioner_inplace_cuda(int64_t N, double *axt, const double *diags, double min_e, double shift)
+{
+    std::lock_guard<std::mutex> g(g_dav_mu);
+    auto &S = dav_scratch();
+    int st = bsim::dav_precondition(S, N, axt, diags, min_e, shift, nullptr, nullptr);
+    if (st == BSIM_OK) cudaDeviceSynchronize();
+    report(st, "apply_preconditioner_inplace_cuda");
+}
+
+double mgs_orthogonalize_cuda(int64_t N, int dim, const double **V, double *vt)
+{
+    std::lock_guard<std::mutex> g(g_dav_mu);
+    auto &S = dav_scratch();
+    int st = S.ensure();
+    if (st == BSIM_OK) st = bsim::dav_mgs<double>(S, N, dim, V, vt, S.res + bsim::kMaxSub, nullptr);
+    report(st, "mgs_orthogonalize_cuda");
+    return st == BSIM_OK ? fetch1(S.res + bsim::kMaxSub) : 0.0;
+}
+
+double inplace_normalize_cuda(int64_t N, double *vec)
+{
+    std::lock_guard<std::mutex> g(g_dav_mu);
+    auto &S = dav_scratch();
+    int st = S.ensure();
+    if (st == BSIM_OK) st = bsim::dav_normalize(S, N, vec, S.res, nullptr);
+    report(st, "inplace_normalize_cuda");
+    return st == BSIM_OK ? fetch1(S.res) : 0.0;
+}
+
+double fast_dot_cuda(int64_t N, const double *v1, const double *v2)
+{
+    std::lock_guard<std::mutex> g(g_dav_mu);
+    auto &S = dav_scratch();
+    int st = S.ensure();
+    if (st == BSIM_OK) st = bsim::dav_dot(S, N, v1, v2, S.res, nullptr);
+    report(st, "fast_dot_cuda");
+    return st == BSIM_OK ? fetch1(S.res) : 0.0;
+}
+
+void compute_heff_col_cuda(int64_t N, int dim, const double **V, const double *AV_dim, double *out_col)
+{
+    std::lock_guard<std::mutex> g(g_dav_mu);
+    auto &S = dav_scratch();
+    int st = S.ensure();
+    if (st == BSIM_OK) st = bsim::dav_multidot<double, double>(S, N, dim, V, AV_dim, S.res, nullptr);
+    if (st == BSIM_OK) {
+        cudaError_t e = cudaMemcpy(out_col, S.res, sizeof(double) * dim, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = bsim::cuda_status(e, "compute_heff_col_cuda");
+    }
+    report(st, "compute_heff_col_cuda");
+}
+
+void rebuild_heff_cuda(int64_t N, int dim, const double **V, const double **AV, double *heff, int ldh)
+{
+    std::lock_guard<std::mutex> g(g_dav_mu);
+    auto &S = dav_scratch();
+    int st = S.ensure();
+    double col[bsim::kMaxSub];
+    for (int j = 0; j < dim && st == BSIM_OK; ++j) {
+        st = bsim::dav_multidot<double, double>(S, N, dim, V, AV[j], S.res, nullptr);
+        if (st == BSIM_OK) {
+            cudaError_t e = cudaMemcpy(col, S.res, sizeof(double) * dim, cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) st = bsim::cuda_status(e, "rebuild_heff_cuda");
+        }
+        for (int i = 0; i < dim && st == BSIM_OK; ++i) heff[i + (int64_t)j * ldh] = col[i];
+    }
+    report(st, "rebuild_heff_cuda");
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// Davidson vector operations and drivers (internal interface).
+#pragma once
+#include "ops.h"
+
+namespace bsim {
+
+constexpr int kMaxSub = 64;   // subspace limit, as the reference's 64-entry locals (diag/davidson.hpp:41)
+
+struct Coeffs { double v[kMaxSub]; };
+
+// Per-driver scratch for reductions: partials and small device result slots.
+struct DavScratch {
+    double *part = nullptr;
+    double *res = nullptr;   // kMaxSub + 8 device doubles
+    int ensure();
+    ~DavScratch();
+};
+
+template <typename TV>
+int dav_ritz_residual(DavScratch &S, i64 n, int k, const double *coeffs, double e, const TV *const *V,
+                      const TV *const *AV, double *axt, double *norm_dev, cudaStream_t s);
+template <typename TV, typename TX>
+int dav_combine(i64 n, int k, const double *coeffs, const TV *const *V, TX *x, cudaStream_t s);
+int dav_precondition(DavScratch &S, i64 n, double *r, const double *d, double e, double shift, double *norm_dev,
+                     cudaStream_t s);
+template <typename TV>
+int dav_mgs(DavScratch &S, i64 n, int k, const TV *const *V, double *v, double *norm_dev, cudaStream_t s);
+int dav_normalize(DavScratch &S, i64 n, double *v, double *norm_dev, cudaStream_t s);
+int dav_dot(DavScratch &S, i64 n, const double *a, const double *b, double *out_dev, cudaStream_t s);
+template <typename TV, typename TW>
+int dav_multidot(DavScratch &S, i64 n, int k, const TV *const *V, const TW *w, double *out_dev, cudaStream_t s);
+
+void jacobi_eigh(int k, const double *A, int lda, double *evals, double *evecs);
+
+// Result/statistics of a Davidson run.
+struct DavStats {
+    double energy;        // converged (or last) Ritz value
+    double residual;      // final FP64 residual norm
+    int iterations;       // subspace expansions (sigma applications after the first)
+    int sigma_fp64;       // FP64 sigma applications
+    int sigma_fp32;       // FP32-bulk sigma applications
+    int converged;        // 1 if the tolerance was met
+};
+
+// Plain FP64 single-root Davidson, jl/davidson.jl:1-185 on device vectors.
+// v0 (device, dim) is the start vector (normalised in place); diags (device)
+// the Hamiltonian diagonal; x_out (device, dim) receives the Ritz vector.
+template <typename Ti>
+int davidson_fp64(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const double *diags, double tol,
+                  int maxiter, int ncv, int maxspace, double *x_out, DavStats *stats, int verbose, cudaStream_t s);
+
+// Mixed precision: FP32 subspace storage and FP32-bulk sigma with FP64
+// accumulation inside, wrapped in FP64 residual refinement (outer loop on the
+// FP64 vector with an FP64 sigma).  Converges on the FP64 residual norm.
+template <typename Ti>
+int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const double *diags, double tol,
+                   int maxiter, int maxspace, double *x_out, DavStats *stats, int verbose, cudaStream_t s);
+
+}  // namespace bsim

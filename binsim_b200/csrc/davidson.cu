@@ -1,0 +1,340 @@
+// Davidson vector operations on device vectors and a device-resident Davidson
+// driver (reference diag/davidson.hpp:31-272 and jl/davidson.jl:1-185).
+//
+// All reductions are deterministic: a fixed grid writes per-CTA partials and a
+// single CTA sums them in index order.  The streaming kernels read each vector
+// once per call, so they run at HBM bandwidth: a k-vector Ritz/residual step
+// moves (2k + 1) * dim * 8 bytes.
+#include "dav.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace bsim {
+
+constexpr int kRedCtas = 148 * 8;
+constexpr int kRedThreads = 256;
+
+template <typename T>
+struct Ptrs { const T *p[kMaxSub]; };
+
+// ---- final reduction: out[j] = sum_b part[b * nout + j] ---------------------------
+__global__ void finish_kernel(const double *__restrict__ part, int nblk, int nout, double *__restrict__ out,
+                              int sqrt_out)
+{
+    __shared__ double red[32];
+    for (int j = 0; j < nout; ++j) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[(i64)b * nout + j];
+        s = warp_sum(s);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+            out[j] = sqrt_out ? sqrt(t) : t;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void cta_partial(double v, double *red, double *dst)
+{
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        *dst = t;
+    }
+    __syncthreads();
+}
+
+// axt = sum_j c_j AV_j - e sum_j c_j V_j ; partial |axt|^2   (davidson.hpp:31-69)
+template <typename TV>
+__global__ void ritz_residual_kernel(i64 n, int k, Coeffs c, double e, Ptrs<TV> V, Ptrs<TV> AV,
+                                     double *__restrict__ axt, double *__restrict__ part)
+{
+    __shared__ double red[32];
+    double s = 0.0;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        double x = 0.0, ax = 0.0;
+        for (int j = 0; j < k; ++j) {
+            x += c.v[j] * (double)V.p[j][i];
+            ax += c.v[j] * (double)AV.p[j][i];
+        }
+        const double rr = ax - e * x;
+        axt[i] = rr;
+        s += rr * rr;
+    }
+    cta_partial(s, red, part + blockIdx.x);
+}
+
+// x = sum_j c_j V_j  (davidson.hpp:71-95); TX may be float or double
+template <typename TV, typename TX>
+__global__ void combine_kernel(i64 n, int k, Coeffs c, Ptrs<TV> V, TX *__restrict__ x)
+{
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < k; ++j) s += c.v[j] * (double)V.p[j][i];
+        x[i] = (TX)s;
+    }
+}
+
+// r_i /= (d_i - e), denominator clamped to +-|shift|  (davidson.hpp:97-117)
+__global__ void precondition_kernel(i64 n, double *__restrict__ r, const double *__restrict__ d, double e,
+                                    double shift, double *__restrict__ part)
+{
+    __shared__ double red[32];
+    const double as = fabs(shift);
+    double s = 0.0;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        double diff = d[i] - e;
+        if (fabs(diff) < as) diff = (diff >= 0) ? as : -as;
+        const double v = r[i] / diff;
+        r[i] = v;
+        s += v * v;
+    }
+    if (part) cta_partial(s, red, part + blockIdx.x);
+}
+
+// One modified Gram-Schmidt step, fused with the next projection:
+// v -= p_prev * Vprev (p_prev read from device), partial <Vnext, v>.
+template <typename TV>
+__global__ void mgs_step_kernel(i64 n, double *__restrict__ v, const TV *__restrict__ vprev,
+                                const double *__restrict__ pprev, const TV *__restrict__ vnext,
+                                double *__restrict__ part)
+{
+    __shared__ double red[32];
+    const double p = vprev ? *pprev : 0.0;
+    double s = 0.0;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        double x = v[i];
+        if (vprev) { x -= p * (double)vprev[i]; v[i] = x; }
+        s += vnext ? (double)vnext[i] * x : x * x;
+    }
+    cta_partial(s, red, part + blockIdx.x);
+}
+
+__global__ void scale_kernel(i64 n, double *__restrict__ v, const double *__restrict__ nrm)
+{
+    const double inv = 1.0 / *nrm;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) v[i] *= inv;
+}
+
+// out_j partials = <V_j, w> for j < k (davidson.hpp:186-219)
+template <typename TV, typename TW>
+__global__ void multidot_kernel(i64 n, int k, Ptrs<TV> V, const TW *__restrict__ w, double *__restrict__ part)
+{
+    __shared__ double red[32];
+    double s[kMaxSub];
+    for (int j = 0; j < k; ++j) s[j] = 0.0;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        const double x = (double)w[i];
+        for (int j = 0; j < k; ++j) s[j] += (double)V.p[j][i] * x;
+    }
+    for (int j = 0; j < k; ++j) cta_partial(s[j], red, part + (i64)blockIdx.x * k + j);
+}
+
+__global__ void dot_kernel(i64 n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ part)
+{
+    __shared__ double red[32];
+    double s = 0.0;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) s += a[i] * b[i];
+    cta_partial(s, red, part + blockIdx.x);
+}
+
+// ---- host wrappers -----------------------------------------------------------------
+DavScratch::~DavScratch()
+{
+    if (part) cudaFree(part);
+    if (res) cudaFree(res);
+}
+
+int DavScratch::ensure()
+{
+    if (part) return BSIM_OK;
+    cudaError_t e = cudaMalloc(&part, sizeof(double) * kRedCtas * kMaxSub);
+    if (e != cudaSuccess) { part = nullptr; return cuda_status(e, "davidson scratch"); }
+    e = cudaMalloc(&res, sizeof(double) * (kMaxSub + 8));
+    if (e != cudaSuccess) { res = nullptr; return cuda_status(e, "davidson scratch"); }
+    return BSIM_OK;
+}
+
+static int grid_for(i64 n) { return (int)std::max<i64>(1, std::min<i64>(kRedCtas, (n + kRedThreads - 1) / kRedThreads)); }
+
+template <typename TV>
+static Ptrs<TV> pack(const TV *const *v, int k)
+{
+    Ptrs<TV> p{};
+    for (int j = 0; j < k; ++j) p.p[j] = v[j];
+    return p;
+}
+
+template <typename TV>
+int dav_ritz_residual(DavScratch &S, i64 n, int k, const double *coeffs, double e, const TV *const *V,
+                      const TV *const *AV, double *axt, double *norm_dev, cudaStream_t s)
+{
+    if (k < 1 || k > kMaxSub) { set_error("subspace size %d out of range", k); return BSIM_ERR_ARG; }
+    int st = S.ensure();
+    if (st) return st;
+    Coeffs c{};
+    for (int j = 0; j < k; ++j) c.v[j] = coeffs[j];
+    const int g = grid_for(n);
+    ritz_residual_kernel<TV><<<g, kRedThreads, 0, s>>>(n, k, c, e, pack(V, k), pack(AV, k), axt, S.part);
+    finish_kernel<<<1, 1024, 0, s>>>(S.part, g, 1, norm_dev, 1);
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+template <typename TV, typename TX>
+int dav_combine(i64 n, int k, const double *coeffs, const TV *const *V, TX *x, cudaStream_t s)
+{
+    if (k < 1 || k > kMaxSub) { set_error("subspace size %d out of range", k); return BSIM_ERR_ARG; }
+    Coeffs c{};
+    for (int j = 0; j < k; ++j) c.v[j] = coeffs[j];
+    combine_kernel<TV, TX><<<grid_for(n), kRedThreads, 0, s>>>(n, k, c, pack(V, k), x);
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+int dav_precondition(DavScratch &S, i64 n, double *r, const double *d, double e, double shift, double *norm_dev,
+                     cudaStream_t s)
+{
+    int st = S.ensure();
+    if (st) return st;
+    const int g = grid_for(n);
+    precondition_kernel<<<g, kRedThreads, 0, s>>>(n, r, d, e, shift, norm_dev ? S.part : nullptr);
+    if (norm_dev) finish_kernel<<<1, 1024, 0, s>>>(S.part, g, 1, norm_dev, 1);
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+template <typename TV>
+int dav_mgs(DavScratch &S, i64 n, int k, const TV *const *V, double *v, double *norm_dev, cudaStream_t s)
+{
+    int st = S.ensure();
+    if (st) return st;
+    if (k < 0 || k > kMaxSub) { set_error("subspace size %d out of range", k); return BSIM_ERR_ARG; }
+    const int g = grid_for(n);
+    // projections p_j land in S.res[j]; the final pass computes |v|^2
+    for (int j = 0; j <= k; ++j) {
+        const TV *prev = j > 0 ? V[j - 1] : nullptr;
+        const TV *next = j < k ? V[j] : nullptr;
+        mgs_step_kernel<TV><<<g, kRedThreads, 0, s>>>(n, v, prev, j > 0 ? S.res + (j - 1) : nullptr, next, S.part);
+        if (j < k) finish_kernel<<<1, 1024, 0, s>>>(S.part, g, 1, S.res + j, 0);
+        else finish_kernel<<<1, 1024, 0, s>>>(S.part, g, 1, norm_dev, 1);
+    }
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+int dav_normalize(DavScratch &S, i64 n, double *v, double *norm_dev, cudaStream_t s)
+{
+    int st = S.ensure();
+    if (st) return st;
+    const int g = grid_for(n);
+    mgs_step_kernel<double><<<g, kRedThreads, 0, s>>>(n, v, nullptr, nullptr, nullptr, S.part);
+    finish_kernel<<<1, 1024, 0, s>>>(S.part, g, 1, norm_dev, 1);
+    scale_kernel<<<g, kRedThreads, 0, s>>>(n, v, norm_dev);
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+int dav_dot(DavScratch &S, i64 n, const double *a, const double *b, double *out_dev, cudaStream_t s)
+{
+    int st = S.ensure();
+    if (st) return st;
+    const int g = grid_for(n);
+    dot_kernel<<<g, kRedThreads, 0, s>>>(n, a, b, S.part);
+    finish_kernel<<<1, 1024, 0, s>>>(S.part, g, 1, out_dev, 0);
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+template <typename TV, typename TW>
+int dav_multidot(DavScratch &S, i64 n, int k, const TV *const *V, const TW *w, double *out_dev, cudaStream_t s)
+{
+    if (k < 1 || k > kMaxSub) { set_error("subspace size %d out of range", k); return BSIM_ERR_ARG; }
+    int st = S.ensure();
+    if (st) return st;
+    const int g = grid_for(n);
+    multidot_kernel<TV, TW><<<g, kRedThreads, 0, s>>>(n, k, pack(V, k), w, S.part);
+    finish_kernel<<<1, 1024, 0, s>>>(S.part, g, k, out_dev, 0);
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+template int dav_ritz_residual<double>(DavScratch &, i64, int, const double *, double, const double *const *,
+                                       const double *const *, double *, double *, cudaStream_t);
+template int dav_ritz_residual<float>(DavScratch &, i64, int, const double *, double, const float *const *,
+                                      const float *const *, double *, double *, cudaStream_t);
+template int dav_combine<double, double>(i64, int, const double *, const double *const *, double *, cudaStream_t);
+template int dav_combine<float, double>(i64, int, const double *, const float *const *, double *, cudaStream_t);
+template int dav_combine<float, float>(i64, int, const double *, const float *const *, float *, cudaStream_t);
+template int dav_combine<double, float>(i64, int, const double *, const double *const *, float *, cudaStream_t);
+template int dav_mgs<double>(DavScratch &, i64, int, const double *const *, double *, double *, cudaStream_t);
+template int dav_mgs<float>(DavScratch &, i64, int, const float *const *, double *, double *, cudaStream_t);
+template int dav_multidot<double, double>(DavScratch &, i64, int, const double *const *, const double *, double *,
+                                          cudaStream_t);
+template int dav_multidot<float, float>(DavScratch &, i64, int, const float *const *, const float *, double *,
+                                        cudaStream_t);
+template int dav_multidot<float, double>(DavScratch &, i64, int, const float *const *, const double *, double *,
+                                         cudaStream_t);
+
+// ---- small symmetric eigensolver (cyclic Jacobi, FP64, k <= 64) --------------------
+void jacobi_eigh(int k, const double *A_in, int lda, double *evals, double *evecs /* k x k col-major */)
+{
+    std::vector<double> A((size_t)k * k);
+    for (int j = 0; j < k; ++j)
+        for (int i = 0; i < k; ++i) A[i + (size_t)j * k] = A_in[i + (size_t)j * lda];
+    for (int i = 0; i < k * k; ++i) evecs[i] = 0.0;
+    for (int i = 0; i < k; ++i) evecs[i + i * k] = 1.0;
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0, tot = 0.0;
+        for (int j = 0; j < k; ++j)
+            for (int i = 0; i < k; ++i) {
+                const double v = A[i + (size_t)j * k] * A[i + (size_t)j * k];
+                tot += v;
+                if (i != j) off += v;
+            }
+        if (off <= 1e-30 * std::max(tot, 1e-300)) break;
+        for (int p = 0; p < k - 1; ++p)
+            for (int q = p + 1; q < k; ++q) {
+                const double apq = A[p + (size_t)q * k];
+                if (fabs(apq) < 1e-300) continue;
+                const double app = A[p + (size_t)p * k], aqq = A[q + (size_t)q * k];
+                const double tau = (aqq - app) / (2.0 * apq);
+                const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                const double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
+                for (int r = 0; r < k; ++r) {   // A = J^T A J
+                    const double arp = A[r + (size_t)p * k], arq = A[r + (size_t)q * k];
+                    A[r + (size_t)p * k] = c * arp - s * arq;
+                    A[r + (size_t)q * k] = s * arp + c * arq;
+                }
+                for (int r = 0; r < k; ++r) {
+                    const double apr = A[p + (size_t)r * k], aqr = A[q + (size_t)r * k];
+                    A[p + (size_t)r * k] = c * apr - s * aqr;
+                    A[q + (size_t)r * k] = s * apr + c * aqr;
+                }
+                for (int r = 0; r < k; ++r) {
+                    const double vrp = evecs[r + p * k], vrq = evecs[r + q * k];
+                    evecs[r + p * k] = c * vrp - s * vrq;
+                    evecs[r + q * k] = s * vrp + c * vrq;
+                }
+            }
+    }
+    // sort ascending
+    std::vector<int> idx(k);
+    for (int i = 0; i < k; ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](int a, int b) { return A[a + (size_t)a * k] < A[b + (size_t)b * k]; });
+    std::vector<double> V(evecs, evecs + (size_t)k * k);
+    for (int j = 0; j < k; ++j) {
+        evals[j] = A[idx[j] + (size_t)idx[j] * k];
+        for (int i = 0; i < k; ++i) evecs[i + (size_t)j * k] = V[i + (size_t)idx[j] * k];
+    }
+}
+
+}  // namespace bsim

@@ -1,0 +1,118 @@
+// Host-side handles of libcuotf: the device basis and the device OTF network.
+//
+// A handle owns one device arena (a single cudaMalloc) holding every table
+// the kernels read.  Handles start with a magic word so that entry points can
+// reject pointers that are not handles of the right kind.
+#pragma once
+#include "common.cuh"
+
+namespace bsim {
+
+constexpr unsigned kBasisMagic = 0xB5B1A515u;
+constexpr unsigned kNetMagic = 0xB5B1E7A1u;
+constexpr int kMaxDenseMapOrb = 26;   // dense string->index tables up to 2^26 entries
+
+// Device arena: one allocation carved into aligned pieces.
+struct Arena {
+    char *base = nullptr;
+    size_t size = 0, used = 0;
+    int reserve(size_t bytes);
+    template <typename T>
+    T *take(size_t n) {
+        size_t a = (used + 255) & ~size_t(255);
+        used = a + n * sizeof(T);
+        return reinterpret_cast<T *>(base + a);
+    }
+    void release();
+};
+
+// Grow-on-demand device scratch owned by a basis handle: the tile table of the
+// tile kernels, an FP32 staging vector, reduction partials and result slots.
+// Growth calls cudaMalloc (synchronous); steady-state calls allocate nothing.
+// Calls that share one basis handle share this scratch, so they must not run
+// concurrently on different streams.
+struct Workspace {
+    i64 *tiles = nullptr;
+    size_t tiles_n = 0;
+    std::vector<i64> tiles_host;
+    float *f32 = nullptr;
+    size_t f32_n = 0;
+    double *part = nullptr;
+    size_t part_n = 0;
+    int tile_table(const std::vector<i64> &pref, const i64 **out);
+    int f32_buffer(size_t n, float **out);
+    int partials(size_t n, double **out);
+    void release();
+};
+
+template <typename Ti>
+struct DevBasis {
+    unsigned magic = kBasisMagic;
+    int norb = 0, num_irreps = 0, num_blocks = 0;
+    i64 dim = 0, total_sym = 0;
+    int max_na = 0, max_nb = 0;
+    // host mirrors
+    std::vector<int> asym, bsym, na, nb, astart, bstart, block_map;
+    std::vector<i64> off;
+    std::vector<Ti> astrs, bstrs;
+    std::vector<i64> orbsym;
+    // device
+    Arena arena;
+    BasisView<Ti> view{};
+    mutable Workspace ws;
+
+    int upload();                       // builds dense maps + copies tables
+    i64 find_det(u64 astr, u64 bstr) const;   // -1 when absent
+    ~DevBasis() { ws.release(); arena.release(); magic = 0; }
+};
+
+template <typename Ti>
+struct DevNet {
+    unsigned magic = kNetMagic;
+    int norb = 0;
+    i64 ngs = 0;
+    std::vector<GroupDev> groups;        // original order
+    std::vector<Ti> z;
+    std::vector<double> w;
+    std::vector<i64> orbsym;
+    // reference-style bookkeeping (ham/otf.hpp:329-344)
+    std::vector<int> excit_type;         // [ngs] original index -> type
+    std::vector<i64> sorted_pos;         // [ngs] original index -> position inside its type list
+    std::vector<int> by_type[4];         // original indices per type, stably sorted by rank
+    int diag_group = -1;                 // first diagonal group (get_diags uses it)
+    int max_rank = 0;
+    // sigma chunk plan: groups in (type, rank) order cut into chunks with uniform
+    // rank <= 2 and at most 32 groups, or a single group of larger rank
+    std::vector<int> plan_groups;        // original indices in plan order
+    std::vector<int4> plan_chunks;       // {start, count, rank, type-mask}
+    // device
+    Arena arena;
+    NetView<Ti> view{};
+    const int *d_plan_groups = nullptr;
+    const int4 *d_plan_chunks = nullptr;
+
+    int finalize();   // derived tables + upload
+    ~DevNet() { arena.release(); magic = 0; }
+};
+
+// ---- constructors -----------------------------------------------------------
+template <typename Ti>
+int make_basis(i64 norb, i64 na, i64 nb, i64 total_sym, const i64 *orbsym, i64 num_irreps,
+               DevBasis<Ti> **out);
+
+template <typename Ti>
+int make_network(const i64 *orbsym, i64 norb, i64 ngs, const Ti *axs, const Ti *bxs,
+                 const i64 *ranks, const i64 *nzas, const i64 *nzbs, const Ti *flat_za,
+                 const Ti *flat_zb, const double *flat_wa, const double *flat_wb,
+                 DevNet<Ti> **out);
+
+// From the reference's own host handles (layout mirrors in refmirror.h).
+int basis_from_ref_handle(const void *host_basis, DevBasis<unsigned> **out);
+int network_from_ref_handle(const void *host_net, DevNet<unsigned> **out);
+
+template <typename Ti>
+inline bool valid(const DevBasis<Ti> *b) { return b && b->magic == kBasisMagic; }
+template <typename Ti>
+inline bool valid(const DevNet<Ti> *n) { return n && n->magic == kNetMagic; }
+
+}  // namespace bsim

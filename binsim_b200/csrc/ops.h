@@ -1,0 +1,45 @@
+// Internal operation entry points of libcuotf (the C-ABI in capi.cu wraps them).
+#pragma once
+#include "handles.h"
+
+namespace bsim {
+
+template <typename Ti>
+inline Workspace &workspace_for(const DevBasis<Ti> *B) { return B->ws; }
+
+// sigma = H src (dst overwritten).  mixed: FP32 bulk, FP64 accumulation; src32
+// may carry an FP32 copy of the input (else one is made in the workspace).
+template <typename Ti>
+int sigma(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32, double *dst,
+          bool mixed, cudaStream_t s);
+
+template <typename Ti>
+int diag_elements(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *diag, cudaStream_t s);
+
+template <typename Ti>
+int tile_prefix(const DevBasis<Ti> *B, Workspace &ws, const i64 **out_dev, i64 *ntiles);
+
+// Single-generator pair operators (original group index gidx).
+//   expm:     v <- exp(theta G) v
+//   grad:     *out_dev = <l, G e^{theta G}>(r) in the reference orientation
+//   backgrad: l <- e^{-theta G} l ; *out_dev = grad term ; r <- e^{-theta G} r
+// out_dev is a device double; with accumulate the term is added to it.
+template <typename Ti>
+int expm(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta, double *v, cudaStream_t s);
+template <typename Ti>
+int grad(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta, const double *l, const double *r,
+         double *out_dev, bool accumulate, cudaStream_t s, double *scratch = nullptr, size_t scratch_n = 0);
+template <typename Ti>
+int backgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta, double *l, double *r,
+             double *out_dev, bool accumulate, cudaStream_t s);
+
+// Pool gradient: grads[orig] = grad of every group at thetas[orig] (device arrays).
+template <typename Ti>
+int batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *thetas, const double *l,
+              const double *r, double *grads, cudaStream_t s);
+
+// Number of CTAs the row-pair kernels launch (size of their partial-sum scratch).
+template <typename Ti>
+inline i64 pair_grid(const DevBasis<Ti> *B) { return (i64)B->max_na * B->num_blocks; }
+
+}  // namespace bsim

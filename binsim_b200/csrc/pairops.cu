@@ -1,0 +1,231 @@
+// Single-generator pair operators: expm, grad, backgrad
+// (reference op/expm.hpp:374-438, op/grad.hpp:397-465, op/backgrad.hpp:406-474,
+//  update rules core/math.hpp:132-215; GPU counterparts cuda/expm.cuh,
+//  cuda/grad.cuh, cuda/backgrad.cuh).
+//
+// Launch shape: one CTA per destination alpha row of every block
+// (grid = max_na x num_blocks).  A CTA whose row is connected to a source row
+// (and passes the once-per-pair rule) walks the row's beta columns with lanes
+// on consecutive columns: the destination row segment is read and written
+// coalesced, the source side is the row a^ax at columns idx(b^bx).  Every
+// unordered pair is owned by exactly one thread, so the in-place updates need
+// no atomics.
+//
+// grad/backgrad reduce deterministically: each CTA writes its partial sum to a
+// scratch slot, and the last CTA to finish (atomic ticket) adds all slots in
+// index order and writes the result.
+#include "ops.h"
+
+namespace bsim {
+
+enum PairOp { kExpm = 0, kGrad = 1, kBackgrad = 2 };
+
+constexpr int kPairThreads = 256;
+
+struct PairAngles { double c0, c1, c2, c3; };
+
+// Ticket counters for the last-CTA reduction live with the partials: the
+// scratch buffer holds [nslots partials][1 counter as unsigned long long].
+template <typename Ti, int OP>
+__global__ void __launch_bounds__(kPairThreads)
+pair_row_kernel(const BasisView<Ti> B, const NetView<Ti> N, int gid, PairAngles ang, double *__restrict__ l,
+                double *__restrict__ r, double *__restrict__ partials, unsigned long long *__restrict__ ticket,
+                double *__restrict__ out, int accumulate)
+{
+    __shared__ double spa[kMaxRank];
+    __shared__ double red[32];
+    __shared__ bool last;
+    const int kd = blockIdx.y, a = blockIdx.x;
+    const GroupDev g = N.g[gid];
+    const int nirr = B.num_irreps;
+    bool active = (g.type != 0) && a < B.blk_na[kd];
+    int ks = -1, sa = -1;
+    Ti s_a = 0;
+    if (active) {
+        const int as = B.blk_asym[kd] ^ g.asym, bs = B.blk_bsym[kd] ^ g.bsym;
+        ks = (as < nirr && bs < nirr) ? B.block_map[as * nirr + bs] : -1;
+        active = ks >= kd;   // ks == -1 fails too
+    }
+    if (active) {
+        s_a = B.astrs[B.blk_astart[kd] + a] ^ (Ti)g.ax;
+        sa = g.ax ? B.amap[s_a] : a;
+        active = sa >= 0 && !(ks == kd && g.type != 2 && sa < a);
+    }
+    double acc = 0.0;
+    if (active) {
+        const int R = g.rank;
+        for (int q = threadIdx.x; q < R; q += blockDim.x)
+            spa[q] = 0.0;
+        __syncthreads();
+        if (threadIdx.x < R) {
+            const Ti *z = N.z + g.za_off;
+            const double *w = N.w + g.wa_off + (i64)threadIdx.x * g.nza;
+            double v = 0.0;
+            for (int q = 0; q < g.nza; ++q) v += par(s_a & z[q]) ? -w[q] : w[q];
+            spa[threadIdx.x] = v;
+        }
+        __syncthreads();
+        const int nb = B.blk_nb[kd], nbs = B.blk_nb[ks];
+        const bool same = (ks == kd);
+        const i64 drow = B.blk_off[kd] + (i64)a * nb;
+        const i64 srow = B.blk_off[ks] + (i64)sa * nbs;
+        const Ti *bstrs = B.bstrs + B.blk_bstart[kd];
+        const Ti *zb = N.z + g.zb_off;
+        const double *wb = N.w + g.wb_off;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            const Ti s_b = bstrs[b] ^ (Ti)g.bx;
+            const int sb = g.bx ? B.bmap[s_b] : b;
+            if (sb < 0 || (same && g.type == 2 && sb < b)) continue;
+            double vt = 0.0;
+            for (int rr = 0; rr < R; ++rr) {
+                double pb = 0.0;
+                const double *w = wb + (i64)rr * g.nzb;
+                for (int q = 0; q < g.nzb; ++q) pb += par(s_b & zb[q]) ? -w[q] : w[q];
+                vt += spa[rr] * pb;
+            }
+            const i64 di = drow + b, si = srow + sb;
+            if (OP == kExpm) {
+                // expm_update, core/math.hpp:132-146: c0 = cos-1, c1 = sin
+                const double vd = 1.0 + ang.c0 * (vt * vt), vo = ang.c1 * vt;
+                const double vi = l[si], vj = l[di];
+                l[si] = vi * vd - vj * vo;
+                l[di] = vj * vd + vi * vo;
+            } else if (OP == kGrad) {
+                // grad_update, core/math.hpp:148-162: c0 = -sin, c1 = cos
+                const double vd = ang.c0 * (vt * vt), vo = ang.c1 * vt;
+                const double rvi = r[si], rvj = r[di];
+                acc += l[si] * (rvi * vd + rvj * vo) + l[di] * (rvj * vd - rvi * vo);
+            } else {
+                // backgrad_update, core/math.hpp:187-215
+                const double evd = 1.0 + ang.c0 * (vt * vt), evo = ang.c1 * vt;
+                const double gvd = ang.c2 * (vt * vt), gvo = ang.c3 * vt;
+                const double lvi = l[si], lvj = l[di], rvi = r[si], rvj = r[di];
+                const double els = lvi * evd - lvj * evo;
+                const double eld = lvj * evd + lvi * evo;
+                acc += els * (rvi * gvd + rvj * gvo) + eld * (rvj * gvd - rvi * gvo);
+                l[si] = els;
+                l[di] = eld;
+                r[si] = rvi * evd - rvj * evo;
+                r[di] = rvj * evd + rvi * evo;
+            }
+        }
+    }
+    if (OP == kExpm) return;
+    // ---- deterministic reduction --------------------------------------------
+    acc = warp_sum(acc);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = acc;
+    __syncthreads();
+    const unsigned nslots = gridDim.x * gridDim.y;
+    const unsigned slot = blockIdx.y * gridDim.x + blockIdx.x;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
+        partials[slot] = s;
+        __threadfence();
+        const unsigned long long t = atomicAdd(ticket, 1ull);
+        last = (t == nslots - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double s = 0.0;
+    for (unsigned i = threadIdx.x; i < nslots; i += blockDim.x) s += __ldcg(partials + i);
+    s = warp_sum(s);
+    if (lane == 0) red[wid] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tot += red[i];
+        out[0] = accumulate ? out[0] + tot : tot;
+        *ticket = 0ull;   // ready for the next launch on this stream
+    }
+}
+
+// ---- host side -----------------------------------------------------------------
+
+template <typename Ti>
+static int check_group(const DevNet<Ti> *N, i64 gidx)
+{
+    if (gidx < 0 || gidx >= N->ngs) {
+        set_error("group index %lld out of range [0, %lld)", gidx, N->ngs);
+        return BSIM_ERR_ARG;
+    }
+    return BSIM_OK;
+}
+
+// scratch layout: [nslots doubles][ticket]; the ticket must start at zero.
+template <typename Ti>
+static int pair_scratch(const DevBasis<Ti> *B, double **part, unsigned long long **ticket, cudaStream_t s)
+{
+    (void)s;
+    const size_t nslots = (size_t)pair_grid(B);
+    Workspace &ws = workspace_for(B);
+    // [nslots partials][ticket][result slot of the synchronous legacy calls]
+    int st = ws.partials(nslots + 2, part);
+    if (st != BSIM_OK) return st;
+    *ticket = reinterpret_cast<unsigned long long *>(*part + nslots);
+    return BSIM_OK;
+}
+
+template <typename Ti, int OP>
+static int launch_pair(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, PairAngles ang, double *l, double *r,
+                       double *out, bool accumulate, cudaStream_t s, double *ext_part, size_t ext_n)
+{
+    int st = check_group(N, gidx);
+    if (st != BSIM_OK) return st;
+    if (B->num_blocks == 0 || B->max_na == 0) {
+        if (OP != kExpm && !accumulate) BSIM_CUDA(cudaMemsetAsync(out, 0, sizeof(double), s));
+        return BSIM_OK;
+    }
+    double *part = nullptr;
+    unsigned long long *ticket = nullptr;
+    if (OP != kExpm) {
+        if (ext_part) {
+            if (ext_n < (size_t)pair_grid(B) + 1) { set_error("scratch too small"); return BSIM_ERR_TOO_LARGE; }
+            part = ext_part;
+            ticket = reinterpret_cast<unsigned long long *>(part + pair_grid(B));
+        } else {
+            st = pair_scratch(B, &part, &ticket, s);
+            if (st != BSIM_OK) return st;
+        }
+    }
+    dim3 grid(B->max_na, B->num_blocks);
+    pair_row_kernel<Ti, OP><<<grid, kPairThreads, 0, s>>>(B->view, N->view, (int)gidx, ang, l, r, part, ticket, out,
+                                                         accumulate ? 1 : 0);
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+template <typename Ti>
+int expm(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta, double *v, cudaStream_t s)
+{
+    PairAngles a{cos(theta) - 1.0, sin(theta), 0.0, 0.0};
+    return launch_pair<Ti, kExpm>(B, N, gidx, a, v, nullptr, nullptr, false, s, nullptr, 0);
+}
+
+template <typename Ti>
+int grad(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta, const double *l, const double *r,
+         double *out_dev, bool accumulate, cudaStream_t s, double *scratch, size_t scratch_n)
+{
+    PairAngles a{-sin(theta), cos(theta), 0.0, 0.0};
+    return launch_pair<Ti, kGrad>(B, N, gidx, a, const_cast<double *>(l), const_cast<double *>(r), out_dev, accumulate,
+                                  s, scratch, scratch_n);
+}
+
+template <typename Ti>
+int backgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta, double *l, double *r,
+             double *out_dev, bool accumulate, cudaStream_t s)
+{
+    // exp(-theta G) with the gradient at +theta (reference op/backgrad.hpp:81-84)
+    PairAngles a{cos(theta) - 1.0, -sin(theta), -sin(theta), cos(theta)};
+    return launch_pair<Ti, kBackgrad>(B, N, gidx, a, l, r, out_dev, accumulate, s, nullptr, 0);
+}
+
+template int expm<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, double, double *, cudaStream_t);
+template int grad<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, double, const double *,
+                            const double *, double *, bool, cudaStream_t, double *, size_t);
+template int backgrad<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, double, double *, double *,
+                                double *, bool, cudaStream_t);
+
+}  // namespace bsim

@@ -1,0 +1,269 @@
+"""ctypes binding of libcuotf and a host layer mirroring the reference's
+``CuOTF_Functions`` (``jl/cuda/cunetwork.jl:74-160``).
+
+Device vectors are ``torch`` CUDA tensors (float64); torch provides device
+memory and streams only -- all arithmetic runs in libcuotf's kernels.  Work is
+enqueued on torch's current stream.  The library is loaded from
+``binsim_b200/lib/libcuotf.so``; a missing library raises immediately (there
+is no fallback path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import network as nw
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libcuotf.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "binsim_cuotf.h")
+
+vp, i64, dbl, ci = C.c_void_p, C.c_int64, C.c_double, C.c_int
+_lib = None
+
+
+class CuOTFError(RuntimeError):
+    """A libcuotf entry point returned a non-zero status."""
+
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: status {status}: {msg}")
+        self.status = status
+
+
+def header_symbols() -> list:
+    """Every function name declared in include/binsim_cuotf.h."""
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", txt)) -
+                  {"extern", "if", "defined", "sizeof"})
+
+
+def lib() -> C.CDLL:
+    """Load libcuotf (once).  Raises FileNotFoundError when it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is missing: run __graft_entry__.build() "
+                                "(or python binsim_b200/build.py)")
+    L = C.CDLL(LIB_PATH)
+    sig = {
+        # part 1
+        "sync_device_cuda": (None, []),
+        "build_basisdev_f64": (vp, [vp]), "destroy_basisdev_f64": (None, [vp]),
+        "build_networkdev_f64": (vp, [vp]), "destroy_networkdev_f64": (None, [vp]),
+        "hvec_cuda": (None, [vp, vp, vp, vp]), "get_diags_elements_cuda": (None, [vp, vp, vp]),
+        "expm_cuda": (None, [vp, vp, i64, dbl, vp]), "grad_cuda": (dbl, [vp, vp, i64, dbl, vp, vp]),
+        "backgrad_cuda": (dbl, [vp, vp, i64, dbl, vp, vp]), "batchgrad_cuda": (None, [vp, vp, vp, vp, vp, vp]),
+        "expm_cuda_2d": (None, [vp, vp, i64, dbl, vp]), "grad_cuda_2d": (dbl, [vp, vp, i64, dbl, vp, vp]),
+        "backgrad_cuda_2d": (dbl, [vp, vp, i64, dbl, vp, vp]),
+        # part 2
+        "bsim_last_error": (C.c_char_p, []), "bsim_version": (C.c_char_p, []),
+        "bsim_basis_create_u32": (ci, [i64, i64, i64, i64, vp, i64, vp]),
+        "bsim_basis_from_host": (ci, [vp, vp]), "bsim_basis_destroy": (ci, [vp]),
+        "bsim_basis_dim": (i64, [vp]), "bsim_basis_find_det": (i64, [vp, C.c_uint64, C.c_uint64]),
+        "bsim_network_create_u32": (ci, [vp, i64, i64] + [vp] * 9 + [vp]),
+        "bsim_network_from_host": (ci, [vp, vp]), "bsim_network_destroy": (ci, [vp]),
+        "bsim_network_ngs": (i64, [vp]),
+        "bsim_hvec": (ci, [vp, vp, vp, vp, vp]), "bsim_hvec_mixed": (ci, [vp, vp, vp, vp, vp]),
+        "bsim_hvec_f32in": (ci, [vp, vp, vp, vp, vp]), "bsim_diag": (ci, [vp, vp, vp, vp]),
+        "bsim_expm": (ci, [vp, vp, i64, dbl, vp, vp]), "bsim_expm_seq": (ci, [vp, vp, i64, vp, vp, vp, vp]),
+        "bsim_grad": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
+        "bsim_backgrad": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
+        "bsim_batchgrad": (ci, [vp, vp, vp, vp, vp, vp, vp]),
+        "bsim_prepare_state": (ci, [vp, vp, i64, vp, vp, vp, vp, vp, i64, vp, vp]),
+        "bsim_vqe_energy_grad": (ci, [vp, vp, vp, i64, vp, vp, i64, vp, vp, vp, i64, i64, vp, vp, vp, vp, vp, vp]),
+        "bsim_davidson": (ci, [vp, vp, vp, vp, dbl, ci, ci, ci, ci, vp, vp, vp, vp, vp, vp, ci, vp]),
+        # part 3
+        "build_ritz_and_residual_cuda": (dbl, [i64, ci, vp, dbl, vp, vp, vp]),
+        "build_ritz_vector_cuda": (None, [i64, ci, vp, vp, vp]),
+        "apply_preconditioner_inplace_cuda": (None, [i64, vp, vp, dbl, dbl]),
+        "mgs_orthogonalize_cuda": (dbl, [i64, ci, vp, vp]),
+        "inplace_normalize_cuda": (dbl, [i64, vp]),
+        "fast_dot_cuda": (dbl, [i64, vp, vp]),
+        "compute_heff_col_cuda": (None, [i64, ci, vp, vp, vp]),
+        "rebuild_heff_cuda": (None, [i64, ci, vp, vp, vp, ci]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(st: int, where: str):
+    if st != 0:
+        raise CuOTFError(st, where, lib().bsim_last_error().decode())
+
+
+def _ptr(x) -> int:
+    """Device pointer of a torch tensor, or host pointer of a numpy array."""
+    if x is None:
+        return None
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    return x.ctypes.data
+
+
+def _stream(stream=None):
+    if stream is not None:
+        return stream
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _host(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class CuBasis:
+    """Device determinant space (``BasisManager`` + ``upload_basis``)."""
+
+    def __init__(self, norb: int, na: int, nb: int, orbsym=None, total_sym: int = 0, num_irreps: int = 16,
+                 host_handle: Optional[int] = None):
+        L = lib()
+        out = vp()
+        if host_handle is not None:
+            _check(L.bsim_basis_from_host(host_handle, C.byref(out)), "bsim_basis_from_host")
+        else:
+            self._orbsym = _host(np.zeros(norb) if orbsym is None else orbsym, np.int64)
+            _check(L.bsim_basis_create_u32(norb, na, nb, total_sym, self._orbsym.ctypes.data, num_irreps,
+                                           C.byref(out)), "bsim_basis_create_u32")
+        self.h = out.value
+        self.norb, self.nelec = norb, (na, nb)
+        self.dim = L.bsim_basis_dim(self.h)
+
+    def find_det(self, astr: int, bstr: int) -> int:
+        return lib().bsim_basis_find_det(self.h, astr, bstr)
+
+    def hf_index(self) -> int:
+        """Index of the Hartree-Fock determinant (``get_hf``, jl/network.jl:81-116)."""
+        na, nb = self.nelec
+        return self.find_det((1 << na) - 1, (1 << nb) - 1)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bsim_basis_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CuNetwork:
+    """Device OTF network (``Network_OTF`` + ``upload_network``)."""
+
+    def __init__(self, net: Optional[nw.OTFNetwork] = None, host_handle: Optional[int] = None):
+        L = lib()
+        out = vp()
+        if host_handle is not None:
+            _check(L.bsim_network_from_host(host_handle, C.byref(out)), "bsim_network_from_host")
+        else:
+            a = net.as_uint32()
+            self._keep = [
+                _host(net.orbsym, np.int64), a["axs"], a["bxs"], _host(net.ranks, np.int64),
+                _host(net.num_zas, np.int64), _host(net.num_zbs, np.int64), a["flat_zas"], a["flat_zbs"],
+                _host(net.flat_wa, np.float64), _host(net.flat_wb, np.float64)]
+            k = self._keep
+            _check(L.bsim_network_create_u32(k[0].ctypes.data, net.norb, net.ngs, *[x.ctypes.data for x in k[1:]],
+                                             C.byref(out)), "bsim_network_create_u32")
+        self.h = out.value
+        self.ngs = L.bsim_network_ngs(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bsim_network_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CuOTFFunctions:
+    """The operator closures of ``CuOTF_Functions`` (jl/cuda/cunetwork.jl:74-160).
+
+    Generator indices are 1-based as in the Julia closures (they pass idx-1 to
+    the C-ABI).  Vectors are float64 torch CUDA tensors of length ``basis.dim``.
+    """
+
+    def __init__(self, basis: CuBasis, ham: Optional[CuNetwork] = None, pool: Optional[CuNetwork] = None):
+        self.basis, self.ham, self.pool = basis, ham, pool
+        import torch
+        self._scalar = torch.zeros(1, dtype=torch.float64, device="cuda")
+
+    # -- jl/cuda/cunetwork.jl:105-150 --------------------------------------
+    def hvec(self, v, Hv, stream=None):
+        _check(lib().bsim_hvec(self.basis.h, self.ham.h, _ptr(v), _ptr(Hv), _stream(stream)), "hvec")
+
+    def hvec_mixed(self, v, Hv, stream=None):
+        _check(lib().bsim_hvec_mixed(self.basis.h, self.ham.h, _ptr(v), _ptr(Hv), _stream(stream)), "hvec_mixed")
+
+    def get_diags(self, dv, stream=None):
+        _check(lib().bsim_diag(self.basis.h, self.ham.h, _ptr(dv), _stream(stream)), "get_diags")
+
+    def expm(self, idx: int, theta: float, v, stream=None):
+        _check(lib().bsim_expm(self.basis.h, self.pool.h, idx - 1, theta, _ptr(v), _stream(stream)), "expm")
+
+    def grad(self, idx: int, theta: float, lv, rv, stream=None) -> float:
+        _check(lib().bsim_grad(self.basis.h, self.pool.h, idx - 1, theta, _ptr(lv), _ptr(rv),
+                               _ptr(self._scalar), _stream(stream)), "grad")
+        return float(self._scalar.item())
+
+    def backgrad(self, idx: int, theta: float, lv, rv, stream=None) -> float:
+        _check(lib().bsim_backgrad(self.basis.h, self.pool.h, idx - 1, theta, _ptr(lv), _ptr(rv),
+                                   _ptr(self._scalar), _stream(stream)), "backgrad")
+        return float(self._scalar.item())
+
+    def batchgrad(self, lv, rv, grads, x, stream=None):
+        _check(lib().bsim_batchgrad(self.basis.h, self.pool.h, _ptr(x), _ptr(lv), _ptr(rv), _ptr(grads),
+                                    _stream(stream)), "batchgrad")
+
+    # -- sequence-level entry points ------------------------------------------
+    def expm_seq(self, idxs: Sequence[int], thetas: Sequence[float], v, stream=None):
+        """Apply exp(theta_i G_{idx_i}) for i in order (1-based idx)."""
+        ii = _host(np.asarray(idxs) - 1, np.int64)
+        tt = _host(thetas, np.float64)
+        _check(lib().bsim_expm_seq(self.basis.h, self.pool.h, len(ii), ii.ctypes.data, tt.ctypes.data, _ptr(v),
+                                   _stream(stream)), "expm_seq")
+
+    def prepare_state(self, op_idx, param_idx, thetas, ref_idx, ref_val, v, stream=None):
+        """v = prod exp(thetas[param_idx[i]] G_{op_idx[i]}) |ref> (0-based indices)."""
+        o, p = _host(op_idx, np.int64), _host(param_idx, np.int64)
+        t, ri, rv = _host(thetas, np.float64), _host(ref_idx, np.int64), _host(ref_val, np.float64)
+        _check(lib().bsim_prepare_state(self.basis.h, self.pool.h, len(o), o.ctypes.data, p.ctypes.data,
+                                        t.ctypes.data, ri.ctypes.data, rv.ctypes.data, len(ri), _ptr(v),
+                                        _stream(stream)), "prepare_state")
+
+    def energy_grad(self, op_idx, param_idx, thetas, ref_idx, ref_val, lv, rv, ckpt_every: int = 64, stream=None):
+        """(energy, gradient[n_params], variance) by the adjoint sweep (jl/vqe.jl:1-21)."""
+        o, p = _host(op_idx, np.int64), _host(param_idx, np.int64)
+        t, ri, rvv = _host(thetas, np.float64), _host(ref_idx, np.int64), _host(ref_val, np.float64)
+        g = np.zeros(len(t))
+        e, var = C.c_double(), C.c_double()
+        _check(lib().bsim_vqe_energy_grad(self.basis.h, self.ham.h, self.pool.h, len(o), o.ctypes.data,
+                                          p.ctypes.data, len(t), t.ctypes.data, ri.ctypes.data, rvv.ctypes.data,
+                                          len(ri), ckpt_every, _ptr(lv), _ptr(rv), C.byref(e), C.byref(var),
+                                          g.ctypes.data, _stream(stream)), "vqe_energy_grad")
+        return e.value, g, var.value
+
+    def davidson(self, v0, diags, x_out, tol=1e-5, maxiter=200, ncv=3, maxspace=23, mixed=False, verbose=False,
+                 stream=None):
+        """Lowest eigenpair (jl/davidson.jl:1-185).  Returns a stats dict."""
+        e, r = C.c_double(), C.c_double()
+        it, s64, s32 = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().bsim_davidson(self.basis.h, self.ham.h, _ptr(v0), _ptr(diags), tol, maxiter, ncv, maxspace,
+                                   1 if mixed else 0, _ptr(x_out), C.byref(e), C.byref(r), C.byref(it),
+                                   C.byref(s64), C.byref(s32), 1 if verbose else 0, _stream(stream)), "davidson")
+        return dict(energy=e.value, residual=r.value, iterations=it.value, sigma_fp64=s64.value,
+                    sigma_fp32=s32.value)

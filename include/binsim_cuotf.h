@@ -1,0 +1,186 @@
+/*
+ * binsim_cuotf.h -- C-ABI of libcuotf, the B200 (sm_100a) implementation of
+ * BinSim's on-the-fly (OTF) operator path.
+ *
+ * Part 1 keeps the reference GPU library's entry points with identical names,
+ * argument lists and semantics, so Julia's ccall sites bind unchanged.  Part 2
+ * adds status-returning, stream-taking entry points.  Part 3 puts libdiag's
+ * Davidson vector helpers on device pointers.
+ *
+ * Conventions (all parts):
+ *   - vectors are device pointers to FP64 arrays of length bsim_basis_dim(),
+ *     ordered block offset + alpha index * n_beta + beta index
+ *     (reference src/include/basis/basis.hpp:327);
+ *   - group / generator indices are 0-based original network indices (the
+ *     Julia layer passes idx-1, reference jl/cuda/cunetwork.jl:124);
+ *   - strings are UInt32 bit strings (orbital p = bit p), norb <= 26.
+ *
+ * Thread safety: a basis handle owns reusable device scratch, so calls that
+ * share one basis handle must be issued from one host thread / one stream at
+ * a time.
+ */
+#ifndef BINSIM_CUOTF_H
+#define BINSIM_CUOTF_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *bsim_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+/* ========================================================================
+ * Part 1: reference-compatible entry points (src/extern/cuotf.cu:7-162).
+ * They run on the legacy default stream.  hvec/expm/batchgrad/diag return
+ * before the GPU finishes; grad/backgrad return the scalar, so they wait.
+ * On failure they print to stderr and leave bsim_last_error() set; they never
+ * exit the process (the reference calls exit(1), common.cuh:42-49).
+ * ====================================================================== */
+
+/* cuotf.cu:9-12 */
+void sync_device_cuda(void);
+/* cuotf.cu:26-31: host_basis is a BasisManager<uint32>* returned by libbasis
+ * create_basis_manager (basis/declare.hpp:24-33); its tables are copied. */
+void *build_basisdev_f64(void *host_basis);
+/* cuotf.cu:14-24 */
+void destroy_basisdev_f64(void *basis);
+/* cuotf.cu:43-48: host_net is a Network_OTF<uint32,double>* returned by
+ * libotf_native build_network_otf_f64 (op/declare.hpp:25-35). */
+void *build_networkdev_f64(void *host_net);
+/* cuotf.cu:33-41 */
+void destroy_networkdev_f64(void *net);
+/* cuotf.cu:50-60: dst = H src (dst overwritten). */
+void hvec_cuda(void *basis, void *net, const double *src, double *dst);
+/* cuotf.cu:62-71: diags += diagonal of H (caller zeroes, as jl/fci.jl:3-4). */
+void get_diags_elements_cuda(void *basis, void *net, double *diags);
+/* cuotf.cu:73-83: vec <- exp(theta G_idx) vec. */
+void expm_cuda(void *basis, void *net, int64_t idx, double theta, double *vec);
+/* cuotf.cu:85-96: <l| G e^{theta G} |r> in the reference's orientation. */
+double grad_cuda(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r);
+/* cuotf.cu:98-109: l <- e^{-theta G} l; returns the gradient term; r <- e^{-theta G} r. */
+double backgrad_cuda(void *basis, void *net, int64_t idx, double theta, double *l, double *r);
+/* cuotf.cu:111-123: grads[g] for every group g at thetas[g] (device arrays,
+ * indexed by original group index); grads is overwritten. */
+void batchgrad_cuda(void *basis, void *net, const double *thetas, const double *l, const double *r, double *grads);
+/* cuotf.cu:125-161: same semantics as the entries above. */
+void expm_cuda_2d(void *basis, void *net, int64_t idx, double theta, double *vec);
+double grad_cuda_2d(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r);
+double backgrad_cuda_2d(void *basis, void *net, int64_t idx, double theta, double *l, double *r);
+
+/* ========================================================================
+ * Part 2: status-returning API.  Every function returns 0 on success or a
+ * negative BSIM_ERR_* code; bsim_last_error() describes the last failure of
+ * the calling thread.  Work is enqueued on `stream`.
+ * ====================================================================== */
+enum {
+    BSIM_OK = 0,
+    BSIM_ERR_NULL = -1,
+    BSIM_ERR_ARG = -2,
+    BSIM_ERR_UNSUPPORTED = -3,
+    BSIM_ERR_ALLOC = -4,
+    BSIM_ERR_TIMEOUT = -5,
+    BSIM_ERR_CUDA = -6,
+    BSIM_ERR_TOO_LARGE = -7
+};
+
+const char *bsim_last_error(void);
+const char *bsim_version(void);
+
+/* Basis: create_basis_manager's arguments (basis/declare.hpp:24-33). */
+int bsim_basis_create_u32(int64_t norb, int64_t na, int64_t nb, int64_t total_sym, const int64_t *orbsym,
+                          int64_t num_irreps, void **out);
+/* Basis from the reference's host BasisManager<uint32>* (as build_basisdev_f64). */
+int bsim_basis_from_host(void *host_basis, void **out);
+int bsim_basis_destroy(void *basis);
+int64_t bsim_basis_dim(void *basis);
+/* Determinant index of (alpha string, beta string) or -1 (set_det_coeff
+ * semantics, basis/basis.hpp:298-330). */
+int64_t bsim_basis_find_det(void *basis, uint64_t astr, uint64_t bstr);
+
+/* Network: build_network_otf_f64's arguments (op/declare.hpp:25-35); flat_wa /
+ * flat_wb hold each group's weights column-major [num_z x rank]. */
+int bsim_network_create_u32(const int64_t *orbsym, int64_t norb, int64_t ngs, const uint32_t *axs,
+                            const uint32_t *bxs, const int64_t *ranks, const int64_t *num_zas,
+                            const int64_t *num_zbs, const uint32_t *flat_zas, const uint32_t *flat_zbs,
+                            const double *flat_wa, const double *flat_wb, void **out);
+/* Network from the reference's host Network_OTF<uint32,double>*. */
+int bsim_network_from_host(void *host_net, void **out);
+int bsim_network_destroy(void *net);
+int64_t bsim_network_ngs(void *net);
+
+/* dst = H src, FP64. */
+int bsim_hvec(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream);
+/* dst = H src with FP32 bulk (FP32 phases, weights and gathered source,
+ * products summed in FP32 per chunk of <= 64 group-ranks) and FP64
+ * accumulation across chunks. */
+int bsim_hvec_mixed(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream);
+/* As bsim_hvec_mixed with an FP32 input vector. */
+int bsim_hvec_f32in(void *basis, void *net, const float *src, double *dst, bsim_stream_t stream);
+/* diags += diagonal of H. */
+int bsim_diag(void *basis, void *net, double *diags, bsim_stream_t stream);
+/* vec <- exp(theta G_idx) vec. */
+int bsim_expm(void *basis, void *net, int64_t idx, double theta, double *vec, bsim_stream_t stream);
+/* vec <- exp(theta[n-1] G_idx[n-1]) ... exp(theta[0] G_idx[0]) vec; idx/theta are host arrays. */
+int bsim_expm_seq(void *basis, void *net, int64_t n, const int64_t *idx, const double *theta, double *vec,
+                  bsim_stream_t stream);
+/* *out_dev (a device double) = grad term; nothing is read back. */
+int bsim_grad(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r,
+              double *out_dev, bsim_stream_t stream);
+/* Fused adjoint step; *out_dev (device) = gradient term. */
+int bsim_backgrad(void *basis, void *net, int64_t idx, double theta, double *l, double *r, double *out_dev,
+                  bsim_stream_t stream);
+/* Pool gradient (thetas, grads: device, original group order). */
+int bsim_batchgrad(void *basis, void *net, const double *thetas, const double *l, const double *r,
+                   double *grads, bsim_stream_t stream);
+/* vec <- prod_i exp(thetas[param_idx[i]] G_{op_idx[i]}) |ref>, |ref> = sum_j ref_val[j] e_{ref_idx[j]};
+ * all index/angle arrays are host arrays. */
+int bsim_prepare_state(void *basis, void *pool, int64_t n_ops, const int64_t *op_idx, const int64_t *param_idx,
+                       const double *thetas, const int64_t *ref_idx, const double *ref_val, int64_t n_ref,
+                       double *vec, bsim_stream_t stream);
+/* VQE energy E = <psi|H|psi>/<psi|psi>, variance <H^2> - E^2 and the adjoint
+ * gradient dE/dtheta_p (jl/vqe.jl:1-21) for psi = prepare_state(...).
+ * Components sharing a parameter (spin-adapted generators) sum their terms.
+ * ckpt_every > 0 stores the forward state every ckpt_every parameters and
+ * restores it during the reverse sweep.  lv, rv: device work vectors (dim).
+ * energy, variance, grad[n_params]: host outputs. */
+int bsim_vqe_energy_grad(void *basis, void *ham, void *pool, int64_t n_ops, const int64_t *op_idx,
+                         const int64_t *param_idx, int64_t n_params, const double *thetas, const int64_t *ref_idx,
+                         const double *ref_val, int64_t n_ref, int64_t ckpt_every, double *lv, double *rv,
+                         double *energy, double *variance, double *grad, bsim_stream_t stream);
+/* Lowest eigenpair by Davidson on device (jl/davidson.jl:1-185).  mixed = 0:
+ * FP64 throughout (ncv, maxspace as the reference); mixed = 1: FP32 subspace
+ * and FP32-bulk sigma inside FP64 residual refinement (ncv unused).  v0 is
+ * normalised in place; x_out receives the eigenvector.  Outputs may be NULL. */
+int bsim_davidson(void *basis, void *net, double *v0, const double *diags, double tol, int maxiter, int ncv,
+                  int maxspace, int mixed, double *x_out, double *energy, double *residual, int *iterations,
+                  int *sigma_fp64, int *sigma_fp32, int verbose, bsim_stream_t stream);
+
+/* ========================================================================
+ * Part 3: libdiag's Davidson helpers (diag/declare.hpp:4-75) on device
+ * vectors.  N, dim, coeffs and the returned scalars are host values; V / AV
+ * are host arrays of device pointers.  Each call completes before returning.
+ * ====================================================================== */
+/* diag/declare.hpp:7-16 */
+double build_ritz_and_residual_cuda(int64_t N, int dim, const double *coeffs, double min_e, const double **V,
+                                    const double **AV, double *axt);
+/* diag/declare.hpp:18-25 */
+void build_ritz_vector_cuda(int64_t N, int dim, const double *coeffs, const double **V, double *xt);
+/* diag/declare.hpp:27-34 */
+void apply_preconditioner_inplace_cuda(int64_t N, double *axt, const double *diags, double min_e, double shift);
+/* diag/declare.hpp:36-42 */
+double mgs_orthogonalize_cuda(int64_t N, int dim, const double **V, double *vt);
+/* diag/declare.hpp:44-49 */
+double inplace_normalize_cuda(int64_t N, double *vec);
+/* diag/declare.hpp:51-57 */
+double fast_dot_cuda(int64_t N, const double *v1, const double *v2);
+/* diag/declare.hpp:59-66: out_col is a host array of dim entries. */
+void compute_heff_col_cuda(int64_t N, int dim, const double **V, const double *AV_dim, double *out_col);
+/* diag/declare.hpp:68-75: heff is a host array (column-major, leading dim ldh). */
+void rebuild_heff_cuda(int64_t N, int dim, const double **V, const double **AV, double *heff, int ldh);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BINSIM_CUOTF_H */

@@ -1,0 +1,342 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes drivers for the checkers.
+
+* ``Oracle`` drives ``oracle/liboracle.so``, the plain-C restatement of the
+  OTF operator path (``oracle/otf_oracle.c``).
+* ``RefLibs`` drives the reference's own CPU libraries compiled by
+  ``oracle/Makefile`` into ``oracle/_ref`` (libotf_native, libbasis, libdiag,
+  libham_real), restating the Julia glue that calls them
+  (``jl/network.jl:17-48, 313-375, 483-608``, ``jl/davidson.jl``).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module.  The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+_lock = threading.Lock()
+
+P = lambda a: a.ctypes.data_as(C.c_void_p)
+i64 = C.c_int64
+dbl = C.c_double
+vp = C.c_void_p
+
+
+def build_oracle(force: bool = False) -> str:
+    """Compile liboracle.so (gcc, a second or two) if it is missing."""
+    path = os.path.join(HERE, "liboracle.so")
+    with _lock:
+        if force or not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(
+                os.path.join(HERE, "otf_oracle.c")):
+            subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    return path
+
+
+def _ptr_array(vecs):
+    arr = (C.c_void_p * len(vecs))()
+    for i, v in enumerate(vecs):
+        arr[i] = v.ctypes.data
+    return arr
+
+
+class Oracle:
+    """The C restatement: basis/network handles and every operator of the path."""
+
+    def __init__(self):
+        lib = C.CDLL(build_oracle())
+        lib.oracle_basis_create.restype = vp
+        lib.oracle_basis_create.argtypes = [i64, i64, i64, i64, vp, i64]
+        lib.oracle_basis_dim.restype = i64
+        lib.oracle_basis_dim.argtypes = [vp]
+        lib.oracle_basis_num_blocks.restype = i64
+        lib.oracle_basis_num_blocks.argtypes = [vp]
+        lib.oracle_basis_blocks.argtypes = [vp, vp]
+        lib.oracle_basis_strings.argtypes = [vp, i64, C.c_int, vp]
+        lib.oracle_basis_destroy.argtypes = [vp]
+        lib.oracle_net_create.restype = vp
+        lib.oracle_net_create.argtypes = [vp, i64, i64] + [vp] * 9
+        lib.oracle_net_destroy.argtypes = [vp]
+        lib.oracle_hvec.argtypes = [vp, vp, vp, vp]
+        lib.oracle_diag.argtypes = [vp, vp, vp]
+        lib.oracle_expm.argtypes = [vp, vp, i64, dbl, vp]
+        lib.oracle_grad.restype = dbl
+        lib.oracle_grad.argtypes = [vp, vp, i64, dbl, vp, vp]
+        lib.oracle_backgrad.restype = dbl
+        lib.oracle_backgrad.argtypes = [vp, vp, i64, dbl, vp, vp]
+        lib.oracle_batchgrad.argtypes = [vp, vp, vp, vp, vp, vp]
+        lib.oracle_ritz_residual.restype = dbl
+        lib.oracle_ritz_residual.argtypes = [i64, C.c_int, vp, dbl, vp, vp, vp]
+        lib.oracle_ritz_vector.argtypes = [i64, C.c_int, vp, vp, vp]
+        lib.oracle_precondition.argtypes = [i64, vp, vp, dbl, dbl]
+        lib.oracle_mgs.restype = dbl
+        lib.oracle_mgs.argtypes = [i64, C.c_int, vp, vp]
+        lib.oracle_normalize.restype = dbl
+        lib.oracle_normalize.argtypes = [i64, vp]
+        lib.oracle_dot.restype = dbl
+        lib.oracle_dot.argtypes = [i64, vp, vp]
+        lib.oracle_heff_col.argtypes = [i64, C.c_int, vp, vp, vp]
+        self.lib = lib
+
+    # -- handles ---------------------------------------------------------
+    def basis(self, norb, na, nb, orbsym=None, total_sym=0, num_irreps=16):
+        orbsym = np.zeros(norb, np.int64) if orbsym is None else np.ascontiguousarray(orbsym, np.int64)
+        h = self.lib.oracle_basis_create(norb, na, nb, total_sym, P(orbsym), num_irreps)
+        return OracleBasis(self, h, norb)
+
+    def network(self, net):
+        a = dict(orbsym=np.ascontiguousarray(net.orbsym, np.int64),
+                 axs=np.ascontiguousarray(net.axs, np.uint64), bxs=np.ascontiguousarray(net.bxs, np.uint64),
+                 ranks=np.ascontiguousarray(net.ranks, np.int64),
+                 nza=np.ascontiguousarray(net.num_zas, np.int64), nzb=np.ascontiguousarray(net.num_zbs, np.int64),
+                 za=np.ascontiguousarray(net.flat_zas, np.uint64), zb=np.ascontiguousarray(net.flat_zbs, np.uint64),
+                 wa=np.ascontiguousarray(net.flat_wa, np.float64), wb=np.ascontiguousarray(net.flat_wb, np.float64))
+        h = self.lib.oracle_net_create(P(a["orbsym"]), net.norb, net.ngs, P(a["axs"]), P(a["bxs"]), P(a["ranks"]),
+                                       P(a["nza"]), P(a["nzb"]), P(a["za"]), P(a["zb"]), P(a["wa"]), P(a["wb"]))
+        return OracleNet(self, h, net.ngs, a)
+
+    # -- operators --------------------------------------------------------
+    def hvec(self, B, N, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(B.dim)
+        self.lib.oracle_hvec(B.h, N.h, P(x), P(y))
+        return y
+
+    def diag(self, B, N):
+        d = np.zeros(B.dim)
+        self.lib.oracle_diag(B.h, N.h, P(d))
+        return d
+
+    def expm(self, B, N, idx, theta, v):
+        v = np.array(v, np.float64, copy=True)
+        self.lib.oracle_expm(B.h, N.h, idx, theta, P(v))
+        return v
+
+    def grad(self, B, N, idx, theta, l, r):
+        l = np.ascontiguousarray(l, np.float64); r = np.ascontiguousarray(r, np.float64)
+        return self.lib.oracle_grad(B.h, N.h, idx, theta, P(l), P(r))
+
+    def backgrad(self, B, N, idx, theta, l, r):
+        """Returns (g, l_new, r_new); inputs are not modified."""
+        l = np.array(l, np.float64, copy=True); r = np.array(r, np.float64, copy=True)
+        g = self.lib.oracle_backgrad(B.h, N.h, idx, theta, P(l), P(r))
+        return g, l, r
+
+    def batchgrad(self, B, N, thetas, l, r):
+        thetas = np.ascontiguousarray(thetas, np.float64)
+        l = np.ascontiguousarray(l, np.float64); r = np.ascontiguousarray(r, np.float64)
+        g = np.zeros(N.ngs)
+        self.lib.oracle_batchgrad(B.h, N.h, P(thetas), P(l), P(r), P(g))
+        return g
+
+    # -- Davidson helpers -------------------------------------------------
+    def ritz_residual(self, coeffs, e, V, AV):
+        n = len(V[0]); out = np.zeros(n)
+        c = np.ascontiguousarray(coeffs, np.float64)
+        nr = self.lib.oracle_ritz_residual(n, len(V), P(c), e, _ptr_array(V), _ptr_array(AV), P(out))
+        return nr, out
+
+    def ritz_vector(self, coeffs, V):
+        n = len(V[0]); out = np.zeros(n)
+        c = np.ascontiguousarray(coeffs, np.float64)
+        self.lib.oracle_ritz_vector(n, len(V), P(c), _ptr_array(V), P(out))
+        return out
+
+    def precondition(self, r, d, e, shift):
+        r = np.array(r, np.float64, copy=True)
+        self.lib.oracle_precondition(len(r), P(r), P(np.ascontiguousarray(d, np.float64)), e, shift)
+        return r
+
+    def mgs(self, V, v):
+        v = np.array(v, np.float64, copy=True)
+        nrm = self.lib.oracle_mgs(len(v), len(V), _ptr_array(V), P(v))
+        return nrm, v
+
+    def normalize(self, v):
+        v = np.array(v, np.float64, copy=True)
+        nrm = self.lib.oracle_normalize(len(v), P(v))
+        return nrm, v
+
+    def heff_col(self, V, av):
+        out = np.zeros(len(V))
+        self.lib.oracle_heff_col(len(av), len(V), _ptr_array(V), P(np.ascontiguousarray(av)), P(out))
+        return out
+
+
+class OracleBasis:
+    def __init__(self, owner, h, norb):
+        self.o, self.h, self.norb = owner, h, norb
+        self.dim = owner.lib.oracle_basis_dim(h)
+        self.num_blocks = owner.lib.oracle_basis_num_blocks(h)
+        blk = np.zeros(5 * max(1, self.num_blocks), np.int64)
+        owner.lib.oracle_basis_blocks(h, P(blk))
+        self.blocks = blk[: 5 * self.num_blocks].reshape(-1, 5)
+
+    def strings(self, k, spin):
+        n = int(self.blocks[k, 2 + spin])
+        out = np.zeros(max(1, n), np.uint64)
+        self.o.lib.oracle_basis_strings(self.h, k, spin, P(out))
+        return out[:n]
+
+    def det_index(self, astr, bstr):
+        for k in range(self.num_blocks):
+            A, Bs = self.strings(k, 0), self.strings(k, 1)
+            ia = np.searchsorted(A, astr); ib = np.searchsorted(Bs, bstr)
+            if ia < len(A) and A[ia] == astr and ib < len(Bs) and Bs[ib] == bstr:
+                return int(self.blocks[k, 4] + ia * len(Bs) + ib)
+        return -1
+
+    def __del__(self):
+        try:
+            self.o.lib.oracle_basis_destroy(self.h)
+        except Exception:
+            pass
+
+
+class OracleNet:
+    def __init__(self, owner, h, ngs, keep):
+        self.o, self.h, self.ngs, self._keep = owner, h, ngs, keep
+
+    def __del__(self):
+        try:
+            self.o.lib.oracle_net_destroy(self.h)
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# the reference's own libraries (built here from its sources)
+# ---------------------------------------------------------------------------
+
+class HamResult(C.Structure):
+    """binsim::ham::HamResult<double>, ham.hpp:482-490."""
+    _fields_ = [("axs", vp), ("azs", vp), ("bxs", vp), ("bzs", vp),
+                ("cs", C.POINTER(C.c_double)), ("ncs", C.c_size_t)]
+
+
+def ref_available() -> bool:
+    return all(os.path.exists(os.path.join(REF_DIR, f)) for f in
+               ("libotf_native.so", "libbasis.so", "libdiag.so", "libham_real.so"))
+
+
+def build_ref() -> bool:
+    """Compile oracle/_ref from the reference sources when they are present."""
+    if ref_available():
+        return True
+    if not os.path.isdir("/root/reference/src/include"):
+        return False
+    subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    return ref_available()
+
+
+class RefLibs:
+    """ctypes access to the reference's compiled CPU libraries (uint32 strings)."""
+
+    def __init__(self):
+        if not ref_available():
+            raise RuntimeError("oracle/_ref libraries are not built")
+        L = lambda n: C.CDLL(os.path.join(REF_DIR, n))
+        self.otf, self.bas, self.diag, self.ham = (L("libotf_native.so"), L("libbasis.so"),
+                                                   L("libdiag.so"), L("libham_real.so"))
+        f = self.ham.generate_hamiltonian_real_64_128_f64
+        f.restype = HamResult
+        f.argtypes = [dbl, vp, vp, C.c_int, dbl, C.c_bool]
+        self.otf.build_network_otf_f64.restype = vp
+        self.otf.build_network_otf_f64.argtypes = [vp, i64, i64] + [vp] * 9
+        self.otf.destroy_network_otf_f64.argtypes = [vp]
+        self.otf.hvec_gather_contract_otf_f64.argtypes = [vp, vp, vp, vp]
+        self.otf.get_diags_elements_f64.argtypes = [vp, vp, vp]
+        self.otf.expm_contract_otf_f64.argtypes = [vp, vp, i64, dbl, vp]
+        self.otf.grad_contract_otf_f64.restype = dbl
+        self.otf.grad_contract_otf_f64.argtypes = [vp, vp, i64, dbl, vp, vp]
+        self.otf.backgrad_contract_otf_f64.restype = dbl
+        self.otf.backgrad_contract_otf_f64.argtypes = [vp, vp, i64, dbl, vp, vp]
+        self.otf.batch_grad_contract_otf_f64.argtypes = [vp, vp, vp, vp, vp, vp]
+        self.bas.create_basis_manager.restype = vp
+        self.bas.create_basis_manager.argtypes = [i64, i64, i64, i64, vp, i64]
+        self.bas.get_subspace_dim.restype = i64
+        self.bas.get_subspace_dim.argtypes = [vp]
+        self.bas.get_num_symmetry_blocks.restype = i64
+        self.bas.get_num_symmetry_blocks.argtypes = [vp]
+        self.bas.destroy_basis_manager.argtypes = [vp]
+        self.bas.set_det_coeff_f64.argtypes = [vp, C.c_uint32, C.c_uint32, dbl, vp]
+        for name in ("build_ritz_and_residual_f64", "mgs_orthogonalize_f64", "inplace_normalize_f64",
+                     "fast_dot_f64"):
+            getattr(self.diag, name).restype = dbl
+        self.diag.build_ritz_and_residual_f64.argtypes = [i64, C.c_int, vp, dbl, vp, vp, vp]
+        self.diag.build_ritz_vector_f64.argtypes = [i64, C.c_int, vp, vp, vp]
+        self.diag.apply_preconditioner_inplace_f64.argtypes = [i64, vp, vp, dbl, dbl]
+        self.diag.mgs_orthogonalize_f64.argtypes = [i64, C.c_int, vp, vp]
+        self.diag.inplace_normalize_f64.argtypes = [i64, vp]
+        self.diag.fast_dot_f64.argtypes = [i64, vp, vp]
+        self.diag.compute_heff_col_f64.argtypes = [i64, C.c_int, vp, vp, vp]
+        self._keep = []
+
+    def hamiltonian_terms(self, h, g, e_nuc=0.0, tol=1e-12):
+        """Raw (ax, az, bx, bz, cs) from generate_hamiltonian_real_64_128_f64
+        (integrals passed column-major as Julia does, ham.hpp:214-241)."""
+        h1 = np.asfortranarray(h, np.float64); g4 = np.asfortranarray(g, np.float64)
+        r = self.ham.generate_hamiltonian_real_64_128_f64(e_nuc, h1.ctypes.data, g4.ctypes.data,
+                                                          h.shape[0], tol, False)
+        n = r.ncs
+        U = lambda p: np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint32)), (n,)).astype(np.uint64)
+        cs = np.ctypeslib.as_array(r.cs, (n,)).copy() if n else np.zeros(0)
+        return U(r.axs), U(r.azs), U(r.bxs), U(r.bzs), cs
+
+    def basis(self, norb, na, nb, orbsym=None, total_sym=0, num_irreps=16):
+        orbsym = np.zeros(norb, np.int64) if orbsym is None else np.ascontiguousarray(orbsym, np.int64)
+        h = self.bas.create_basis_manager(norb, na, nb, total_sym, P(orbsym), num_irreps)
+        self._keep.append(orbsym)
+        return h, self.bas.get_subspace_dim(h)
+
+    def network(self, net):
+        a = [np.ascontiguousarray(net.orbsym, np.int64)]
+        arrs = [np.ascontiguousarray(net.axs, np.uint32), np.ascontiguousarray(net.bxs, np.uint32),
+                np.ascontiguousarray(net.ranks, np.int64), np.ascontiguousarray(net.num_zas, np.int64),
+                np.ascontiguousarray(net.num_zbs, np.int64), np.ascontiguousarray(net.flat_zas, np.uint32),
+                np.ascontiguousarray(net.flat_zbs, np.uint32), np.ascontiguousarray(net.flat_wa, np.float64),
+                np.ascontiguousarray(net.flat_wb, np.float64)]
+        h = self.otf.build_network_otf_f64(P(a[0]), net.norb, net.ngs, *[P(x) for x in arrs])
+        self._keep.append((a, arrs))
+        return h
+
+    def hvec(self, b, n, x, dim):
+        x = np.ascontiguousarray(x, np.float64); y = np.zeros(dim)
+        self.otf.hvec_gather_contract_otf_f64(b, n, P(x), P(y))
+        return y
+
+    def diag_elems(self, b, n, dim):
+        d = np.zeros(dim)
+        self.otf.get_diags_elements_f64(b, n, P(d))
+        return d
+
+    def expm(self, b, n, idx, theta, v):
+        v = np.array(v, np.float64, copy=True)
+        self.otf.expm_contract_otf_f64(b, n, idx, theta, P(v))
+        return v
+
+    def grad(self, b, n, idx, theta, l, r):
+        return self.otf.grad_contract_otf_f64(b, n, idx, theta, P(np.ascontiguousarray(l)), P(np.ascontiguousarray(r)))
+
+    def backgrad(self, b, n, idx, theta, l, r):
+        l = np.array(l, np.float64, copy=True); r = np.array(r, np.float64, copy=True)
+        g = self.otf.backgrad_contract_otf_f64(b, n, idx, theta, P(l), P(r))
+        return g, l, r
+
+    def batchgrad(self, b, n, thetas, l, r, ngs):
+        g = np.zeros(ngs)
+        self.otf.batch_grad_contract_otf_f64(b, n, P(np.ascontiguousarray(thetas, np.float64)),
+                                             P(np.ascontiguousarray(l)), P(np.ascontiguousarray(r)), P(g))
+        return g
+
+    def det_index(self, b, astr, bstr, dim):
+        v = np.zeros(dim)
+        self.bas.set_det_coeff_f64(b, astr, bstr, 1.0, P(v))
+        nz = np.flatnonzero(v)
+        return int(nz[0]) if len(nz) else -1

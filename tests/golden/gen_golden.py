@@ -1,0 +1,76 @@
+"""Generate the golden fixtures of tests/golden/ from the reference's own CPU
+libraries (oracle/_ref, compiled from the reference sources by oracle/Makefile).
+
+Each fixture stores the inputs (the OTF network as flat arrays, basis
+parameters, seeded vectors, angles) and the reference outputs of
+hvec_gather_contract_otf_f64, get_diags_elements_f64, expm/grad/backgrad/
+batch_grad_contract_otf_f64 and a few libdiag helpers.  Run:
+
+    python tests/golden/gen_golden.py
+
+Small sizes only (dim <= 4900) so the fixtures stay a few hundred KB.
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from binsim_b200 import network as nw  # noqa: E402
+from oracle.oracle import RefLibs, build_ref  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+CASES = [
+    # name, norb, na, nb, orbsym, total_sym, num_irreps, seed
+    ("h6_3a3b", 6, 3, 3, None, 0, 16, 11),
+    ("h8_4a3b_sym", 8, 4, 3, [0, 1, 0, 1, 2, 3, 2, 3], 1, 4, 12),
+    ("h8_4a4b", 8, 4, 4, None, 0, 16, 13),
+]
+
+
+def net_arrays(prefix, net):
+    return {f"{prefix}_{k}": np.asarray(getattr(net, k)) for k in
+            ("orbsym", "axs", "bxs", "ranks", "num_zas", "num_zbs", "flat_zas", "flat_zbs", "flat_wa", "flat_wb")} | \
+        {f"{prefix}_norb": np.asarray(net.norb)}
+
+
+def main():
+    if not build_ref():
+        raise SystemExit("reference libraries unavailable (need the reference sources)")
+    ref = RefLibs()
+    for name, norb, na, nb, orbsym, tsym, nirr, seed in CASES:
+        ham = nw.hamiltonian_network(norb, seed=seed)
+        pool = nw.ucc_pool(norb).network
+        osym = np.zeros(norb, np.int64) if orbsym is None else np.asarray(orbsym, np.int64)
+        ham.orbsym = osym
+        pool.orbsym = osym
+        rb, dim = ref.basis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=nirr)
+        rh, rp = ref.network(ham), ref.network(pool)
+        rng = np.random.default_rng(seed)
+        x = rng.normal(size=dim); x /= np.linalg.norm(x)
+        y = rng.normal(size=dim); y /= np.linalg.norm(y)
+        sigma = ref.hvec(rb, rh, x, dim)
+        diag = ref.diag_elems(rb, rh, dim)
+        ops = rng.choice(pool.ngs, size=min(12 if dim <= 1000 else 4, pool.ngs), replace=False)
+        thetas = rng.normal(0, 0.7, size=len(ops))
+        expm = np.stack([ref.expm(rb, rp, int(i), t, x) for i, t in zip(ops, thetas)])
+        grad = np.array([ref.grad(rb, rp, int(i), t, x, y) for i, t in zip(ops, thetas)])
+        bg = [ref.backgrad(rb, rp, int(i), t, x, y) for i, t in zip(ops, thetas)]
+        bth = rng.normal(0, 0.3, size=pool.ngs)
+        batch = ref.batchgrad(rb, rp, bth, x, sigma, pool.ngs)
+        hf = ref.det_index(rb, (1 << na) - 1, (1 << nb) - 1, dim)
+        np.savez_compressed(
+            os.path.join(OUT, f"{name}.npz"),
+            norb=norb, na=na, nb=nb, orbsym=osym, total_sym=tsym, num_irreps=nirr, dim=dim, hf=hf,
+            x=x, y=y, sigma=sigma, diag=diag, ops=ops, thetas=thetas, expm=expm, grad=grad,
+            backgrad=np.array([b[0] for b in bg]), backgrad_l=np.stack([b[1] for b in bg]),
+            backgrad_r=np.stack([b[2] for b in bg]), batch_thetas=bth, batchgrad=batch,
+            **net_arrays("ham", ham), **net_arrays("pool", pool))
+        print(name, "dim", dim, "ham groups", ham.ngs, "pool groups", pool.ngs)
+
+
+if __name__ == "__main__":
+    main()

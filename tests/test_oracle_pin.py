@@ -1,0 +1,96 @@
+"""Pin the C restatement (oracle/otf_oracle.c) against the reference.
+
+* against the golden fixtures made by the reference's own libraries
+  (tests/golden/gen_golden.py) -- runs everywhere;
+* against the reference libraries directly (oracle/_ref) on fresh seeded
+  inputs -- runs where they are built.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, load_golden
+
+TOL = 1e-12
+
+
+def _basis(oracle, z):
+    return oracle.basis(int(z["norb"]), int(z["na"]), int(z["nb"]), orbsym=z["orbsym"],
+                        total_sym=int(z["total_sym"]), num_irreps=int(z["num_irreps"]))
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_matches_golden(oracle, name):
+    z, ham, pool = load_golden(name)
+    B = _basis(oracle, z)
+    assert B.dim == int(z["dim"])
+    H, P = oracle.network(ham), oracle.network(pool)
+    x, y = z["x"], z["y"]
+    scale = np.abs(z["sigma"]).max()
+    np.testing.assert_allclose(oracle.hvec(B, H, x), z["sigma"], rtol=0, atol=TOL * scale)
+    np.testing.assert_allclose(oracle.diag(B, H), z["diag"], rtol=0, atol=TOL * np.abs(z["diag"]).max())
+    for k, (i, t) in enumerate(zip(z["ops"], z["thetas"])):
+        np.testing.assert_allclose(oracle.expm(B, P, int(i), t, x), z["expm"][k], rtol=0, atol=1e-14)
+        assert abs(oracle.grad(B, P, int(i), t, x, y) - z["grad"][k]) < 1e-13
+        g, l2, r2 = oracle.backgrad(B, P, int(i), t, x, y)
+        assert abs(g - z["backgrad"][k]) < 1e-13
+        np.testing.assert_allclose(l2, z["backgrad_l"][k], rtol=0, atol=1e-14)
+        np.testing.assert_allclose(r2, z["backgrad_r"][k], rtol=0, atol=1e-14)
+    bg = oracle.batchgrad(B, P, z["batch_thetas"], x, z["sigma"])
+    np.testing.assert_allclose(bg, z["batchgrad"], rtol=0, atol=TOL * max(1.0, np.abs(z["batchgrad"]).max()))
+    assert B.det_index((1 << int(z["na"])) - 1, (1 << int(z["nb"])) - 1) == int(z["hf"])
+
+
+@pytest.mark.parametrize("norb,na,nb,orbsym,tsym", [
+    (5, 2, 3, None, 0),
+    (7, 3, 3, [0, 1, 2, 3, 0, 1, 2], 2),
+    (8, 4, 4, [0, 1, 1, 0, 2, 3, 3, 2], 0),
+])
+def test_oracle_matches_reference_libs(oracle, reflibs, norb, na, nb, orbsym, tsym):
+    from binsim_b200 import network as nw
+    osym = np.zeros(norb, np.int64) if orbsym is None else np.asarray(orbsym, np.int64)
+    ham = nw.hamiltonian_network(norb, seed=norb * 7 + 1)
+    pool = nw.ucc_pool(norb).network
+    ham.orbsym = osym; pool.orbsym = osym
+    rb, dim = reflibs.basis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
+    B = oracle.basis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
+    assert B.dim == dim
+    rh, rp = reflibs.network(ham), reflibs.network(pool)
+    H, P = oracle.network(ham), oracle.network(pool)
+    rng = np.random.default_rng(norb)
+    x, y = rng.normal(size=dim), rng.normal(size=dim)
+    s_ref = reflibs.hvec(rb, rh, x, dim)
+    np.testing.assert_allclose(oracle.hvec(B, H, x), s_ref, rtol=0, atol=1e-12 * np.abs(s_ref).max())
+    np.testing.assert_allclose(oracle.diag(B, H), reflibs.diag_elems(rb, rh, dim), rtol=0, atol=1e-12)
+    for i in rng.choice(pool.ngs, 25, replace=False):
+        t = rng.normal()
+        np.testing.assert_allclose(oracle.expm(B, P, int(i), t, x), reflibs.expm(rb, rp, int(i), t, x), atol=1e-13)
+        assert abs(oracle.grad(B, P, int(i), t, x, y) - reflibs.grad(rb, rp, int(i), t, x, y)) < 1e-11
+    th = rng.normal(size=pool.ngs)
+    np.testing.assert_allclose(oracle.batchgrad(B, P, th, x, y), reflibs.batchgrad(rb, rp, th, x, y, pool.ngs),
+                               atol=1e-10)
+
+
+def test_oracle_davidson_helpers_match_libdiag(oracle, reflibs):
+    import ctypes as C
+    rng = np.random.default_rng(5)
+    n, k = 3001, 5
+    Q = np.linalg.qr(rng.normal(size=(n, k)))[0]
+    V = [np.ascontiguousarray(Q[:, j]) for j in range(k)]
+    AV = [rng.normal(size=n) for _ in range(k)]
+    c = rng.normal(size=k)
+    d = rng.normal(size=n)
+    arr = lambda vs: (C.c_void_p * len(vs))(*[v.ctypes.data for v in vs])
+    out = np.zeros(n)
+    nr = reflibs.diag.build_ritz_and_residual_f64(n, k, c.ctypes.data, 0.3, arr(V), arr(AV), out.ctypes.data)
+    nr2, out2 = oracle.ritz_residual(c, 0.3, V, AV)
+    assert abs(nr - nr2) < 1e-10 and np.abs(out - out2).max() < 1e-12
+    r = rng.normal(size=n); r1 = r.copy()
+    reflibs.diag.apply_preconditioner_inplace_f64(n, r1.ctypes.data, d.ctypes.data, 0.1, 0.05)
+    np.testing.assert_allclose(oracle.precondition(r, d, 0.1, 0.05), r1, rtol=1e-15)
+    v = rng.normal(size=n); v1 = v.copy()
+    m1 = reflibs.diag.mgs_orthogonalize_f64(n, k, arr(V), v1.ctypes.data)
+    m2, v2 = oracle.mgs(V, v)
+    assert abs(m1 - m2) < 1e-12 * m1 and np.abs(v1 - v2).max() < 1e-12
+    col = np.zeros(k)
+    reflibs.diag.compute_heff_col_f64(n, k, arr(V), AV[0].ctypes.data, col.ctypes.data)
+    np.testing.assert_allclose(oracle.heff_col(V, AV[0]), col, rtol=1e-12)

@@ -241,6 +241,16 @@ int bsim_hvec_f32in(void *basis, void *net, const float *src, double *dst, bsim_
     return bsim::sigma(B(basis), N(net), nullptr, src, dst, true, stream);
 }
 
+int64_t bsim_hvec_num_tiles(void *basis) { return check(basis, nullptr) == BSIM_OK ? bsim::num_tiles(B(basis)) : -1; }
+
+int bsim_hvec_tiles(void *basis, void *net, const double *src, double *dst, int64_t tile_lo, int64_t tile_hi,
+                    int mixed, bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(src); NEED(dst);
+    return bsim::sigma_tiles(B(basis), N(net), src, nullptr, dst, mixed != 0, tile_lo, tile_hi, stream);
+}
+
 int bsim_diag(void *basis, void *net, double *diags, bsim_stream_t stream)
 {
     CHECK2(basis, net);

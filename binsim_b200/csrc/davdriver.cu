@@ -57,6 +57,13 @@ __global__ void resid_kernel(i64 n, const double *__restrict__ x, const double *
         r[i] = ax[i] - e * x[i];
 }
 
+// x = a * x + t
+__global__ void axpby_kernel(i64 n, double a, double *__restrict__ x, const double *__restrict__ t)
+{
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+        x[i] = a * x[i] + t[i];
+}
+
 }  // namespace
 
 #define TRY(...) do { int st__ = (__VA_ARGS__); if (st__ != BSIM_OK) return st__; } while (0)
@@ -177,10 +184,13 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
         TRY(alloc<float>(vb[j], n, s)); TRY(alloc<float>(avb[j], n, s));
         V[j] = (float *)vb[j].p; AV[j] = (float *)avb[j].p;
     }
-    DevBuf xb, axb, rb, tb;
+    DevBuf xb, axb, rb, tb, ayb;
     TRY(alloc<double>(xb, n, s)); TRY(alloc<double>(axb, n, s)); TRY(alloc<double>(rb, n, s));
-    TRY(alloc<double>(tb, n, s));
+    TRY(alloc<double>(tb, n, s)); TRY(alloc<double>(ayb, n, s));
+    // x: current FP64 vector, ax = H x (FP64), r = ax - E x, t: expansion vector,
+    // ay: FP32-bulk sigma of the newest subspace vector
     double *x = (double *)xb.p, *ax = (double *)axb.p, *r = (double *)rb.p, *t = (double *)tb.p;
+    double *ay = (double *)ayb.p;
     double *sc = S.res + kMaxSub;
     DavStats st{};
     const int grid = 1184;
@@ -227,23 +237,37 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
             TRY(dav_normalize(S, n, t, sc, s));
             cvt_kernel_d2f<<<grid, 256, 0, s>>>(t, V[dim], n);
             // FP32-bulk sigma straight from the FP32 basis vector
-            TRY(sigma(B, N, nullptr, V[dim], ax, true, s));
+            TRY(sigma(B, N, nullptr, V[dim], ay, true, s));
             st.sigma_fp32++;
             ++total_inner;
-            cvt_kernel_d2f<<<grid, 256, 0, s>>>(ax, AV[dim], n);
+            cvt_kernel_d2f<<<grid, 256, 0, s>>>(ay, AV[dim], n);
             ++dim;
             TRY(dav_multidot<float, float>(S, n, dim, V.data(), AV[dim - 1], S.res, s));
-            TRY(fetch(col, S.res, dim, s));
+            // the coupling to the current vector, <x|H|V_j> = <H x|V_j>, from the
+            // FP64 sigma of x: near convergence it drives the correction, so it
+            // must not carry the FP32-bulk sigma's rounding
+            TRY(dav_multidot<float, double>(S, n, 1, V.data() + (dim - 1), ax, S.res + dim, s));
+            TRY(fetch(col, S.res, dim + 1, s));
+            col[0] = col[dim];
             for (int i = 0; i < dim; ++i) h[i + (dim - 1) * kMaxSub] = h[(dim - 1) + i * kMaxSub] = col[i];
             jacobi_eigh(dim, h, kMaxSub, es, vs);
             e_in = es[0];
+            const double rprev = rin;
             TRY(dav_ritz_residual<float>(S, n, dim, vs, e_in, V.data(), AV.data(), t, sc, s));
             TRY(fetch(&rin, sc, 1, s));
             if (verbose) printf("    inner %02d: residual %.4e e %.14f\n", it, rin, e_in);
-            if (rin < 0.05 * rnorm || rin < 0.5 * tol || total_inner >= maxiter) break;
+            // leave for an FP64 refinement once the inner residual dropped enough or
+            // stalls at the FP32 noise floor
+            if (rin < 0.05 * rnorm || rin < 0.5 * tol || (it >= 1 && rin > 0.8 * rprev) || total_inner >= maxiter)
+                break;
         }
         jacobi_eigh(dim, h, kMaxSub, es, vs);
-        TRY(dav_combine<float, double>(n, dim, vs, V.data(), x, s));
+        // x <- y0 * x + sum_{j>=1} y_j V_j: the FP64 vector keeps its precision and
+        // only the correction, small near convergence, carries FP32 rounding.
+        if (dim > 1) {
+            TRY(dav_combine<float, double>(n, dim - 1, vs + 1, V.data() + 1, t, s));
+            axpby_kernel<<<grid, 256, 0, s>>>(n, vs[0], x, t);
+        }
         TRY(dav_normalize(S, n, x, sc, s));
     }
     st.iterations = total_inner;

@@ -13,6 +13,14 @@ template <typename Ti>
 int sigma(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32, double *dst,
           bool mixed, cudaStream_t s);
 
+// As sigma, restricted to flat tiles [tile_lo, tile_hi) (32-row x 32-column
+// destination tiles, block-major then row-major); other elements untouched.
+template <typename Ti>
+int sigma_tiles(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32, double *dst,
+                bool mixed, i64 tile_lo, i64 tile_hi, cudaStream_t s);
+template <typename Ti>
+i64 num_tiles(const DevBasis<Ti> *B);
+
 template <typename Ti>
 int diag_elements(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *diag, cudaStream_t s);
 

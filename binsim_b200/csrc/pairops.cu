@@ -48,7 +48,7 @@ pair_row_kernel(const BasisView<Ti> B, const NetView<Ti> N, int gid, PairAngles 
     }
     if (active) {
         s_a = B.astrs[B.blk_astart[kd] + a] ^ (Ti)g.ax;
-        sa = g.ax ? B.amap[s_a] : a;
+        sa = g.ax ? (((u64)s_a >> B.norb) ? -1 : B.amap[s_a]) : a;
         active = sa >= 0 && !(ks == kd && g.type != 2 && sa < a);
     }
     double acc = 0.0;
@@ -74,7 +74,7 @@ pair_row_kernel(const BasisView<Ti> B, const NetView<Ti> N, int gid, PairAngles 
         const double *wb = N.w + g.wb_off;
         for (int b = threadIdx.x; b < nb; b += blockDim.x) {
             const Ti s_b = bstrs[b] ^ (Ti)g.bx;
-            const int sb = g.bx ? B.bmap[s_b] : b;
+            const int sb = g.bx ? (((u64)s_b >> B.norb) ? -1 : B.bmap[s_b]) : b;
             if (sb < 0 || (same && g.type == 2 && sb < b)) continue;
             double vt = 0.0;
             for (int rr = 0; rr < R; ++rr) {

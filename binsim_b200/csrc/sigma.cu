@@ -18,11 +18,12 @@ template <typename Ti, bool MIXED>
 __global__ void __launch_bounds__(kTileThreads)
 sigma_tile_kernel(const BasisView<Ti> B, const NetView<Ti> N, const int *__restrict__ plan_g,
                   const int4 *__restrict__ chunks, int nchunks, const i64 *__restrict__ tile_start,
-                  const double *__restrict__ src, const float *__restrict__ src32, double *__restrict__ dst)
+                  const double *__restrict__ src, const float *__restrict__ src32, double *__restrict__ dst,
+                  i64 tile_lo)
 {
     using Tw = typename std::conditional<MIXED, float, double>::type;
     __shared__ TileSmem<Tw> S;
-    const TileCoord c = decode_tile(B, tile_start, blockIdx.x);
+    const TileCoord c = decode_tile(B, tile_start, tile_lo + blockIdx.x);
     const int lane = threadIdx.x & 31, wrow = (threadIdx.x >> 5) * kRowsPerWarp;
     double acc[kRowsPerWarp] = {0.0, 0.0, 0.0, 0.0};
 
@@ -128,8 +129,17 @@ int tile_prefix(const DevBasis<Ti> *B, Workspace &ws, const i64 **out_dev, i64 *
 }
 
 template <typename Ti>
-int sigma(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32, double *dst,
-          bool mixed, cudaStream_t s)
+i64 num_tiles(const DevBasis<Ti> *B)
+{
+    i64 t = 0;
+    for (int k = 0; k < B->num_blocks; ++k)
+        t += (i64)((B->na[k] + kTile - 1) / kTile) * ((B->nb[k] + kTile - 1) / kTile);
+    return t;
+}
+
+template <typename Ti>
+int sigma_tiles(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32, double *dst,
+                bool mixed, i64 tile_lo, i64 tile_hi, cudaStream_t s)
 {
     if (B->dim == 0) return BSIM_OK;
     Workspace &ws = workspace_for(B);
@@ -137,9 +147,16 @@ int sigma(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const f
     i64 ntiles = 0;
     int st = tile_prefix(B, ws, &tp, &ntiles);
     if (st != BSIM_OK) return st;
-    if (ntiles > 0x7fffffffLL) { set_error("too many tiles"); return BSIM_ERR_TOO_LARGE; }
+    if (tile_lo < 0 || tile_hi > ntiles || tile_lo > tile_hi) {
+        set_error("tile range [%lld, %lld) outside [0, %lld)", tile_lo, tile_hi, ntiles);
+        return BSIM_ERR_ARG;
+    }
+    const i64 nt = tile_hi - tile_lo;
+    if (nt == 0) return BSIM_OK;
+    if (nt > 0x7fffffffLL) { set_error("too many tiles"); return BSIM_ERR_TOO_LARGE; }
     if (N->plan_chunks.empty()) {
-        BSIM_CUDA(cudaMemsetAsync(dst, 0, sizeof(double) * B->dim, s));
+        if (tile_lo == 0 && tile_hi == ntiles) BSIM_CUDA(cudaMemsetAsync(dst, 0, sizeof(double) * B->dim, s));
+        else { set_error("empty network with a partial tile range"); return BSIM_ERR_ARG; }
         return BSIM_OK;
     }
     if (mixed && !src32) {
@@ -150,13 +167,22 @@ int sigma(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const f
         src32 = tmp;
     }
     if (mixed)
-        sigma_tile_kernel<Ti, true><<<(unsigned)ntiles, kTileThreads, 0, s>>>(
-            B->view, N->view, N->d_plan_groups, N->d_plan_chunks, (int)N->plan_chunks.size(), tp, nullptr, src32, dst);
+        sigma_tile_kernel<Ti, true><<<(unsigned)nt, kTileThreads, 0, s>>>(
+            B->view, N->view, N->d_plan_groups, N->d_plan_chunks, (int)N->plan_chunks.size(), tp, nullptr, src32, dst,
+            tile_lo);
     else
-        sigma_tile_kernel<Ti, false><<<(unsigned)ntiles, kTileThreads, 0, s>>>(
-            B->view, N->view, N->d_plan_groups, N->d_plan_chunks, (int)N->plan_chunks.size(), tp, src, nullptr, dst);
+        sigma_tile_kernel<Ti, false><<<(unsigned)nt, kTileThreads, 0, s>>>(
+            B->view, N->view, N->d_plan_groups, N->d_plan_chunks, (int)N->plan_chunks.size(), tp, src, nullptr, dst,
+            tile_lo);
     BSIM_CUDA(cudaGetLastError());
     return BSIM_OK;
+}
+
+template <typename Ti>
+int sigma(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32, double *dst,
+          bool mixed, cudaStream_t s)
+{
+    return sigma_tiles(B, N, src, src32, dst, mixed, 0, num_tiles(B), s);
 }
 
 template <typename Ti>
@@ -176,6 +202,9 @@ int diag_elements(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *diag, cuda
 template int tile_prefix<unsigned>(const DevBasis<unsigned> *, Workspace &, const i64 **, i64 *);
 template int sigma<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *, const float *,
                              double *, bool, cudaStream_t);
+template int sigma_tiles<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *,
+                                   const float *, double *, bool, i64, i64, cudaStream_t);
+template i64 num_tiles<unsigned>(const DevBasis<unsigned> *);
 template int diag_elements<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, double *, cudaStream_t);
 
 }  // namespace bsim

@@ -70,7 +70,8 @@ def lib() -> C.CDLL:
         "bsim_network_from_host": (ci, [vp, vp]), "bsim_network_destroy": (ci, [vp]),
         "bsim_network_ngs": (i64, [vp]),
         "bsim_hvec": (ci, [vp, vp, vp, vp, vp]), "bsim_hvec_mixed": (ci, [vp, vp, vp, vp, vp]),
-        "bsim_hvec_f32in": (ci, [vp, vp, vp, vp, vp]), "bsim_diag": (ci, [vp, vp, vp, vp]),
+        "bsim_hvec_f32in": (ci, [vp, vp, vp, vp, vp]),
+        "bsim_hvec_num_tiles": (i64, [vp]), "bsim_hvec_tiles": (ci, [vp, vp, vp, vp, i64, i64, ci, vp]), "bsim_diag": (ci, [vp, vp, vp, vp]),
         "bsim_expm": (ci, [vp, vp, i64, dbl, vp, vp]), "bsim_expm_seq": (ci, [vp, vp, i64, vp, vp, vp, vp]),
         "bsim_grad": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_backgrad": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
@@ -208,6 +209,14 @@ class CuOTFFunctions:
 
     def hvec_mixed(self, v, Hv, stream=None):
         _check(lib().bsim_hvec_mixed(self.basis.h, self.ham.h, _ptr(v), _ptr(Hv), _stream(stream)), "hvec_mixed")
+
+    def hvec_tiles(self, v, Hv, tile_lo: int, tile_hi: int, mixed=False, stream=None):
+        """sigma on destination tiles [tile_lo, tile_hi) only (row sharding)."""
+        _check(lib().bsim_hvec_tiles(self.basis.h, self.ham.h, _ptr(v), _ptr(Hv), tile_lo, tile_hi,
+                                     1 if mixed else 0, _stream(stream)), "hvec_tiles")
+
+    def num_tiles(self) -> int:
+        return lib().bsim_hvec_num_tiles(self.basis.h)
 
     def get_diags(self, dv, stream=None):
         _check(lib().bsim_diag(self.basis.h, self.ham.h, _ptr(dv), _stream(stream)), "get_diags")

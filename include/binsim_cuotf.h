@@ -117,6 +117,14 @@ int bsim_hvec(void *basis, void *net, const double *src, double *dst, bsim_strea
 int bsim_hvec_mixed(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream);
 /* As bsim_hvec_mixed with an FP32 input vector. */
 int bsim_hvec_f32in(void *basis, void *net, const float *src, double *dst, bsim_stream_t stream);
+/* Number of 32 x 32 destination tiles of sigma (block-major, then row-major). */
+int64_t bsim_hvec_num_tiles(void *basis);
+/* sigma restricted to destination tiles [tile_lo, tile_hi): the rows of those
+ * tiles get (H src) there, every other element of dst is left untouched.  A
+ * contiguous tile range is a contiguous range of 32-row bands, so ranks that
+ * split [0, num_tiles) share sigma by destination rows.  mixed selects FP32 bulk. */
+int bsim_hvec_tiles(void *basis, void *net, const double *src, double *dst, int64_t tile_lo, int64_t tile_hi,
+                    int mixed, bsim_stream_t stream);
 /* diags += diagonal of H. */
 int bsim_diag(void *basis, void *net, double *diags, bsim_stream_t stream);
 /* vec <- exp(theta G_idx) vec. */

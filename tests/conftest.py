@@ -42,3 +42,24 @@ def reflibs():
     if not ref_available():
         pytest.skip("oracle/_ref (the reference's compiled CPU libraries) not built")
     return RefLibs()
+
+
+@pytest.fixture(scope="session")
+def cuda():
+    """torch with a CUDA device; GPU tests fail (not skip) without one."""
+    import torch
+    assert torch.cuda.is_available(), "GPU test run without a CUDA device"
+    return torch
+
+
+def dev(torch, a, dtype=None):
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda", dtype=dtype or torch.float64)
+
+
+def cu_setup(z, ham, pool):
+    from binsim_b200 import cuotf
+    B = cuotf.CuBasis(int(z["norb"]), int(z["na"]), int(z["nb"]), orbsym=z["orbsym"],
+                      total_sym=int(z["total_sym"]), num_irreps=int(z["num_irreps"]))
+    H = cuotf.CuNetwork(ham) if ham is not None else None
+    P = cuotf.CuNetwork(pool) if pool is not None else None
+    return B, H, P, cuotf.CuOTFFunctions(B, H, P)

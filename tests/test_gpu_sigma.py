@@ -1,0 +1,105 @@
+"""sigma = H c and diag(H) on the GPU against the oracle and the golden fixtures."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, cu_setup, dev, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_sigma_and_diag_match_golden(cuda, name):
+    z, ham, pool = load_golden(name)
+    B, H, P, f = cu_setup(z, ham, None)
+    assert B.dim == int(z["dim"])
+    x = dev(cuda, z["x"])
+    y = cuda.empty_like(x)
+    f.hvec(x, y)
+    scale = np.abs(z["sigma"]).max()
+    np.testing.assert_allclose(y.cpu().numpy(), z["sigma"], rtol=0, atol=1e-12 * scale)
+    d = cuda.zeros_like(x)
+    f.get_diags(d)
+    np.testing.assert_allclose(d.cpu().numpy(), z["diag"], rtol=0, atol=1e-12 * np.abs(z["diag"]).max())
+    assert B.hf_index() == int(z["hf"])
+
+
+@pytest.mark.parametrize("norb,na,nb,orbsym,tsym", [
+    (10, 5, 5, None, 0),
+    (10, 4, 5, [0, 1, 2, 3, 0, 1, 2, 3, 0, 1], 3),
+    (11, 3, 6, None, 0),
+])
+def test_sigma_matches_oracle(cuda, oracle, norb, na, nb, orbsym, tsym):
+    from binsim_b200 import cuotf, network as nw
+    osym = np.zeros(norb, np.int64) if orbsym is None else np.asarray(orbsym, np.int64)
+    net = nw.hamiltonian_network(norb, seed=norb + na)
+    net.orbsym = osym
+    Bo = oracle.basis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
+    No = oracle.network(net)
+    B = cuotf.CuBasis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    assert B.dim == Bo.dim
+    x = np.random.default_rng(norb).normal(size=B.dim)
+    ref = oracle.hvec(Bo, No, x)
+    y = cuda.empty(B.dim, dtype=cuda.float64, device="cuda")
+    f.hvec(dev(cuda, x), y)
+    np.testing.assert_allclose(y.cpu().numpy(), ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+    # FP32 bulk: per-chunk FP32 sums, FP64 across chunks
+    ym = cuda.empty_like(y)
+    f.hvec_mixed(dev(cuda, x), ym)
+    err = np.abs(ym.cpu().numpy() - ref).max() / np.abs(ref).max()
+    assert err < 2e-6, err
+    # FP32 input variant
+    from binsim_b200.cuotf import lib
+    y32 = cuda.empty_like(y)
+    assert lib().bsim_hvec_f32in(B.h, f.ham.h, dev(cuda, x, cuda.float32).data_ptr(), y32.data_ptr(), None) == 0
+    cuda.cuda.synchronize()
+    assert np.abs(y32.cpu().numpy() - ref).max() / np.abs(ref).max() < 2e-6
+
+
+def test_sigma_is_symmetric_operator(cuda):
+    """<u|H v> == <H u|v> on a 12-orbital case (size-independent property)."""
+    from binsim_b200 import cuotf, network as nw
+    net = nw.hamiltonian_network(12, seed=0)
+    B = cuotf.CuBasis(12, 6, 6)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    g = cuda.Generator(device="cuda").manual_seed(0)
+    u = cuda.randn(B.dim, dtype=cuda.float64, device="cuda", generator=g)
+    v = cuda.randn(B.dim, dtype=cuda.float64, device="cuda", generator=g)
+    hu, hv = cuda.empty_like(u), cuda.empty_like(v)
+    f.hvec(u, hu)
+    f.hvec(v, hv)
+    a, b = float(u @ hv), float(hu @ v)
+    assert abs(a - b) < 1e-10 * max(abs(a), 1.0)
+    # linearity: H(2u + 3v) = 2Hu + 3Hv
+    w = 2 * u + 3 * v
+    hw = cuda.empty_like(w)
+    f.hvec(w, hw)
+    assert float((hw - 2 * hu - 3 * hv).abs().max()) < 1e-10 * float(hw.abs().max())
+
+
+def test_reference_host_handles(cuda, reflibs):
+    """build_basisdev_f64 / build_networkdev_f64 accept the reference's host handles."""
+    from binsim_b200 import cuotf, network as nw
+    L = cuotf.lib()
+    norb, na, nb = 8, 4, 3
+    osym = np.array([0, 1, 0, 1, 2, 3, 2, 3], np.int64)
+    net = nw.hamiltonian_network(norb, seed=4)
+    net.orbsym = osym
+    rb, dim = reflibs.basis(norb, na, nb, orbsym=osym, total_sym=2, num_irreps=4)
+    rn = reflibs.network(net)
+    db = L.build_basisdev_f64(rb)
+    dn = L.build_networkdev_f64(rn)
+    assert db and dn
+    x = np.random.default_rng(2).normal(size=dim)
+    xd = dev(cuda, x)
+    yd = cuda.zeros_like(xd)
+    L.hvec_cuda(db, dn, xd.data_ptr(), yd.data_ptr())
+    L.sync_device_cuda()
+    ref = reflibs.hvec(rb, rn, x, dim)
+    np.testing.assert_allclose(yd.cpu().numpy(), ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+    d = cuda.zeros_like(xd)
+    L.get_diags_elements_cuda(db, dn, d.data_ptr())
+    L.sync_device_cuda()
+    np.testing.assert_allclose(d.cpu().numpy(), reflibs.diag_elems(rb, rn, dim), atol=1e-12)
+    L.destroy_networkdev_f64(dn)
+    L.destroy_basisdev_f64(db)

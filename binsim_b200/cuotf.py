@@ -75,6 +75,7 @@ def lib() -> C.CDLL:
         "bsim_expm": (ci, [vp, vp, i64, dbl, vp, vp]), "bsim_expm_seq": (ci, [vp, vp, i64, vp, vp, vp, vp]),
         "bsim_grad": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_backgrad": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
+        "bsim_grad_noalloc": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_batchgrad": (ci, [vp, vp, vp, vp, vp, vp, vp]),
         "bsim_prepare_state": (ci, [vp, vp, i64, vp, vp, vp, vp, vp, i64, vp, vp]),
         "bsim_vqe_energy_grad": (ci, [vp, vp, vp, i64, vp, vp, i64, vp, vp, vp, i64, i64, vp, vp, vp, vp, vp, vp]),

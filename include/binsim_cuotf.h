@@ -135,6 +135,18 @@ int bsim_expm_seq(void *basis, void *net, int64_t n, const int64_t *idx, const d
 /* *out_dev (a device double) = grad term; nothing is read back. */
 int bsim_grad(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r,
               double *out_dev, bsim_stream_t stream);
+/* No counterpart in the reference.  The same result as bsim_grad, for callers
+ * that must not allocate device memory once running (a host whose memory pool
+ * already owns the device, or a loop that cannot afford cudaMalloc's implicit
+ * synchronisation): its reduction scratch is a fixed array inside the library
+ * (65536 partial sums, 512 KiB per GPU, held until the process exits), so no
+ * call allocates.  Limit: (alpha strings of the largest block) x (symmetry
+ * blocks) <= 65536, else BSIM_ERR_TOO_LARGE and nothing runs.  The first call
+ * on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU (other streams or host threads) race, so issue them on one stream. */
+int bsim_grad_noalloc(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r,
+                      double *out_dev, bsim_stream_t stream);
 /* Fused adjoint step; *out_dev (device) = gradient term. */
 int bsim_backgrad(void *basis, void *net, int64_t idx, double theta, double *l, double *r, double *out_dev,
                   bsim_stream_t stream);

@@ -260,7 +260,12 @@ def gpu_sigma(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
 
     def step(mixed=False):
-        f.hvec_tiles(x, y, lo, hi, mixed=mixed)
+        if world == 1:
+            (f.hvec_mixed if mixed else f.hvec)(x, y)
+        else:
+            f.hvec_tiles(x, y, lo, hi, mixed=mixed)
+    path = f.sigma_path()
+    log(f"[rank {rank}] sigma path {path}")
 
     def timed(fn, k, w):
         for _ in range(w):
@@ -299,7 +304,7 @@ def gpu_sigma(args, rank, world, local_rank):
 
     def e2e_step():
         x.copy_(xpin, non_blocking=True)
-        f.hvec_tiles(x, y, lo, hi)
+        step(False)
         ypin.copy_(y, non_blocking=True)
     ms_e2e = timed(e2e_step, max(1, args.steps // 2), 1)
 
@@ -334,6 +339,7 @@ def gpu_sigma(args, rank, world, local_rank):
                                  "flops_per_sigma": flops, "note": "(2r+1) flops per connected pair; "
                                                                    "peak is the nominal FP64 figure"},
             "pair_updates_per_s": float(pairs.sum()) / (ms * 1e-3),
+            "sigma_path": {"path": path[0], "reason": path[1], "residual_groups": path[2]},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
         }

@@ -241,6 +241,18 @@ int bsim_hvec_f32in(void *basis, void *net, const float *src, double *dst, bsim_
     return bsim::sigma(B(basis), N(net), nullptr, src, dst, true, stream);
 }
 
+int bsim_hvec_path(void *basis, void *net, char *why, int why_len, int *residual_groups)
+{
+    CHECK2(basis, net);
+    std::string w;
+    int nres = 0;
+    int r = bsim::fast_sigma_info(B(basis), N(net), &w, &nres);
+    if (r < 0) return r;
+    if (why && why_len > 0) snprintf(why, why_len, "%s", w.c_str());
+    if (residual_groups) *residual_groups = nres;
+    return r;
+}
+
 int64_t bsim_hvec_num_tiles(void *basis) { return check(basis, nullptr) == BSIM_OK ? bsim::num_tiles(B(basis)) : -1; }
 
 int bsim_hvec_tiles(void *basis, void *net, const double *src, double *dst, int64_t tile_lo, int64_t tile_hi,

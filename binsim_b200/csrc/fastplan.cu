@@ -1,0 +1,307 @@
+// Host-side construction of the structured sigma plan (see fastplan.h).
+#include "fastplan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <unordered_map>
+
+namespace bsim {
+
+namespace {
+
+inline int popc(u64 x) { return __builtin_popcountll(x); }
+
+// Ma(bx): alpha orbitals with an odd number of bx bits strictly below them.
+u64 mask_below_odd(u64 x, int norb)
+{
+    u64 m = 0;
+    for (int i = 0; i < norb; ++i)
+        if (popc(x & ((1ull << i) - 1)) & 1) m |= 1ull << i;
+    return m;
+}
+
+// Mb(ax): beta orbitals with an odd number of ax bits strictly above them.
+u64 mask_above_odd(u64 x, int norb)
+{
+    u64 m = 0;
+    for (int j = 0; j < norb; ++j)
+        if (popc(x >> (j + 1)) & 1) m |= 1ull << j;
+    return m;
+}
+
+template <typename Ti>
+double phase_r(u64 s, const Ti *z, int nz, const double *w, int r, u64 zxor)
+{
+    const double *wr = w + (i64)r * nz;
+    double v = 0.0;
+    for (int k = 0; k < nz; ++k) v += (popc(s & ((u64)z[k] ^ zxor)) & 1) ? -wr[k] : wr[k];
+    return v;
+}
+
+u64 comb_count(int n, int k)
+{
+    if (k < 0 || k > n) return 0;
+    u64 r = 1;
+    for (int i = 1; i <= k; ++i) r = r * (u64)(n - k + i) / (u64)i;
+    return r;
+}
+
+}  // namespace
+
+template <typename Ti>
+int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
+{
+    P->ok = false;
+    P->basis = B;
+    P->basis_dim = B->dim;
+    if (B->num_blocks != 1) { P->why = "more than one symmetry block"; return BSIM_OK; }
+    const int norb = B->norb;
+    const int nA = B->na[0], nB = B->nb[0];
+    const auto &A = B->astrs;
+    const auto &Bs = B->bstrs;
+    const int nelA = popc((u64)A[0]), nelB = popc((u64)Bs[0]);
+    if ((u64)nA != comb_count(norb, nelA) || (u64)nB != comb_count(norb, nelB)) {
+        P->why = "string lists are not complete (symmetry-restricted)";
+        return BSIM_OK;
+    }
+    if (norb > 24) { P->why = "norb > 24"; return BSIM_OK; }
+    P->norb = norb; P->nA = nA; P->nB = nB; P->nelA = nelA; P->nelB = nelB;
+    P->Ka.resize(nA);
+    for (int a = 0; a < nA; ++a) {
+        u64 k = 0, s = (u64)A[a];
+        for (int i = 0; i < norb; ++i)
+            if ((s >> i) & 1u) k ^= (1ull << i) - 1;
+        P->Ka[a] = k;
+    }
+
+    const Ti *z = N->z.data();
+    const double *w = N->w.data();
+    std::vector<int> diag, pa, pb, mixed;
+    for (i64 g = 0; g < N->ngs; ++g) {
+        const GroupDev &G = N->groups[g];
+        if (G.rank == 0) continue;
+        if (G.type == 0) (diag.empty() ? diag : P->residual).push_back((int)g);
+        else if (G.type == 1) (G.rank <= kSideMaxRank ? pa : P->residual).push_back((int)g);
+        else if (G.type == 2) (G.rank <= kSideMaxRank ? pb : P->residual).push_back((int)g);
+        else mixed.push_back((int)g);
+    }
+
+    // ---- diagonal tables --------------------------------------------------------
+    std::vector<double> PAd, PBd;
+    if (!diag.empty()) {
+        const GroupDev &G = N->groups[diag[0]];
+        P->rank_d = G.rank;
+        PAd.resize((size_t)nA * G.rank);
+        PBd.resize((size_t)nB * G.rank);
+        for (int a = 0; a < nA; ++a)
+            for (int r = 0; r < G.rank; ++r) PAd[(size_t)a * G.rank + r] = phase_r(A[a], z + G.za_off, G.nza, w + G.wa_off, r, 0);
+        for (int b = 0; b < nB; ++b)
+            for (int r = 0; r < G.rank; ++r) PBd[(size_t)b * G.rank + r] = phase_r(Bs[b], z + G.zb_off, G.nzb, w + G.wb_off, r, 0);
+    }
+
+    // ---- pure sides: row-spin data + column factor in the alpha-first frame -----
+    struct SideHost {
+        std::vector<u64> x, zmask;
+        std::vector<int> rank, nz, colmode;
+        std::vector<i64> z_off, w_off, ctab_off;
+        std::vector<double> wv, cconst, ctab;
+    } sh[2];
+    auto add_side = [&](int side, const std::vector<int> &gl) {
+        SideHost &S = sh[side];
+        const auto &colstr = side == 0 ? Bs : A;
+        const int ncol = side == 0 ? nB : nA;
+        for (int g : gl) {
+            const GroupDev &G = N->groups[g];
+            const u64 rowx = side == 0 ? G.ax : G.bx;
+            const Ti *rz = z + (side == 0 ? G.za_off : G.zb_off);
+            const int rnz = side == 0 ? G.nza : G.nzb;
+            const double *rw = w + (side == 0 ? G.wa_off : G.wb_off);
+            const Ti *cz = z + (side == 0 ? G.zb_off : G.za_off);
+            const int cnz = side == 0 ? G.nzb : G.nza;
+            const double *cw = w + (side == 0 ? G.wb_off : G.wa_off);
+            // the frame flips the column factor by (-1)^{popc(col & M)}
+            const u64 cm = side == 0 ? mask_above_odd(rowx, norb) : mask_below_odd(rowx, norb);
+            std::vector<double> col((size_t)G.rank * ncol);
+            bool constant = true;
+            for (int r = 0; r < G.rank; ++r)
+                for (int c = 0; c < ncol; ++c) {
+                    double v = phase_r((u64)colstr[c], cz, cnz, cw, r, cm);
+                    col[(size_t)r * ncol + c] = v;
+                    if (std::fabs(v - col[(size_t)r * ncol]) > 1e-13 * std::max(1.0, std::fabs(col[(size_t)r * ncol])))
+                        constant = false;
+                }
+            S.x.push_back(rowx);
+            S.rank.push_back(G.rank);
+            S.nz.push_back(rnz);
+            S.z_off.push_back((i64)S.zmask.size());
+            for (int k = 0; k < rnz; ++k) S.zmask.push_back((u64)rz[k]);
+            S.w_off.push_back((i64)S.wv.size());
+            S.wv.insert(S.wv.end(), rw, rw + (i64)rnz * G.rank);
+            for (int r = 0; r < kSideMaxRank; ++r) S.cconst.push_back(r < G.rank ? col[(size_t)r * ncol] : 0.0);
+            S.colmode.push_back(constant ? 0 : 1);
+            S.ctab_off.push_back(constant ? -1 : (i64)S.ctab.size());
+            if (!constant) S.ctab.insert(S.ctab.end(), col.begin(), col.end());
+        }
+    };
+    add_side(0, pa);
+    add_side(1, pb);
+    P->nPA = (int)pa.size();
+    P->nPB = (int)pb.size();
+
+    // ---- mixed single-single groups: Kronecker factorisation --------------------
+    std::unordered_map<u64, int> eidx, fidx;
+    struct MixedRec { int E, F; double coef; };
+    std::vector<MixedRec> recs;
+    std::vector<int> connA, connB;   // scratch: connected string indices
+    for (int g : mixed) {
+        const GroupDev &G = N->groups[g];
+        if (G.rank != 1 || popc(G.ax) != 2 || popc(G.bx) != 2) { P->residual.push_back(g); continue; }
+        const u64 ma = mask_below_odd(G.bx, norb), mb = mask_above_odd(G.ax, norb);
+        const double csign = (popc(G.ax & ma) & 1) ? -1.0 : 1.0;
+        auto ei = eidx.find(G.ax);
+        auto fi = fidx.find(G.bx);
+        // sign masks of a new excitation: the first transformed Z mask of this group
+        const u64 mA = ei == eidx.end() ? ((u64)z[G.za_off] ^ ma) : P->mA[ei->second];
+        const u64 mB = fi == fidx.end() ? ((u64)z[G.zb_off] ^ mb) : P->mB[fi->second];
+        // lam / mu from one connected string each, then verified on all of them
+        auto factor = [&](const auto &strs, int n, u64 x, const Ti *zz, int nz, const double *ww, u64 zx, u64 sm,
+                          double *out) {
+            double f = 0.0;
+            bool have = false;
+            for (int i = 0; i < n; ++i) {
+                const u64 s = (u64)strs[i];
+                if (popc(s & x) != 1) continue;
+                const double v = phase_r(s, zz, nz, ww, 0, zx);
+                const double sg = (popc(s & sm) & 1) ? -1.0 : 1.0;
+                if (!have) { f = v * sg; have = true; continue; }
+                if (std::fabs(v - f * sg) > 1e-12 * std::max(1.0, std::fabs(f))) return false;
+            }
+            *out = f;
+            return have;
+        };
+        double lam = 0.0, mu = 0.0;
+        if (!factor(A, nA, G.ax, z + G.za_off, G.nza, w + G.wa_off, ma, mA, &lam) ||
+            !factor(Bs, nB, G.bx, z + G.zb_off, G.nzb, w + G.wb_off, mb, mB, &mu)) {
+            P->residual.push_back(g);
+            continue;
+        }
+        int E, F;
+        if (ei == eidx.end()) {
+            E = (int)P->Emask.size();
+            eidx[G.ax] = E;
+            P->Emask.push_back(G.ax);
+            P->mA.push_back(mA);
+        } else E = ei->second;
+        if (fi == fidx.end()) {
+            F = (int)P->Fmask.size();
+            fidx[G.bx] = F;
+            P->Fmask.push_back(G.bx);
+            P->mB.push_back(mB);
+        } else F = fi->second;
+        recs.push_back({E, F, csign * lam * mu});
+        P->mixed_pairs += 0;
+    }
+    P->nE = (int)P->Emask.size();
+    P->nF = (int)P->Fmask.size();
+    if (P->nE > 256 || P->nF > 512) {
+        // too many excitations for the shared-memory tiles: everything generic
+        for (auto &r : recs) (void)r;
+        P->why = "too many single excitations for the structured mixed kernel";
+        return BSIM_OK;
+    }
+    P->Lam.assign((size_t)P->nE * P->nF, 0.0);
+    for (auto &r : recs) P->Lam[(size_t)r.E * P->nF + r.F] += r.coef;
+    // M: connected alpha singles per source row (max over rows)
+    int M = 0;
+    for (int a = 0; a < nA; ++a) {
+        int m = 0;
+        for (int e = 0; e < P->nE; ++e) m += popc((u64)A[a] & P->Emask[e]) == 1;
+        M = std::max(M, m);
+    }
+    P->M = M;
+    if (M > 64 && P->nE > 0) { P->why = "more than 64 connected alpha singles per string"; return BSIM_OK; }
+    if (P->nPA > 4096 || P->nPB > 4096) { P->why = "more than 4096 pure groups on one side"; return BSIM_OK; }
+
+    P->fits64 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 8) <= 227 * 1024;
+    P->fits32 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 4) <= 227 * 1024;
+    if (!P->fits64 && !P->fits32) { P->why = "beta row too long for the mixed kernel's shared memory"; return BSIM_OK; }
+
+    // ---- upload -------------------------------------------------------------------
+    auto bytes = [](size_t n, size_t sz) { return ((std::max<size_t>(n, 1) * sz) + 255) & ~size_t(255); };
+    size_t tot = bytes(nA, sizeof(Ti)) + bytes(nB, sizeof(Ti)) + bytes(nA, 8) + bytes(PAd.size(), 8) +
+                 bytes(PBd.size(), 8) + 4 * bytes(P->nE + P->nF, 8) + 2 * bytes(P->Lam.size(), 8) +
+                 bytes(33 * 33, 4) + bytes(P->residual.size(), 4) + bytes(P->residual.size() + 1, 16);
+    for (auto &S : sh)
+        tot += 4 * bytes(S.x.size(), 8) + 3 * bytes(S.x.size(), 4) + bytes(S.cconst.size(), 8) +
+               bytes(S.zmask.size(), 8) + bytes(S.wv.size(), 8) + bytes(S.ctab.size(), 8) + bytes(S.ctab.size(), 4);
+    int st = P->arena.reserve(tot);
+    if (st != BSIM_OK) return st;
+    auto put = [&](const auto &v) {
+        using T = typename std::decay_t<decltype(v)>::value_type;
+        T *d = P->arena.template take<T>(std::max<size_t>(v.size(), 1));
+        if (!v.empty()) cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+        return (const T *)d;
+    };
+    P->d_astr = put(A);
+    P->d_bstr = put(Bs);
+    P->d_Ka = put(P->Ka);
+    P->d_PAd = put(PAd);
+    P->d_PBd = put(PBd);
+    P->d_Emask = put(P->Emask);
+    P->d_Fmask = put(P->Fmask);
+    P->d_mA = put(P->mA);
+    P->d_mB = put(P->mB);
+    P->d_Lam = put(P->Lam);
+    std::vector<float> lam32(P->Lam.begin(), P->Lam.end());
+    P->d_Lam32 = put(lam32);
+    std::vector<int> binom(33 * 33, 0);
+    for (int n = 0; n <= 32; ++n)
+        for (int k = 0; k <= 32; ++k) binom[n * 33 + k] = (int)std::min<u64>(comb_count(n, k), 0x7fffffff);
+    P->d_binom = put(binom);
+    for (int side = 0; side < 2; ++side) {
+        SideHost &S = sh[side];
+        SideDev &D = side == 0 ? P->sideA : P->sideB;
+        D.ng = (int)S.x.size();
+        D.ncols = side == 0 ? nB : nA;
+        D.x = put(S.x);
+        D.rank = put(S.rank);
+        D.nz = put(S.nz);
+        D.z_off = put(S.z_off);
+        D.w_off = put(S.w_off);
+        D.colmode = put(S.colmode);
+        D.cconst = put(S.cconst);
+        D.ctab_off = put(S.ctab_off);
+        D.zmask = put(S.zmask);
+        D.w = put(S.wv);
+        D.ctab = put(S.ctab);
+        std::vector<float> c32(S.ctab.begin(), S.ctab.end());
+        D.ctab32 = put(c32);
+    }
+    // residual groups through the generic tile kernel (chunks as in DevNet::finalize)
+    std::vector<int> res = P->residual;
+    std::stable_sort(res.begin(), res.end(), [&](int a, int b) {
+        const GroupDev &x = N->groups[a], &y = N->groups[b];
+        return x.type != y.type ? x.type < y.type : x.rank < y.rank;
+    });
+    std::vector<int4> ch;
+    for (size_t i = 0; i < res.size();) {
+        const int r = N->groups[res[i]].rank, ty = N->groups[res[i]].type;
+        size_t j = i + 1;
+        if (r <= 2)
+            while (j < res.size() && j - i < 32 && N->groups[res[j]].rank == r && N->groups[res[j]].type == ty) ++j;
+        ch.push_back(make_int4((int)i, (int)(j - i), r, ty));
+        i = j;
+    }
+    P->d_resid = put(res);
+    P->d_resid_chunks = put(ch);
+    P->n_resid_chunks = (int)ch.size();
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_status(e, "fast plan upload");
+    P->ok = true;
+    return BSIM_OK;
+}
+
+template int build_fast_plan<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, FastPlan<unsigned> *);
+
+}  // namespace bsim

@@ -91,8 +91,16 @@ struct DevNet {
     const int *d_plan_groups = nullptr;
     const int4 *d_plan_chunks = nullptr;
 
+    // cached structured-sigma plan for the last basis it was used with
+    void *fast_state = nullptr;
+    void (*fast_free)(void *) = nullptr;
+
     int finalize();   // derived tables + upload
-    ~DevNet() { arena.release(); magic = 0; }
+    ~DevNet() {
+        if (fast_state && fast_free) fast_free(fast_state);
+        arena.release();
+        magic = 0;
+    }
 };
 
 // ---- constructors -----------------------------------------------------------

@@ -21,6 +21,21 @@ int sigma_tiles(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, c
 template <typename Ti>
 i64 num_tiles(const DevBasis<Ti> *B);
 
+// Structured sigma (single-block bases); *used tells whether it ran.
+template <typename Ti>
+int sigma_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32, double *dst,
+               bool mixed, cudaStream_t s, bool *used);
+// 1: structured path (FP64 and FP32), 2: structured for FP32 only, 0: generic.
+template <typename Ti>
+int fast_sigma_info(const DevBasis<Ti> *B, const DevNet<Ti> *N, std::string *why, int *nresid);
+template <typename Ti>
+bool fast_sigma_available(const DevBasis<Ti> *B, const DevNet<Ti> *N);
+// The generic tile kernel over an explicit chunk plan, adding into dst.
+template <typename Ti>
+int sigma_generic_accumulate(const DevBasis<Ti> *B, const DevNet<Ti> *N, const int *plan_g, const int4 *chunks,
+                             int nchunks, const double *src, const float *src32, double *dst, bool mixed,
+                             cudaStream_t s);
+
 template <typename Ti>
 int diag_elements(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *diag, cudaStream_t s);
 

@@ -12,6 +12,8 @@
 #include "ops.h"
 #include "tiles.cuh"
 
+#include <cstdlib>
+
 namespace bsim {
 
 template <typename Ti, bool MIXED>
@@ -19,7 +21,7 @@ __global__ void __launch_bounds__(kTileThreads)
 sigma_tile_kernel(const BasisView<Ti> B, const NetView<Ti> N, const int *__restrict__ plan_g,
                   const int4 *__restrict__ chunks, int nchunks, const i64 *__restrict__ tile_start,
                   const double *__restrict__ src, const float *__restrict__ src32, double *__restrict__ dst,
-                  i64 tile_lo)
+                  i64 tile_lo, int accumulate)
 {
     using Tw = typename std::conditional<MIXED, float, double>::type;
     __shared__ TileSmem<Tw> S;
@@ -64,7 +66,10 @@ sigma_tile_kernel(const BasisView<Ti> B, const NetView<Ti> N, const int *__restr
 #pragma unroll
         for (int i = 0; i < kRowsPerWarp; ++i) {
             const int a = c.ta * kTile + wrow + i;
-            if (a < c.na) dst[base + (i64)a * c.nb + b] = acc[i];
+            if (a < c.na) {
+                const i64 di = base + (i64)a * c.nb + b;
+                dst[di] = accumulate ? dst[di] + acc[i] : acc[i];
+            }
         }
     }
 }
@@ -169,19 +174,59 @@ int sigma_tiles(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, c
     if (mixed)
         sigma_tile_kernel<Ti, true><<<(unsigned)nt, kTileThreads, 0, s>>>(
             B->view, N->view, N->d_plan_groups, N->d_plan_chunks, (int)N->plan_chunks.size(), tp, nullptr, src32, dst,
-            tile_lo);
+            tile_lo, 0);
     else
         sigma_tile_kernel<Ti, false><<<(unsigned)nt, kTileThreads, 0, s>>>(
             B->view, N->view, N->d_plan_groups, N->d_plan_chunks, (int)N->plan_chunks.size(), tp, src, nullptr, dst,
-            tile_lo);
+            tile_lo, 0);
     BSIM_CUDA(cudaGetLastError());
     return BSIM_OK;
 }
 
 template <typename Ti>
+int sigma_generic_accumulate(const DevBasis<Ti> *B, const DevNet<Ti> *N, const int *plan_g, const int4 *chunks,
+                             int nchunks, const double *src, const float *src32, double *dst, bool mixed,
+                             cudaStream_t s)
+{
+    if (nchunks == 0 || B->dim == 0) return BSIM_OK;
+    Workspace &ws = workspace_for(B);
+    const i64 *tp = nullptr;
+    i64 ntiles = 0;
+    int st = tile_prefix(B, ws, &tp, &ntiles);
+    if (st != BSIM_OK) return st;
+    if (mixed && !src32) {
+        float *tmp = nullptr;
+        st = ws.f32_buffer(B->dim, &tmp);
+        if (st != BSIM_OK) return st;
+        to_f32_kernel<<<1184, 256, 0, s>>>(src, tmp, B->dim);
+        src32 = tmp;
+    }
+    if (mixed)
+        sigma_tile_kernel<Ti, true><<<(unsigned)ntiles, kTileThreads, 0, s>>>(B->view, N->view, plan_g, chunks,
+                                                                             nchunks, tp, nullptr, src32, dst, 0, 1);
+    else
+        sigma_tile_kernel<Ti, false><<<(unsigned)ntiles, kTileThreads, 0, s>>>(B->view, N->view, plan_g, chunks,
+                                                                              nchunks, tp, src, nullptr, dst, 0, 1);
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+// Structured path when the plan accepts the (basis, network) pair, else the
+// generic tile kernel.  BSIM_SIGMA_GENERIC=1 forces the generic kernel.
+template <typename Ti>
 int sigma(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32, double *dst,
           bool mixed, cudaStream_t s)
 {
+    static const bool force_generic = [] {
+        const char *e = getenv("BSIM_SIGMA_GENERIC");
+        return e && e[0] == '1';
+    }();
+    if (!force_generic && B->dim > 0) {
+        bool used = false;
+        int st = sigma_fast(B, N, src, src32, dst, mixed, s, &used);
+        if (st != BSIM_OK) return st;
+        if (used) return BSIM_OK;
+    }
     return sigma_tiles(B, N, src, src32, dst, mixed, 0, num_tiles(B), s);
 }
 
@@ -205,6 +250,9 @@ template int sigma<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> 
 template int sigma_tiles<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *,
                                    const float *, double *, bool, i64, i64, cudaStream_t);
 template i64 num_tiles<unsigned>(const DevBasis<unsigned> *);
+template int sigma_generic_accumulate<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const int *,
+                                                const int4 *, int, const double *, const float *, double *, bool,
+                                                cudaStream_t);
 template int diag_elements<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, double *, cudaStream_t);
 
 }  // namespace bsim

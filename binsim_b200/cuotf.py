@@ -71,6 +71,7 @@ def lib() -> C.CDLL:
         "bsim_network_ngs": (i64, [vp]),
         "bsim_hvec": (ci, [vp, vp, vp, vp, vp]), "bsim_hvec_mixed": (ci, [vp, vp, vp, vp, vp]),
         "bsim_hvec_f32in": (ci, [vp, vp, vp, vp, vp]),
+        "bsim_hvec_path": (ci, [vp, vp, C.c_char_p, ci, vp]),
         "bsim_hvec_num_tiles": (i64, [vp]), "bsim_hvec_tiles": (ci, [vp, vp, vp, vp, i64, i64, ci, vp]), "bsim_diag": (ci, [vp, vp, vp, vp]),
         "bsim_expm": (ci, [vp, vp, i64, dbl, vp, vp]), "bsim_expm_seq": (ci, [vp, vp, i64, vp, vp, vp, vp]),
         "bsim_grad": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
@@ -215,6 +216,15 @@ class CuOTFFunctions:
         """sigma on destination tiles [tile_lo, tile_hi) only (row sharding)."""
         _check(lib().bsim_hvec_tiles(self.basis.h, self.ham.h, _ptr(v), _ptr(Hv), tile_lo, tile_hi,
                                      1 if mixed else 0, _stream(stream)), "hvec_tiles")
+
+    def sigma_path(self):
+        """(path, reason, residual groups): path 1 structured, 2 structured FP32 only, 0 generic."""
+        buf = C.create_string_buffer(256)
+        nres = C.c_int()
+        r = lib().bsim_hvec_path(self.basis.h, self.ham.h, buf, 256, C.byref(nres))
+        if r < 0:
+            _check(r, "hvec_path")
+        return r, buf.value.decode(), nres.value
 
     def num_tiles(self) -> int:
         return lib().bsim_hvec_num_tiles(self.basis.h)

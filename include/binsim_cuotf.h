@@ -117,6 +117,12 @@ int bsim_hvec(void *basis, void *net, const double *src, double *dst, bsim_strea
 int bsim_hvec_mixed(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream);
 /* As bsim_hvec_mixed with an FP32 input vector. */
 int bsim_hvec_f32in(void *basis, void *net, const float *src, double *dst, bsim_stream_t stream);
+/* Which sigma kernel bsim_hvec uses for this (basis, network) pair: 1 the
+ * structured path (FP64 and FP32-bulk), 2 structured for FP32 bulk only, 0 the
+ * generic tile kernel; negative on error.  why receives the reason, and
+ * residual_groups the number of groups the structured path leaves to the
+ * generic kernel.  Builds (and caches) the plan on first use. */
+int bsim_hvec_path(void *basis, void *net, char *why, int why_len, int *residual_groups);
 /* Number of 32 x 32 destination tiles of sigma (block-major, then row-major). */
 int64_t bsim_hvec_num_tiles(void *basis);
 /* sigma restricted to destination tiles [tile_lo, tile_hi): the rows of those

@@ -38,6 +38,8 @@ def test_sigma_matches_oracle(cuda, oracle, norb, na, nb, orbsym, tsym):
     B = cuotf.CuBasis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
     f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
     assert B.dim == Bo.dim
+    path, why, nres = f.sigma_path()
+    assert path == (0 if orbsym is not None else 1), (path, why)
     x = np.random.default_rng(norb).normal(size=B.dim)
     ref = oracle.hvec(Bo, No, x)
     y = cuda.empty(B.dim, dtype=cuda.float64, device="cuda")

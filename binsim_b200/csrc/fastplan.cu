@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <thread>
 #include <unordered_map>
 
 namespace bsim {
@@ -146,6 +147,88 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     };
     add_side(0, pa);
     add_side(1, pb);
+    // per-row contribution lists (CSR), built with a few host threads
+    struct CSRHost {
+        std::vector<i64> cptr, tptr;
+        std::vector<int> csrc, tsrc, tgid;
+        std::vector<double> ccoef, tpa;
+    } csr[2];
+    {
+        std::vector<int> amap((size_t)1 << norb, -1), bmap((size_t)1 << norb, -1);
+        for (int a = 0; a < nA; ++a) amap[(size_t)A[a]] = a;
+        for (int b = 0; b < nB; ++b) bmap[(size_t)Bs[b]] = b;
+        for (int side = 0; side < 2; ++side) {
+            const SideHost &S = sh[side];
+            const auto &rows = side == 0 ? A : Bs;
+            const std::vector<int> &rmap = side == 0 ? amap : bmap;
+            const int nrows = side == 0 ? nA : nB;
+            const int ng = (int)S.x.size();
+            const int nth = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+            struct Part {
+                std::vector<i64> cn, tn;
+                std::vector<int> csrc, tsrc, tgid;
+                std::vector<double> ccoef, tpa;
+            };
+            std::vector<Part> parts(nth);
+            auto work = [&](int t) {
+                Part &pt = parts[t];
+                const int r0 = (int)((i64)nrows * t / nth), r1 = (int)((i64)nrows * (t + 1) / nth);
+                for (int r = r0; r < r1; ++r) {
+                    const u64 s0 = (u64)rows[r];
+                    i64 cc = 0, tc = 0;
+                    for (int g = 0; g < ng; ++g) {
+                        const u64 x = S.x[g];
+                        if (2 * popc(s0 & x) != popc(x)) continue;
+                        const u64 sv = s0 ^ x;
+                        if (sv >> norb) continue;
+                        const int src = rmap[(size_t)sv];
+                        if (src < 0) continue;
+                        double pa[kSideMaxRank] = {0, 0, 0, 0};
+                        const int R = S.rank[g], nz = S.nz[g];
+                        for (int q = 0; q < nz; ++q) {
+                            const bool odd = popc(sv & S.zmask[S.z_off[g] + q]) & 1;
+                            for (int rr = 0; rr < R; ++rr) {
+                                const double v = S.wv[S.w_off[g] + (i64)rr * nz + q];
+                                pa[rr] += odd ? -v : v;
+                            }
+                        }
+                        if (S.colmode[g] == 0) {
+                            double coef = 0.0;
+                            for (int rr = 0; rr < R; ++rr) coef += pa[rr] * S.cconst[(size_t)g * kSideMaxRank + rr];
+                            pt.csrc.push_back(src);
+                            pt.ccoef.push_back(coef);
+                            ++cc;
+                        } else {
+                            pt.tsrc.push_back(src);
+                            pt.tgid.push_back(g);
+                            for (int rr = 0; rr < kSideMaxRank; ++rr) pt.tpa.push_back(pa[rr]);
+                            ++tc;
+                        }
+                    }
+                    pt.cn.push_back(cc);
+                    pt.tn.push_back(tc);
+                }
+            };
+            std::vector<std::thread> th;
+            for (int t = 1; t < nth; ++t) th.emplace_back(work, t);
+            work(0);
+            for (auto &x : th) x.join();
+            CSRHost &C = csr[side];
+            C.cptr.assign(1, 0);
+            C.tptr.assign(1, 0);
+            for (auto &pt : parts) {
+                for (i64 v : pt.cn) C.cptr.push_back(C.cptr.back() + v);
+                for (i64 v : pt.tn) C.tptr.push_back(C.tptr.back() + v);
+                C.csrc.insert(C.csrc.end(), pt.csrc.begin(), pt.csrc.end());
+                C.ccoef.insert(C.ccoef.end(), pt.ccoef.begin(), pt.ccoef.end());
+                C.tsrc.insert(C.tsrc.end(), pt.tsrc.begin(), pt.tsrc.end());
+                C.tgid.insert(C.tgid.end(), pt.tgid.begin(), pt.tgid.end());
+                C.tpa.insert(C.tpa.end(), pt.tpa.begin(), pt.tpa.end());
+            }
+        }
+    }
+    P->nnzA = (i64)csr[0].csrc.size();
+    P->nnzB = (i64)csr[1].csrc.size();
     P->nPA = (int)pa.size();
     P->nPB = (int)pb.size();
 
@@ -231,7 +314,10 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     auto bytes = [](size_t n, size_t sz) { return ((std::max<size_t>(n, 1) * sz) + 255) & ~size_t(255); };
     size_t tot = bytes(nA, sizeof(Ti)) + bytes(nB, sizeof(Ti)) + bytes(nA, 8) + bytes(PAd.size(), 8) +
                  bytes(PBd.size(), 8) + 4 * bytes(P->nE + P->nF, 8) + 2 * bytes(P->Lam.size(), 8) +
-                 bytes(33 * 33, 4) + bytes(P->residual.size(), 4) + bytes(P->residual.size() + 1, 16);
+                 bytes(33 * 33, 4) + bytes(kRankTabInts, 4) + bytes(P->residual.size(), 4) + bytes(P->residual.size() + 1, 16);
+    for (auto &C : csr)
+        tot += 2 * bytes(C.cptr.size(), 8) + bytes(C.csrc.size(), 4) + bytes(C.ccoef.size(), 8) +
+               2 * bytes(C.tsrc.size(), 4) + bytes(C.tpa.size(), 8);
     for (auto &S : sh)
         tot += 4 * bytes(S.x.size(), 8) + 3 * bytes(S.x.size(), 4) + bytes(S.cconst.size(), 8) +
                bytes(S.zmask.size(), 8) + bytes(S.wv.size(), 8) + bytes(S.ctab.size(), 8) + bytes(S.ctab.size(), 4);
@@ -259,6 +345,19 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     for (int n = 0; n <= 32; ++n)
         for (int k = 0; k <= 32; ++k) binom[n * 33 + k] = (int)std::min<u64>(comb_count(n, k), 0x7fffffff);
     P->d_binom = put(binom);
+    // byte tables: T_k[byte][o] = sum over set bits of byte (ascending, j = o+1, o+2, ...) of C(8k + p, j)
+    std::vector<int> rt(kRankTabInts, 0);
+    const int tbase[3] = {0, 256, 256 + 256 * 9}, nofs[3] = {1, 9, 17};
+    for (int k = 0; k < 3; ++k)
+        for (int byte = 0; byte < 256; ++byte)
+            for (int o = 0; o < nofs[k]; ++o) {
+                u64 v = 0;
+                int j = o;
+                for (int p = 0; p < 8; ++p)
+                    if ((byte >> p) & 1) v += comb_count(8 * k + p, ++j);
+                rt[tbase[k] + byte * nofs[k] + o] = (int)std::min<u64>(v, 0x7fffffff);
+            }
+    P->d_ranktab = put(rt);
     for (int side = 0; side < 2; ++side) {
         SideHost &S = sh[side];
         SideDev &D = side == 0 ? P->sideA : P->sideB;
@@ -277,6 +376,17 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
         D.ctab = put(S.ctab);
         std::vector<float> c32(S.ctab.begin(), S.ctab.end());
         D.ctab32 = put(c32);
+    }
+    for (int side = 0; side < 2; ++side) {
+        CSRHost &C = csr[side];
+        SideCSR &D = side == 0 ? P->csrA : P->csrB;
+        D.cptr = put(C.cptr);
+        D.csrc = put(C.csrc);
+        D.ccoef = put(C.ccoef);
+        D.tptr = put(C.tptr);
+        D.tsrc = put(C.tsrc);
+        D.tgid = put(C.tgid);
+        D.tpa = put(C.tpa);
     }
     // residual groups through the generic tile kernel (chunks as in DevNet::finalize)
     std::vector<int> res = P->residual;

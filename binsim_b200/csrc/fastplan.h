@@ -44,6 +44,18 @@ struct SideDev {
 
 constexpr int kSideMaxRank = 4;
 
+// Static list of the pure-spin contributions of every row (depends only on the
+// basis and the network): constant-factor entries (source row, coefficient)
+// and table entries (source row, group, row-spin phases).
+struct SideCSR {
+    const i64 *cptr;      // [nrows + 1]
+    const int *csrc;      // [nnz_c]
+    const double *ccoef;  // [nnz_c]
+    const i64 *tptr;      // [nrows + 1]
+    const int *tsrc, *tgid;   // [nnz_t]
+    const double *tpa;    // [nnz_t * kSideMaxRank]
+};
+
 template <typename Ti>
 struct FastPlan {
     bool ok = false;
@@ -70,10 +82,13 @@ struct FastPlan {
     const u64 *d_Ka = nullptr;
     const double *d_PAd = nullptr, *d_PBd = nullptr;
     SideDev sideA{}, sideB{};
+    SideCSR csrA{}, csrB{};
+    i64 nnzA = 0, nnzB = 0;
     const u64 *d_Emask = nullptr, *d_Fmask = nullptr, *d_mA = nullptr, *d_mB = nullptr;
     const double *d_Lam = nullptr;
     const float *d_Lam32 = nullptr;
     const int *d_binom = nullptr;      // [33 x 33] binomials for string ranking
+    const int *d_ranktab = nullptr;    // [kRankTabInts] byte tables for string ranking
     const int *d_resid = nullptr;      // residual group plan (for the generic kernel)
     const int4 *d_resid_chunks = nullptr;
     int n_resid_chunks = 0;
@@ -82,9 +97,15 @@ struct FastPlan {
 
 // Shared memory of the mixed GEMM kernel: source row, Lam_conn [K x 64], an
 // X slice [32 x 64], the binomial table and the excitation lists.
+// Byte tables for the colex rank of a string: table k covers bits 8k..8k+7
+// and is indexed [byte][number of set bits below the byte].
+constexpr int kRankTabInts = 256 + 256 * 9 + 256 * 17;   // up to 24 orbitals
+constexpr int kMixCols = 128;                             // columns per GEMM chunk
+
 inline size_t mixed_smem_bytes(int nB, int nF, size_t elem)
 {
-    return (((size_t)nB + 7) & ~size_t(7)) * elem + (size_t)nF * 64 * elem + 32 * 64 * elem + 33 * 33 * 4 + 128 * 4;
+    return (((size_t)nB + 7) & ~size_t(7)) * elem + (size_t)nF * 64 * elem + 32 * (size_t)kMixCols * elem +
+           (size_t)kRankTabInts * 4 + kMixCols * 8 + 128 * 4;
 }
 
 template <typename Ti>

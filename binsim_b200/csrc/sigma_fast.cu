@@ -23,20 +23,6 @@
 namespace bsim {
 
 constexpr int kRowChunk = 1024;        // columns per CTA in the row kernels
-constexpr int kMaxTab = 512;           // table-mode pure groups connected to one row
-
-// ---- colex rank of a string (index in Gosper order of all strings with its popcount)
-__device__ __forceinline__ int colex_rank(u64 s, const int *__restrict__ binom)
-{
-    int r = 0, i = 1;
-    while (s) {
-        const int p = __ffsll((long long)s) - 1;
-        r += binom[p * 33 + i];
-        ++i;
-        s &= s - 1;
-    }
-    return r;
-}
 
 // ---- 1. frame + transpose ---------------------------------------------------------
 template <typename Ti, typename Tin, typename T>
@@ -65,80 +51,14 @@ __global__ void frame_transpose_kernel(int nA, int nB, const Ti *__restrict__ as
     }
 }
 
-// ---- 2/3. pure groups of one spin: row AXPY --------------------------------------
-template <typename Ti, typename T>
+// ---- 2/3. pure groups of one spin: row AXPY over the precomputed row lists -----------
+template <typename T>
 __global__ void __launch_bounds__(256)
-pure_rows_kernel(const SideDev S, int nrows, const Ti *__restrict__ rowstr, const int *__restrict__ rowmap,
-                 int norb, const T *__restrict__ in, double *__restrict__ out, const double *__restrict__ PAd,
-                 const double *__restrict__ PBd, int rank_d)
+pure_rows_kernel(const SideDev S, const SideCSR L, const T *__restrict__ in, double *__restrict__ out,
+                 const double *__restrict__ PAd, const double *__restrict__ PBd, int rank_d)
 {
-    // dynamic shared memory: [cap_c] src, [cap_c] coef, [cap_t] src, gid, [cap_t][4] pa
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int cap_c = S.ng, cap_t = min(S.ng, kMaxTab);
-    double *ccoef = reinterpret_cast<double *>(smem_raw);
-    double *tpa = ccoef + cap_c;                                  // [cap_t * kSideMaxRank]
-    int *csrc = reinterpret_cast<int *>(tpa + (size_t)cap_t * kSideMaxRank);
-    int *tsrc = csrc + cap_c;
-    int *tgid = tsrc + cap_t;
-    __shared__ int wcount[2][8], wbase[2][8];
-    __shared__ int ntot[2];
     const int row = blockIdx.x;
     const int ncols = S.ncols;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const u64 s0 = (u64)rowstr[row];
-    if (threadIdx.x < 2) ntot[threadIdx.x] = 0;
-    __syncthreads();
-    // phase 1: connected groups of this row, compacted in group order
-    for (int base = 0; base < S.ng; base += blockDim.x) {
-        const int g = base + threadIdx.x;
-        int src = -1, mode = 0;
-        double pa[kSideMaxRank] = {0.0, 0.0, 0.0, 0.0};
-        double coef = 0.0;
-        if (g < S.ng) {
-            const u64 x = S.x[g];
-            const u64 s = s0 ^ x;
-            if (((s >> norb) == 0) && 2 * __popcll(s0 & x) == __popcll(x)) src = rowmap[s];
-            if (src >= 0) {
-                const int R = S.rank[g], nz = S.nz[g];
-                const u64 *z = S.zmask + S.z_off[g];
-                const double *w = S.w + S.w_off[g];
-                for (int q = 0; q < nz; ++q) {
-                    const bool odd = __popcll(s & z[q]) & 1;
-                    for (int r = 0; r < R; ++r) {
-                        const double v = w[(i64)r * nz + q];
-                        pa[r] += odd ? -v : v;
-                    }
-                }
-                mode = S.colmode[g];
-                if (mode == 0)
-                    for (int r = 0; r < R; ++r) coef += pa[r] * S.cconst[g * kSideMaxRank + r];
-            }
-        }
-        const unsigned mc = __ballot_sync(0xffffffffu, src >= 0 && mode == 0);
-        const unsigned mt = __ballot_sync(0xffffffffu, src >= 0 && mode == 1);
-        if (lane == 0) { wcount[0][wid] = __popc(mc); wcount[1][wid] = __popc(mt); }
-        __syncthreads();
-        if (threadIdx.x < 2) {
-            int acc = ntot[threadIdx.x];
-            for (int w2 = 0; w2 < 8; ++w2) { wbase[threadIdx.x][w2] = acc; acc += wcount[threadIdx.x][w2]; }
-            ntot[threadIdx.x] = acc;
-        }
-        __syncthreads();
-        const unsigned below = (1u << lane) - 1u;
-        if (src >= 0 && mode == 0) {
-            const int pos = wbase[0][wid] + __popc(mc & below);
-            if (pos < cap_c) { csrc[pos] = src; ccoef[pos] = coef; }
-        } else if (src >= 0) {
-            const int pos = wbase[1][wid] + __popc(mt & below);
-            if (pos < cap_t) {
-                tsrc[pos] = src; tgid[pos] = g;
-                for (int r = 0; r < kSideMaxRank; ++r) tpa[pos * kSideMaxRank + r] = pa[r];
-            }
-        }
-        __syncthreads();
-    }
-    const int nc = min(ntot[0], cap_c), nt = min(ntot[1], cap_t);
-    // phase 2: one column chunk
     const int c0 = blockIdx.y * kRowChunk;
     constexpr int K = kRowChunk / 256;
     double acc[K];
@@ -153,15 +73,30 @@ pure_rows_kernel(const SideDev S, int nrows, const Ti *__restrict__ rowstr, cons
             acc[k] = d * (double)in[(i64)row * ncols + col[k]];
         }
     }
-    constexpr int kBatch = 64;
-    for (int e0 = 0; e0 < nc; e0 += kBatch) {
-        const int e1 = min(nc, e0 + kBatch);
+    const i64 e_beg = L.cptr[row], e_end = L.cptr[row + 1];
+    constexpr int kBatch = 64;   // FP32 partial sums span at most this many entries
+    for (i64 e0 = e_beg; e0 < e_end; e0 += kBatch) {
+        const i64 e1 = min(e_end, e0 + kBatch);
         T part[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) part[k] = T(0);
-        for (int e = e0; e < e1; ++e) {
-            const T cf = (T)ccoef[e];
-            const T *srow = in + (i64)csrc[e] * ncols;
+        i64 e = e0;
+        for (; e + 4 <= e1; e += 4) {   // 4 entries x K columns of independent loads in flight
+            const T *s0 = in + (i64)__ldg(L.csrc + e) * ncols, *s1 = in + (i64)__ldg(L.csrc + e + 1) * ncols;
+            const T *s2 = in + (i64)__ldg(L.csrc + e + 2) * ncols, *s3 = in + (i64)__ldg(L.csrc + e + 3) * ncols;
+            const T k0 = (T)__ldg(L.ccoef + e), k1 = (T)__ldg(L.ccoef + e + 1);
+            const T k2 = (T)__ldg(L.ccoef + e + 2), k3 = (T)__ldg(L.ccoef + e + 3);
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                if (col[k] < ncols) {
+                    const T v0 = __ldg(s0 + col[k]), v1 = __ldg(s1 + col[k]);
+                    const T v2 = __ldg(s2 + col[k]), v3 = __ldg(s3 + col[k]);
+                    part[k] += k0 * v0 + k1 * v1 + k2 * v2 + k3 * v3;
+                }
+        }
+        for (; e < e1; ++e) {
+            const T cf = (T)__ldg(L.ccoef + e);
+            const T *srow = in + (i64)__ldg(L.csrc + e) * ncols;
 #pragma unroll
             for (int k = 0; k < K; ++k)
                 if (col[k] < ncols) part[k] += cf * __ldg(srow + col[k]);
@@ -169,16 +104,16 @@ pure_rows_kernel(const SideDev S, int nrows, const Ti *__restrict__ rowstr, cons
 #pragma unroll
         for (int k = 0; k < K; ++k) acc[k] += (double)part[k];
     }
-    for (int e = 0; e < nt; ++e) {
-        const int g = tgid[e];
+    for (i64 e = L.tptr[row]; e < L.tptr[row + 1]; ++e) {
+        const int g = L.tgid[e];
         const int R = S.rank[g];
-        const T *srow = in + (i64)tsrc[e] * ncols;
+        const T *srow = in + (i64)L.tsrc[e] * ncols;
         const i64 toff = S.ctab_off[g];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             if (col[k] >= ncols) continue;
             double f = 0.0;
-            for (int r = 0; r < R; ++r) f += tpa[e * kSideMaxRank + r] * S.ctab[toff + (i64)r * ncols + col[k]];
+            for (int r = 0; r < R; ++r) f += L.tpa[e * kSideMaxRank + r] * S.ctab[toff + (i64)r * ncols + col[k]];
             acc[k] += f * (double)__ldg(srow + col[k]);
         }
     }
@@ -192,27 +127,46 @@ struct MixedArgs {
     int nA, nB, nE, nF, M, norb;
     const u64 *Emask, *Fmask, *mA, *mB;
     const void *Lam;        // T [nE x nF]
-    const int *binom;
+    const int *ranktab;     // colex byte tables
 };
 
+// colex rank from the byte tables (strings of up to 24 orbitals)
+__device__ __forceinline__ int rank_bytes(unsigned s, const int *__restrict__ t)
+{
+    const unsigned b0 = s & 255u, b1 = (s >> 8) & 255u, b2 = (s >> 16) & 255u;
+    const int o1 = __popc(b0), o2 = o1 + __popc(b1);
+    return t[b0] + t[256 + b1 * 9 + o1] + t[256 + 256 * 9 + b2 * 17 + o2];
+}
+
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+constexpr int kGemmThreads = 512;
+
+// One CTA per source row a'.  Warp w owns excitations 4w..4w+3 of the row's
+// connected list, lane l owns columns 4l..4l+3 of a kMixCols-column chunk.
 template <typename Ti, typename T>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(kGemmThreads, 1)
 mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const Ti *__restrict__ bstr,
                   const T *__restrict__ ct, T *__restrict__ Z, int z0, int W)
 {
+    using V2 = typename Vec2<T>::type;
+    constexpr int NW = kGemmThreads / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nB = P.nB, K = P.nF, M = P.M;
     T *srow = reinterpret_cast<T *>(smem_raw);                               // [nB]
     T *lam = srow + ((nB + 7) & ~7);                                          // [K][64]
-    T *xs = lam + (size_t)K * 64;                                             // [32][64]
-    int *binom = reinterpret_cast<int *>(xs + 32 * 64);                       // [33*33]
-    int *conn = binom + 33 * 33;                                              // [64]
+    T *xs = lam + (size_t)K * 64;                                             // [32][kMixCols]
+    int *rtab = reinterpret_cast<int *>(xs + 32 * kMixCols);                  // [kRankTabInts]
+    unsigned long long *cstr = reinterpret_cast<unsigned long long *>(rtab + kRankTabInts);   // [kMixCols]
+    int *conn = reinterpret_cast<int *>(cstr + kMixCols);                     // [64]
     int *sgn = conn + 64;                                                     // [64]
-    __shared__ int wcnt[8], cnt;
+    __shared__ int wcnt[NW], cnt;
     const int a = blockIdx.x;
     const u64 sa = (u64)astr[a];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) binom[i] = P.binom[i];
+    for (int i = threadIdx.x; i < kRankTabInts; i += blockDim.x) rtab[i] = P.ranktab[i];
     // connected alpha excitations of this source row, in E order
     if (threadIdx.x == 0) cnt = 0;
     __syncthreads();
@@ -229,7 +183,7 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const Ti *__re
             if (j < 64) { conn[j] = e; sgn[j] = (__popcll(sa & P.mA[e]) & 1) ? -1 : 1; }
         }
         __syncthreads();
-        if (threadIdx.x == 0) for (int w2 = 0; w2 < 8; ++w2) cnt += wcnt[w2];
+        if (threadIdx.x == 0) for (int w2 = 0; w2 < NW; ++w2) cnt += wcnt[w2];
         __syncthreads();
     }
     const int m = min(cnt, 64);
@@ -241,51 +195,61 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const Ti *__re
         const int f = i >> 6, j = i & 63;
         lam[i] = j < m ? (T)sgn[j] * Lam[(i64)conn[j] * K + f] : T(0);
     }
-    __syncthreads();
     const int zend = min(nB, z0 + W);
-    for (int cb = z0; cb < zend; cb += 64) {
-        T acc[8][2];
+    const bool active = wid * 4 < m;
+    for (int cb = z0; cb < zend; cb += kMixCols) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < kMixCols; i += blockDim.x)
+            cstr[i] = (cb + i < zend) ? (unsigned long long)bstr[cb + i] : 0ull;
+        T acc[4][4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = T(0);
+        for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = T(0);
         for (int f0 = 0; f0 < K; f0 += 32) {
             const int nf = min(32, K - f0);
             __syncthreads();
-            for (int i = threadIdx.x; i < 32 * 64; i += blockDim.x) {
-                const int f = i >> 6, cl = i & 63, b = cb + cl;
+            // X slice: X[f][col] = sB_F(b^F) c~[a', rank(b^F)] for connected (F, b), else 0
+            for (int i = threadIdx.x; i < 32 * kMixCols; i += blockDim.x) {
+                const int f = i / kMixCols, cl = i % kMixCols;
                 T x = T(0);
-                if (f < nf && b < zend) {
-                    const u64 bs = (u64)bstr[b], fm = P.Fmask[f0 + f];
+                if (f < nf && cb + cl < zend) {
+                    const u64 bs = cstr[cl], fm = P.Fmask[f0 + f];
                     if (__popcll(bs & fm) == 1) {
-                        const u64 s = bs ^ fm;
-                        x = srow[colex_rank(s, binom)];
-                        if (__popcll(s & P.mB[f0 + f]) & 1) x = -x;
+                        const u64 sv = bs ^ fm;
+                        x = srow[rank_bytes((unsigned)sv, rtab)];
+                        if (__popcll(sv & P.mB[f0 + f]) & 1) x = -x;
                     }
                 }
                 xs[i] = x;
             }
             __syncthreads();
-            if (wid * 8 < m) {
+            if (active) {
+#pragma unroll 4
                 for (int f = 0; f < nf; ++f) {
-                    const T *lr = lam + (size_t)(f0 + f) * 64 + wid * 8;
-                    const T x0 = xs[f * 64 + 2 * lane], x1 = xs[f * 64 + 2 * lane + 1];
+                    const V2 *lr = reinterpret_cast<const V2 *>(lam + (size_t)(f0 + f) * 64 + wid * 4);
+                    const V2 *xr = reinterpret_cast<const V2 *>(xs + f * kMixCols + 4 * lane);
+                    const V2 xa = xr[0], xb = xr[1];
+                    const V2 la = lr[0], lb = lr[1];
+                    const T l[4] = {la.x, la.y, lb.x, lb.y};
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const T l = lr[i];
-                        acc[i][0] += l * x0;
-                        acc[i][1] += l * x1;
+                    for (int i = 0; i < 4; ++i) {
+                        acc[i][0] += l[i] * xa.x;
+                        acc[i][1] += l[i] * xa.y;
+                        acc[i][2] += l[i] * xb.x;
+                        acc[i][3] += l[i] * xb.y;
                     }
                 }
             }
         }
-        if (wid * 8 < m) {
+        if (active) {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int j = wid * 8 + i;
+            for (int i = 0; i < 4; ++i) {
+                const int j = wid * 4 + i;
                 if (j >= m) break;
                 T *zr = Z + ((i64)a * M + j) * W;
-                const int b = cb + 2 * lane;
-                if (b < zend) zr[b - z0] = acc[i][0];
-                if (b + 1 < zend) zr[b + 1 - z0] = acc[i][1];
+                const int b = cb + 4 * lane;
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (b + q < zend) zr[b + q - z0] = acc[i][q];
             }
         }
     }
@@ -362,12 +326,6 @@ __global__ void final_kernel(int nA, int nB, const Ti *__restrict__ bstr, const 
 }
 
 // ---- host ------------------------------------------------------------------------------------
-static size_t pure_smem(int ng)
-{
-    const size_t ct = (size_t)std::min(ng, kMaxTab);
-    return std::max<size_t>(16, (size_t)ng * (8 + 4) + ct * (kSideMaxRank * 8 + 8));
-}
-
 template <typename Ti>
 struct FastScratch {
     void *ct = nullptr, *ctT = nullptr, *Z = nullptr, *tT = nullptr;
@@ -451,33 +409,28 @@ static int run_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastState<Ti> *s
     // 2. pure alpha + diagonal -> dst (the frame's s~)
     {
         dim3 g(nA, (nB + kRowChunk - 1) / kRowChunk);
-        const size_t sm = pure_smem(P.sideA.ng);
-        BSIM_CUDA(cudaFuncSetAttribute(pure_rows_kernel<Ti, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        pure_rows_kernel<Ti, T><<<g, 256, sm, s>>>(P.sideA, nA, P.d_astr, B->view.amap, P.norb, ct, dst,
-                                                  P.rank_d ? P.d_PAd : nullptr, P.d_PBd, P.rank_d);
+        pure_rows_kernel<T><<<g, 256, 0, s>>>(P.sideA, P.csrA, ct, dst, P.rank_d ? P.d_PAd : nullptr, P.d_PBd,
+                                              P.rank_d);
     }
     // 3. pure beta on the transposed vector -> tT
     {
         dim3 g(nB, (nA + kRowChunk - 1) / kRowChunk);
-        const size_t sm = pure_smem(P.sideB.ng);
-        BSIM_CUDA(cudaFuncSetAttribute(pure_rows_kernel<Ti, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        pure_rows_kernel<Ti, T><<<g, 256, sm, s>>>(P.sideB, nB, P.d_bstr, B->view.bmap, P.norb, ctT, tT, nullptr,
-                                                  nullptr, 0);
+        pure_rows_kernel<T><<<g, 256, 0, s>>>(P.sideB, P.csrB, ctT, tT, nullptr, nullptr, 0);
     }
     // 4. mixed
     if (P.nE > 0 && P.nF > 0 && P.M > 0) {
         const size_t per_col = (size_t)nA * P.M * sizeof(T);
-        size_t Wz = std::max<size_t>(64, (scratch_budget() / per_col) / 64 * 64);
-        Wz = std::min<size_t>(Wz, ((size_t)nB + 63) / 64 * 64);
+        size_t Wz = std::max<size_t>(kMixCols, (scratch_budget() / per_col) / kMixCols * kMixCols);
+        Wz = std::min<size_t>(Wz, ((size_t)nB + kMixCols - 1) / kMixCols * kMixCols);
         if ((rc = ensure(&S.Z, &S.z_n, per_col * Wz)) != BSIM_OK) return rc;
         MixedArgs ma{nA, nB, P.nE, P.nF, P.M, P.norb, P.d_Emask, P.d_Fmask, P.d_mA, P.d_mB,
-                     sizeof(T) == 8 ? (const void *)P.d_Lam : (const void *)P.d_Lam32, P.d_binom};
+                     sizeof(T) == 8 ? (const void *)P.d_Lam : (const void *)P.d_Lam32, P.d_ranktab};
         const size_t smem = mixed_smem_bytes(nB, P.nF, sizeof(T));
         if (smem > 227 * 1024) { set_error("mixed kernel needs %zu bytes of shared memory", smem); return BSIM_ERR_UNSUPPORTED; }
         BSIM_CUDA(cudaFuncSetAttribute(mixed_gemm_kernel<Ti, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         T *Z = static_cast<T *>(S.Z);
         for (int z0 = 0; z0 < nB; z0 += (int)Wz) {
-            mixed_gemm_kernel<Ti, T><<<nA, 256, smem, s>>>(ma, P.d_astr, P.d_bstr, ct, Z, z0, (int)Wz);
+            mixed_gemm_kernel<Ti, T><<<nA, kGemmThreads, smem, s>>>(ma, P.d_astr, P.d_bstr, ct, Z, z0, (int)Wz);
             dim3 g(nA, (unsigned)((std::min<size_t>(Wz, nB - z0) + kRowChunk - 1) / kRowChunk));
             mixed_gather_kernel<Ti, T><<<g, 256, 0, s>>>(ma, P.d_astr, B->view.amap, Z, dst, z0, (int)Wz);
         }

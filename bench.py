@@ -346,6 +346,339 @@ def gpu_sigma(args, rank, world, local_rank):
     return result
 
 
+def count_launches(fn, prefix="bsim::"):
+    """Kernels of this library launched by one call of fn, counted in an
+    untimed pass under the CUDA activity tracer."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    torch.cuda.synchronize()
+    try:
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize()
+    except Exception as e:  # tracer unavailable
+        log(f"launch count unavailable: {e}")
+        return None
+    n = 0
+    for ev in prof.events():
+        if prefix in ev.name and getattr(ev, "device_type", None) is not None and "CUDA" in str(ev.device_type):
+            n += 1
+    return n
+
+
+def timed_events(fn, k, w):
+    """Device time of k calls of fn after w warm-up calls (CUDA events on the
+    current stream, synchronised on both sides); ms per call."""
+    import torch
+    for _ in range(w):
+        fn()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / k
+
+
+# ---------------------------------------------------------------------------
+# FCI Davidson workload: time to the lowest root, FP64 vs FP32-bulk mixed
+# ---------------------------------------------------------------------------
+
+DAV_CFGS = {
+    # BASELINE config 0: plain FP64 FCI Davidson, 12 orbitals 6a+6b, subspace 8
+    "12o": dict(norb=12, na=6, nb=6, seed=0, maxspace=8, ncv=3),
+    # the sigma microbenchmark's space, where sigma dominates the step
+    "16o": dict(norb=16, na=8, nb=8, seed=0, maxspace=8, ncv=3),
+}
+DAV_TOL = 1e-5          # residual norm (jl/davidson.jl convergence test); energy error checked against 1e-8 Eh
+DAV_METRIC = "FCI Davidson time to the lowest root within 1e-8 Eh (FP64 path)"
+
+
+def gpu_davidson(args):
+    import torch
+    from binsim_b200 import cuotf, network as nw
+    cfg = DAV_CFGS[args.dav_size]
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    net = nw.hamiltonian_network(cfg["norb"], seed=cfg["seed"])
+    B = cuotf.CuBasis(cfg["norb"], cfg["na"], cfg["nb"])
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    dim = B.dim
+    diags = torch.zeros(dim, dtype=torch.float64, device="cuda")
+    f.get_diags(diags)
+    hf = B.hf_index()
+    v0h = np.zeros(dim)
+    v0h[hf] = 1.0
+    v0 = torch.from_numpy(v0h).cuda()
+    x = torch.empty_like(v0)
+    y = torch.empty_like(v0)
+    f.hvec(v0, y)           # builds the sigma plan outside the timed region
+    f.hvec_mixed(v0, y)
+    torch.cuda.synchronize()
+    log(f"davidson setup {time.time() - t0:.1f}s dim={dim} sigma path {f.sigma_path()}")
+    stats = {}
+
+    def run(mixed, tol=DAV_TOL):
+        def go():
+            stats[mixed] = f.davidson(v0.clone(), diags, x, tol=tol, maxiter=500, ncv=cfg["ncv"],
+                                      maxspace=cfg["maxspace"], mixed=mixed)
+        return go
+    # tight FP64 energy: the GPU FP64 path to a 1e-9 residual
+    run(False, 1e-9)()
+    e_tight = stats[False]["energy"]
+    steps, warm = max(1, args.steps), max(3, args.warmup)
+    ms64 = timed_events(run(False), steps, warm)
+    st64 = dict(stats[False])
+    ms32 = timed_events(run(True), steps, warm)
+    st32 = dict(stats[True])
+    launches = count_launches(run(False))
+    # e2e: host start vector and diagonal in, host eigenvector out, per solve
+    v0pin = torch.from_numpy(v0h).pin_memory()
+    dpin = diags.cpu().pin_memory()
+    xpin = torch.empty(dim, dtype=torch.float64).pin_memory()
+
+    def e2e():
+        v0.copy_(v0pin, non_blocking=True)
+        diags.copy_(dpin, non_blocking=True)
+        run(False)()
+        xpin.copy_(x, non_blocking=True)
+    ms_e2e = timed_events(e2e, steps, 1)
+    cpu = None
+    if not args.no_cpu_baseline and args.dav_size == "12o":
+        cpu = run_cpu_davidson(args)
+    e_oracle = cpu["energy"] if cpu and "energy" in cpu else e_tight
+    sig = dim * 16.0
+    res = {
+        "metric": DAV_METRIC, "value": ms64 * 1e-3, "unit": "s", "n_gpus": 1, "steps": steps, "warmup": warm,
+        "ms_per_step": ms64, "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"FCI Davidson, lowest root, {cfg['norb']} orbitals {cfg['na']}a+{cfg['nb']}b, "
+                               f"{dim:,} dets, UInt32 strings, seeded synthetic integrals (seed {cfg['seed']}), "
+                               f"HF start, subspace {cfg['maxspace']}, restart to {cfg['ncv']}, residual tol {DAV_TOL}",
+                   "dim": dim, "l2": "vectors larger than L2" if sig > 126e6 else "vectors fit in L2"},
+        "fp64": {"seconds": ms64 * 1e-3, "iterations": st64["iterations"], "sigma_fp64": st64["sigma_fp64"],
+                 "energy": st64["energy"], "abs_err_vs_oracle": abs(st64["energy"] - e_oracle)},
+        "mixed": {"seconds": ms32 * 1e-3, "iterations": st32["iterations"], "sigma_fp64": st32["sigma_fp64"],
+                  "sigma_fp32": st32["sigma_fp32"], "energy": st32["energy"],
+                  "abs_err_vs_oracle": abs(st32["energy"] - e_oracle), "speedup_vs_fp64": ms64 / ms32},
+        "oracle_energy": {"value": e_oracle, "source": "reference CPU Davidson (libotf_native + libdiag), "
+                                                       "residual 1e-9" if cpu and "energy" in cpu else
+                          "GPU FP64 Davidson to residual 1e-9 (parity-tested path)"},
+        "e2e": {"value": ms_e2e * 1e-3, "unit": "s", "h2d_bytes_per_step": 2 * dim * 8, "d2h_bytes_per_step": dim * 8,
+                "ms_per_step": ms_e2e},
+        "gpu_launches": launches * steps if launches is not None else None,
+    }
+    if cpu:
+        res["cpu_baseline"] = {"value": cpu.get("seconds"), "unit": "s", "cores": cpu.get("cores"),
+                               "kind": "reference", "sample": cpu.get("sample")}
+    return res
+
+
+# ---------------------------------------------------------------------------
+# VQE workload: energy + full gradient by the adjoint sweep
+# ---------------------------------------------------------------------------
+
+VQE_CFG = dict(norb=14, na=7, nb=7, seed=0, n_gen=2000, amp=0.05, ckpt=64)
+VQE_METRIC = "VQE UCCGSD energy + adjoint gradient evaluations per second"
+
+
+def vqe_problem(cfg):
+    from binsim_b200 import network as nw
+    ham = nw.hamiltonian_network(cfg["norb"], seed=cfg["seed"])
+    pool = nw.ucc_pool(cfg["norb"])
+    op_idx, param_idx, th = nw.draw_generators(pool, cfg["n_gen"], seed=cfg["seed"], amp_sigma=cfg["amp"])
+    return ham, pool, op_idx, param_idx, th
+
+
+def gpu_vqe(args):
+    import torch
+    from binsim_b200 import cuotf
+    cfg = VQE_CFG
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    ham, pool, op_idx, param_idx, th = vqe_problem(cfg)
+    B = cuotf.CuBasis(cfg["norb"], cfg["na"], cfg["nb"])
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(ham), cuotf.CuNetwork(pool.network))
+    dim = B.dim
+    ref_idx, ref_val = np.array([B.hf_index()]), np.array([1.0])
+    lv = torch.empty(dim, dtype=torch.float64, device="cuda")
+    rv = torch.empty_like(lv)
+    f.hvec(lv.zero_(), rv)
+    torch.cuda.synchronize()
+    log(f"vqe setup {time.time() - t0:.1f}s dim={dim} components={len(op_idx)} params={len(th)}")
+    out = {}
+
+    def adjoint():
+        out["adj"] = f.energy_grad(op_idx, param_idx, th, ref_idx, ref_val, lv, rv, ckpt_every=cfg["ckpt"])
+    steps, warm = max(1, args.steps), max(3, args.warmup)
+    with Clocks(0) as clk:
+        ms_adj = timed_events(adjoint, steps, warm)
+    E, g, var = out["adj"]
+    launches = count_launches(adjoint)
+
+    # the reference's energy_objective (jl/vqe.jl:1-21) step by step through the
+    # legacy entry points: one expm per component, hvec, one backgrad per
+    # component with its host round trip
+    def ref_sweep():
+        lv.zero_()
+        lv[int(ref_idx[0])] = 1.0
+        for i, p in zip(op_idx, param_idx):
+            f.expm(int(i) + 1, float(th[p]), lv)
+        f.hvec(lv, rv)
+        ln = float(lv @ lv)
+        gg = np.zeros(len(th))
+        for i, p in zip(op_idx[::-1], param_idx[::-1]):
+            gg[p] += f.backgrad(int(i) + 1, float(th[p]), lv, rv) * 2 / ln
+        out["sweep"] = gg
+    ms_sweep = timed_events(ref_sweep, 1, 1)
+
+    # plain per-parameter gradient: central differences, two energies per parameter
+    def energy(t):
+        f.prepare_state(op_idx, param_idx, t, ref_idx, ref_val, lv)
+        f.hvec(lv, rv)
+        return float(lv @ rv) / float(lv @ lv)
+    ms_energy = timed_events(lambda: energy(th), steps, 1)
+    h = 1e-5
+    fd_err = 0.0
+    for p in range(4):
+        tp, tm = th.copy(), th.copy()
+        tp[p] += h
+        tm[p] -= h
+        fd_err = max(fd_err, abs((energy(tp) - energy(tm)) / (2 * h) - g[p]))
+    ms_fd = 2 * len(th) * ms_energy
+    # e2e: parameters from the host, energy and gradient back to the host (the call does both)
+    res = {
+        "metric": VQE_METRIC, "value": 1000.0 / ms_adj, "unit": "evals/s", "n_gpus": 1, "steps": steps,
+        "warmup": warm, "ms_per_step": ms_adj, "higher_is_better": True, "scaling": "replicas",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"VQE energy + gradient, {cfg['norb']} orbitals {cfg['na']}a+{cfg['nb']}b, {dim:,} dets, "
+                               f"{cfg['n_gen']} spin-adapted generalised singles/doubles drawn with seed {cfg['seed']} "
+                               f"({len(op_idx)} spin-orbital components), amplitudes N(0, {cfg['amp']}^2), HF reference, "
+                               f"checkpoint every {cfg['ckpt']} generators",
+                   "dim": dim, "components": int(len(op_idx)), "params": int(len(th)),
+                   "l2": "state vectors 94 MB each; two of them plus checkpoints exceed L2"},
+        "energy": E, "variance": var,
+        "adjoint_vs_reference_sweep": {"sweep_ms": ms_sweep, "speedup": ms_sweep / ms_adj,
+                                       "max_abs_grad_diff": float(np.abs(out["sweep"] - g).max()),
+                                       "note": "jl/vqe.jl energy_objective on this library's legacy entry points"},
+        "adjoint_vs_per_parameter": {"fd_ms": ms_fd, "energy_ms": ms_energy, "speedup": ms_fd / ms_adj,
+                                     "max_abs_fd_err_first4": fd_err,
+                                     "note": "central differences h=1e-5: 2 energies per parameter, "
+                                             "time = 2 * params * one energy evaluation"},
+        "e2e": {"value": 1000.0 / ms_adj, "unit": "evals/s", "h2d_bytes_per_step": int(8 * (len(th) + 2 * len(op_idx))),
+                "d2h_bytes_per_step": int(8 * (len(th) + 2)), "ms_per_step": ms_adj,
+                "note": "the public call takes host parameters and returns host energy and gradient"},
+        "gpu_launches": launches * steps if launches is not None else None,
+        "clocks": clk.summary(),
+    }
+    return res
+
+
+def cpu_davidson_worker(args):
+    from binsim_b200 import network as nw
+    from oracle.oracle import RefLibs, ref_available
+    if not ref_available():
+        print(json.dumps({"unavailable": "oracle/_ref not built"}))
+        return
+    cfg = DAV_CFGS[args.dav_size]
+    R = RefLibs()
+    net = nw.hamiltonian_network(cfg["norb"], seed=cfg["seed"])
+    b, dim = R.basis(cfg["norb"], cfg["na"], cfg["nb"])
+    n = R.network(net)
+    d = R.diag_elems(b, n, dim)
+    v0 = np.zeros(dim)
+    v0[R.det_index(b, (1 << cfg["na"]) - 1, (1 << cfg["nb"]) - 1, dim)] = 1.0
+    t0 = time.perf_counter()
+    e, _, it, ns = R.davidson(b, n, v0, d, tol=DAV_TOL, ncv=cfg["ncv"], maxspace=cfg["maxspace"])
+    sec = time.perf_counter() - t0
+    out = {"seconds": sec, "energy_at_tol": e, "iterations": it, "sigma": ns}
+    if args.dav_oracle:
+        e2, _, _, _ = R.davidson(b, n, v0, d, tol=1e-9, ncv=cfg["ncv"], maxspace=cfg["maxspace"])
+        out["energy"] = e2
+    print(json.dumps(out))
+
+
+def cpu_vqe_worker(args):
+    """The reference's energy_objective (jl/vqe.jl:1-21) on libotf_native: a
+    bounded prefix of the forward expm sweep and of the backgrad sweep, one full
+    hvec, scaled to the whole component sequence."""
+    import ctypes as C
+    from oracle.oracle import RefLibs, ref_available
+    if not ref_available():
+        print(json.dumps({"unavailable": "oracle/_ref not built"}))
+        return
+    cfg = VQE_CFG
+    R = RefLibs()
+    ham, pool, op_idx, param_idx, th = vqe_problem(cfg)
+    b, dim = R.basis(cfg["norb"], cfg["na"], cfg["nb"])
+    hn, pn = R.network(ham), R.network(pool.network)
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    lv = np.zeros(dim)
+    lv[R.det_index(b, (1 << cfg["na"]) - 1, (1 << cfg["nb"]) - 1, dim)] = 1.0
+    rv = np.zeros(dim)
+    k = min(len(op_idx), args.vqe_sample)
+    t0 = time.perf_counter()
+    for i in range(k):
+        R.otf.expm_contract_otf_f64(b, pn, int(op_idx[i]), float(th[param_idx[i]]), P(lv))
+    t_exp = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    R.otf.hvec_gather_contract_otf_f64(b, hn, P(lv), P(rv))
+    t_h = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for i in reversed(range(k)):
+        R.otf.backgrad_contract_otf_f64(b, pn, int(op_idx[i]), float(th[param_idx[i]]), P(lv), P(rv))
+    t_bg = time.perf_counter() - t0
+    n = len(op_idx)
+    sec = (t_exp + t_bg) * n / k + t_h
+    print(json.dumps({"seconds": sec, "sample_components": k, "components": n, "t_expm": t_exp, "t_backgrad": t_bg,
+                      "t_hvec": t_h}))
+
+
+def run_cpu_worker(args, extra):
+    cores = physical_cores()
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close", OMP_PLACES="cores")
+    env.pop("CUDA_VISIBLE_DEVICES", None)
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker"] + extra
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
+    if r.returncode != 0:
+        log(r.stderr[-2000:])
+        return None, cores
+    return json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1]), cores
+
+
+def run_cpu_vqe(args):
+    out, cores = run_cpu_worker(args, ["--workload", "vqe", "--vqe-sample", str(args.vqe_sample)])
+    if out is None or "seconds" not in out:
+        return out
+    out["cores"] = cores
+    out["sample"] = (f"reference energy_objective on libotf_native: first {out['sample_components']} of "
+                     f"{out['components']} components of the expm and backgrad sweeps, scaled by the component count, "
+                     f"plus one full hvec; {cpu_model()}")
+    return out
+
+
+def run_cpu_davidson(args, oracle_energy=True):
+    out, cores = run_cpu_worker(args, ["--workload", "davidson", "--dav-size", args.dav_size] +
+                                (["--dav-oracle"] if oracle_energy else []))
+    if out is None or "seconds" not in out:
+        return out
+    out["cores"] = cores
+    out["sample"] = (f"whole solve: reference Davidson driver (jl/davidson.jl restated over libdiag) with "
+                     f"libotf_native sigma, residual tol {DAV_TOL}, {out.get('iterations')} iterations; {cpu_model()}")
+    return out
+
+
+def physical_cores():
+    try:
+        import psutil
+        return psutil.cpu_count(logical=False) or os.cpu_count()
+    except Exception:
+        return os.cpu_count()
+
+
 # ---------------------------------------------------------------------------
 # main
 # ---------------------------------------------------------------------------
@@ -356,7 +689,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="sigma", choices=["sigma"])
+    ap.add_argument("--workload", default="sigma", choices=["sigma", "davidson", "vqe"])
+    ap.add_argument("--dav-size", default="12o", choices=sorted(DAV_CFGS))
+    ap.add_argument("--dav-oracle", action="store_true")
+    ap.add_argument("--vqe-sample", type=int, default=200)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--cpu-reps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -364,7 +700,7 @@ def main():
     args = ap.parse_args()
 
     if args.cpu_worker:
-        cpu_worker(args)
+        {"sigma": cpu_worker, "davidson": cpu_davidson_worker, "vqe": cpu_vqe_worker}[args.workload](args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -374,21 +710,20 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        res, cores = run_cpu_baseline(args)
-        if res is None or "unavailable" in res:
-            print(json.dumps({"impl": "reference", "unavailable": (res or {}).get("unavailable", "worker failed")}))
+        reference_arm(args)
+        return
+
+    if args.workload != "sigma":
+        # Davidson and VQE are single-state solves: one GPU (further ranks would be replicas)
+        if rank != 0:
             return
-        sample = (f"reference libotf_native hvec_gather_contract_otf_f64 on every {res['stride']}-th off-diagonal "
-                  f"group ({res['sample_groups']} groups, {res['sample_pairs']:.3e} of {res['full_pairs']:.3e} pair "
-                  f"updates), scaled by exact pair counts; {cpu_model()}")
-        line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
-                "steps": res["reps"], "warmup": 1, "ms_per_step": res["sec_per_sigma"] * 1e3,
-                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": "sigma microbenchmark (config 1): H*c, 16 orbitals 8a+8b"},
-                "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": cores, "kind": "reference",
-                                 "sample": sample},
-                "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        result = gpu_davidson(args) if args.workload == "davidson" else gpu_vqe(args)
+        if args.workload == "vqe" and not args.no_cpu_baseline:
+            cpu = run_cpu_vqe(args)
+            if cpu and "seconds" in cpu:
+                result["cpu_baseline"] = {"value": 1.0 / cpu["seconds"], "unit": "evals/s", "cores": cpu["cores"],
+                                          "kind": "reference", "sample": cpu["sample"]}
+        print(json.dumps(result))
         return
 
     if world > 1:
@@ -414,6 +749,54 @@ def main():
                 result["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
                                           "sample": "unavailable: oracle/_ref not built"}
         print(json.dumps(result))
+
+
+def reference_arm(args):
+    """The reference's own CPU implementation of the workload, on the host cores."""
+    base = {"impl": "reference", "n_gpus": args.gpus, "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
+    if args.workload == "sigma":
+        res, cores = run_cpu_baseline(args)
+        if res is None or "unavailable" in res:
+            print(json.dumps({"impl": "reference", "unavailable": (res or {}).get("unavailable", "worker failed")}))
+            return
+        sample = (f"reference libotf_native hvec_gather_contract_otf_f64 on every {res['stride']}-th off-diagonal "
+                  f"group ({res['sample_groups']} groups, {res['sample_pairs']:.3e} of {res['full_pairs']:.3e} pair "
+                  f"updates), scaled by exact pair counts; {cpu_model()}")
+        line = dict(base, metric=METRIC, value=res["value"], unit=UNIT, steps=res["reps"], warmup=1,
+                    ms_per_step=res["sec_per_sigma"] * 1e3, higher_is_better=True, scaling="strong",
+                    config={"workload": "sigma microbenchmark (config 1): H*c, 16 orbitals 8a+8b"},
+                    cpu_baseline={"value": res["value"], "unit": UNIT, "cores": cores, "kind": "reference",
+                                  "sample": sample},
+                    e2e={"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    elif args.workload == "davidson":
+        if args.dav_size != "12o":
+            print(json.dumps({"impl": "reference", "unavailable": "the CPU reference solve of the 16-orbital space "
+                                                                  "takes tens of minutes; timed on 12 orbitals only"}))
+            return
+        cpu = run_cpu_davidson(args, oracle_energy=False)
+        if not cpu or "seconds" not in cpu:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+            return
+        cfg = DAV_CFGS[args.dav_size]
+        line = dict(base, metric=DAV_METRIC, value=cpu["seconds"], unit="s", steps=1, warmup=0,
+                    ms_per_step=cpu["seconds"] * 1e3, higher_is_better=False, scaling="strong",
+                    config={"workload": f"FCI Davidson, lowest root, {cfg['norb']} orbitals {cfg['na']}a+{cfg['nb']}b"},
+                    cpu_baseline={"value": cpu["seconds"], "unit": "s", "cores": cpu["cores"], "kind": "reference",
+                                  "sample": cpu["sample"]},
+                    e2e={"value": cpu["seconds"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    else:
+        cpu = run_cpu_vqe(args)
+        if not cpu or "seconds" not in cpu:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+            return
+        v = 1.0 / cpu["seconds"]
+        line = dict(base, metric=VQE_METRIC, value=v, unit="evals/s", steps=1, warmup=0,
+                    ms_per_step=cpu["seconds"] * 1e3, higher_is_better=True, scaling="replicas",
+                    config={"workload": "VQE energy + gradient, 14 orbitals 7a+7b, 2000 generators"},
+                    cpu_baseline={"value": v, "unit": "evals/s", "cores": cpu["cores"], "kind": "reference",
+                                  "sample": cpu["sample"]},
+                    e2e={"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    print(json.dumps(line))
 
 
 if __name__ == "__main__":

@@ -68,6 +68,9 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     }
     if (norb > 24) { P->why = "norb > 24"; return BSIM_OK; }
     P->norb = norb; P->nA = nA; P->nB = nB; P->nelA = nelA; P->nelB = nelB;
+    P->ldA = (nB + 7) & ~7;
+    P->ldB = (nA + 7) & ~7;
+    P->ldG = (nB + kMixCols - 1) / kMixCols * kMixCols;
     P->Ka.resize(nA);
     for (int a = 0; a < nA; ++a) {
         u64 k = 0, s = (u64)A[a];
@@ -94,11 +97,11 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
         const GroupDev &G = N->groups[diag[0]];
         P->rank_d = G.rank;
         PAd.resize((size_t)nA * G.rank);
-        PBd.resize((size_t)nB * G.rank);
+        PBd.assign((size_t)G.rank * P->ldA, 0.0);
         for (int a = 0; a < nA; ++a)
             for (int r = 0; r < G.rank; ++r) PAd[(size_t)a * G.rank + r] = phase_r(A[a], z + G.za_off, G.nza, w + G.wa_off, r, 0);
         for (int b = 0; b < nB; ++b)
-            for (int r = 0; r < G.rank; ++r) PBd[(size_t)b * G.rank + r] = phase_r(Bs[b], z + G.zb_off, G.nzb, w + G.wb_off, r, 0);
+            for (int r = 0; r < G.rank; ++r) PBd[(size_t)r * P->ldA + b] = phase_r(Bs[b], z + G.zb_off, G.nzb, w + G.wb_off, r, 0);
     }
 
     // ---- pure sides: row-spin data + column factor in the alpha-first frame -----
@@ -112,6 +115,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
         SideHost &S = sh[side];
         const auto &colstr = side == 0 ? Bs : A;
         const int ncol = side == 0 ? nB : nA;
+        const int ld = side == 0 ? P->ldA : P->ldB;
         for (int g : gl) {
             const GroupDev &G = N->groups[g];
             const u64 rowx = side == 0 ? G.ax : G.bx;
@@ -142,7 +146,11 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
             for (int r = 0; r < kSideMaxRank; ++r) S.cconst.push_back(r < G.rank ? col[(size_t)r * ncol] : 0.0);
             S.colmode.push_back(constant ? 0 : 1);
             S.ctab_off.push_back(constant ? -1 : (i64)S.ctab.size());
-            if (!constant) S.ctab.insert(S.ctab.end(), col.begin(), col.end());
+            if (!constant)
+                for (int r = 0; r < G.rank; ++r) {
+                    S.ctab.insert(S.ctab.end(), col.begin() + (size_t)r * ncol, col.begin() + (size_t)(r + 1) * ncol);
+                    S.ctab.resize(S.ctab.size() + (ld - ncol), 0.0);
+                }
         }
     };
     add_side(0, pa);
@@ -150,8 +158,8 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     // per-row contribution lists (CSR), built with a few host threads
     struct CSRHost {
         std::vector<i64> cptr, tptr;
-        std::vector<int> csrc, tsrc, tgid;
-        std::vector<double> ccoef, tpa;
+        std::vector<CEnt> cent;
+        std::vector<TEnt> tent;
     } csr[2];
     {
         std::vector<int> amap((size_t)1 << norb, -1), bmap((size_t)1 << norb, -1);
@@ -164,10 +172,11 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
             const int nrows = side == 0 ? nA : nB;
             const int ng = (int)S.x.size();
             const int nth = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+            const i64 ld_in = side == 0 ? P->ldA : P->ldB;
             struct Part {
                 std::vector<i64> cn, tn;
-                std::vector<int> csrc, tsrc, tgid;
-                std::vector<double> ccoef, tpa;
+                std::vector<CEnt> cent;
+                std::vector<TEnt> tent;
             };
             std::vector<Part> parts(nth);
             auto work = [&](int t) {
@@ -195,13 +204,12 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
                         if (S.colmode[g] == 0) {
                             double coef = 0.0;
                             for (int rr = 0; rr < R; ++rr) coef += pa[rr] * S.cconst[(size_t)g * kSideMaxRank + rr];
-                            pt.csrc.push_back(src);
-                            pt.ccoef.push_back(coef);
+                            pt.cent.push_back(CEnt{(long long)src * ld_in, coef});
                             ++cc;
                         } else {
-                            pt.tsrc.push_back(src);
-                            pt.tgid.push_back(g);
-                            for (int rr = 0; rr < kSideMaxRank; ++rr) pt.tpa.push_back(pa[rr]);
+                            TEnt t{(long long)src * ld_in, (long long)S.ctab_off[g] | R, {0, 0, 0, 0}};
+                            for (int rr = 0; rr < kSideMaxRank; ++rr) t.pa[rr] = pa[rr];
+                            pt.tent.push_back(t);
                             ++tc;
                         }
                     }
@@ -219,16 +227,13 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
             for (auto &pt : parts) {
                 for (i64 v : pt.cn) C.cptr.push_back(C.cptr.back() + v);
                 for (i64 v : pt.tn) C.tptr.push_back(C.tptr.back() + v);
-                C.csrc.insert(C.csrc.end(), pt.csrc.begin(), pt.csrc.end());
-                C.ccoef.insert(C.ccoef.end(), pt.ccoef.begin(), pt.ccoef.end());
-                C.tsrc.insert(C.tsrc.end(), pt.tsrc.begin(), pt.tsrc.end());
-                C.tgid.insert(C.tgid.end(), pt.tgid.begin(), pt.tgid.end());
-                C.tpa.insert(C.tpa.end(), pt.tpa.begin(), pt.tpa.end());
+                C.cent.insert(C.cent.end(), pt.cent.begin(), pt.cent.end());
+                C.tent.insert(C.tent.end(), pt.tent.begin(), pt.tent.end());
             }
         }
     }
-    P->nnzA = (i64)csr[0].csrc.size();
-    P->nnzB = (i64)csr[1].csrc.size();
+    P->nnzA = (i64)csr[0].cent.size();
+    P->nnzB = (i64)csr[1].cent.size();
     P->nPA = (int)pa.size();
     P->nPB = (int)pb.size();
 
@@ -310,17 +315,31 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     P->fits32 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 4) <= 227 * 1024;
     if (!P->fits64 && !P->fits32) { P->why = "beta row too long for the mixed kernel's shared memory"; return BSIM_OK; }
 
+    // ---- gather-index table of the mixed GEMM: X[F][b] = sB_F(b^F) c~[a', b^F] ------
+    std::vector<int> gidx((size_t)P->nF * P->ldG, -1);
+    {
+        std::unordered_map<u64, int> bidx;
+        bidx.reserve((size_t)nB * 2);
+        for (int b = 0; b < nB; ++b) bidx[(u64)Bs[b]] = b;
+        for (int f = 0; f < P->nF; ++f)
+            for (int b = 0; b < nB; ++b) {
+                const u64 s0 = (u64)Bs[b], fm = P->Fmask[f];
+                if (popc(s0 & fm) != 1) continue;
+                const u64 sv = s0 ^ fm;
+                auto it = bidx.find(sv);
+                if (it == bidx.end()) continue;
+                gidx[(size_t)f * P->ldG + b] = (it->second << 1) | (popc(sv & P->mB[f]) & 1);
+            }
+    }
+
     // ---- upload -------------------------------------------------------------------
     auto bytes = [](size_t n, size_t sz) { return ((std::max<size_t>(n, 1) * sz) + 255) & ~size_t(255); };
     size_t tot = bytes(nA, sizeof(Ti)) + bytes(nB, sizeof(Ti)) + bytes(nA, 8) + bytes(PAd.size(), 8) +
-                 bytes(PBd.size(), 8) + 4 * bytes(P->nE + P->nF, 8) + 2 * bytes(P->Lam.size(), 8) +
-                 bytes(33 * 33, 4) + bytes(kRankTabInts, 4) + bytes(P->residual.size(), 4) + bytes(P->residual.size() + 1, 16);
-    for (auto &C : csr)
-        tot += 2 * bytes(C.cptr.size(), 8) + bytes(C.csrc.size(), 4) + bytes(C.ccoef.size(), 8) +
-               2 * bytes(C.tsrc.size(), 4) + bytes(C.tpa.size(), 8);
-    for (auto &S : sh)
-        tot += 4 * bytes(S.x.size(), 8) + 3 * bytes(S.x.size(), 4) + bytes(S.cconst.size(), 8) +
-               bytes(S.zmask.size(), 8) + bytes(S.wv.size(), 8) + bytes(S.ctab.size(), 8) + bytes(S.ctab.size(), 4);
+                 bytes(PBd.size(), 8) + 2 * bytes(P->nE, 8) + 2 * bytes(P->Lam.size(), 8) + bytes(gidx.size(), 4) +
+                 bytes(P->residual.size(), 4) + bytes(P->residual.size() + 1, 16);
+    for (int side = 0; side < 2; ++side)
+        tot += 2 * bytes(csr[side].cptr.size(), 8) + bytes(csr[side].cent.size(), sizeof(CEnt)) +
+               bytes(csr[side].tent.size(), sizeof(TEnt)) + bytes(sh[side].ctab.size(), 8);
     int st = P->arena.reserve(tot);
     if (st != BSIM_OK) return st;
     auto put = [&](const auto &v) {
@@ -333,60 +352,21 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     P->d_bstr = put(Bs);
     P->d_Ka = put(P->Ka);
     P->d_PAd = put(PAd);
-    P->d_PBd = put(PBd);
+    P->d_PBdT = put(PBd);
     P->d_Emask = put(P->Emask);
-    P->d_Fmask = put(P->Fmask);
     P->d_mA = put(P->mA);
-    P->d_mB = put(P->mB);
     P->d_Lam = put(P->Lam);
     std::vector<float> lam32(P->Lam.begin(), P->Lam.end());
     P->d_Lam32 = put(lam32);
-    std::vector<int> binom(33 * 33, 0);
-    for (int n = 0; n <= 32; ++n)
-        for (int k = 0; k <= 32; ++k) binom[n * 33 + k] = (int)std::min<u64>(comb_count(n, k), 0x7fffffff);
-    P->d_binom = put(binom);
-    // byte tables: T_k[byte][o] = sum over set bits of byte (ascending, j = o+1, o+2, ...) of C(8k + p, j)
-    std::vector<int> rt(kRankTabInts, 0);
-    const int tbase[3] = {0, 256, 256 + 256 * 9}, nofs[3] = {1, 9, 17};
-    for (int k = 0; k < 3; ++k)
-        for (int byte = 0; byte < 256; ++byte)
-            for (int o = 0; o < nofs[k]; ++o) {
-                u64 v = 0;
-                int j = o;
-                for (int p = 0; p < 8; ++p)
-                    if ((byte >> p) & 1) v += comb_count(8 * k + p, ++j);
-                rt[tbase[k] + byte * nofs[k] + o] = (int)std::min<u64>(v, 0x7fffffff);
-            }
-    P->d_ranktab = put(rt);
-    for (int side = 0; side < 2; ++side) {
-        SideHost &S = sh[side];
-        SideDev &D = side == 0 ? P->sideA : P->sideB;
-        D.ng = (int)S.x.size();
-        D.ncols = side == 0 ? nB : nA;
-        D.x = put(S.x);
-        D.rank = put(S.rank);
-        D.nz = put(S.nz);
-        D.z_off = put(S.z_off);
-        D.w_off = put(S.w_off);
-        D.colmode = put(S.colmode);
-        D.cconst = put(S.cconst);
-        D.ctab_off = put(S.ctab_off);
-        D.zmask = put(S.zmask);
-        D.w = put(S.wv);
-        D.ctab = put(S.ctab);
-        std::vector<float> c32(S.ctab.begin(), S.ctab.end());
-        D.ctab32 = put(c32);
-    }
+    P->d_gidx = put(gidx);
     for (int side = 0; side < 2; ++side) {
         CSRHost &C = csr[side];
         SideCSR &D = side == 0 ? P->csrA : P->csrB;
         D.cptr = put(C.cptr);
-        D.csrc = put(C.csrc);
-        D.ccoef = put(C.ccoef);
+        D.cent = put(C.cent);
         D.tptr = put(C.tptr);
-        D.tsrc = put(C.tsrc);
-        D.tgid = put(C.tgid);
-        D.tpa = put(C.tpa);
+        D.tent = put(C.tent);
+        D.ctab = put(sh[side].ctab);
     }
     // residual groups through the generic tile kernel (chunks as in DevNet::finalize)
     std::vector<int> res = P->residual;

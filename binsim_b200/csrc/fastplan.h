@@ -22,38 +22,33 @@
 
 namespace bsim {
 
-// Groups acting on one spin ("row" spin) with a factor on the other ("col")
-// spin.  For pure-alpha groups the rows are alpha strings; for pure-beta groups
-// the kernels run on the transposed vector, so rows are beta strings.
-struct SideDev {
-    int ng;              // groups on this side
-    int ncols;           // length of the other-spin list
-    const u64 *x;        // [ng] row-spin X mask
-    const int *rank;     // [ng]
-    const int *nz;       // [ng] row-spin Z count
-    const i64 *z_off;    // [ng] into zmask
-    const i64 *w_off;    // [ng] into w (column-major nz x rank)
-    const int *colmode;  // [ng] 0: constant column factor, 1: table
-    const double *cconst;  // [ng * kSideMaxRank]
-    const i64 *ctab_off;   // [ng] into ctab ([rank][ncols])
-    const u64 *zmask;
-    const double *w;
-    const double *ctab;
-    const float *ctab32;
-};
-
+// Pure groups act on one spin (the "row" spin) with a factor on the other
+// (column) spin.  Pure-alpha rows are alpha strings; pure-beta groups run on the
+// transposed vector, so their rows are beta strings.
 constexpr int kSideMaxRank = 4;
 
 // Static list of the pure-spin contributions of every row (depends only on the
-// basis and the network): constant-factor entries (source row, coefficient)
-// and table entries (source row, group, row-spin phases).
+// basis and the network).  Constant-factor entries carry the source row's
+// element offset in the padded input and the combined coefficient; table
+// entries carry the source offset, the offset of the group's column-factor
+// table (rank in the low 3 bits, tables start on multiples of 8) and the
+// row-spin phases.
+struct CEnt {
+    long long off;
+    double coef;
+};
+struct TEnt {
+    long long off;
+    long long toff_rank;
+    double pa[kSideMaxRank];
+};
+
 struct SideCSR {
     const i64 *cptr;      // [nrows + 1]
-    const int *csrc;      // [nnz_c]
-    const double *ccoef;  // [nnz_c]
+    const CEnt *cent;     // [nnz_c]
     const i64 *tptr;      // [nrows + 1]
-    const int *tsrc, *tgid;   // [nnz_t]
-    const double *tpa;    // [nnz_t * kSideMaxRank]
+    const TEnt *tent;     // [nnz_t]
+    const double *ctab;   // column-factor tables, rows padded to ld_in
 };
 
 template <typename Ti>
@@ -63,6 +58,9 @@ struct FastPlan {
     const void *basis = nullptr;
     i64 basis_dim = -1;
     int norb = 0, nA = 0, nB = 0, nelA = 0, nelB = 0;
+    // padded row strides: ldA for rows of c~ (alpha rows, beta columns), ldB for
+    // rows of c~^T and of the beta-side result, ldG for the gather-index table
+    int ldA = 0, ldB = 0, ldG = 0;
     // frame
     std::vector<u64> Ka;       // [nA] eps masks K(a)
     // diagonal D = PAd * PBd^T (tables [n x rank])
@@ -80,32 +78,27 @@ struct FastPlan {
     Arena arena;
     const Ti *d_astr = nullptr, *d_bstr = nullptr;
     const u64 *d_Ka = nullptr;
-    const double *d_PAd = nullptr, *d_PBd = nullptr;
-    SideDev sideA{}, sideB{};
+    const double *d_PAd = nullptr;     // [nA x rank_d] alpha diagonal factors
     SideCSR csrA{}, csrB{};
     i64 nnzA = 0, nnzB = 0;
-    const u64 *d_Emask = nullptr, *d_Fmask = nullptr, *d_mA = nullptr, *d_mB = nullptr;
+    const u64 *d_Emask = nullptr, *d_mA = nullptr;
     const double *d_Lam = nullptr;
     const float *d_Lam32 = nullptr;
-    const int *d_binom = nullptr;      // [33 x 33] binomials for string ranking
-    const int *d_ranktab = nullptr;    // [kRankTabInts] byte tables for string ranking
+    const double *d_PBdT = nullptr;    // [rank_d x ldA] beta diagonal factors, transposed
+    const int *d_gidx = nullptr;       // [nF x ldG] (rank(b^F) << 1 | sign) or -1
     const int *d_resid = nullptr;      // residual group plan (for the generic kernel)
     const int4 *d_resid_chunks = nullptr;
     int n_resid_chunks = 0;
     ~FastPlan() { arena.release(); }
 };
 
-// Shared memory of the mixed GEMM kernel: source row, Lam_conn [K x 64], an
-// X slice [32 x 64], the binomial table and the excitation lists.
-// Byte tables for the colex rank of a string: table k covers bits 8k..8k+7
-// and is indexed [byte][number of set bits below the byte].
-constexpr int kRankTabInts = 256 + 256 * 9 + 256 * 17;   // up to 24 orbitals
 constexpr int kMixCols = 128;                             // columns per GEMM chunk
 
+// Shared memory of the mixed GEMM kernel: source row, Lam_conn [K x 64], an
+// X slice [32 x kMixCols] and the connected-excitation lists.
 inline size_t mixed_smem_bytes(int nB, int nF, size_t elem)
 {
-    return (((size_t)nB + 7) & ~size_t(7)) * elem + (size_t)nF * 64 * elem + 32 * (size_t)kMixCols * elem +
-           (size_t)kRankTabInts * 4 + kMixCols * 8 + 128 * 4;
+    return (((size_t)nB + 7) & ~size_t(7)) * elem + (size_t)nF * 64 * elem + 32 * (size_t)kMixCols * elem + 128 * 4;
 }
 
 template <typename Ti>

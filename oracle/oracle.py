@@ -340,3 +340,83 @@ class RefLibs:
         self.bas.set_det_coeff_f64(b, astr, bstr, 1.0, P(v))
         nz = np.flatnonzero(v)
         return int(nz[0]) if len(nz) else -1
+
+    def davidson(self, b, n, v0, diags, tol=1e-5, ncv=3, maxspace=23, maxiter=100000):
+        """Lowest eigenpair by the reference driver jl/davidson.jl:1-160 over the
+        reference's libdiag helpers and hvec_gather_contract_otf_f64.
+
+        Returns (energy, vector, iterations, sigma_calls)."""
+        N = len(v0)
+        vpp = C.c_void_p * maxspace
+        V, AV = [np.array(v0, np.float64, copy=True)], [np.empty(N)]
+        Vp, AVp = vpp(), vpp()
+        Vp[0], AVp[0] = V[0].ctypes.data, AV[0].ctypes.data
+        axt = np.empty(N)
+        heff = np.zeros((maxspace, maxspace), order="F")
+        col = np.empty(maxspace)
+        d = self.diag
+        d.rebuild_heff_f64.argtypes = [i64, C.c_int, vp, vp, vp, C.c_int]
+        d.inplace_normalize_f64(N, P(V[0]))
+        nsig = 0
+
+        def aop(x, y):
+            nonlocal nsig
+            y[:] = 0.0
+            self.otf.hvec_gather_contract_otf_f64(b, n, P(x), P(y))
+            nsig += 1
+
+        aop(V[0], AV[0])
+        heff[0, 0] = d.fast_dot_f64(N, P(V[0]), P(AV[0]))
+        dim = 1
+        e_best = heff[0, 0]
+        Vt, AVt = [], []
+        for it in range(1, maxiter + 1):
+            es, vs = np.linalg.eigh(heff[:dim, :dim])
+            k = int(np.argmin(es))
+            e_best = float(es[k])
+            coeffs = np.ascontiguousarray(vs[:, k])
+            norm_r = d.build_ritz_and_residual_f64(N, dim, P(coeffs), e_best, Vp, AVp, P(axt))
+            if norm_r < tol:
+                xt = np.empty(N)
+                d.build_ritz_vector_f64(N, dim, P(coeffs), Vp, P(xt))
+                return e_best, xt, it, nsig
+            if dim >= maxspace:
+                nsave = min(ncv, dim)
+                order = np.argsort(es)
+                while len(Vt) < nsave:
+                    Vt.append(np.empty(N)); AVt.append(np.empty(N))
+                for i in range(nsave):
+                    c = vs[:, order[i]]
+                    Vt[i][:] = 0.0; AVt[i][:] = 0.0
+                    for j in range(dim):
+                        Vt[i] += c[j] * V[j]
+                        AVt[i] += c[j] * AV[j]
+                for i in range(nsave):
+                    V[i][:] = Vt[i]; AV[i][:] = AVt[i]
+                dim = nsave
+                d.rebuild_heff_f64(N, dim, Vp, AVp, heff.ctypes.data, maxspace)
+            shift = max(norm_r * 1e-2, 1e-4)
+            d.apply_preconditioner_inplace_f64(N, P(axt), P(diags), e_best, shift)
+            nb_ = float(np.linalg.norm(axt))
+            na_ = d.mgs_orthogonalize_f64(N, dim, Vp, P(axt))
+            if na_ < 0.717 * nb_:
+                na_ = d.mgs_orthogonalize_f64(N, dim, Vp, P(axt))
+            if na_ < 1e-12:
+                xt = np.empty(N)
+                d.build_ritz_vector_f64(N, dim, P(coeffs), Vp, P(xt))
+                return e_best, xt, it, nsig
+            d.inplace_normalize_f64(N, P(axt))
+            dim += 1
+            if len(V) < dim:
+                V.append(np.empty(N)); AV.append(np.empty(N))
+                Vp[dim - 1], AVp[dim - 1] = V[-1].ctypes.data, AV[-1].ctypes.data
+            V[dim - 1][:] = axt
+            aop(V[dim - 1], AV[dim - 1])
+            d.compute_heff_col_f64(N, dim, Vp, P(AV[dim - 1]), P(col))
+            heff[:dim, dim - 1] = col[:dim]
+            heff[dim - 1, :dim] = col[:dim]
+        es, vs = np.linalg.eigh(heff[:dim, :dim])
+        coeffs = np.ascontiguousarray(vs[:, int(np.argmin(es))])
+        xt = np.empty(N)
+        d.build_ritz_vector_f64(N, dim, P(coeffs), Vp, P(xt))
+        return e_best, xt, maxiter, nsig

@@ -198,6 +198,89 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
     TRY(dav_normalize(S, n, x, sc, s));
     double h[kMaxSub * kMaxSub], es[kMaxSub], vs[kMaxSub * kMaxSub], col[kMaxSub];
     int total_inner = 0;
+
+    // ---- phase A: the reference driver's Davidson (restart to ncv Ritz vectors)
+    // on FP32 subspace storage with the FP32-bulk sigma; it stops at the
+    // tolerance or where the FP32 residual stalls, and the FP64 refinement below
+    // takes over from its Ritz vector.
+    {
+        const int ncv = std::min(3, maxspace - 1);
+        std::vector<DevBuf> tvb(ncv), tavb(ncv);
+        std::vector<float *> Vt(ncv), AVt(ncv);
+        for (int j = 0; j < ncv; ++j) {
+            TRY(alloc<float>(tvb[j], n, s)); TRY(alloc<float>(tavb[j], n, s));
+            Vt[j] = (float *)tvb[j].p; AVt[j] = (float *)tavb[j].p;
+        }
+        cvt_kernel_d2f<<<grid, 256, 0, s>>>(x, V[0], n);
+        TRY(sigma(B, N, nullptr, V[0], ay, true, s));
+        st.sigma_fp32++;
+        cvt_kernel_d2f<<<grid, 256, 0, s>>>(ay, AV[0], n);
+        TRY(dav_multidot<float, float>(S, n, 1, V.data(), AV[0], S.res, s));
+        TRY(fetch(&h[0], S.res, 1, s));
+        int dim = 1;
+        double best = 1e300;   // smallest residual so far and the iterations since it
+        int since_best = 0;
+        for (int iter = 1; iter <= maxiter; ++iter) {
+            jacobi_eigh(dim, h, kMaxSub, es, vs);
+            const double e = es[0];
+            double norm_r;
+            TRY(dav_ritz_residual<float>(S, n, dim, vs, e, V.data(), AV.data(), t, sc, s));
+            TRY(fetch(&norm_r, sc, 1, s));
+            if (verbose) printf("  fp32 step %03d: residual %.4e e %.14f\n", iter, norm_r, e);
+            // leave at the tolerance, or when the FP32 residual has stopped improving
+            // (its noise floor) for a whole subspace cycle
+            if (norm_r < best) { best = norm_r; since_best = 0; }
+            else ++since_best;
+            if (norm_r < tol || since_best >= maxspace || total_inner >= maxiter) break;
+            if (dim >= maxspace) {
+                const int nsave = std::min(ncv, dim);
+                for (int i = 0; i < nsave; ++i) {
+                    TRY(dav_combine<float, float>(n, dim, vs + (size_t)i * dim, V.data(), Vt[i], s));
+                    TRY(dav_combine<float, float>(n, dim, vs + (size_t)i * dim, AV.data(), AVt[i], s));
+                }
+                for (int i = 0; i < nsave; ++i) { std::swap(V[i], Vt[i]); std::swap(AV[i], AVt[i]); }
+                dim = nsave;
+                for (int j = 0; j < dim; ++j) {
+                    TRY(dav_multidot<float, float>(S, n, dim, V.data(), AV[j], S.res, s));
+                    TRY(fetch(col, S.res, dim, s));
+                    for (int i = 0; i < dim; ++i) h[i + j * kMaxSub] = col[i];
+                }
+                for (int j = 0; j < dim; ++j)
+                    for (int i = 0; i < j; ++i)
+                        h[i + j * kMaxSub] = h[j + i * kMaxSub] = 0.5 * (h[i + j * kMaxSub] + h[j + i * kMaxSub]);
+            }
+            const double shift = std::max(norm_r * 1e-2, 1e-4);
+            double nrm[2];
+            TRY(dav_precondition(S, n, t, diags, e, shift, sc, s));
+            TRY(fetch(&nrm[0], sc, 1, s));
+            TRY(dav_mgs<float>(S, n, dim, V.data(), t, sc + 1, s));
+            TRY(fetch(&nrm[1], sc + 1, 1, s));
+            if (nrm[1] < 0.717 * nrm[0]) {
+                TRY(dav_mgs<float>(S, n, dim, V.data(), t, sc + 1, s));
+                TRY(fetch(&nrm[1], sc + 1, 1, s));
+            }
+            if (nrm[1] < 1e-12) break;
+            TRY(dav_normalize(S, n, t, sc, s));
+            cvt_kernel_d2f<<<grid, 256, 0, s>>>(t, V[dim], n);
+            TRY(sigma(B, N, nullptr, V[dim], ay, true, s));
+            st.sigma_fp32++;
+            ++total_inner;
+            cvt_kernel_d2f<<<grid, 256, 0, s>>>(ay, AV[dim], n);
+            ++dim;
+            TRY(dav_multidot<float, float>(S, n, dim, V.data(), AV[dim - 1], S.res, s));
+            TRY(fetch(col, S.res, dim, s));
+            for (int i = 0; i < dim; ++i) h[i + (dim - 1) * kMaxSub] = h[(dim - 1) + i * kMaxSub] = col[i];
+        }
+        jacobi_eigh(dim, h, kMaxSub, es, vs);
+        TRY(dav_combine<float, double>(n, dim, vs, V.data(), x, s));
+        TRY(dav_normalize(S, n, x, sc, s));
+        // restarts swapped subspace slots with the temporaries freed at the end of
+        // this scope (stream-ordered, after the combine): point V/AV back at the
+        // buffers that live through phase B
+        for (int j = 0; j < maxspace; ++j) { V[j] = (float *)vb[j].p; AV[j] = (float *)avb[j].p; }
+    }
+
+    // ---- phase B: FP64 residual refinement ----
     for (int outer = 0; outer < maxiter; ++outer) {
         // ---- FP64 residual of the current vector ----
         TRY(sigma(B, N, x, nullptr, ax, false, s));
@@ -258,7 +341,7 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
             if (verbose) printf("    inner %02d: residual %.4e e %.14f\n", it, rin, e_in);
             // leave for an FP64 refinement once the inner residual dropped enough or
             // stalls at the FP32 noise floor
-            if (rin < 0.05 * rnorm || rin < 0.5 * tol || (it >= 1 && rin > 0.8 * rprev) || total_inner >= maxiter)
+            if (rin < 0.05 * rnorm || rin < 0.5 * tol || (it >= 2 && rin > rprev) || total_inner >= maxiter)
                 break;
         }
         jacobi_eigh(dim, h, kMaxSub, es, vs);

@@ -94,10 +94,14 @@ struct DevNet {
     // cached structured-sigma plan for the last basis it was used with
     void *fast_state = nullptr;
     void (*fast_free)(void *) = nullptr;
+    // cached pair lists of the pair operators for the last basis they were used with
+    void *pair_state = nullptr;
+    void (*pair_free)(void *) = nullptr;
 
     int finalize();   // derived tables + upload
     ~DevNet() {
         if (fast_state && fast_free) fast_free(fast_state);
+        if (pair_state && pair_free) pair_free(pair_state);
         arena.release();
         magic = 0;
     }

@@ -65,4 +65,16 @@ int batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *thetas, 
 template <typename Ti>
 inline i64 pair_grid(const DevBasis<Ti> *B) { return (i64)B->max_na * B->num_blocks; }
 
+// Angle terms of the pair updates (core/math.hpp:132-215).
+struct PairAngles { double c0, c1, c2, c3; };
+enum PairOpKind { kPairExpm = 0, kPairGrad = 1, kPairBackgrad = 2 };
+
+// Pair operator over the precomputed pair lists (single-block bases, rank <= 4).
+// Sets *used = false (and launches nothing) when the row kernel must serve the
+// call.  grad/backgrad write at most max_slots partials before the ticket.
+template <typename Ti, int OP>
+int pair_list_launch(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, PairAngles ang, double *l, double *r,
+                     double *part, unsigned long long *ticket, i64 max_slots, double *out, bool accumulate,
+                     cudaStream_t s, bool *used);
+
 }  // namespace bsim

@@ -18,11 +18,8 @@
 
 namespace bsim {
 
-enum PairOp { kExpm = 0, kGrad = 1, kBackgrad = 2 };
-
 constexpr int kPairThreads = 256;
-
-struct PairAngles { double c0, c1, c2, c3; };
+constexpr int kExpm = kPairExpm, kGrad = kPairGrad, kBackgrad = kPairBackgrad;
 
 // Ticket counters for the last-CTA reduction live with the partials: the
 // scratch buffer holds [nslots partials][1 counter as unsigned long long].
@@ -190,6 +187,9 @@ static int launch_pair(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, Pai
             if (st != BSIM_OK) return st;
         }
     }
+    bool used = false;
+    st = pair_list_launch<Ti, OP>(B, N, gidx, ang, l, r, part, ticket, pair_grid(B), out, accumulate, s, &used);
+    if (st != BSIM_OK || used) return st;
     dim3 grid(B->max_na, B->num_blocks);
     pair_row_kernel<Ti, OP><<<grid, kPairThreads, 0, s>>>(B->view, N->view, (int)gidx, ang, l, r, part, ticket, out,
                                                          accumulate ? 1 : 0);

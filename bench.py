@@ -10,9 +10,10 @@ FP32-bulk/FP64-accumulate sigma is timed beside it.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                   [--workload sigma|davidson|vqe]
 
-N > 1 (torchrun, one rank per GPU): the destination tiles of one sigma are
-split into N contiguous row bands (strong scaling, input replicated on every
-rank, no data-path collective); the step time is the max over ranks.
+N > 1 (torchrun, one rank per GPU): one sigma is split into N beta-column
+bands (strong scaling); each rank computes its band from the whole input and
+the bands are all-gathered over NCCL, so every rank ends the step with the
+whole sigma.  The step time is the max over ranks.
 
 --impl reference times the reference's own CPU implementation
 (libotf_native built from the reference sources into oracle/_ref) on the
@@ -33,7 +34,11 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-SIGMA_CFG = dict(norb=16, na=8, nb=8, seed=0)
+SIGMA_CFGS = {
+    "16o": dict(norb=16, na=8, nb=8, seed=0),   # the sigma microbenchmark
+    "15o": dict(norb=15, na=7, nb=8, seed=0),   # a smaller case of the same kernels, for ncu captures
+}
+SIGMA_CFG = SIGMA_CFGS["16o"]
 METRIC = "sigma H*c builds per second (FP64), 16 orbitals 8a+8b"
 UNIT = "sigma/s"
 FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (non-tensor) nominal; no measured figure on this pool
@@ -93,7 +98,7 @@ def cpu_worker(args):
         print(json.dumps({"unavailable": "oracle/_ref not built"}))
         return
     ref = RefLibs()
-    cfg = SIGMA_CFG
+    cfg = SIGMA_CFGS[args.sigma_size]
     net = nw.hamiltonian_network(cfg["norb"], seed=cfg["seed"])
     pairs = pair_counts(net, cfg["norb"], cfg["na"], cfg["nb"])
     rb, dim = ref.basis(cfg["norb"], cfg["na"], cfg["nb"])
@@ -145,7 +150,7 @@ def run_cpu_baseline(args):
     env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close", OMP_PLACES="cores")
     env.pop("CUDA_VISIBLE_DEVICES", None)
     cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--cpu-seconds", str(args.cpu_seconds),
-           "--cpu-reps", str(args.cpu_reps)]
+           "--cpu-reps", str(args.cpu_reps), "--sigma-size", args.sigma_size]
     r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
     if r.returncode != 0:
         log(r.stderr[-2000:])
@@ -225,13 +230,65 @@ def peaks():
         return {}
 
 
-def profile_traffic():
-    """DRAM bytes per sigma launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "sigma_tile_kernel_16o8e.json")
+def profile_traffic(name):
+    """Figures of a committed ncu summary (profiles/<name>.json), or None."""
     try:
-        return json.load(open(p)).get("dram_bytes_per_launch")
+        return json.load(open(os.path.join(ROOT, "profiles", name + ".json")))
     except Exception:
         return None
+
+
+def sigma_roofline(net, pairs, cfg, dim, stages, hbm, fp64_peak, world, ms):
+    """Roofline of the dominant kernel of the structured sigma, from the per-stage
+    CUDA-event times measured in this run.  Returns (roofline dict, launches per sigma)."""
+    if not stages:
+        return ({"bound": "hbm", "achieved": dim * 16.0 / world / (ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                 "frac": None, "traffic": None, "note": "whole sigma (no per-stage times on this path)"}, None)
+    launches = int(sum(v[1] for v in stages.values()))
+    # stages -> kernels: both pure-spin stages launch pure_rows_kernel
+    kern = {}
+    for k, (t, n) in stages.items():
+        name = "pure_rows" if k in ("pure_alpha", "pure_beta") else k
+        t0, n0 = kern.get(name, (0.0, 0))
+        kern[name] = (t0 + t, n0 + n)
+    top = max(kern, key=lambda k: kern[k][0])
+    t_ms, n_launch = kern[top]
+    per_launch_s = t_ms * 1e-3 / max(1, n_launch)
+    nA, nB = math.comb(cfg["norb"], cfg["na"]), math.comb(cfg["norb"], cfg["nb"])
+    types = net.type_codes()
+    if top == "mixed_gemm":
+        # compulsory bytes of the GEMM stage: each source row of c~ read once, the
+        # intermediate Z[a'][j][b] (M = connected alpha singles per row) written once
+        M = cfg["na"] * (cfg["norb"] - cfg["na"])
+        bytes_total = dim * 8.0 + nA * M * nB * 8.0
+        flops_total = float(np.sum(pairs[types == 3] * (2 * net.ranks[types == 3] + 1)))
+    elif top == "pure_rows":
+        # per launch (one spin side) the compulsory HBM bytes are one read of the
+        # input (c~ or its transpose) and one write of the result; the source-row
+        # re-reads of the row AXPYs are served by L2 (see l2_bytes)
+        bytes_total = 2 * dim * 16.0
+        sel = (types == 1) | (types == 2)
+        flops_total = float(np.sum(pairs[sel] * (2 * net.ranks[sel] + 1)))
+    else:
+        bytes_total = dim * 16.0
+        flops_total = 0.0
+    achieved = bytes_total / max(1, n_launch) / per_launch_s / 1e9
+    prof = profile_traffic(f"sigma_{top}_15o7a8b")
+    traffic = None
+    if prof and prof.get("dram_bytes_per_launch") and prof.get("units_per_launch"):
+        # scale the captured launch (15 orbitals) by the determinants one launch covers here
+        units_here = dim / max(1, n_launch)
+        traffic = prof["dram_bytes_per_launch"] * units_here / prof["units_per_launch"]
+    roof = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm if hbm else None, "traffic": traffic,
+            "launches_per_sigma": n_launch, "ms_per_launch": per_launch_s * 1e3,
+            "fp64_tflops": flops_total / max(1, n_launch) / per_launch_s / 1e12,
+            "fp64_frac_of_measured_fma_peak": flops_total / max(1, n_launch) / per_launch_s / 1e12 / fp64_peak,
+            "note": "dominant kernel of the structured sigma, timed live per launch with CUDA events; achieved = "
+                    "its compulsory HBM bytes per launch / launch time, of the measured HBM copy peak; the kernel "
+                    "is bound by FP64 issue and shared-memory gathers, see fp64_frac_of_measured_fma_peak; traffic "
+                    "= ncu dram bytes of a 15-orbital launch scaled by determinants per launch"}
+    return roof, launches
 
 
 def gpu_sigma(args, rank, world, local_rank):
@@ -240,7 +297,7 @@ def gpu_sigma(args, rank, world, local_rank):
     from binsim_b200 import cuotf, network as nw
 
     torch.cuda.set_device(local_rank)
-    cfg = SIGMA_CFG
+    cfg = SIGMA_CFGS[args.sigma_size]
     t0 = time.time()
     net = nw.hamiltonian_network(cfg["norb"], seed=cfg["seed"])
     pairs = pair_counts(net, cfg["norb"], cfg["na"], cfg["nb"])
@@ -255,15 +312,19 @@ def gpu_sigma(args, rank, world, local_rank):
     xh /= np.linalg.norm(xh)
     x = torch.from_numpy(xh).cuda()
     y = torch.empty_like(x)
-    ntiles = f.num_tiles()
-    lo, hi = rank * ntiles // world, (rank + 1) * ntiles // world
     stream = torch.cuda.current_stream()
+    shard = None
+    if world > 1:
+        # beta-column bands per rank, then an NCCL all-gather of the bands: every
+        # rank ends the step holding the whole sigma (the next step's input)
+        from binsim_b200.shard import ColumnShardedSigma
+        shard = ColumnShardedSigma(f.hvec_cols, math.comb(cfg["norb"], cfg["na"]), math.comb(cfg["norb"], cfg["nb"]))
 
     def step(mixed=False):
         if world == 1:
             (f.hvec_mixed if mixed else f.hvec)(x, y)
         else:
-            f.hvec_tiles(x, y, lo, hi, mixed=mixed)
+            shard(x, y, mixed=mixed)
     path = f.sigma_path()
     log(f"[rank {rank}] sigma path {path}")
 
@@ -298,6 +359,17 @@ def gpu_sigma(args, rank, world, local_rank):
     step(True)
     err_mixed = float((y - y64).abs().max() / y64.abs().max())
 
+    # per-stage device times of one sigma (CUDA events around every launch of
+    # the structured path), FP64 and FP32 bulk; the median of 3 runs per stage
+    stages, stages32 = None, None
+    if world == 1 and path[0] == 1:
+        runs = [f.sigma_stage_times(x, y) for _ in range(3)]
+        stages = {k: (float(np.median([r[k][0] for r in runs])), runs[0][k][1]) for k in runs[0]}
+        runs = [f.sigma_stage_times(x, y, mixed=True) for _ in range(3)]
+        stages32 = {k: (float(np.median([r[k][0] for r in runs])), runs[0][k][1]) for k in runs[0]}
+    fp64_peak = cuotf.fma_peak(True)
+    fp32_peak = cuotf.fma_peak(False)
+
     # e2e through the public API with host buffers: H2D c, sigma, D2H sigma
     xpin = torch.from_numpy(xh).pin_memory()
     ypin = torch.empty(dim, dtype=torch.float64).pin_memory()
@@ -312,35 +384,41 @@ def gpu_sigma(args, rank, world, local_rank):
     if rank == 0:
         pk = peaks()
         hbm = pk.get("hbm_gbs")
-        bytes_alg = dim * 16.0 / world        # c read + sigma written per launch (rows of this rank)
-        achieved = bytes_alg / (ms * 1e-3) / 1e9
-        traffic = profile_traffic()
         tflops = flops / world / (ms * 1e-3) / 1e12
+        roof, launches = sigma_roofline(net, pairs, cfg, dim, stages, hbm, fp64_peak, world, ms)
+        if launches is None:
+            launches = count_launches(step)
         result = {
-            "metric": METRIC, "value": 1000.0 / ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC if args.sigma_size == "16o" else
+            f"sigma H*c builds per second (FP64), {cfg['norb']} orbitals {cfg['na']}a+{cfg['nb']}b",
+            "value": 1000.0 / ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "sigma microbenchmark (config 1): H*c, 16 orbitals 8a+8b, 165,636,900 dets, "
-                                   "UInt32 strings, seeded synthetic integrals (seed 0), c ~ N(0,1) normalised",
+            "config": {"workload": f"sigma microbenchmark: H*c, {cfg['norb']} orbitals {cfg['na']}a+{cfg['nb']}b, "
+                                   f"{dim:,} dets, UInt32 strings, seeded synthetic integrals (seed {cfg['seed']}), "
+                                   "c ~ N(0,1) normalised",
                        "dim": dim, "groups": int(net.ngs), "pair_updates": float(pairs.sum()),
-                       "l2": "inputs larger than L2 (c and sigma are 1.33 GB each)",
-                       "sharding": f"{world} row bands of one sigma" if world > 1 else "single GPU"},
+                       "l2": f"inputs larger than L2 (c and sigma are {dim * 8 / 1e9:.2f} GB each)",
+                       "sharding": (f"{world} beta-column bands of one sigma + NCCL all-gather of the bands "
+                                    f"({shard.exchange_bytes() / 1e9:.2f} GB received per rank per step)")
+                       if world > 1 else "single GPU"},
             "e2e": {"value": 1000.0 / ms_e2e, "unit": UNIT, "h2d_bytes_per_step": dim * 8,
                     "d2h_bytes_per_step": dim * 8, "ms_per_step": ms_e2e},
             "mixed": {"value": 1000.0 / ms_mixed, "unit": UNIT, "ms_per_step": ms_mixed,
                       "dtype": "f32 bulk, f64 accumulate", "max_rel_err_vs_fp64": err_mixed,
                       "speedup_vs_fp64": ms / ms_mixed},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": (achieved / hbm) if hbm else None, "traffic": traffic,
-                         "note": "compulsory bytes dim*(8+8) per sigma, of measured HBM copy peak; sigma is "
-                                 "bound by FP64 issue and gathers, see compute_roofline"},
-            "compute_roofline": {"bound": "fp64", "achieved": tflops, "peak": FP64_NOMINAL_TFLOPS,
-                                 "unit": "TFLOP/s", "frac": tflops / FP64_NOMINAL_TFLOPS,
-                                 "flops_per_sigma": flops, "note": "(2r+1) flops per connected pair; "
-                                                                   "peak is the nominal FP64 figure"},
+            "roofline": roof,
+            "compute_roofline": {"bound": "fp64 CUDA cores", "achieved": tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+                                 "frac": tflops / fp64_peak, "flops_per_sigma": flops,
+                                 "note": "whole sigma: (2r+1) flops per connected pair of a rank-r group; peak = "
+                                         "FP64 FMA-chain throughput measured on this GPU by bsim_fma_peak (no FP64 "
+                                         "figure in MEASURED_PEAKS.json)"},
+            "stages_ms": {k: round(v[0], 3) for k, v in stages.items()} if stages else None,
+            "stages_ms_fp32_bulk": {k: round(v[0], 3) for k, v in stages32.items()} if stages32 else None,
+            "fp32_fma_peak_tflops": fp32_peak,
             "pair_updates_per_s": float(pairs.sum()) / (ms * 1e-3),
             "sigma_path": {"path": path[0], "reason": path[1], "residual_groups": path[2]},
-            "gpu_launches": args.steps,
+            "gpu_launches": launches * args.steps if launches else None,
             "clocks": clk.summary(),
         }
     return result
@@ -693,6 +771,7 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--workload", default="sigma", choices=["sigma", "davidson", "vqe"])
     ap.add_argument("--dav-size", default="12o", choices=sorted(DAV_CFGS))
+    ap.add_argument("--sigma-size", default="16o", choices=sorted(SIGMA_CFGS))
     ap.add_argument("--dav-oracle", action="store_true")
     ap.add_argument("--vqe-sample", type=int, default=200)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

@@ -253,6 +253,28 @@ int bsim_hvec_path(void *basis, void *net, char *why, int why_len, int *residual
     return r;
 }
 
+int bsim_hvec_cols(void *basis, void *net, const double *src, double *dst, int64_t col_lo, int64_t col_hi,
+                   int mixed, bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(src); NEED(dst);
+    return bsim::sigma_fast_cols(B(basis), N(net), src, dst, mixed != 0, col_lo, col_hi, stream);
+}
+
+int bsim_hvec_stage_times(void *basis, void *net, const double *src, double *dst, int mixed, double *ms_out,
+                          int *launches_out, int nstages, bsim_stream_t stream)
+{
+    CHECK2(basis, net);
+    NEED(src); NEED(dst); NEED(ms_out); NEED(launches_out);
+    return bsim::sigma_fast_stages(B(basis), N(net), src, dst, mixed != 0, stream, ms_out, launches_out, nstages);
+}
+
+int bsim_fma_peak(int fp64, double *tflops_out, bsim_stream_t stream)
+{
+    NEED(tflops_out);
+    return bsim::fma_peak(fp64 != 0, tflops_out, stream);
+}
+
 int64_t bsim_hvec_num_tiles(void *basis) { return check(basis, nullptr) == BSIM_OK ? bsim::num_tiles(B(basis)) : -1; }
 
 int bsim_hvec_tiles(void *basis, void *net, const double *src, double *dst, int64_t tile_lo, int64_t tile_hi,

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <thread>
 #include <unordered_map>
@@ -155,17 +156,105 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     };
     add_side(0, pa);
     add_side(1, pb);
-    // per-row contribution lists (CSR), built with a few host threads
+    std::vector<int> amap((size_t)1 << norb, -1), bmap((size_t)1 << norb, -1);
+    for (int a = 0; a < nA; ++a) amap[(size_t)A[a]] = a;
+    for (int b = 0; b < nB; ++b) bmap[(size_t)Bs[b]] = b;
+    const int nth_host = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+
+    // ---- same-spin doubles through intermediate strings: extract and verify W ----
+    const int nP = norb * (norb - 1) / 2;
+    auto pair_id = [norb](int p, int q) { return p * (2 * norb - p - 1) / 2 + (q - p - 1); };
+    auto spair = [](u64 m, int p, int q) { return (popc(m & ((1ull << p) - 1)) + popc(m & ((1ull << q) - 1))) & 1; };
+    // which 2 of the 4 bits of x form pq, as a 4-bit pattern (one slot per split)
+    auto split_id = [](u64 x, u64 pq) {
+        int id = 0, k = 0;
+        for (u64 y = x; y; y &= y - 1, ++k)
+            if (pq & (y & (~y + 1))) id |= 1 << k;
+        return id;
+    };
+    std::vector<char> ri_grp[2];
+    std::vector<double> Wri[2];
+    bool ri_on[2] = {false, false};
+    for (int side = 0; side < 2; ++side) {
+        const SideHost &S = sh[side];
+        const int ng = (int)S.x.size();
+        const int nel = side == 0 ? nelA : nelB;
+        const int nU = (int)comb_count(norb - nel + 2, 2), npr = (int)comb_count(nel, 2);
+        ri_grp[side].assign(ng, 0);
+        const char *ri_env = getenv("BSIM_SIGMA_RI");   // BSIM_SIGMA_RI=0 keeps these groups in the row lists
+        if (nel < 2 || norb - nel < 2 || nU > 64 || npr > 64 || (ri_env && ri_env[0] == '0')) continue;
+        Wri[side].assign((size_t)nP * nP, 0.0);
+        const auto &rows = side == 0 ? A : Bs;
+        const std::vector<int> &rmap = side == 0 ? amap : bmap;
+        const int nrows = side == 0 ? nA : nB;
+        std::vector<int> cand;
+        for (int g = 0; g < ng; ++g)
+            if (popc(S.x[g]) == 4 && S.colmode[g] == 0) cand.push_back(g);
+        auto work = [&](int t) {
+            for (size_t ci = t; ci < cand.size(); ci += nth_host) {
+                const int g = cand[ci];
+                const u64 x = S.x[g];
+                const int R = S.rank[g], nz = S.nz[g];
+                double wv[16];
+                bool have[16] = {false};
+                bool ok = true;
+                for (int r = 0; r < nrows && ok; ++r) {
+                    const u64 d = (u64)rows[r];
+                    if (popc(d & x) != 2) continue;
+                    const u64 sv = d ^ x;
+                    if (rmap[(size_t)sv] < 0) { ok = false; break; }
+                    double pa[kSideMaxRank] = {0, 0, 0, 0};
+                    for (int q = 0; q < nz; ++q) {
+                        const bool odd = popc(sv & S.zmask[S.z_off[g] + q]) & 1;
+                        for (int rr = 0; rr < R; ++rr) {
+                            const double v = S.wv[S.w_off[g] + (i64)rr * nz + q];
+                            pa[rr] += odd ? -v : v;
+                        }
+                    }
+                    double coef = 0.0;
+                    for (int rr = 0; rr < R; ++rr) coef += pa[rr] * S.cconst[(size_t)g * kSideMaxRank + rr];
+                    const u64 pq = d & x, rs = sv & x, m = d & ~x;
+                    const int p = __builtin_ctzll(pq), q2 = 63 - __builtin_clzll(pq);
+                    const int r1 = __builtin_ctzll(rs), s1 = 63 - __builtin_clzll(rs);
+                    const double w = ((spair(m, p, q2) ^ spair(m, r1, s1)) ? -coef : coef);
+                    const int id = split_id(x, pq);
+                    if (!have[id]) { have[id] = true; wv[id] = w; }
+                    else if (std::fabs(w - wv[id]) > 1e-12 * std::max(1.0, std::fabs(wv[id]))) ok = false;
+                }
+                if (!ok) continue;
+                // record W for every split seen (each split maps to its own (pq, rs) entry)
+                for (int r = 0; r < nrows; ++r) {
+                    const u64 d = (u64)rows[r];
+                    if (popc(d & x) != 2) continue;
+                    const u64 pq = d & x, rs = (d ^ x) & x;
+                    const int id = split_id(x, pq);
+                    const int p = __builtin_ctzll(pq), q2 = 63 - __builtin_clzll(pq);
+                    const int r1 = __builtin_ctzll(rs), s1 = 63 - __builtin_clzll(rs);
+                    Wri[side][(size_t)pair_id(p, q2) * nP + pair_id(r1, s1)] = wv[id];
+                }
+                ri_grp[side][g] = 1;
+            }
+        };
+        std::vector<std::thread> th;
+        for (int t = 1; t < nth_host; ++t) th.emplace_back(work, t);
+        work(0);
+        for (auto &t : th) t.join();
+        for (int g = 0; g < ng; ++g) ri_on[side] = ri_on[side] || ri_grp[side][g];
+    }
+
+    // per-row contribution lists (CSR), built with a few host threads: alpha
+    // (without the intermediate-string groups when that side uses them), beta
+    // with every group (column bands), beta without them (whole sigma)
     struct CSRHost {
         std::vector<i64> cptr, tptr;
         std::vector<CEnt> cent;
         std::vector<TEnt> tent;
-    } csr[2];
+    } csr[3];
     {
-        std::vector<int> amap((size_t)1 << norb, -1), bmap((size_t)1 << norb, -1);
-        for (int a = 0; a < nA; ++a) amap[(size_t)A[a]] = a;
-        for (int b = 0; b < nB; ++b) bmap[(size_t)Bs[b]] = b;
-        for (int side = 0; side < 2; ++side) {
+        for (int li = 0; li < 3; ++li) {
+            const int side = li == 0 ? 0 : 1;
+            const bool skip_ri = li == 0 ? ri_on[0] : (li == 2);
+            if (li == 2 && !ri_on[1]) continue;
             const SideHost &S = sh[side];
             const auto &rows = side == 0 ? A : Bs;
             const std::vector<int> &rmap = side == 0 ? amap : bmap;
@@ -186,6 +275,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
                     const u64 s0 = (u64)rows[r];
                     i64 cc = 0, tc = 0;
                     for (int g = 0; g < ng; ++g) {
+                        if (skip_ri && ri_grp[side][g]) continue;
                         const u64 x = S.x[g];
                         if (2 * popc(s0 & x) != popc(x)) continue;
                         const u64 sv = s0 ^ x;
@@ -221,7 +311,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
             for (int t = 1; t < nth; ++t) th.emplace_back(work, t);
             work(0);
             for (auto &x : th) x.join();
-            CSRHost &C = csr[side];
+            CSRHost &C = csr[li];
             C.cptr.assign(1, 0);
             C.tptr.assign(1, 0);
             for (auto &pt : parts) {
@@ -332,14 +422,85 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
             }
     }
 
+    // ---- intermediate-string tables ----------------------------------------------
+    struct RIHost {
+        int nM = 0, nU = 0, npr = 0;
+        std::vector<int> src, pid;
+        std::vector<int2> gath;
+        std::vector<float> W32;
+    } rih[2];
+    for (int side = 0; side < 2; ++side) {
+        if (!ri_on[side]) continue;
+        RIHost &H = rih[side];
+        const int nel = side == 0 ? nelA : nelB;
+        const auto &rows = side == 0 ? A : Bs;
+        const std::vector<int> &rmap = side == 0 ? amap : bmap;
+        const int nrows = side == 0 ? nA : nB;
+        H.nU = (int)comb_count(norb - nel + 2, 2);
+        H.npr = (int)comb_count(nel, 2);
+        // intermediates in colex order (Gosper), as the string lists
+        std::vector<u64> Ms;
+        std::unordered_map<u64, int> midx;
+        const int k = nel - 2;
+        if (k == 0) Ms.push_back(0);
+        else
+            for (u64 v = (1ull << k) - 1; v < (1ull << norb);) {
+                Ms.push_back(v);
+                const u64 t = v | (v - 1);
+                v = (t + 1) | (((~t & (t + 1)) - 1) >> (__builtin_ctzll(v) + 1));
+            }
+        H.nM = (int)Ms.size();
+        midx.reserve(Ms.size() * 2);
+        for (int i = 0; i < H.nM; ++i) midx[Ms[i]] = i;
+        H.src.assign((size_t)H.nM * H.nU, -1);
+        H.pid.assign((size_t)H.nM * H.nU, 0);
+        const u64 full = norb == 64 ? ~0ull : ((1ull << norb) - 1);
+        for (int i = 0; i < H.nM; ++i) {
+            const u64 m = Ms[i], comp = full & ~m;
+            int slot = 0;
+            for (u64 yp = comp; yp; yp &= yp - 1) {
+                const int p = __builtin_ctzll(yp);
+                for (u64 yq = yp & (yp - 1); yq; yq &= yq - 1) {
+                    const int q = __builtin_ctzll(yq);
+                    const int row = rmap[(size_t)(m | (1ull << p) | (1ull << q))];
+                    H.src[(size_t)i * H.nU + slot] = (row << 1) | spair(m, p, q);
+                    H.pid[(size_t)i * H.nU + slot] = pair_id(p, q);
+                    ++slot;
+                }
+            }
+        }
+        H.gath.assign((size_t)nrows * H.npr, make_int2(0, 0));
+        for (int r = 0; r < nrows; ++r) {
+            const u64 a = (u64)rows[r];
+            int e = 0;
+            for (u64 yp = a; yp; yp &= yp - 1) {
+                const int p = __builtin_ctzll(yp);
+                for (u64 yq = yp & (yp - 1); yq; yq &= yq - 1) {
+                    const int q = __builtin_ctzll(yq);
+                    const u64 m = a & ~((1ull << p) | (1ull << q));
+                    const u64 comp = full & ~m;
+                    const int pp = popc(comp & ((1ull << p) - 1)), qq = popc(comp & ((1ull << q) - 1));
+                    const int nc = popc(comp);
+                    const int slot = pp * (2 * nc - pp - 1) / 2 + (qq - pp - 1);
+                    H.gath[(size_t)r * H.npr + e] = make_int2(midx[m] * H.nU + slot, spair(m, p, q));
+                    ++e;
+                }
+            }
+        }
+        H.W32.assign(Wri[side].begin(), Wri[side].end());
+    }
+
     // ---- upload -------------------------------------------------------------------
     auto bytes = [](size_t n, size_t sz) { return ((std::max<size_t>(n, 1) * sz) + 255) & ~size_t(255); };
     size_t tot = bytes(nA, sizeof(Ti)) + bytes(nB, sizeof(Ti)) + bytes(nA, 8) + bytes(PAd.size(), 8) +
                  bytes(PBd.size(), 8) + 2 * bytes(P->nE, 8) + 2 * bytes(P->Lam.size(), 8) + bytes(gidx.size(), 4) +
                  bytes(P->residual.size(), 4) + bytes(P->residual.size() + 1, 16);
+    for (int li = 0; li < 3; ++li)
+        tot += 2 * bytes(csr[li].cptr.size(), 8) + bytes(csr[li].cent.size(), sizeof(CEnt)) +
+               bytes(csr[li].tent.size(), sizeof(TEnt)) + bytes(sh[li == 0 ? 0 : 1].ctab.size(), 8);
     for (int side = 0; side < 2; ++side)
-        tot += 2 * bytes(csr[side].cptr.size(), 8) + bytes(csr[side].cent.size(), sizeof(CEnt)) +
-               bytes(csr[side].tent.size(), sizeof(TEnt)) + bytes(sh[side].ctab.size(), 8);
+        tot += 2 * bytes(rih[side].src.size(), 4) + bytes(rih[side].gath.size(), 8) + bytes(Wri[side].size(), 8) +
+               bytes(rih[side].W32.size(), 4);
     int st = P->arena.reserve(tot);
     if (st != BSIM_OK) return st;
     auto put = [&](const auto &v) {
@@ -359,14 +520,31 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     std::vector<float> lam32(P->Lam.begin(), P->Lam.end());
     P->d_Lam32 = put(lam32);
     P->d_gidx = put(gidx);
-    for (int side = 0; side < 2; ++side) {
-        CSRHost &C = csr[side];
-        SideCSR &D = side == 0 ? P->csrA : P->csrB;
+    for (int li = 0; li < 3; ++li) {
+        CSRHost &C = csr[li];
+        if (li == 2 && !ri_on[1]) continue;
+        SideCSR &D = li == 0 ? P->csrA : li == 1 ? P->csrB : P->csrBri;
         D.cptr = put(C.cptr);
         D.cent = put(C.cent);
         D.tptr = put(C.tptr);
         D.tent = put(C.tent);
-        D.ctab = put(sh[side].ctab);
+        D.ctab = put(sh[li == 0 ? 0 : 1].ctab);
+    }
+    for (int side = 0; side < 2; ++side) {
+        RISide &R = side == 0 ? P->riA : P->riB;
+        R = RISide{};
+        if (!ri_on[side]) continue;
+        const RIHost &H = rih[side];
+        R.on = 1;
+        R.nM = H.nM;
+        R.nU = H.nU;
+        R.npr = H.npr;
+        R.nP = nP;
+        R.src = put(H.src);
+        R.pid = put(H.pid);
+        R.gath = put(H.gath);
+        R.W = put(Wri[side]);
+        R.W32 = put(H.W32);
     }
     // residual groups through the generic tile kernel (chunks as in DevNet::finalize)
     std::vector<int> res = P->residual;

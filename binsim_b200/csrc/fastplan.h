@@ -51,6 +51,28 @@ struct SideCSR {
     const double *ctab;   // column-factor tables, rows padded to ld_in
 };
 
+// Same-spin double excitations through (n-2)-electron intermediate strings m
+// (resolution of the identity on one spin):
+//   sigma~[a, b] += sum_{pq in a} s(m, pq) sum_{rs not in m} W[pq][rs] s(m, rs) c~[m + rs, b],
+//   m = a - pq,  s(m, pq) = <m + pq| a+_p a+_q |m> = (-1)^(#m below p + #m below q).
+// Per m the inner sum is a dense (nU x nU) x (nU x columns) product over the nU
+// pairs outside m; the outer sum gathers C(n, 2) rows of its result per string.
+// W is extracted from the 4-orbital pure groups and verified on every connected
+// string pair when the plan is built; a group that does not factor this way
+// stays in the row lists.
+struct RISide {
+    int on = 0;           // the side uses the intermediate-string product
+    int nM = 0;           // intermediate strings, C(norb, n - 2)
+    int nU = 0;           // pairs outside an intermediate, C(norb - n + 2, 2)
+    int npr = 0;          // pairs inside a string, C(n, 2)
+    int nP = 0;           // all pairs, C(norb, 2)
+    const int *src = nullptr;     // [nM x nU]: (row of m + pair) << 1 | sign
+    const int *pid = nullptr;     // [nM x nU]: pair index of each slot
+    const int2 *gath = nullptr;   // [nrows x npr]: {m * nU + slot, sign}
+    const double *W = nullptr;    // [nP x nP]
+    const float *W32 = nullptr;
+};
+
 template <typename Ti>
 struct FastPlan {
     bool ok = false;
@@ -80,6 +102,8 @@ struct FastPlan {
     const u64 *d_Ka = nullptr;
     const double *d_PAd = nullptr;     // [nA x rank_d] alpha diagonal factors
     SideCSR csrA{}, csrB{};
+    SideCSR csrBri{};                  // beta rows without the intermediate-string groups
+    RISide riA{}, riB{};
     i64 nnzA = 0, nnzB = 0;
     const u64 *d_Emask = nullptr, *d_mA = nullptr;
     const double *d_Lam = nullptr;
@@ -93,6 +117,12 @@ struct FastPlan {
 };
 
 constexpr int kMixCols = 128;                             // columns per GEMM chunk
+
+// Shared memory of the intermediate-string GEMM: W_m [nU x 64] and an X slice.
+inline size_t ri_smem_bytes(int nU, size_t elem)
+{
+    return (size_t)nU * 64 * elem + 32 * (size_t)kMixCols * elem + 64 * 8;
+}
 
 // Shared memory of the mixed GEMM kernel: source row, Lam_conn [K x 64], an
 // X slice [32 x kMixCols] and the connected-excitation lists.

@@ -26,6 +26,22 @@ template <typename Ti>
 int sigma_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32, double *dst,
                bool mixed, cudaStream_t s, bool *used);
 // 1: structured path (FP64 and FP32), 2: structured for FP32 only, 0: generic.
+// Columns [col_lo, col_hi) of sigma through the structured path (col_lo a
+// multiple of 128): the unit of work of one rank when sigma is split by beta
+// columns.  Every other element of dst is left untouched.
+template <typename Ti>
+int sigma_fast_cols(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, double *dst, bool mixed,
+                    i64 col_lo, i64 col_hi, cudaStream_t s);
+
+// One structured sigma with CUDA events around every launch: per-stage device
+// milliseconds and launch counts (stages as in sigma_fast.cu's StageTimer).
+template <typename Ti>
+int sigma_fast_stages(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, double *dst, bool mixed,
+                      cudaStream_t s, double *ms, int *launches, int nstages);
+
+// Arithmetic peak of the CUDA cores (FMA chains), TFLOP/s, FP64 or FP32.
+int fma_peak(bool fp64, double *tflops, cudaStream_t s);
+
 template <typename Ti>
 int fast_sigma_info(const DevBasis<Ti> *B, const DevNet<Ti> *N, std::string *why, int *nresid);
 template <typename Ti>

@@ -71,16 +71,18 @@ __global__ void frame_transpose_kernel(int nA, int nB, int ldA, int ldB, const T
 }
 
 // ---- 2/3. pure groups of one spin: row AXPY over the precomputed row lists -----------
-// One CTA per (row, 1024-column chunk); each thread owns 4 consecutive columns.
+// One CTA per (row, 1024-column chunk) of rows row_begin.. and columns
+// [col_begin, ncols); each thread owns 4 consecutive columns.
 // Constant-factor entries accumulate in T over batches of 64 entries, then in
 // FP64; table entries and the diagonal are FP64 throughout.
 template <typename T>
 __global__ void __launch_bounds__(256)
-pure_rows_kernel(int ncols, int ld_in, const SideCSR L, const T *__restrict__ in, double *__restrict__ out,
-                 int ld_out, const double *__restrict__ PAd, const double *__restrict__ PBdT, int rank_d)
+pure_rows_kernel(int row_begin, int col_begin, int ncols, int ld_in, const SideCSR L, const T *__restrict__ in,
+                 double *__restrict__ out, int ld_out, const double *__restrict__ PAd, const double *__restrict__ PBdT,
+                 int rank_d)
 {
-    const int row = blockIdx.x;
-    const int c = blockIdx.y * kRowChunk + 4 * threadIdx.x;
+    const int row = row_begin + blockIdx.x;
+    const int c = col_begin + blockIdx.y * kRowChunk + 4 * threadIdx.x;
     if (c >= ncols) return;
     const T *in_c = in + c;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -152,6 +154,7 @@ pure_rows_kernel(int ncols, int ld_in, const SideCSR L, const T *__restrict__ in
 // ---- 4a. mixed GEMM -----------------------------------------------------------------
 struct MixedArgs {
     int nA, nB, nE, nF, M, ldA, ldG;
+    int cend;               // end of the column range being computed (nB for a whole sigma)
     const u64 *Emask, *mA;
     const void *Lam;        // T [nE x nF]
     const int *gidx;        // [nF x ldG]: (rank(b^F) << 1 | sign) or -1
@@ -202,6 +205,65 @@ __device__ __forceinline__ void load_lam(const float *p, float l[EPT])
     l[4] = q1.x; l[5] = q1.y; l[6] = q1.z; l[7] = q1.w;
 }
 
+// Register tile of the two GEMMs: EPT output rows x the lane's 4 columns
+// {2l, 2l+1, 64+2l, 64+2l+1}.  The FP32 tile keeps its accumulators as f32x2
+// pairs and issues Blackwell's packed fma.rn.f32x2 (two IEEE single-precision
+// FMAs per instruction, each rounded as a scalar fmaf), halving the FMA issue
+// slots of the FP32-bulk GEMMs.
+template <typename T, int EPT>
+struct GemmTile {
+    T v[EPT][4];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) v[i][0] = v[i][1] = v[i][2] = v[i][3] = T(0);
+    }
+    __device__ __forceinline__ void step(const T *l, const T *xa, const T *xb)
+    {
+        const typename Vec2<T>::type a = *reinterpret_cast<const typename Vec2<T>::type *>(xa);
+        const typename Vec2<T>::type b = *reinterpret_cast<const typename Vec2<T>::type *>(xb);
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            v[i][0] += l[i] * a.x;
+            v[i][1] += l[i] * a.y;
+            v[i][2] += l[i] * b.x;
+            v[i][3] += l[i] * b.y;
+        }
+    }
+    __device__ __forceinline__ void pair(int i, typename Vec2<T>::type &p0, typename Vec2<T>::type &p1) const
+    {
+        p0.x = v[i][0]; p0.y = v[i][1];
+        p1.x = v[i][2]; p1.y = v[i][3];
+    }
+};
+
+template <int EPT>
+struct GemmTile<float, EPT> {
+    unsigned long long p[EPT][2];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) p[i][0] = p[i][1] = 0ull;   // +0.0f in both halves
+    }
+    __device__ __forceinline__ void step(const float *l, const float *xa, const float *xb)
+    {
+        const unsigned long long a = *reinterpret_cast<const unsigned long long *>(xa);
+        const unsigned long long b = *reinterpret_cast<const unsigned long long *>(xb);
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            unsigned long long ll;
+            asm("mov.b64 %0, {%1, %1};" : "=l"(ll) : "f"(l[i]));
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(p[i][0]) : "l"(ll), "l"(a));
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(p[i][1]) : "l"(ll), "l"(b));
+        }
+    }
+    __device__ __forceinline__ void pair(int i, float2 &p0, float2 &p1) const
+    {
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(p0.x), "=f"(p0.y) : "l"(p[i][0]));
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(p1.x), "=f"(p1.y) : "l"(p[i][1]));
+    }
+};
+
 // One CTA per source row a'.  Warp w owns excitations w*EPT .. w*EPT+EPT-1 of
 // the row's connected list; lane l owns columns {2l, 2l+1, 64+2l, 64+2l+1} of a
 // kMixCols-column chunk (conflict-free 2-element shared loads).  The X slice for
@@ -238,7 +300,7 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
         const int f = i >> 6, j = i & 63;
         lam[i] = j < m ? (T)sgn[j] * Lam[(i64)conn[j] * K + f] : T(0);
     }
-    const int zend = min(P.nB, z0 + W);
+    const int zend = min(P.cend, z0 + W);
     const int ncb = (zend - z0 + kMixCols - 1) / kMixCols;
     const int nfc = (K + 31) / 32;
     const int nsteps = ncb * nfc;
@@ -253,9 +315,8 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
             gpre[it] = f0 + f < K ? __ldg(P.gidx + (i64)(f0 + f) * P.ldG + cb + cl) : -1;
         }
     };
-    T acc[EPT][4];
-#pragma unroll
-    for (int i = 0; i < EPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = T(0);
+    GemmTile<T, EPT> acc;
+    acc.zero();
     if (nsteps > 0) load_g(0);
     for (int step = 0; step < nsteps; ++step) {
         const int cbi = step / nfc, fci = step % nfc;
@@ -278,15 +339,7 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
             for (int f = 0; f < nf; ++f) {
                 T l[EPT];
                 load_lam<EPT>(lam + (size_t)(f0 + f) * 64 + wid * EPT, l);
-                const V2 xa = *reinterpret_cast<const V2 *>(xs + f * kMixCols + 2 * lane);
-                const V2 xb = *reinterpret_cast<const V2 *>(xs + f * kMixCols + 64 + 2 * lane);
-#pragma unroll
-                for (int i = 0; i < EPT; ++i) {
-                    acc[i][0] += l[i] * xa.x;
-                    acc[i][1] += l[i] * xa.y;
-                    acc[i][2] += l[i] * xb.x;
-                    acc[i][3] += l[i] * xb.y;
-                }
+                acc.step(l, xs + f * kMixCols + 2 * lane, xs + f * kMixCols + 64 + 2 * lane);
             }
         }
         if (fci == nfc - 1) {
@@ -297,15 +350,13 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
                     if (j < m) {
                         T *zr = Z + ((i64)a * M + j) * W + cbi * kMixCols;
                         V2 v0, v1;
-                        v0.x = acc[i][0]; v0.y = acc[i][1];
-                        v1.x = acc[i][2]; v1.y = acc[i][3];
+                        acc.pair(i, v0, v1);
                         *reinterpret_cast<V2 *>(zr + 2 * lane) = v0;
                         *reinterpret_cast<V2 *>(zr + 64 + 2 * lane) = v1;
                     }
                 }
             }
-#pragma unroll
-            for (int i = 0; i < EPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = T(0);
+            acc.zero();
         }
     }
 }
@@ -347,7 +398,7 @@ mixed_gather_kernel(const MixedArgs P, const Ti *__restrict__ astr, const int *_
         __syncthreads();
     }
     const int n = min(cnt, 64);
-    const int zend = min(P.nB, z0 + W);
+    const int zend = min(P.cend, z0 + W);
     for (int b = z0 + blockIdx.y * kRowChunk + threadIdx.x; b < min(zend, z0 + (blockIdx.y + 1) * kRowChunk);
          b += blockDim.x) {
         T part = T(0);
@@ -356,22 +407,148 @@ mixed_gather_kernel(const MixedArgs P, const Ti *__restrict__ astr, const int *_
     }
 }
 
+// ---- 2b/3b. same-spin doubles through intermediate strings ----------------------------
+struct RIArgs {
+    int nM, nU, npr, nP, ld_in, cend;
+    const int *src, *pid;
+    const void *W;          // T [nP x nP]
+};
+
+// One CTA per intermediate m: X[k][col] = s(m, pair_k) c~[m + pair_k][col] for the
+// nU pairs outside m (coalesced row segments, the next slice prefetched into
+// registers), Z[m][j][col] = sum_k W[pair_j][pair_k] X[k][col].  Same tiling as
+// the mixed GEMM: warp w owns output rows w*EPT.., lane l owns columns
+// {2l, 2l+1, 64+2l, 64+2l+1} of a kMixCols chunk.
+template <typename T, int EPT>
+__global__ void __launch_bounds__((64 / EPT) * 32, EPT == 8 ? 2 : 1)
+ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int z0, int W)
+{
+    constexpr int NT = (64 / EPT) * 32;
+    constexpr int ITEMS = 32 * kMixCols / NT;
+    using V2 = typename Vec2<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int K = P.nU;
+    T *wm = reinterpret_cast<T *>(smem_raw);                          // [K][64]
+    T *xs = wm + (size_t)K * 64;                                       // [32][kMixCols]
+    long long *soff = reinterpret_cast<long long *>(xs + 32 * kMixCols);   // [64]
+    const int m = blockIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int *srcm = P.src + (i64)m * K, *pidm = P.pid + (i64)m * K;
+    for (int i = threadIdx.x; i < 64; i += NT) {
+        long long o = 0;
+        if (i < K) {
+            const int v = srcm[i];
+            o = ((long long)(v >> 1) * P.ld_in) * 2 + (v & 1);   // row offset, sign in the low bit
+        }
+        soff[i] = o;
+    }
+    const T *Wt = static_cast<const T *>(P.W);
+    for (int i = threadIdx.x; i < K * 64; i += NT) {
+        const int k = i >> 6, j = i & 63;
+        wm[i] = j < K ? Wt[(i64)pidm[j] * P.nP + pidm[k]] : T(0);
+    }
+    __syncthreads();
+    const int zend = min(P.cend, z0 + W);
+    const int ncb = (zend - z0 + kMixCols - 1) / kMixCols;
+    const int nfc = (K + 31) / 32;
+    const int nsteps = ncb * nfc;
+    const bool active = wid * EPT < K;
+    T gpre[ITEMS];
+    auto load_x = [&](int step) {
+        const int cb = z0 + (step / nfc) * kMixCols, f0 = (step % nfc) * 32;
+#pragma unroll
+        for (int it = 0; it < ITEMS; ++it) {
+            const int i = threadIdx.x + it * NT;
+            const int k = f0 + i / kMixCols, col = cb + i % kMixCols;
+            T v = T(0);
+            if (k < K && col < zend) {
+                const long long o = soff[k];
+                v = __ldg(in + (o >> 1) + col);
+                if (o & 1) v = -v;
+            }
+            gpre[it] = v;
+        }
+    };
+    GemmTile<T, EPT> acc;
+    acc.zero();
+    if (nsteps > 0) load_x(0);
+    for (int step = 0; step < nsteps; ++step) {
+        const int cbi = step / nfc, fci = step % nfc;
+        const int f0 = fci * 32, nf = min(32, K - f0);
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < ITEMS; ++it) xs[threadIdx.x + it * NT] = gpre[it];
+        __syncthreads();
+        if (step + 1 < nsteps) load_x(step + 1);
+        if (active) {
+#pragma unroll 4
+            for (int f = 0; f < nf; ++f) {
+                T l[EPT];
+                load_lam<EPT>(wm + (size_t)(f0 + f) * 64 + wid * EPT, l);
+                acc.step(l, xs + f * kMixCols + 2 * lane, xs + f * kMixCols + 64 + 2 * lane);
+            }
+        }
+        if (fci == nfc - 1) {
+            if (active) {
+#pragma unroll
+                for (int i = 0; i < EPT; ++i) {
+                    const int j = wid * EPT + i;
+                    if (j < K) {
+                        T *zr = Z + ((i64)m * K + j) * W + cbi * kMixCols;
+                        V2 v0, v1;
+                        acc.pair(i, v0, v1);
+                        *reinterpret_cast<V2 *>(zr + 2 * lane) = v0;
+                        *reinterpret_cast<V2 *>(zr + 64 + 2 * lane) = v1;
+                    }
+                }
+            }
+            acc.zero();
+        }
+    }
+}
+
+// out[row][b] += sum over the pairs pq in the row's string of s(m, pq) Z[m][slot(pq)][b]
+template <typename T>
+__global__ void __launch_bounds__(256)
+ri_gather_kernel(const RIArgs P, const int2 *__restrict__ gath, const T *__restrict__ Z, double *__restrict__ out,
+                 int ld_out, int z0, int W)
+{
+    __shared__ long long eoff[64];
+    const int row = blockIdx.x;
+    for (int e = threadIdx.x; e < P.npr; e += blockDim.x) {
+        const int2 g = gath[(i64)row * P.npr + e];
+        eoff[e] = (long long)g.x * W * 2 + (g.y & 1);
+    }
+    __syncthreads();
+    const int zend = min(P.cend, z0 + W);
+    for (int b = z0 + blockIdx.y * kRowChunk + threadIdx.x; b < min(zend, z0 + (blockIdx.y + 1) * kRowChunk);
+         b += blockDim.x) {
+        T part = T(0);
+        for (int e = 0; e < P.npr; ++e) {
+            const long long o = eoff[e];
+            const T v = __ldg(Z + (o >> 1) + (b - z0));
+            part += (o & 1) ? -v : v;
+        }
+        out[(i64)row * ld_out + b] += (double)part;
+    }
+}
+
 // ---- 5. final: sigma = eps * (s~ + t^T) ---------------------------------------------
 template <typename Ti>
-__global__ void final_kernel(int nA, int nB, int ldB, const Ti *__restrict__ bstr, const u64 *__restrict__ Ka,
-                             const double *__restrict__ tT, double *__restrict__ sig)
+__global__ void final_kernel(int nA, int nB, int ldB, int col_begin, int col_end, const Ti *__restrict__ bstr,
+                             const u64 *__restrict__ Ka, const double *__restrict__ tT, double *__restrict__ sig)
 {
     __shared__ double tile[32][33];
-    const int b0 = blockIdx.x * 32, a0 = blockIdx.y * 32;
+    const int b0 = col_begin + blockIdx.x * 32, a0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int i = ty; i < 32; i += blockDim.y) {   // t^T tile: rows b, cols a
         const int b = b0 + i, a = a0 + tx;
-        tile[i][tx] = (a < nA && b < nB) ? tT[(i64)b * ldB + a] : 0.0;
+        tile[i][tx] = (a < nA && b < col_end) ? tT[(i64)b * ldB + a] : 0.0;
     }
     __syncthreads();
     for (int i = ty; i < 32; i += blockDim.y) {
         const int a = a0 + i, b = b0 + tx;
-        if (a < nA && b < nB) {
+        if (a < nA && b < col_end) {
             const i64 idx = (i64)a * nB + b;
             double v = sig[idx] + tile[tx][i];
             if (par((u64)bstr[b] & Ka[a])) v = -v;
@@ -443,35 +620,106 @@ bool fast_sigma_available(const DevBasis<Ti> *B, const DevNet<Ti> *N)
     return st->plan.ok;
 }
 
+// Optional per-stage CUDA-event timing of one structured sigma (measurement
+// entry point bsim_hvec_stage_times); stages: 0 frame+transpose, 1 pure alpha,
+// 2 pure beta, 3 mixed GEMM, 4 mixed gather, 5 final combine, 6 residual groups,
+// 7 intermediate-string GEMM, 8 intermediate-string gather.
+struct StageTimer {
+    struct Mark { cudaEvent_t e0, e1; int stage; };
+    std::vector<Mark> marks;
+    int begin(int stage, cudaStream_t s)
+    {
+        Mark m{nullptr, nullptr, stage};
+        BSIM_CUDA(cudaEventCreate(&m.e0));
+        BSIM_CUDA(cudaEventCreate(&m.e1));
+        BSIM_CUDA(cudaEventRecord(m.e0, s));
+        marks.push_back(m);
+        return BSIM_OK;
+    }
+    int end(cudaStream_t s)
+    {
+        BSIM_CUDA(cudaEventRecord(marks.back().e1, s));
+        return BSIM_OK;
+    }
+    int collect(double *ms, int *launches, int n)
+    {
+        for (int i = 0; i < n; ++i) { ms[i] = 0.0; launches[i] = 0; }
+        for (auto &m : marks) {
+            float t = 0.f;
+            BSIM_CUDA(cudaEventSynchronize(m.e1));
+            BSIM_CUDA(cudaEventElapsedTime(&t, m.e0, m.e1));
+            if (m.stage < n) { ms[m.stage] += t; launches[m.stage] += 1; }
+        }
+        return BSIM_OK;
+    }
+    ~StageTimer()
+    {
+        for (auto &m : marks) { cudaEventDestroy(m.e0); cudaEventDestroy(m.e1); }
+    }
+};
+
+#define STAGE(tm, id, s, ...)                                   \
+    do {                                                        \
+        if (tm) { int rc__ = (tm)->begin(id, s); if (rc__) return rc__; } \
+        __VA_ARGS__;                                            \
+        if (tm) { int rc__ = (tm)->end(s); if (rc__) return rc__; } \
+    } while (0)
+
 template <typename Ti, typename T, int EPT>
 static int launch_mixed(const DevBasis<Ti> *B, FastPlan<Ti> &P, FastScratch<Ti> &S, const T *ct, double *dst,
-                        cudaStream_t s)
+                        int c0, int c1, cudaStream_t s, StageTimer *tm)
 {
     constexpr int NT = (64 / EPT) * 32;
     const int nA = P.nA, nB = P.nB;
     const size_t per_col = (size_t)nA * P.M * sizeof(T);
     size_t Wz = std::max<size_t>(kMixCols, (scratch_budget() / per_col) / kMixCols * kMixCols);
-    Wz = std::min<size_t>(Wz, ((size_t)nB + kMixCols - 1) / kMixCols * kMixCols);
+    Wz = std::min<size_t>(Wz, ((size_t)(c1 - c0) + kMixCols - 1) / kMixCols * kMixCols);
     int rc;
     if ((rc = ensure(&S.Z, &S.z_n, per_col * Wz)) != BSIM_OK) return rc;
-    MixedArgs ma{nA, nB, P.nE, P.nF, P.M, P.ldA, P.ldG, P.d_Emask, P.d_mA,
+    MixedArgs ma{nA, nB, P.nE, P.nF, P.M, P.ldA, P.ldG, c1, P.d_Emask, P.d_mA,
                  sizeof(T) == 8 ? (const void *)P.d_Lam : (const void *)P.d_Lam32, P.d_gidx};
     const size_t smem = mixed_smem_bytes(nB, P.nF, sizeof(T));
     if (smem > 227 * 1024) { set_error("mixed kernel needs %zu bytes of shared memory", smem); return BSIM_ERR_UNSUPPORTED; }
     BSIM_CUDA(cudaFuncSetAttribute(mixed_gemm_kernel<Ti, T, EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
     T *Z = static_cast<T *>(S.Z);
-    for (int z0 = 0; z0 < nB; z0 += (int)Wz) {
-        mixed_gemm_kernel<Ti, T, EPT><<<nA, NT, smem, s>>>(ma, P.d_astr, ct, Z, z0, (int)Wz);
-        dim3 g(nA, (unsigned)((std::min<size_t>(Wz, nB - z0) + kRowChunk - 1) / kRowChunk));
-        mixed_gather_kernel<Ti, T><<<g, 256, 0, s>>>(ma, P.d_astr, B->view.amap, Z, dst, z0, (int)Wz);
+    for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
+        STAGE(tm, 3, s, (mixed_gemm_kernel<Ti, T, EPT><<<nA, NT, smem, s>>>(ma, P.d_astr, ct, Z, z0, (int)Wz)));
+        dim3 g(nA, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
+        STAGE(tm, 4, s, (mixed_gather_kernel<Ti, T><<<g, 256, 0, s>>>(ma, P.d_astr, B->view.amap, Z, dst, z0, (int)Wz)));
+    }
+    return BSIM_OK;
+}
+
+// Same-spin doubles of one side through the intermediate strings, columns [c0, c1)
+// of the side's rows (all rows), accumulated into out.
+template <typename T, int EPT>
+static int launch_ri(const RISide &R, const T *in, int ld_in, double *out, int ld_out, int nrows, int c0, int c1,
+                     void **zbuf, size_t *zhave, cudaStream_t s, StageTimer *tm)
+{
+    constexpr int NT = (64 / EPT) * 32;
+    if (c1 <= c0) return BSIM_OK;
+    const size_t per_col = (size_t)R.nM * R.nU * sizeof(T);
+    size_t Wz = std::max<size_t>(kMixCols, (scratch_budget() / per_col) / kMixCols * kMixCols);
+    Wz = std::min<size_t>(Wz, ((size_t)(c1 - c0) + kMixCols - 1) / kMixCols * kMixCols);
+    int rc;
+    if ((rc = ensure(zbuf, zhave, per_col * Wz)) != BSIM_OK) return rc;
+    RIArgs ra{R.nM, R.nU, R.npr, R.nP, ld_in, c1, R.src, R.pid,
+              sizeof(T) == 8 ? (const void *)R.W : (const void *)R.W32};
+    const size_t smem = ri_smem_bytes(R.nU, sizeof(T));
+    BSIM_CUDA(cudaFuncSetAttribute(ri_gemm_kernel<T, EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    T *Z = static_cast<T *>(*zbuf);
+    for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
+        STAGE(tm, 7, s, (ri_gemm_kernel<T, EPT><<<R.nM, NT, smem, s>>>(ra, in, Z, z0, (int)Wz)));
+        dim3 g(nrows, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
+        STAGE(tm, 8, s, (ri_gather_kernel<T><<<g, 256, 0, s>>>(ra, R.gath, Z, out, ld_out, z0, (int)Wz)));
     }
     return BSIM_OK;
 }
 
 template <typename Ti, typename T>
 static int run_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastState<Ti> *st, const double *src,
-                    const float *src32, double *dst, cudaStream_t s)
+                    const float *src32, double *dst, int c0, int c1, cudaStream_t s, StageTimer *tm)
 {
     FastPlan<Ti> &P = st->plan;
     FastScratch<Ti> &S = st->scratch;
@@ -485,29 +733,66 @@ static int run_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastState<Ti> *s
     // 1. frame + transpose (grid covers the padded strides)
     dim3 tgrid((nB + 31) / 32, (nA + 31) / 32), tblk(32, 8);
     if (src32)
-        frame_transpose_kernel<Ti, float, T><<<tgrid, tblk, 0, s>>>(nA, nB, P.ldA, P.ldB, P.d_bstr, P.d_Ka, src32, ct, ctT);
+        STAGE(tm, 0, s, (frame_transpose_kernel<Ti, float, T><<<tgrid, tblk, 0, s>>>(nA, nB, P.ldA, P.ldB, P.d_bstr,
+                                                                                   P.d_Ka, src32, ct, ctT)));
     else
-        frame_transpose_kernel<Ti, double, T><<<tgrid, tblk, 0, s>>>(nA, nB, P.ldA, P.ldB, P.d_bstr, P.d_Ka, src, ct, ctT);
+        STAGE(tm, 0, s, (frame_transpose_kernel<Ti, double, T><<<tgrid, tblk, 0, s>>>(nA, nB, P.ldA, P.ldB, P.d_bstr,
+                                                                                    P.d_Ka, src, ct, ctT)));
     // 2. pure alpha + diagonal -> dst (the frame's s~)
     {
-        dim3 g(nA, (nB + kRowChunk - 1) / kRowChunk);
-        pure_rows_kernel<T><<<g, 256, 0, s>>>(nB, P.ldA, P.csrA, ct, dst, nB, P.rank_d ? P.d_PAd : nullptr,
-                                              P.d_PBdT, P.rank_d);
+        dim3 g(nA, (c1 - c0 + kRowChunk - 1) / kRowChunk);
+        STAGE(tm, 1, s, (pure_rows_kernel<T><<<g, 256, 0, s>>>(0, c0, c1, P.ldA, P.csrA, ct, dst, nB,
+                                                               P.rank_d ? P.d_PAd : nullptr, P.d_PBdT, P.rank_d)));
     }
-    // 3. pure beta on the transposed vector -> tT
+    constexpr int kEPT = sizeof(T) == 8 ? 4 : 8;
+    // 2b. same-spin alpha doubles through intermediate strings -> dst
+    if (P.riA.on) {
+        rc = launch_ri<T, kEPT>(P.riA, ct, P.ldA, dst, nB, nA, c0, c1, &S.Z, &S.z_n, s, tm);
+        if (rc != BSIM_OK) return rc;
+    }
+    // 3. pure beta on the transposed vector -> tT (the beta doubles through
+    //    intermediates when the whole sigma is computed, else through the rows)
+    const bool ri_b = P.riB.on && c0 == 0 && c1 == nB;
     {
-        dim3 g(nB, (nA + kRowChunk - 1) / kRowChunk);
-        pure_rows_kernel<T><<<g, 256, 0, s>>>(nA, P.ldB, P.csrB, ctT, tT, P.ldB, nullptr, nullptr, 0);
+        dim3 g(c1 - c0, (nA + kRowChunk - 1) / kRowChunk);
+        STAGE(tm, 2, s, (pure_rows_kernel<T><<<g, 256, 0, s>>>(c0, 0, nA, P.ldB, ri_b ? P.csrBri : P.csrB, ctT, tT,
+                                                               P.ldB, nullptr, nullptr, 0)));
+    }
+    if (ri_b) {
+        rc = launch_ri<T, kEPT>(P.riB, ctT, P.ldB, tT, P.ldB, nB, 0, nA, &S.Z, &S.z_n, s, tm);
+        if (rc != BSIM_OK) return rc;
     }
     // 4. mixed
     if (P.nE > 0 && P.nF > 0 && P.M > 0) {
-        if constexpr (sizeof(T) == 8) rc = launch_mixed<Ti, T, 4>(B, P, S, ct, dst, s);
-        else rc = launch_mixed<Ti, T, 8>(B, P, S, ct, dst, s);
+        if constexpr (sizeof(T) == 8) rc = launch_mixed<Ti, T, 4>(B, P, S, ct, dst, c0, c1, s, tm);
+        else rc = launch_mixed<Ti, T, 8>(B, P, S, ct, dst, c0, c1, s, tm);
         if (rc != BSIM_OK) return rc;
     }
     // 5. final combine
-    final_kernel<Ti><<<tgrid, tblk, 0, s>>>(nA, nB, P.ldB, P.d_bstr, P.d_Ka, tT, dst);
+    dim3 fgrid((c1 - c0 + 31) / 32, (nA + 31) / 32);
+    STAGE(tm, 5, s, (final_kernel<Ti><<<fgrid, tblk, 0, s>>>(nA, nB, P.ldB, c0, c1, P.d_bstr, P.d_Ka, tT, dst)));
     BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+template <typename Ti>
+static int sigma_fast_impl(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32,
+                           double *dst, bool mixed, cudaStream_t s, bool *used, StageTimer *tm)
+{
+    *used = false;
+    FastState<Ti> *st = nullptr;
+    int rc = get_fast(B, N, &st);
+    if (rc != BSIM_OK) return rc;
+    if (!st->plan.ok || (mixed ? !st->plan.fits32 : !st->plan.fits64)) return BSIM_OK;
+    rc = mixed ? run_fast<Ti, float>(B, N, st, src, src32, dst, 0, st->plan.nB, s, tm)
+               : run_fast<Ti, double>(B, N, st, src, nullptr, dst, 0, st->plan.nB, s, tm);
+    if (rc != BSIM_OK) return rc;
+    if (!st->plan.residual.empty()) {
+        STAGE(tm, 6, s, rc = sigma_generic_accumulate(B, N, st->plan.d_resid, st->plan.d_resid_chunks,
+                                                      st->plan.n_resid_chunks, src, src32, dst, mixed, s));
+        if (rc != BSIM_OK) return rc;
+    }
+    *used = true;
     return BSIM_OK;
 }
 
@@ -515,20 +800,42 @@ template <typename Ti>
 int sigma_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const float *src32, double *dst,
                bool mixed, cudaStream_t s, bool *used)
 {
-    *used = false;
+    return sigma_fast_impl(B, N, src, src32, dst, mixed, s, used, (StageTimer *)nullptr);
+}
+
+template <typename Ti>
+int sigma_fast_cols(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, double *dst, bool mixed,
+                    i64 col_lo, i64 col_hi, cudaStream_t s)
+{
     FastState<Ti> *st = nullptr;
     int rc = get_fast(B, N, &st);
     if (rc != BSIM_OK) return rc;
-    if (!st->plan.ok || (mixed ? !st->plan.fits32 : !st->plan.fits64)) return BSIM_OK;
-    rc = mixed ? run_fast<Ti, float>(B, N, st, src, src32, dst, s) : run_fast<Ti, double>(B, N, st, src, nullptr, dst, s);
-    if (rc != BSIM_OK) return rc;
-    if (!st->plan.residual.empty()) {
-        rc = sigma_generic_accumulate(B, N, st->plan.d_resid, st->plan.d_resid_chunks, st->plan.n_resid_chunks, src,
-                                      src32, dst, mixed, s);
-        if (rc != BSIM_OK) return rc;
+    const FastPlan<Ti> &P = st->plan;
+    if (!P.ok || (mixed ? !P.fits32 : !P.fits64) || !P.residual.empty()) {
+        set_error("column-band sigma needs the structured path with no residual groups (%s)",
+                  P.ok ? "residual groups or shared memory" : P.why.c_str());
+        return BSIM_ERR_UNSUPPORTED;
     }
-    *used = true;
-    return BSIM_OK;
+    if (col_lo < 0 || col_hi > P.nB || col_lo > col_hi || (col_lo % kMixCols) != 0) {
+        set_error("column band [%lld, %lld) must lie in [0, %d) and start on a multiple of %d", (long long)col_lo,
+                  (long long)col_hi, P.nB, kMixCols);
+        return BSIM_ERR_ARG;
+    }
+    if (col_lo == col_hi) return BSIM_OK;
+    return mixed ? run_fast<Ti, float>(B, N, st, src, nullptr, dst, (int)col_lo, (int)col_hi, s, nullptr)
+                 : run_fast<Ti, double>(B, N, st, src, nullptr, dst, (int)col_lo, (int)col_hi, s, nullptr);
+}
+
+template <typename Ti>
+int sigma_fast_stages(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, double *dst, bool mixed,
+                      cudaStream_t s, double *ms, int *launches, int nstages)
+{
+    StageTimer tm;
+    bool used = false;
+    int rc = sigma_fast_impl(B, N, src, nullptr, dst, mixed, s, &used, &tm);
+    if (rc != BSIM_OK) return rc;
+    if (!used) { set_error("the structured sigma path is off for this basis and network"); return BSIM_ERR_UNSUPPORTED; }
+    return tm.collect(ms, launches, nstages);
 }
 
 template <typename Ti>
@@ -546,5 +853,9 @@ template int fast_sigma_info<unsigned>(const DevBasis<unsigned> *, const DevNet<
 template bool fast_sigma_available<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *);
 template int sigma_fast<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *, const float *,
                                   double *, bool, cudaStream_t, bool *);
+template int sigma_fast_cols<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *, double *,
+                                       bool, i64, i64, cudaStream_t);
+template int sigma_fast_stages<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *, double *,
+                                         bool, cudaStream_t, double *, int *, int);
 
 }  // namespace bsim

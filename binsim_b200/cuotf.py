@@ -72,6 +72,9 @@ def lib() -> C.CDLL:
         "bsim_hvec": (ci, [vp, vp, vp, vp, vp]), "bsim_hvec_mixed": (ci, [vp, vp, vp, vp, vp]),
         "bsim_hvec_f32in": (ci, [vp, vp, vp, vp, vp]),
         "bsim_hvec_path": (ci, [vp, vp, C.c_char_p, ci, vp]),
+        "bsim_hvec_stage_times": (ci, [vp, vp, vp, vp, ci, vp, vp, ci, vp]),
+        "bsim_hvec_cols": (ci, [vp, vp, vp, vp, i64, i64, ci, vp]),
+        "bsim_fma_peak": (ci, [ci, vp, vp]),
         "bsim_hvec_num_tiles": (i64, [vp]), "bsim_hvec_tiles": (ci, [vp, vp, vp, vp, i64, i64, ci, vp]), "bsim_diag": (ci, [vp, vp, vp, vp]),
         "bsim_expm": (ci, [vp, vp, i64, dbl, vp, vp]), "bsim_expm_seq": (ci, [vp, vp, i64, vp, vp, vp, vp]),
         "bsim_grad": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
@@ -122,6 +125,13 @@ def _stream(stream=None):
 
 def _host(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
+
+
+def fma_peak(fp64: bool = True, stream=None) -> float:
+    """CUDA-core FMA throughput of the current GPU, TFLOP/s."""
+    t = C.c_double()
+    _check(lib().bsim_fma_peak(1 if fp64 else 0, C.byref(t), _stream(stream)), "fma_peak")
+    return t.value
 
 
 class CuBasis:
@@ -225,6 +235,22 @@ class CuOTFFunctions:
         if r < 0:
             _check(r, "hvec_path")
         return r, buf.value.decode(), nres.value
+
+    def hvec_cols(self, v, Hv, col_lo: int, col_hi: int, mixed=False, stream=None):
+        """sigma on beta columns [col_lo, col_hi) only (column-band sharding)."""
+        _check(lib().bsim_hvec_cols(self.basis.h, self.ham.h, _ptr(v), _ptr(Hv), col_lo, col_hi, 1 if mixed else 0,
+                                    _stream(stream)), "hvec_cols")
+
+    STAGES = ("frame_transpose", "pure_alpha", "pure_beta", "mixed_gemm", "mixed_gather", "final", "residual",
+              "ri_gemm", "ri_gather")
+
+    def sigma_stage_times(self, v, Hv, mixed=False, stream=None):
+        """One structured sigma with CUDA events per launch: {stage: (ms, launches)}."""
+        n = len(self.STAGES)
+        ms, nl = (C.c_double * n)(), (C.c_int * n)()
+        _check(lib().bsim_hvec_stage_times(self.basis.h, self.ham.h, _ptr(v), _ptr(Hv), 1 if mixed else 0, ms, nl, n,
+                                           _stream(stream)), "hvec_stage_times")
+        return {k: (ms[i], nl[i]) for i, k in enumerate(self.STAGES)}
 
     def num_tiles(self) -> int:
         return lib().bsim_hvec_num_tiles(self.basis.h)

@@ -123,6 +123,26 @@ int bsim_hvec_f32in(void *basis, void *net, const float *src, double *dst, bsim_
  * residual_groups the number of groups the structured path leaves to the
  * generic kernel.  Builds (and caches) the plan on first use. */
 int bsim_hvec_path(void *basis, void *net, char *why, int why_len, int *residual_groups);
+/* Beta-column band of sigma: dst[a, b] = (H src)[a, b] for every alpha row a and
+ * col_lo <= b < col_hi (within the single symmetry block; col_lo a multiple of
+ * 128), every other element of dst untouched.  src must hold the whole vector.
+ * Ranks that split [0, num_b) into such bands compute disjoint parts of one
+ * sigma.  Needs the structured path (bsim_hvec_path == 1) with no residual
+ * groups, else BSIM_ERR_UNSUPPORTED.  mixed selects FP32 bulk. */
+int bsim_hvec_cols(void *basis, void *net, const double *src, double *dst, int64_t col_lo, int64_t col_hi,
+                   int mixed, bsim_stream_t stream);
+/* Measurement: one structured sigma (dst = H src, FP64 or FP32 bulk) with CUDA
+ * events around every launch.  ms_out[i] / launches_out[i] receive the device
+ * milliseconds and launch count of stage i for i < nstages: 0 frame+transpose,
+ * 1 pure-alpha rows (+ diagonal), 2 pure-beta rows, 3 mixed GEMM, 4 mixed
+ * gather, 5 final combine, 6 groups left to the generic kernel, 7 same-spin
+ * doubles' intermediate-string GEMM, 8 their gather.  Fails with
+ * BSIM_ERR_UNSUPPORTED when the structured path is off. */
+int bsim_hvec_stage_times(void *basis, void *net, const double *src, double *dst, int mixed, double *ms_out,
+                          int *launches_out, int nstages, bsim_stream_t stream);
+/* Measurement: CUDA-core FMA throughput of this GPU in TFLOP/s (fp64 != 0:
+ * FP64, else FP32), from chains of dependent FMAs on every SM. */
+int bsim_fma_peak(int fp64, double *tflops_out, bsim_stream_t stream);
 /* Number of 32 x 32 destination tiles of sigma (block-major, then row-major). */
 int64_t bsim_hvec_num_tiles(void *basis);
 /* sigma restricted to destination tiles [tile_lo, tile_hi): the rows of those

@@ -105,3 +105,42 @@ def test_reference_host_handles(cuda, reflibs):
     np.testing.assert_allclose(d.cpu().numpy(), reflibs.diag_elems(rb, rn, dim), atol=1e-12)
     L.destroy_networkdev_f64(dn)
     L.destroy_basisdev_f64(db)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_column_bands_reassemble_sigma(cuda, mixed):
+    """Column-band sigma (the per-rank unit of the sharded path): bands computed
+    separately reproduce the whole sigma (to rounding: a band sums the same-spin
+    doubles of the beta side through the row lists, a whole sigma through the
+    intermediate strings), every split gives the same bits, and a call leaves the
+    columns outside its band untouched."""
+    import math
+    from binsim_b200 import cuotf, network as nw
+    from binsim_b200.shard import column_bands
+    norb, na, nb = 11, 4, 5                      # 330 x 462 determinants
+    net = nw.hamiltonian_network(norb, seed=12)
+    B = cuotf.CuBasis(norb, na, nb)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    assert f.sigma_path()[0] == 1
+    nA, nB = math.comb(norb, na), math.comb(norb, nb)
+    x = dev(cuda, np.random.default_rng(4).normal(size=B.dim))
+    full = cuda.empty_like(x)
+    (f.hvec_mixed if mixed else f.hvec)(x, full)
+    first = None
+    for world in (2, 3, 4):
+        y = cuda.full_like(x, float("nan"))
+        for lo, hi in column_bands(nB, world):
+            before = y.clone()
+            f.hvec_cols(x, y, lo, hi, mixed=mixed)
+            changed = (y != before) & ~(y.isnan() & before.isnan())
+            outside = changed.view(nA, nB).clone()
+            outside[:, lo:hi] = False
+            assert not bool(outside.any()), "wrote outside its column band"
+        tol = (2e-6 if mixed else 1e-13) * float(full.abs().max())
+        assert float((y - full).abs().max()) <= tol
+        if first is None:
+            first = y.clone()
+        assert cuda.equal(y, first)
+    # misaligned band start is an argument error
+    with pytest.raises(cuotf.CuOTFError):
+        f.hvec_cols(x, y, 5, 40)

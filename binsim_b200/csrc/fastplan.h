@@ -119,16 +119,21 @@ struct FastPlan {
 constexpr int kMixCols = 128;                             // columns per GEMM chunk
 
 // Shared memory of the intermediate-string GEMM: W_m [nU x 64] and an X slice.
+// (Row strides: 68 / kMixCols + 4 elements for FP64, 64 / kMixCols for FP32;
+// rows rounded up to a multiple of 4.)
+inline size_t gemm_ls(size_t elem) { return elem == 8 ? 68 : 64; }
+inline size_t gemm_xs(size_t elem) { return elem == 8 ? kMixCols + 4 : kMixCols; }
 inline size_t ri_smem_bytes(int nU, size_t elem)
 {
-    return (size_t)nU * 64 * elem + 32 * (size_t)kMixCols * elem + 64 * 8;
+    return (((size_t)nU + 3) & ~size_t(3)) * gemm_ls(elem) * elem + 32 * gemm_xs(elem) * elem + 64 * 8;
 }
 
 // Shared memory of the mixed GEMM kernel: source row, Lam_conn [K x 64], an
 // X slice [32 x kMixCols] and the connected-excitation lists.
 inline size_t mixed_smem_bytes(int nB, int nF, size_t elem)
 {
-    return (((size_t)nB + 7) & ~size_t(7)) * elem + (size_t)nF * 64 * elem + 32 * (size_t)kMixCols * elem + 128 * 4;
+    return (((size_t)nB + 7) & ~size_t(7)) * elem + (((size_t)nF + 3) & ~size_t(3)) * gemm_ls(elem) * elem +
+           32 * gemm_xs(elem) * elem + 128 * 4;
 }
 
 template <typename Ti>

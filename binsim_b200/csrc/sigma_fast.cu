@@ -192,9 +192,13 @@ __device__ __forceinline__ int connected_excitations(const MixedArgs &P, u64 sa,
 template <int EPT>
 __device__ __forceinline__ void load_lam(const double *p, double l[EPT])
 {
-    static_assert(EPT == 4, "FP64 GEMM uses 4 excitations per thread");
-    const double2 q0 = reinterpret_cast<const double2 *>(p)[0], q1 = reinterpret_cast<const double2 *>(p)[1];
-    l[0] = q0.x; l[1] = q0.y; l[2] = q1.x; l[3] = q1.y;
+    static_assert(EPT % 2 == 0, "pairs of excitations per 16-byte load");
+#pragma unroll
+    for (int i = 0; i < EPT / 2; ++i) {
+        const double2 q = reinterpret_cast<const double2 *>(p)[i];
+        l[2 * i] = q.x;
+        l[2 * i + 1] = q.y;
+    }
 }
 template <int EPT>
 __device__ __forceinline__ void load_lam(const float *p, float l[EPT])
@@ -264,13 +268,103 @@ struct GemmTile<float, EPT> {
     }
 };
 
+// Shared-memory strides of the GEMM operands: Lam/W_m rows of LS elements and
+// X-slice rows of XS elements.  The FP64 tiles are read as mma fragments (lane
+// (g, t) = (lane / 4, lane % 4) reads row t, column g of a 4 x 8 block); a row
+// stride of 4 mod 16 doubles puts the 16 lanes of each half-warp on distinct
+// banks.
+template <typename T> struct GemmLayout { static constexpr int LS = 64, XS = kMixCols; };
+template <> struct GemmLayout<double> { static constexpr int LS = 68, XS = kMixCols + 4; };
+
+// FP64 core: warp w computes rows 8*(w/2)..+7 and columns 64*(w%2)..+63 of the
+// 64 x kMixCols output chunk as eight 8x8 tiles with mma.sync m8n8k4 (FP64 on
+// the tensor cores' DMMA path), 4 slice rows per instruction.
+__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <typename T, int EPT>
+struct GemmCore {
+    // FP32 bulk: EPT rows x 4 columns per thread with packed f32x2 FMAs
+    GemmTile<T, EPT> acc;
+    __device__ __forceinline__ void zero() { acc.zero(); }
+    __device__ __forceinline__ static bool active(int rows) { return (int)(threadIdx.x >> 5) * EPT < rows; }
+    __device__ __forceinline__ void step(const T *lam, const T *xs, int f0, int nf)
+    {
+        constexpr int LS = GemmLayout<T>::LS, XS = GemmLayout<T>::XS;
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll 4
+        for (int f = 0; f < nf; ++f) {
+            T l[EPT];
+            load_lam<EPT>(lam + (size_t)(f0 + f) * LS + wid * EPT, l);
+            acc.step(l, xs + f * XS + 2 * lane, xs + f * XS + 64 + 2 * lane);
+        }
+    }
+    __device__ __forceinline__ void store(T *zbase, int W, int rows) const
+    {
+        using V2 = typename Vec2<T>::type;
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int j = wid * EPT + i;
+            if (j < rows) {
+                V2 v0, v1;
+                acc.pair(i, v0, v1);
+                *reinterpret_cast<V2 *>(zbase + (i64)j * W + 2 * lane) = v0;
+                *reinterpret_cast<V2 *>(zbase + (i64)j * W + 64 + 2 * lane) = v1;
+            }
+        }
+    }
+};
+
+template <int EPT>
+struct GemmCore<double, EPT> {
+    static_assert(EPT == 4, "16 warps: 8 row blocks x 2 column halves");
+    double c[8][2];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) c[k][0] = c[k][1] = 0.0;
+    }
+    __device__ __forceinline__ static bool active(int rows) { return (int)(threadIdx.x >> 6) * 8 < rows; }
+    __device__ __forceinline__ void step(const double *lam, const double *xs, int f0, int nf)
+    {
+        constexpr int LS = GemmLayout<double>::LS, XS = GemmLayout<double>::XS;
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const int g = lane >> 2, t = lane & 3, rb = wid >> 1, ch = wid & 1;
+        const double *la = lam + (size_t)(f0 + t) * LS + rb * 8 + g;
+        const double *xb = xs + t * XS + ch * 64 + g;
+        for (int kk = 0; kk < nf; kk += 4) {   // slice rows past nf are zero in X and in Lam
+            const double a = la[(size_t)kk * LS];
+            double b[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) b[k] = xb[kk * XS + 8 * k];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) dmma_8x8x4(c[k][0], c[k][1], a, b[k]);
+        }
+    }
+    __device__ __forceinline__ void store(double *zbase, int W, int rows) const
+    {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const int g = lane >> 2, t = lane & 3, rb = wid >> 1, ch = wid & 1;
+        const int j = rb * 8 + g;
+        if (j >= rows) return;
+        double *zr = zbase + (i64)j * W + ch * 64 + 2 * t;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) *reinterpret_cast<double2 *>(zr + 8 * k) = make_double2(c[k][0], c[k][1]);
+    }
+};
+
 // One CTA per source row a'.  Warp w owns excitations w*EPT .. w*EPT+EPT-1 of
 // the row's connected list; lane l owns columns {2l, 2l+1, 64+2l, 64+2l+1} of a
 // kMixCols-column chunk (conflict-free 2-element shared loads).  The X slice for
 // (chunk, 32 F) is filled from the gather-index table, whose next slice is
 // loaded into registers while the current one is multiplied.
 template <typename Ti, typename T, int EPT>
-__global__ void __launch_bounds__((64 / EPT) * 32, EPT == 8 ? 2 : 1)
+__global__ void __launch_bounds__((64 / EPT) * 32, sizeof(T) == 4 ? 2 : 1)
 mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__restrict__ ct, T *__restrict__ Z,
                   int z0, int W)
 {
@@ -280,13 +374,14 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.nF, M = P.M;
     T *srow = reinterpret_cast<T *>(smem_raw);                    // [ldA]
-    T *lam = srow + P.ldA;                                         // [K][64]
-    T *xs = lam + (size_t)K * 64;                                  // [32][kMixCols]
-    int *conn = reinterpret_cast<int *>(xs + 32 * kMixCols);       // [64]
+    constexpr int LS = GemmLayout<T>::LS, XS = GemmLayout<T>::XS;
+    const int Kp = (K + 3) & ~3;
+    T *lam = srow + P.ldA;                                         // [Kp][LS], rows >= K zero
+    T *xs = lam + (size_t)Kp * LS;                                 // [32][XS]
+    int *conn = reinterpret_cast<int *>(xs + 32 * XS);             // [64]
     int *sgn = conn + 64;                                          // [64]
     __shared__ int wcnt[NW], cnt;
     const int a = blockIdx.x;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int m = connected_excitations<NT>(P, (u64)astr[a], conn, sgn, wcnt, &cnt);
     // stage the source row (16-byte copies) and Lam restricted to the connected excitations
     {
@@ -296,15 +391,15 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
         for (int i = threadIdx.x; i < n16; i += NT) dst[i] = __ldg(src + i);
     }
     const T *Lam = static_cast<const T *>(P.Lam);
-    for (int i = threadIdx.x; i < K * 64; i += NT) {
-        const int f = i >> 6, j = i & 63;
-        lam[i] = j < m ? (T)sgn[j] * Lam[(i64)conn[j] * K + f] : T(0);
+    for (int i = threadIdx.x; i < Kp * LS; i += NT) {
+        const int f = i / LS, j = i % LS;
+        lam[i] = (j < m && f < K) ? (T)sgn[j] * Lam[(i64)conn[j] * K + f] : T(0);
     }
     const int zend = min(P.cend, z0 + W);
     const int ncb = (zend - z0 + kMixCols - 1) / kMixCols;
     const int nfc = (K + 31) / 32;
     const int nsteps = ncb * nfc;
-    const bool active = wid * EPT < m;
+    const bool active = GemmCore<T, EPT>::active(m);
     int gpre[ITEMS];
     auto load_g = [&](int step) {
         const int cb = z0 + (step / nfc) * kMixCols, f0 = (step % nfc) * 32;
@@ -315,7 +410,7 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
             gpre[it] = f0 + f < K ? __ldg(P.gidx + (i64)(f0 + f) * P.ldG + cb + cl) : -1;
         }
     };
-    GemmTile<T, EPT> acc;
+    GemmCore<T, EPT> acc;
     acc.zero();
     if (nsteps > 0) load_g(0);
     for (int step = 0; step < nsteps; ++step) {
@@ -330,32 +425,14 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
                 x = srow[g >> 1];
                 if (g & 1) x = -x;
             }
-            xs[threadIdx.x + it * NT] = x;
+            const int i = threadIdx.x + it * NT;
+            xs[(i / kMixCols) * XS + i % kMixCols] = x;
         }
         __syncthreads();
         if (step + 1 < nsteps) load_g(step + 1);
-        if (active) {
-#pragma unroll 4
-            for (int f = 0; f < nf; ++f) {
-                T l[EPT];
-                load_lam<EPT>(lam + (size_t)(f0 + f) * 64 + wid * EPT, l);
-                acc.step(l, xs + f * kMixCols + 2 * lane, xs + f * kMixCols + 64 + 2 * lane);
-            }
-        }
+        if (active) acc.step(lam, xs, f0, nf);
         if (fci == nfc - 1) {
-            if (active) {
-#pragma unroll
-                for (int i = 0; i < EPT; ++i) {
-                    const int j = wid * EPT + i;
-                    if (j < m) {
-                        T *zr = Z + ((i64)a * M + j) * W + cbi * kMixCols;
-                        V2 v0, v1;
-                        acc.pair(i, v0, v1);
-                        *reinterpret_cast<V2 *>(zr + 2 * lane) = v0;
-                        *reinterpret_cast<V2 *>(zr + 64 + 2 * lane) = v1;
-                    }
-                }
-            }
+            if (active) acc.store(Z + (i64)a * M * W + cbi * kMixCols, W, m);
             acc.zero();
         }
     }
@@ -420,7 +497,7 @@ struct RIArgs {
 // the mixed GEMM: warp w owns output rows w*EPT.., lane l owns columns
 // {2l, 2l+1, 64+2l, 64+2l+1} of a kMixCols chunk.
 template <typename T, int EPT>
-__global__ void __launch_bounds__((64 / EPT) * 32, EPT == 8 ? 2 : 1)
+__global__ void __launch_bounds__((64 / EPT) * 32, sizeof(T) == 4 ? 2 : 1)
 ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int z0, int W)
 {
     constexpr int NT = (64 / EPT) * 32;
@@ -428,11 +505,12 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
     using V2 = typename Vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.nU;
-    T *wm = reinterpret_cast<T *>(smem_raw);                          // [K][64]
-    T *xs = wm + (size_t)K * 64;                                       // [32][kMixCols]
-    long long *soff = reinterpret_cast<long long *>(xs + 32 * kMixCols);   // [64]
+    constexpr int LS = GemmLayout<T>::LS, XS = GemmLayout<T>::XS;
+    const int Kp = (K + 3) & ~3;
+    T *wm = reinterpret_cast<T *>(smem_raw);                          // [Kp][LS], rows >= K zero
+    T *xs = wm + (size_t)Kp * LS;                                      // [32][XS]
+    long long *soff = reinterpret_cast<long long *>(xs + 32 * XS);     // [64]
     const int m = blockIdx.x;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int *srcm = P.src + (i64)m * K, *pidm = P.pid + (i64)m * K;
     for (int i = threadIdx.x; i < 64; i += NT) {
         long long o = 0;
@@ -443,16 +521,16 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
         soff[i] = o;
     }
     const T *Wt = static_cast<const T *>(P.W);
-    for (int i = threadIdx.x; i < K * 64; i += NT) {
-        const int k = i >> 6, j = i & 63;
-        wm[i] = j < K ? Wt[(i64)pidm[j] * P.nP + pidm[k]] : T(0);
+    for (int i = threadIdx.x; i < Kp * LS; i += NT) {
+        const int k = i / LS, j = i % LS;
+        wm[i] = (j < K && k < K) ? Wt[(i64)pidm[j] * P.nP + pidm[k]] : T(0);
     }
     __syncthreads();
     const int zend = min(P.cend, z0 + W);
     const int ncb = (zend - z0 + kMixCols - 1) / kMixCols;
     const int nfc = (K + 31) / 32;
     const int nsteps = ncb * nfc;
-    const bool active = wid * EPT < K;
+    const bool active = GemmCore<T, EPT>::active(K);
     T gpre[ITEMS];
     auto load_x = [&](int step) {
         const int cb = z0 + (step / nfc) * kMixCols, f0 = (step % nfc) * 32;
@@ -469,7 +547,7 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
             gpre[it] = v;
         }
     };
-    GemmTile<T, EPT> acc;
+    GemmCore<T, EPT> acc;
     acc.zero();
     if (nsteps > 0) load_x(0);
     for (int step = 0; step < nsteps; ++step) {
@@ -477,31 +555,15 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
         const int f0 = fci * 32, nf = min(32, K - f0);
         __syncthreads();
 #pragma unroll
-        for (int it = 0; it < ITEMS; ++it) xs[threadIdx.x + it * NT] = gpre[it];
+        for (int it = 0; it < ITEMS; ++it) {
+            const int i = threadIdx.x + it * NT;
+            xs[(i / kMixCols) * XS + i % kMixCols] = gpre[it];
+        }
         __syncthreads();
         if (step + 1 < nsteps) load_x(step + 1);
-        if (active) {
-#pragma unroll 4
-            for (int f = 0; f < nf; ++f) {
-                T l[EPT];
-                load_lam<EPT>(wm + (size_t)(f0 + f) * 64 + wid * EPT, l);
-                acc.step(l, xs + f * kMixCols + 2 * lane, xs + f * kMixCols + 64 + 2 * lane);
-            }
-        }
+        if (active) acc.step(wm, xs, f0, nf);
         if (fci == nfc - 1) {
-            if (active) {
-#pragma unroll
-                for (int i = 0; i < EPT; ++i) {
-                    const int j = wid * EPT + i;
-                    if (j < K) {
-                        T *zr = Z + ((i64)m * K + j) * W + cbi * kMixCols;
-                        V2 v0, v1;
-                        acc.pair(i, v0, v1);
-                        *reinterpret_cast<V2 *>(zr + 2 * lane) = v0;
-                        *reinterpret_cast<V2 *>(zr + 64 + 2 * lane) = v1;
-                    }
-                }
-            }
+            if (active) acc.store(Z + (i64)m * K * W + cbi * kMixCols, W, K);
             acc.zero();
         }
     }
@@ -744,6 +806,7 @@ static int run_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastState<Ti> *s
         STAGE(tm, 1, s, (pure_rows_kernel<T><<<g, 256, 0, s>>>(0, c0, c1, P.ldA, P.csrA, ct, dst, nB,
                                                                P.rank_d ? P.d_PAd : nullptr, P.d_PBdT, P.rank_d)));
     }
+    // FP64: 16 warps of DMMA 8x8 tiles; FP32: 8 warps of 8 x 4 f32x2 register tiles
     constexpr int kEPT = sizeof(T) == 8 ? 4 : 8;
     // 2b. same-spin alpha doubles through intermediate strings -> dst
     if (P.riA.on) {
@@ -764,8 +827,7 @@ static int run_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastState<Ti> *s
     }
     // 4. mixed
     if (P.nE > 0 && P.nF > 0 && P.M > 0) {
-        if constexpr (sizeof(T) == 8) rc = launch_mixed<Ti, T, 4>(B, P, S, ct, dst, c0, c1, s, tm);
-        else rc = launch_mixed<Ti, T, 8>(B, P, S, ct, dst, c0, c1, s, tm);
+        rc = launch_mixed<Ti, T, kEPT>(B, P, S, ct, dst, c0, c1, s, tm);
         if (rc != BSIM_OK) return rc;
     }
     // 5. final combine

@@ -124,18 +124,26 @@ __global__ void scale_kernel(i64 n, double *__restrict__ v, const double *__rest
     for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) v[i] *= inv;
 }
 
-// out_j partials = <V_j, w> for j < k (davidson.hpp:186-219)
+// out_j partials = <V_j, w> for j < k <= kDotChunk (davidson.hpp:186-219); the
+// sums stay in registers (a fixed-size, fully unrolled array), the host splits
+// larger subspaces into chunks
+constexpr int kDotChunk = 8;
 template <typename TV, typename TW>
 __global__ void multidot_kernel(i64 n, int k, Ptrs<TV> V, const TW *__restrict__ w, double *__restrict__ part)
 {
     __shared__ double red[32];
-    double s[kMaxSub];
-    for (int j = 0; j < k; ++j) s[j] = 0.0;
+    double s[kDotChunk];
+#pragma unroll
+    for (int j = 0; j < kDotChunk; ++j) s[j] = 0.0;
     for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
         const double x = (double)w[i];
-        for (int j = 0; j < k; ++j) s[j] += (double)V.p[j][i] * x;
+#pragma unroll
+        for (int j = 0; j < kDotChunk; ++j)
+            if (j < k) s[j] += (double)V.p[j][i] * x;
     }
-    for (int j = 0; j < k; ++j) cta_partial(s[j], red, part + (i64)blockIdx.x * k + j);
+#pragma unroll
+    for (int j = 0; j < kDotChunk; ++j)
+        if (j < k) cta_partial(s[j], red, part + (i64)blockIdx.x * k + j);
 }
 
 __global__ void dot_kernel(i64 n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ part)
@@ -261,8 +269,11 @@ int dav_multidot(DavScratch &S, i64 n, int k, const TV *const *V, const TW *w, d
     int st = S.ensure();
     if (st) return st;
     const int g = grid_for(n);
-    multidot_kernel<TV, TW><<<g, kRedThreads, 0, s>>>(n, k, pack(V, k), w, S.part);
-    finish_kernel<<<1, 1024, 0, s>>>(S.part, g, k, out_dev, 0);
+    for (int j0 = 0; j0 < k; j0 += kDotChunk) {
+        const int kc = std::min(kDotChunk, k - j0);
+        multidot_kernel<TV, TW><<<g, kRedThreads, 0, s>>>(n, kc, pack(V + j0, kc), w, S.part);
+        finish_kernel<<<1, 1024, 0, s>>>(S.part, g, kc, out_dev + j0, 0);
+    }
     BSIM_CUDA(cudaGetLastError());
     return BSIM_OK;
 }

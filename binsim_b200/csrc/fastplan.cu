@@ -497,7 +497,8 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
                  bytes(P->residual.size(), 4) + bytes(P->residual.size() + 1, 16);
     for (int li = 0; li < 3; ++li)
         tot += 2 * bytes(csr[li].cptr.size(), 8) + bytes(csr[li].cent.size(), sizeof(CEnt)) +
-               bytes(csr[li].tent.size(), sizeof(TEnt)) + bytes(sh[li == 0 ? 0 : 1].ctab.size(), 8);
+               bytes(csr[li].tent.size(), sizeof(TEnt)) + bytes(sh[li == 0 ? 0 : 1].ctab.size(), 8) +
+               bytes(sh[li == 0 ? 0 : 1].ctab.size(), 4);
     for (int side = 0; side < 2; ++side)
         tot += 2 * bytes(rih[side].src.size(), 4) + bytes(rih[side].gath.size(), 8) + bytes(Wri[side].size(), 8) +
                bytes(rih[side].W32.size(), 4);
@@ -529,6 +530,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
         D.tptr = put(C.tptr);
         D.tent = put(C.tent);
         D.ctab = put(sh[li == 0 ? 0 : 1].ctab);
+        D.ctab32 = put(std::vector<float>(sh[li == 0 ? 0 : 1].ctab.begin(), sh[li == 0 ? 0 : 1].ctab.end()));
     }
     for (int side = 0; side < 2; ++side) {
         RISide &R = side == 0 ? P->riA : P->riB;

@@ -49,6 +49,7 @@ struct SideCSR {
     const i64 *tptr;      // [nrows + 1]
     const TEnt *tent;     // [nnz_t]
     const double *ctab;   // column-factor tables, rows padded to ld_in
+    const float *ctab32;  // the same in FP32 (FP32-bulk sigma)
 };
 
 // Same-spin double excitations through (n-2)-electron intermediate strings m

@@ -21,6 +21,7 @@
 
 #include <cstdlib>
 #include <mutex>
+#include <type_traits>
 
 namespace bsim {
 
@@ -129,16 +130,19 @@ pure_rows_kernel(int row_begin, int col_begin, int ncols, int ld_in, const SideC
 #pragma unroll
         for (int k = 0; k < 4; ++k) acc[k] += (double)part[k];
     }
+    // column-factor tables in the bulk precision (FP64 sums of the factor)
+    const T *ctab = std::is_same<T, float>::value ? reinterpret_cast<const T *>(L.ctab32)
+                                                  : reinterpret_cast<const T *>(L.ctab);
     for (i64 e = L.tptr[row]; e < L.tptr[row + 1]; ++e) {
         const TEnt t = L.tent[e];
         const int R = (int)(t.toff_rank & 7);
-        const double *tab = L.ctab + (t.toff_rank & ~7ll) + c;
+        const T *tab = ctab + (t.toff_rank & ~7ll) + c;
         double f[4] = {0.0, 0.0, 0.0, 0.0};
         for (int r = 0; r < R; ++r) {
-            double cr[4];
+            T cr[4];
             load4(tab + (i64)r * ld_in, cr);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) f[k] += t.pa[r] * cr[k];
+            for (int k = 0; k < 4; ++k) f[k] += t.pa[r] * (double)cr[k];
         }
         T v[4];
         load4(in_c + t.off, v);

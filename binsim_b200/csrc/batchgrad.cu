@@ -90,5 +90,7 @@ int batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *thetas, 
 
 template int batchgrad<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *, const double *,
                                  const double *, double *, cudaStream_t);
+template int batchgrad<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, const double *, const double *,
+                                 const double *, double *, cudaStream_t);
 
 }  // namespace bsim

@@ -4,6 +4,7 @@
 #include "vqe.h"
 
 #include <cstdio>
+#include <initializer_list>
 #include <mutex>
 
 using bsim::DevBasis;
@@ -24,6 +25,15 @@ int check(void *b, void *n)
 
 Basis *B(void *p) { return static_cast<Basis *>(p); }
 Net *N(void *p) { return static_cast<Net *>(p); }
+
+// f(basis) for a valid basis handle of either string type (no-op otherwise)
+template <class F>
+void with_handles_basis(void *basis, F &&f)
+{
+    if (bsim::is_u64_basis(basis)) f(static_cast<DevBasis<unsigned long long> *>(basis));
+    else if (bsim::valid(B(basis))) f(B(basis));
+    else bsim::set_error("invalid basis handle");
+}
 
 // Legacy entry points report like the reference (stderr) but do not exit.
 void report(int st, const char *where)
@@ -48,6 +58,36 @@ bsim::DavScratch &dav_scratch()
     static bsim::DavScratch S;
     return S;
 }
+
+// Calls f(basis, net...) with handles of the basis' string type (UInt32 or UInt64,
+// told by the handles' magic words); every network must match the basis' type.
+template <class F>
+int with_handles(void *basis, std::initializer_list<void *> nets, F &&f)
+{
+    if (bsim::is_u64_basis(basis)) {
+        auto *b = static_cast<DevBasis<unsigned long long> *>(basis);
+        for (void *n : nets)
+            if (!bsim::valid(static_cast<DevNet<unsigned long long> *>(n))) {
+                bsim::set_error("network handle is not a UInt64 network of this library");
+                return BSIM_ERR_ARG;
+            }
+        return f(b);
+    }
+    if (!bsim::valid(B(basis))) { bsim::set_error("invalid basis handle"); return BSIM_ERR_ARG; }
+    for (void *n : nets)
+        if (!bsim::valid(N(n))) { bsim::set_error("invalid network handle (or string type differs from the basis)"); return BSIM_ERR_ARG; }
+    return f(B(basis));
+}
+// handle validation first (bad handles report BSIM_ERR_ARG before argument checks)
+int check_handles(void *basis, std::initializer_list<void *> nets)
+{
+    return with_handles(basis, nets, [](auto *) { return (int)BSIM_OK; });
+}
+
+template <typename Ti>
+DevNet<Ti> *net_of(DevBasis<Ti> *, void *n) { return static_cast<DevNet<Ti> *>(n); }
+template <typename Ti>
+constexpr bool is_u32(DevBasis<Ti> *) { return sizeof(Ti) == 4; }
 
 }  // namespace
 
@@ -171,18 +211,39 @@ int bsim_basis_from_host(void *host_basis, void **out)
     return st;
 }
 
+int bsim_basis_create_u64(int64_t norb, int64_t na, int64_t nb, int64_t total_sym, const int64_t *orbsym,
+                          int64_t num_irreps, void **out)
+{
+    if (!out) { bsim::set_error("null out"); return BSIM_ERR_NULL; }
+    DevBasis<unsigned long long> *b = nullptr;
+    int st = bsim::make_basis<unsigned long long>(norb, na, nb, total_sym, (const i64 *)orbsym, num_irreps, &b);
+    *out = b;
+    return st;
+}
+
 int bsim_basis_destroy(void *basis)
 {
+    if (bsim::is_u64_basis(basis)) {
+        delete static_cast<DevBasis<unsigned long long> *>(basis);
+        return BSIM_OK;
+    }
     int st = check(basis, nullptr);
     if (st == BSIM_OK) delete B(basis);
     return st;
 }
 
-int64_t bsim_basis_dim(void *basis) { return check(basis, nullptr) == BSIM_OK ? B(basis)->dim : -1; }
+int64_t bsim_basis_dim(void *basis)
+{
+    int64_t d = -1;
+    with_handles_basis(basis, [&](auto *b) { d = b->dim; });
+    return d;
+}
 
 int64_t bsim_basis_find_det(void *basis, uint64_t astr, uint64_t bstr)
 {
-    return check(basis, nullptr) == BSIM_OK ? B(basis)->find_det(astr, bstr) : -1;
+    int64_t i = -1;
+    with_handles_basis(basis, [&](auto *b) { i = b->find_det(astr, bstr); });
+    return i;
 }
 
 int bsim_network_create_u32(const int64_t *orbsym, int64_t norb, int64_t ngs, const uint32_t *axs,
@@ -208,65 +269,101 @@ int bsim_network_from_host(void *host_net, void **out)
     return st;
 }
 
+int bsim_network_create_u64(const int64_t *orbsym, int64_t norb, int64_t ngs, const uint64_t *axs,
+                            const uint64_t *bxs, const int64_t *ranks, const int64_t *num_zas,
+                            const int64_t *num_zbs, const uint64_t *flat_zas, const uint64_t *flat_zbs,
+                            const double *flat_wa, const double *flat_wb, void **out)
+{
+    if (!out) { bsim::set_error("null out"); return BSIM_ERR_NULL; }
+    DevNet<unsigned long long> *n = nullptr;
+    using U = unsigned long long;
+    int st = bsim::make_network<U>((const i64 *)orbsym, norb, ngs, (const U *)axs, (const U *)bxs,
+                                   (const i64 *)ranks, (const i64 *)num_zas, (const i64 *)num_zbs,
+                                   (const U *)flat_zas, (const U *)flat_zbs, flat_wa, flat_wb, &n);
+    *out = n;
+    return st;
+}
+
 int bsim_network_destroy(void *net)
 {
+    if (bsim::is_u64_net(net)) {
+        delete static_cast<DevNet<unsigned long long> *>(net);
+        return BSIM_OK;
+    }
     if (!bsim::valid(N(net))) { bsim::set_error("invalid network handle"); return BSIM_ERR_ARG; }
     delete N(net);
     return BSIM_OK;
 }
 
-int64_t bsim_network_ngs(void *net) { return bsim::valid(N(net)) ? N(net)->ngs : -1; }
+int64_t bsim_network_ngs(void *net)
+{
+    if (bsim::is_u64_net(net)) return static_cast<DevNet<unsigned long long> *>(net)->ngs;
+    return bsim::valid(N(net)) ? N(net)->ngs : -1;
+}
 
-#define CHECK2(b, n) do { int st__ = check(b, n); if (st__ != BSIM_OK) return st__; } while (0)
 #define NEED(p) do { if (!(p)) { bsim::set_error("null pointer argument: %s", #p); return BSIM_ERR_NULL; } } while (0)
 
 int bsim_hvec(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(src); NEED(dst);
-    return bsim::sigma(B(basis), N(net), src, nullptr, dst, false, stream);
+    return with_handles(basis, {net}, [&](auto *b) { return bsim::sigma(b, net_of(b, net), src, nullptr, dst, false, stream); });
 }
 
 int bsim_hvec_mixed(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(src); NEED(dst);
-    return bsim::sigma(B(basis), N(net), src, nullptr, dst, true, stream);
+    return with_handles(basis, {net}, [&](auto *b) { return bsim::sigma(b, net_of(b, net), src, nullptr, dst, true, stream); });
 }
 
 int bsim_hvec_f32in(void *basis, void *net, const float *src, double *dst, bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(src); NEED(dst);
-    return bsim::sigma(B(basis), N(net), nullptr, src, dst, true, stream);
+    return with_handles(basis, {net}, [&](auto *b) { return bsim::sigma(b, net_of(b, net), nullptr, src, dst, true, stream); });
 }
 
 int bsim_hvec_path(void *basis, void *net, char *why, int why_len, int *residual_groups)
 {
-    CHECK2(basis, net);
-    std::string w;
-    int nres = 0;
-    int r = bsim::fast_sigma_info(B(basis), N(net), &w, &nres);
-    if (r < 0) return r;
-    if (why && why_len > 0) snprintf(why, why_len, "%s", w.c_str());
-    if (residual_groups) *residual_groups = nres;
-    return r;
+    return with_handles(basis, {net}, [&](auto *b) -> int {
+        std::string w = "UInt64 strings: generic tile kernel";
+        int nres = 0, r = 0;
+        if constexpr (is_u32((decltype(b))nullptr)) {
+            r = bsim::fast_sigma_info(b, net_of(b, net), &w, &nres);
+            if (r < 0) return r;
+        }
+        if (why && why_len > 0) snprintf(why, why_len, "%s", w.c_str());
+        if (residual_groups) *residual_groups = nres;
+        return r;
+    });
 }
 
 int bsim_hvec_cols(void *basis, void *net, const double *src, double *dst, int64_t col_lo, int64_t col_hi,
                    int mixed, bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(src); NEED(dst);
-    return bsim::sigma_fast_cols(B(basis), N(net), src, dst, mixed != 0, col_lo, col_hi, stream);
+    return with_handles(basis, {net}, [&](auto *b) -> int {
+        if constexpr (is_u32((decltype(b))nullptr))
+            return bsim::sigma_fast_cols(b, net_of(b, net), src, dst, mixed != 0, col_lo, col_hi, stream);
+        bsim::set_error("column-band sigma needs the structured path (UInt32 strings)");
+        return BSIM_ERR_UNSUPPORTED;
+    });
 }
 
 int bsim_hvec_stage_times(void *basis, void *net, const double *src, double *dst, int mixed, double *ms_out,
                           int *launches_out, int nstages, bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(src); NEED(dst); NEED(ms_out); NEED(launches_out);
-    return bsim::sigma_fast_stages(B(basis), N(net), src, dst, mixed != 0, stream, ms_out, launches_out, nstages);
+    return with_handles(basis, {net}, [&](auto *b) -> int {
+        if constexpr (is_u32((decltype(b))nullptr))
+            return bsim::sigma_fast_stages(b, net_of(b, net), src, dst, mixed != 0, stream, ms_out, launches_out,
+                                           nstages);
+        bsim::set_error("stage timing covers the structured path (UInt32 strings)");
+        return BSIM_ERR_UNSUPPORTED;
+    });
 }
 
 int bsim_fma_peak(int fp64, double *tflops_out, bsim_stream_t stream)
@@ -275,82 +372,100 @@ int bsim_fma_peak(int fp64, double *tflops_out, bsim_stream_t stream)
     return bsim::fma_peak(fp64 != 0, tflops_out, stream);
 }
 
-int64_t bsim_hvec_num_tiles(void *basis) { return check(basis, nullptr) == BSIM_OK ? bsim::num_tiles(B(basis)) : -1; }
+int64_t bsim_hvec_num_tiles(void *basis)
+{
+    int64_t n = -1;
+    with_handles(basis, {}, [&](auto *b) { n = bsim::num_tiles(b); return BSIM_OK; });
+    return n;
+}
 
 int bsim_hvec_tiles(void *basis, void *net, const double *src, double *dst, int64_t tile_lo, int64_t tile_hi,
                     int mixed, bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(src); NEED(dst);
-    return bsim::sigma_tiles(B(basis), N(net), src, nullptr, dst, mixed != 0, tile_lo, tile_hi, stream);
+    return with_handles(basis, {net}, [&](auto *b) {
+        return bsim::sigma_tiles(b, net_of(b, net), src, nullptr, dst, mixed != 0, tile_lo, tile_hi, stream);
+    });
 }
 
 int bsim_diag(void *basis, void *net, double *diags, bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(diags);
-    return bsim::diag_elements(B(basis), N(net), diags, stream);
+    return with_handles(basis, {net}, [&](auto *b) { return bsim::diag_elements(b, net_of(b, net), diags, stream); });
 }
 
 int bsim_expm(void *basis, void *net, int64_t idx, double theta, double *vec, bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(vec);
-    return bsim::expm(B(basis), N(net), idx, theta, vec, stream);
+    return with_handles(basis, {net}, [&](auto *b) { return bsim::expm(b, net_of(b, net), idx, theta, vec, stream); });
 }
 
 int bsim_expm_seq(void *basis, void *net, int64_t n, const int64_t *idx, const double *theta, double *vec,
                   bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(vec);
     if (n > 0) { NEED(idx); NEED(theta); }
-    for (int64_t i = 0; i < n; ++i) {
-        int st = bsim::expm(B(basis), N(net), idx[i], theta[i], vec, stream);
-        if (st != BSIM_OK) return st;
-    }
-    return BSIM_OK;
+    return with_handles(basis, {net}, [&](auto *b) {
+        for (int64_t i = 0; i < n; ++i) {
+            int st = bsim::expm(b, net_of(b, net), idx[i], theta[i], vec, stream);
+            if (st != BSIM_OK) return st;
+        }
+        return (int)BSIM_OK;
+    });
 }
 
 int bsim_grad(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r,
               double *out_dev, bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(l); NEED(r); NEED(out_dev);
-    return bsim::grad(B(basis), N(net), idx, theta, l, r, out_dev, false, stream);
+    return with_handles(basis, {net}, [&](auto *b) {
+        return bsim::grad(b, net_of(b, net), idx, theta, l, r, out_dev, false, stream);
+    });
 }
 
 int bsim_backgrad(void *basis, void *net, int64_t idx, double theta, double *l, double *r, double *out_dev,
                   bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(l); NEED(r); NEED(out_dev);
-    return bsim::backgrad(B(basis), N(net), idx, theta, l, r, out_dev, false, stream);
+    return with_handles(basis, {net}, [&](auto *b) {
+        return bsim::backgrad(b, net_of(b, net), idx, theta, l, r, out_dev, false, stream);
+    });
 }
 
 int bsim_batchgrad(void *basis, void *net, const double *thetas, const double *l, const double *r, double *grads,
                    bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(thetas); NEED(l); NEED(r); NEED(grads);
-    return bsim::batchgrad(B(basis), N(net), thetas, l, r, grads, stream);
+    return with_handles(basis, {net}, [&](auto *b) {
+        return bsim::batchgrad(b, net_of(b, net), thetas, l, r, grads, stream);
+    });
 }
 
 int bsim_prepare_state(void *basis, void *pool, int64_t n_ops, const int64_t *op_idx, const int64_t *param_idx,
                        const double *thetas, const int64_t *ref_idx, const double *ref_val, int64_t n_ref,
                        double *vec, bsim_stream_t stream)
 {
-    CHECK2(basis, pool);
+    if (int st0 = check_handles(basis, {pool})) return st0;
     NEED(vec);
     if (n_ops > 0) { NEED(op_idx); NEED(param_idx); NEED(thetas); }
     if (n_ref > 0) { NEED(ref_idx); NEED(ref_val); }
-    for (int64_t i = 0; i < n_ops; ++i)
-        if (op_idx[i] < 0 || op_idx[i] >= N(pool)->ngs || param_idx[i] < 0) {
-            bsim::set_error("op_idx/param_idx[%lld] out of range", (long long)i);
-            return BSIM_ERR_ARG;
-        }
-    return bsim::prepare_state(B(basis), N(pool), n_ops, (const i64 *)op_idx, (const i64 *)param_idx, thetas,
-                               (const i64 *)ref_idx, ref_val, n_ref, vec, stream);
+    return with_handles(basis, {pool}, [&](auto *b) -> int {
+        auto *P = net_of(b, pool);
+        for (int64_t i = 0; i < n_ops; ++i)
+            if (op_idx[i] < 0 || op_idx[i] >= P->ngs || param_idx[i] < 0) {
+                bsim::set_error("op_idx/param_idx[%lld] out of range", (long long)i);
+                return BSIM_ERR_ARG;
+            }
+        return bsim::prepare_state(b, P, n_ops, (const i64 *)op_idx, (const i64 *)param_idx, thetas,
+                                   (const i64 *)ref_idx, ref_val, n_ref, vec, stream);
+    });
 }
 
 int bsim_vqe_energy_grad(void *basis, void *ham, void *pool, int64_t n_ops, const int64_t *op_idx,
@@ -358,27 +473,30 @@ int bsim_vqe_energy_grad(void *basis, void *ham, void *pool, int64_t n_ops, cons
                          const double *ref_val, int64_t n_ref, int64_t ckpt_every, double *lv, double *rv,
                          double *energy, double *variance, double *grad, bsim_stream_t stream)
 {
-    CHECK2(basis, ham);
-    CHECK2(basis, pool);
+    if (int st0 = check_handles(basis, {ham, pool})) return st0;
     NEED(lv); NEED(rv);
     if (n_ops > 0) { NEED(op_idx); NEED(param_idx); NEED(thetas); }
     if (n_ref > 0) { NEED(ref_idx); NEED(ref_val); }
-    return bsim::vqe_energy_grad(B(basis), N(ham), N(pool), n_ops, (const i64 *)op_idx, (const i64 *)param_idx,
-                                 n_params, thetas, (const i64 *)ref_idx, ref_val, n_ref, ckpt_every, lv, rv, energy,
-                                 variance, grad, stream);
+    return with_handles(basis, {ham, pool}, [&](auto *b) {
+        return bsim::vqe_energy_grad(b, net_of(b, ham), net_of(b, pool), n_ops, (const i64 *)op_idx,
+                                     (const i64 *)param_idx, n_params, thetas, (const i64 *)ref_idx, ref_val, n_ref,
+                                     ckpt_every, lv, rv, energy, variance, grad, stream);
+    });
 }
 
 int bsim_davidson(void *basis, void *net, double *v0, const double *diags, double tol, int maxiter, int ncv,
                   int maxspace, int mixed, double *x_out, double *energy, double *residual, int *iterations,
                   int *sigma_fp64, int *sigma_fp32, int verbose, bsim_stream_t stream)
 {
-    CHECK2(basis, net);
+    if (int st0 = check_handles(basis, {net})) return st0;
     NEED(v0); NEED(diags); NEED(x_out);
     bsim::DavStats st{};
-    int rc = mixed ? bsim::davidson_mixed(B(basis), N(net), v0, diags, tol, maxiter, maxspace, x_out, &st, verbose,
-                                          stream)
-                   : bsim::davidson_fp64(B(basis), N(net), v0, diags, tol, maxiter, ncv, maxspace, x_out, &st,
-                                         verbose, stream);
+    int rc = with_handles(basis, {net}, [&](auto *b) {
+        return mixed ? bsim::davidson_mixed(b, net_of(b, net), v0, diags, tol, maxiter, maxspace, x_out, &st, verbose,
+                                            stream)
+                     : bsim::davidson_fp64(b, net_of(b, net), v0, diags, tol, maxiter, ncv, maxspace, x_out, &st,
+                                           verbose, stream);
+    });
     if (rc == BSIM_OK) {
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) rc = bsim::cuda_status(e, "davidson");

@@ -52,9 +52,29 @@ struct BasisView {
     const int *blk_asym, *blk_bsym, *blk_na, *blk_nb, *blk_astart, *blk_bstart;
     const i64 *blk_off;
     const Ti *astrs, *bstrs;   // per-block string lists (alpha, beta)
-    const int *amap, *bmap;    // dense string -> index in its irrep list, or -1
+    const int *amap, *bmap;    // string -> index in its irrep list, or -1: indexed by the
+                               // string itself (dense) or by its colex rank (rank_maps)
     const int *block_map;      // [num_irreps^2] -> block or -1
+    int nel_a, nel_b, rank_maps;
+    const long long *binom;    // [65 x 65] binomials for the colex rank (rank_maps)
 };
+
+// Index of string s in its irrep's list (or -1 when s is not a string of the
+// basis).  Dense tables up to 2^26 entries; above that, the colex rank of s
+// among all strings with its electron count (Gosper order is colex order)
+// indexes a table of C(norb, n) entries.
+template <typename Ti>
+__device__ __forceinline__ int string_index(const BasisView<Ti> &B, const int *map, int nel, Ti s)
+{
+    const unsigned long long x = (unsigned long long)s;
+    if (B.norb < 64 && (x >> B.norb)) return -1;
+    if (!B.rank_maps) return map[x];
+    if (__popcll(x) != nel) return -1;
+    long long r = 0;
+    int i = 1;
+    for (unsigned long long y = x; y; y &= y - 1, ++i) r += B.binom[(__ffsll((long long)y) - 1) * 65 + i];
+    return map[r];
+}
 
 // One group of the OTF network (reference ham/otf.hpp:67-112).
 struct GroupDev {

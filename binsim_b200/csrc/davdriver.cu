@@ -364,5 +364,9 @@ template int davidson_fp64<unsigned>(const DevBasis<unsigned> *, const DevNet<un
                                      double, int, int, int, double *, DavStats *, int, cudaStream_t);
 template int davidson_mixed<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, double *, const double *,
                                       double, int, int, double *, DavStats *, int, cudaStream_t);
+template int davidson_fp64<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, double *, const double *,
+                                     double, int, int, int, double *, DavStats *, int, cudaStream_t);
+template int davidson_mixed<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, double *, const double *,
+                                      double, int, int, double *, DavStats *, int, cudaStream_t);
 
 }  // namespace bsim

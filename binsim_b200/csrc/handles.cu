@@ -147,8 +147,9 @@ int make_basis(i64 norb, i64 na, i64 nb, i64 total_sym, const i64 *orbsym, i64 n
 {
     if (!out || (!orbsym && norb > 0)) { set_error("null argument"); return BSIM_ERR_NULL; }
     *out = nullptr;
-    if (norb < 1 || norb > kMaxDenseMapOrb || norb > (i64)(8 * sizeof(Ti))) {
-        set_error("norb=%lld unsupported (1..%d for this string type)", norb, kMaxDenseMapOrb);
+    const i64 max_orb = sizeof(Ti) == 4 ? 32 : kMaxOrb64;
+    if (norb < 1 || norb > max_orb) {
+        set_error("norb=%lld unsupported (1..%lld for this string type)", norb, max_orb);
         return BSIM_ERR_UNSUPPORTED;
     }
     if (na < 0 || nb < 0 || na > norb || nb > norb || num_irreps < 1 || num_irreps > kMaxIrreps) {
@@ -186,6 +187,8 @@ int make_basis(i64 norb, i64 na, i64 nb, i64 total_sym, const i64 *orbsym, i64 n
     }
     B->num_blocks = (int)B->asym.size();
     B->dim = dim;
+    B->nel_a = (int)na;
+    B->nel_b = (int)nb;
     int st = B->upload();
     if (st != BSIM_OK) { delete B; return st; }
     *out = B;
@@ -200,18 +203,50 @@ int DevBasis<Ti>::upload()
         max_na = std::max(max_na, na[k]);
         max_nb = std::max(max_nb, nb[k]);
     }
-    const size_t map_n = size_t(1) << norb;
-    std::vector<int> amap(map_n, -1), bmap(map_n, -1);
-    // index of a string inside its irrep list (reference basis.hpp:271-285)
+    if (!astrs.empty()) nel_a = __builtin_popcountll((u64)astrs[0]);
+    if (!bstrs.empty()) nel_b = __builtin_popcountll((u64)bstrs[0]);
+    // index of a string inside its irrep list (reference basis.hpp:271-285): a
+    // dense table up to 2^26 strings (the reference's map), else a table over
+    // the colex rank of the string among all strings with its electron count
+    std::vector<long long> binom(65 * 65, 0);
+    for (int n = 0; n <= 64; ++n) {
+        binom[n * 65] = 1;
+        for (int k = 1; k <= n; ++k) {
+            const unsigned long long a = (unsigned long long)binom[(n - 1) * 65 + k - 1];
+            const unsigned long long b = k <= n - 1 ? (unsigned long long)binom[(n - 1) * 65 + k] : 0ull;
+            const unsigned long long c = a + b;
+            binom[n * 65 + k] = (c < a || c > 0x7fffffffffffffffull) ? 0x7fffffffffffffffll : (long long)c;
+        }
+    }
+    const bool ranked = norb > kMaxDenseMapOrb;
+    auto rank_of = [&](u64 x) {
+        long long r = 0;
+        int i = 1;
+        for (u64 y = x; y; y &= y - 1, ++i) r += binom[__builtin_ctzll(y) * 65 + i];
+        return r;
+    };
+    const size_t amap_n = ranked ? (size_t)binom[norb * 65 + nel_a] : size_t(1) << norb;
+    const size_t bmap_n = ranked ? (size_t)binom[norb * 65 + nel_b] : size_t(1) << norb;
+    if (amap_n > (size_t(1) << 30) || bmap_n > (size_t(1) << 30)) {
+        set_error("string index tables of %zu / %zu entries are too large", amap_n, bmap_n);
+        return BSIM_ERR_UNSUPPORTED;
+    }
+    std::vector<int> amap(amap_n, -1), bmap(bmap_n, -1);
     for (int k = 0; k < num_blocks; ++k) {
-        for (int a = 0; a < na[k]; ++a) amap[(size_t)astrs[astart[k] + a]] = a;
-        for (int b = 0; b < nb[k]; ++b) bmap[(size_t)bstrs[bstart[k] + b]] = b;
+        for (int a = 0; a < na[k]; ++a) {
+            const u64 x = (u64)astrs[astart[k] + a];
+            amap[ranked ? (size_t)rank_of(x) : (size_t)x] = a;
+        }
+        for (int b = 0; b < nb[k]; ++b) {
+            const u64 x = (u64)bstrs[bstart[k] + b];
+            bmap[ranked ? (size_t)rank_of(x) : (size_t)x] = b;
+        }
     }
     const int nbk = std::max(1, num_blocks);
     size_t bytes = 7 * al(nbk * sizeof(int)) + al(nbk * sizeof(i64)) +
                    al(std::max<size_t>(1, astrs.size()) * sizeof(Ti)) +
-                   al(std::max<size_t>(1, bstrs.size()) * sizeof(Ti)) + 2 * al(map_n * sizeof(int)) +
-                   al(block_map.size() * sizeof(int));
+                   al(std::max<size_t>(1, bstrs.size()) * sizeof(Ti)) + al(amap_n * sizeof(int)) +
+                   al(bmap_n * sizeof(int)) + al(block_map.size() * sizeof(int)) + al(binom.size() * 8);
     int st = arena.reserve(bytes);
     if (st != BSIM_OK) return st;
     auto put = [&](auto *dst, const auto &src) {
@@ -228,13 +263,14 @@ int DevBasis<Ti>::upload()
     i64 *d_off = put(arena.take<i64>(nbk), off);
     Ti *d_astrs = put(arena.take<Ti>(std::max<size_t>(1, astrs.size())), astrs);
     Ti *d_bstrs = put(arena.take<Ti>(std::max<size_t>(1, bstrs.size())), bstrs);
-    int *d_amap = put(arena.take<int>(map_n), amap);
-    int *d_bmap = put(arena.take<int>(map_n), bmap);
+    int *d_amap = put(arena.take<int>(amap_n), amap);
+    int *d_bmap = put(arena.take<int>(bmap_n), bmap);
     int *d_bm = put(arena.take<int>(block_map.size()), block_map);
+    long long *d_binom = put(arena.take<long long>(binom.size()), binom);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_status(e, "basis upload");
     view = BasisView<Ti>{num_blocks, num_irreps, norb, dim, d_asym, d_bsym, d_na, d_nb, d_as, d_bs,
-                         d_off, d_astrs, d_bstrs, d_amap, d_bmap, d_bm};
+                         d_off, d_astrs, d_bstrs, d_amap, d_bmap, d_bm, nel_a, nel_b, ranked ? 1 : 0, d_binom};
     return BSIM_OK;
 }
 
@@ -472,5 +508,12 @@ template int make_network<unsigned>(const i64 *, i64, i64, const unsigned *, con
                                     const double *, const double *, DevNet<unsigned> **);
 template struct DevBasis<unsigned>;
 template struct DevNet<unsigned>;
+template int make_basis<unsigned long long>(i64, i64, i64, i64, const i64 *, i64, DevBasis<unsigned long long> **);
+template int make_network<unsigned long long>(const i64 *, i64, i64, const unsigned long long *,
+                                              const unsigned long long *, const i64 *, const i64 *, const i64 *,
+                                              const unsigned long long *, const unsigned long long *, const double *,
+                                              const double *, DevNet<unsigned long long> **);
+template struct DevBasis<unsigned long long>;
+template struct DevNet<unsigned long long>;
 
 }  // namespace bsim

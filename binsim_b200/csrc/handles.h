@@ -8,9 +8,19 @@
 
 namespace bsim {
 
-constexpr unsigned kBasisMagic = 0xB5B1A515u;
-constexpr unsigned kNetMagic = 0xB5B1E7A1u;
-constexpr int kMaxDenseMapOrb = 26;   // dense string->index tables up to 2^26 entries
+// Magic words per string type: UInt32 handles (the reference's GPU library's
+// type) and UInt64 handles (up to 63 spatial orbitals).
+template <typename Ti> struct HandleMagic;
+template <> struct HandleMagic<unsigned> {
+    static constexpr unsigned basis = 0xB5B1A515u, net = 0xB5B1E7A1u;
+};
+template <> struct HandleMagic<unsigned long long> {
+    static constexpr unsigned basis = 0xB5B1A564u, net = 0xB5B1E764u;
+};
+constexpr unsigned kBasisMagic = HandleMagic<unsigned>::basis;
+constexpr unsigned kNetMagic = HandleMagic<unsigned>::net;
+constexpr int kMaxDenseMapOrb = 26;   // dense string->index tables up to 2^26 entries; ranked above
+constexpr int kMaxOrb64 = 63;         // UInt64 strings (Gosper enumeration needs one spare bit)
 
 // Device arena: one allocation carved into aligned pieces.
 struct Arena {
@@ -47,8 +57,9 @@ struct Workspace {
 
 template <typename Ti>
 struct DevBasis {
-    unsigned magic = kBasisMagic;
+    unsigned magic = HandleMagic<Ti>::basis;
     int norb = 0, num_irreps = 0, num_blocks = 0;
+    int nel_a = 0, nel_b = 0;
     i64 dim = 0, total_sym = 0;
     int max_na = 0, max_nb = 0;
     // host mirrors
@@ -68,7 +79,7 @@ struct DevBasis {
 
 template <typename Ti>
 struct DevNet {
-    unsigned magic = kNetMagic;
+    unsigned magic = HandleMagic<Ti>::net;
     int norb = 0;
     i64 ngs = 0;
     std::vector<GroupDev> groups;        // original order
@@ -123,8 +134,11 @@ int basis_from_ref_handle(const void *host_basis, DevBasis<unsigned> **out);
 int network_from_ref_handle(const void *host_net, DevNet<unsigned> **out);
 
 template <typename Ti>
-inline bool valid(const DevBasis<Ti> *b) { return b && b->magic == kBasisMagic; }
+inline bool valid(const DevBasis<Ti> *b) { return b && b->magic == HandleMagic<Ti>::basis; }
 template <typename Ti>
-inline bool valid(const DevNet<Ti> *n) { return n && n->magic == kNetMagic; }
+inline bool valid(const DevNet<Ti> *n) { return n && n->magic == HandleMagic<Ti>::net; }
+// The first word of a handle tells its string type.
+inline bool is_u64_basis(const void *h) { return h && *static_cast<const unsigned *>(h) == HandleMagic<unsigned long long>::basis; }
+inline bool is_u64_net(const void *h) { return h && *static_cast<const unsigned *>(h) == HandleMagic<unsigned long long>::net; }
 
 }  // namespace bsim

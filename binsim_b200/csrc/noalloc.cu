@@ -72,16 +72,24 @@ int grad_noalloc(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double th
 
 template int grad_noalloc<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, double,
                                     const double *, const double *, double *, cudaStream_t);
+template int grad_noalloc<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, i64, double,
+                                    const double *, const double *, double *, cudaStream_t);
 
 }  // namespace bsim
 
 extern "C" int bsim_grad_noalloc(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r,
                                  double *out_dev, bsim_stream_t stream)
 {
+    if (!l || !r || !out_dev) { bsim::set_error("null vector or output pointer"); return bsim::BSIM_ERR_NULL; }
+    if (bsim::is_u64_basis(basis)) {   // UInt64 strings
+        auto *b = static_cast<bsim::DevBasis<unsigned long long> *>(basis);
+        auto *n = static_cast<bsim::DevNet<unsigned long long> *>(net);
+        if (!bsim::valid(n)) { bsim::set_error("invalid network handle"); return bsim::BSIM_ERR_ARG; }
+        return bsim::grad_noalloc(b, n, idx, theta, l, r, out_dev, stream);
+    }
     auto *b = static_cast<bsim::DevBasis<unsigned> *>(basis);
     auto *n = static_cast<bsim::DevNet<unsigned> *>(net);
     if (!bsim::valid(b)) { bsim::set_error("invalid basis handle"); return bsim::BSIM_ERR_ARG; }
     if (!bsim::valid(n)) { bsim::set_error("invalid network handle"); return bsim::BSIM_ERR_ARG; }
-    if (!l || !r || !out_dev) { bsim::set_error("null vector or output pointer"); return bsim::BSIM_ERR_NULL; }
     return bsim::grad_noalloc(b, n, idx, theta, l, r, out_dev, stream);
 }

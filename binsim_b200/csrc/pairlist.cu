@@ -325,8 +325,16 @@ int pair_list_launch(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, PairA
     template int pair_list_launch<unsigned, OP>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64,     \
                                                 PairAngles, double *, double *, double *, unsigned long long *, \
                                                 i64, double *, bool, cudaStream_t, bool *);
+#define PAIR_LIST_INST64(OP)                                                                                 \
+    template int pair_list_launch<unsigned long long, OP>(const DevBasis<unsigned long long> *,                 \
+                                                          const DevNet<unsigned long long> *, i64, PairAngles,  \
+                                                          double *, double *, double *, unsigned long long *,   \
+                                                          i64, double *, bool, cudaStream_t, bool *);
 PAIR_LIST_INST(kPairExpm)
 PAIR_LIST_INST(kPairGrad)
 PAIR_LIST_INST(kPairBackgrad)
+PAIR_LIST_INST64(kPairExpm)
+PAIR_LIST_INST64(kPairGrad)
+PAIR_LIST_INST64(kPairBackgrad)
 
 }  // namespace bsim

@@ -45,7 +45,7 @@ pair_row_kernel(const BasisView<Ti> B, const NetView<Ti> N, int gid, PairAngles 
     }
     if (active) {
         s_a = B.astrs[B.blk_astart[kd] + a] ^ (Ti)g.ax;
-        sa = g.ax ? (((u64)s_a >> B.norb) ? -1 : B.amap[s_a]) : a;
+        sa = g.ax ? string_index(B, B.amap, B.nel_a, s_a) : a;
         active = sa >= 0 && !(ks == kd && g.type != 2 && sa < a);
     }
     double acc = 0.0;
@@ -71,7 +71,7 @@ pair_row_kernel(const BasisView<Ti> B, const NetView<Ti> N, int gid, PairAngles 
         const double *wb = N.w + g.wb_off;
         for (int b = threadIdx.x; b < nb; b += blockDim.x) {
             const Ti s_b = bstrs[b] ^ (Ti)g.bx;
-            const int sb = g.bx ? (((u64)s_b >> B.norb) ? -1 : B.bmap[s_b]) : b;
+            const int sb = g.bx ? string_index(B, B.bmap, B.nel_b, s_b) : b;
             if (sb < 0 || (same && g.type == 2 && sb < b)) continue;
             double vt = 0.0;
             for (int rr = 0; rr < R; ++rr) {
@@ -226,6 +226,11 @@ template int expm<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *
 template int grad<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, double, const double *,
                             const double *, double *, bool, cudaStream_t, double *, size_t);
 template int backgrad<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, double, double *, double *,
+                                double *, bool, cudaStream_t);
+template int expm<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, i64, double, double *, cudaStream_t);
+template int grad<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, i64, double, const double *,
+                            const double *, double *, bool, cudaStream_t, double *, size_t);
+template int backgrad<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, i64, double, double *, double *,
                                 double *, bool, cudaStream_t);
 
 }  // namespace bsim

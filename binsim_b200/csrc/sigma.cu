@@ -221,11 +221,13 @@ int sigma(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const f
         const char *e = getenv("BSIM_SIGMA_GENERIC");
         return e && e[0] == '1';
     }();
-    if (!force_generic && B->dim > 0) {
-        bool used = false;
-        int st = sigma_fast(B, N, src, src32, dst, mixed, s, &used);
-        if (st != BSIM_OK) return st;
-        if (used) return BSIM_OK;
+    if constexpr (sizeof(Ti) == 4) {   // the structured path addresses strings of up to 24 orbitals
+        if (!force_generic && B->dim > 0) {
+            bool used = false;
+            int st = sigma_fast(B, N, src, src32, dst, mixed, s, &used);
+            if (st != BSIM_OK) return st;
+            if (used) return BSIM_OK;
+        }
     }
     return sigma_tiles(B, N, src, src32, dst, mixed, 0, num_tiles(B), s);
 }
@@ -254,5 +256,15 @@ template int sigma_generic_accumulate<unsigned>(const DevBasis<unsigned> *, cons
                                                 const int4 *, int, const double *, const float *, double *, bool,
                                                 cudaStream_t);
 template int diag_elements<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, double *, cudaStream_t);
+template int tile_prefix<unsigned long long>(const DevBasis<unsigned long long> *, Workspace &, const i64 **, i64 *);
+template int sigma<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, const double *, const float *,
+                             double *, bool, cudaStream_t);
+template int sigma_tiles<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, const double *,
+                                   const float *, double *, bool, i64, i64, cudaStream_t);
+template i64 num_tiles<unsigned long long>(const DevBasis<unsigned long long> *);
+template int sigma_generic_accumulate<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, const int *,
+                                                const int4 *, int, const double *, const float *, double *, bool,
+                                                cudaStream_t);
+template int diag_elements<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, double *, cudaStream_t);
 
 }  // namespace bsim

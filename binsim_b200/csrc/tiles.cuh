@@ -80,7 +80,7 @@ __device__ __forceinline__ void fill_chunk(const BasisView<Ti> &B, const NetView
         const int b = c.tb * kTile + j;
         if (ks >= 0 && b < c.nb) {
             const Ti s = B.bstrs[B.blk_bstart[c.k] + b] ^ (Ti)gd.bx;
-            sc = gd.bx ? (((u64)s >> B.norb) ? -1 : B.bmap[s]) : b;
+            sc = gd.bx ? string_index(B, B.bmap, B.nel_b, s) : b;
             if (ONCE && same && gd.type == 2 && sc >= 0 && sc < b) sc = -1;
             if (sc >= 0) {
                 const Ti *z = N.z + gd.zb_off;
@@ -100,7 +100,7 @@ __device__ __forceinline__ void fill_chunk(const BasisView<Ti> &B, const NetView
         const int a = c.ta * kTile + j;
         if (ks >= 0 && a < c.na) {
             const Ti s = B.astrs[B.blk_astart[c.k] + a] ^ (Ti)gd.ax;
-            int sa = gd.ax ? (((u64)s >> B.norb) ? -1 : B.amap[s]) : a;
+            int sa = gd.ax ? string_index(B, B.amap, B.nel_a, s) : a;
             if (ONCE && same && (gd.type == 1 || gd.type == 3) && sa >= 0 && sa < a) sa = -1;
             if (sa >= 0) {
                 row = B.blk_off[ks] + (i64)sa * B.blk_nb[ks];

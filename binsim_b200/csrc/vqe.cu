@@ -139,5 +139,12 @@ template int vqe_energy_grad<unsigned>(const DevBasis<unsigned> *, const DevNet<
                                        const DevNet<unsigned> *, i64, const i64 *, const i64 *, i64, const double *,
                                        const i64 *, const double *, i64, i64, double *, double *, double *, double *,
                                        double *, cudaStream_t);
+template int prepare_state<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, i64, const i64 *,
+                                     const i64 *, const double *, const i64 *, const double *, i64, double *,
+                                     cudaStream_t);
+template int vqe_energy_grad<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *,
+                                       const DevNet<unsigned long long> *, i64, const i64 *, const i64 *, i64, const double *,
+                                       const i64 *, const double *, i64, i64, double *, double *, double *, double *,
+                                       double *, cudaStream_t);
 
 }  // namespace bsim

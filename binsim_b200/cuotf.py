@@ -64,6 +64,8 @@ def lib() -> C.CDLL:
         # part 2
         "bsim_last_error": (C.c_char_p, []), "bsim_version": (C.c_char_p, []),
         "bsim_basis_create_u32": (ci, [i64, i64, i64, i64, vp, i64, vp]),
+        "bsim_basis_create_u64": (ci, [i64, i64, i64, i64, vp, i64, vp]),
+        "bsim_network_create_u64": (ci, [vp, i64, i64] + [vp] * 9 + [vp]),
         "bsim_basis_from_host": (ci, [vp, vp]), "bsim_basis_destroy": (ci, [vp]),
         "bsim_basis_dim": (i64, [vp]), "bsim_basis_find_det": (i64, [vp, C.c_uint64, C.c_uint64]),
         "bsim_network_create_u32": (ci, [vp, i64, i64] + [vp] * 9 + [vp]),
@@ -138,15 +140,23 @@ class CuBasis:
     """Device determinant space (``BasisManager`` + ``upload_basis``)."""
 
     def __init__(self, norb: int, na: int, nb: int, orbsym=None, total_sym: int = 0, num_irreps: int = 16,
-                 host_handle: Optional[int] = None):
+                 host_handle: Optional[int] = None, string_bits: Optional[int] = None):
+        """string_bits: 32 (UInt32 strings, the reference GPU library's type) or 64
+        (UInt64, up to 63 orbitals); default 32 up to 32 orbitals, else 64."""
         L = lib()
         out = vp()
+        self.string_bits = 32
         if host_handle is not None:
             _check(L.bsim_basis_from_host(host_handle, C.byref(out)), "bsim_basis_from_host")
         else:
+            bits = string_bits or (32 if norb <= 32 else 64)
+            if bits not in (32, 64):
+                raise ValueError("string_bits must be 32 or 64")
+            self.string_bits = bits
             self._orbsym = _host(np.zeros(norb) if orbsym is None else orbsym, np.int64)
-            _check(L.bsim_basis_create_u32(norb, na, nb, total_sym, self._orbsym.ctypes.data, num_irreps,
-                                           C.byref(out)), "bsim_basis_create_u32")
+            create = L.bsim_basis_create_u32 if bits == 32 else L.bsim_basis_create_u64
+            _check(create(norb, na, nb, total_sym, self._orbsym.ctypes.data, num_irreps, C.byref(out)),
+                   f"bsim_basis_create_u{bits}")
         self.h = out.value
         self.norb, self.nelec = norb, (na, nb)
         self.dim = L.bsim_basis_dim(self.h)
@@ -174,20 +184,28 @@ class CuBasis:
 class CuNetwork:
     """Device OTF network (``Network_OTF`` + ``upload_network``)."""
 
-    def __init__(self, net: Optional[nw.OTFNetwork] = None, host_handle: Optional[int] = None):
+    def __init__(self, net: Optional[nw.OTFNetwork] = None, host_handle: Optional[int] = None,
+                 string_bits: Optional[int] = None):
+        """string_bits must match the basis the network is used with (default: 32
+        up to 32 orbitals, else 64)."""
         L = lib()
         out = vp()
         if host_handle is not None:
             _check(L.bsim_network_from_host(host_handle, C.byref(out)), "bsim_network_from_host")
         else:
-            a = net.as_uint32()
+            bits = string_bits or (32 if net.norb <= 32 else 64)
+            if bits == 32:
+                a = net.as_uint32()
+            else:
+                a = {k: _host(getattr(net, k), np.uint64) for k in ("axs", "bxs", "flat_zas", "flat_zbs")}
             self._keep = [
                 _host(net.orbsym, np.int64), a["axs"], a["bxs"], _host(net.ranks, np.int64),
                 _host(net.num_zas, np.int64), _host(net.num_zbs, np.int64), a["flat_zas"], a["flat_zbs"],
                 _host(net.flat_wa, np.float64), _host(net.flat_wb, np.float64)]
             k = self._keep
-            _check(L.bsim_network_create_u32(k[0].ctypes.data, net.norb, net.ngs, *[x.ctypes.data for x in k[1:]],
-                                             C.byref(out)), "bsim_network_create_u32")
+            create = L.bsim_network_create_u32 if bits == 32 else L.bsim_network_create_u64
+            _check(create(k[0].ctypes.data, net.norb, net.ngs, *[x.ctypes.data for x in k[1:]], C.byref(out)),
+                   f"bsim_network_create_u{bits}")
         self.h = out.value
         self.ngs = L.bsim_network_ngs(self.h)
 

@@ -90,6 +90,14 @@ const char *bsim_version(void);
 /* Basis: create_basis_manager's arguments (basis/declare.hpp:24-33). */
 int bsim_basis_create_u32(int64_t norb, int64_t na, int64_t nb, int64_t total_sym, const int64_t *orbsym,
                           int64_t num_irreps, void **out);
+/* UInt64 strings (up to 63 spatial orbitals), the string type of the reference's
+ * _ui64_f64 operator exports (src/extern/otf_native.cpp:5; jl/network.jl binds
+ * build_network_otf_ui64_f64).  Above 26 orbitals a string is addressed by its
+ * colex rank instead of a dense 2^norb table (basis.hpp:271 overflows there).
+ * Every entry point taking a basis handle accepts either string type; its
+ * networks must have the same type. */
+int bsim_basis_create_u64(int64_t norb, int64_t na, int64_t nb, int64_t total_sym, const int64_t *orbsym,
+                          int64_t num_irreps, void **out);
 /* Basis from the reference's host BasisManager<uint32>* (as build_basisdev_f64). */
 int bsim_basis_from_host(void *host_basis, void **out);
 int bsim_basis_destroy(void *basis);
@@ -103,6 +111,11 @@ int64_t bsim_basis_find_det(void *basis, uint64_t astr, uint64_t bstr);
 int bsim_network_create_u32(const int64_t *orbsym, int64_t norb, int64_t ngs, const uint32_t *axs,
                             const uint32_t *bxs, const int64_t *ranks, const int64_t *num_zas,
                             const int64_t *num_zbs, const uint32_t *flat_zas, const uint32_t *flat_zbs,
+                            const double *flat_wa, const double *flat_wb, void **out);
+/* build_network_otf_ui64_f64's arguments (otf_native.cpp:5, op/declare.hpp:25-35). */
+int bsim_network_create_u64(const int64_t *orbsym, int64_t norb, int64_t ngs, const uint64_t *axs,
+                            const uint64_t *bxs, const int64_t *ranks, const int64_t *num_zas,
+                            const int64_t *num_zbs, const uint64_t *flat_zas, const uint64_t *flat_zbs,
                             const double *flat_wa, const double *flat_wb, void **out);
 /* Network from the reference's host Network_OTF<uint32,double>*. */
 int bsim_network_from_host(void *host_net, void **out);

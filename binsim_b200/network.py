@@ -56,12 +56,15 @@ def popcount_u64(x: np.ndarray) -> np.ndarray:
     return ((x * U64(0x0101010101010101)) >> U64(56)).astype(np.int64)
 
 
-def _deinterleave(mask: np.ndarray, nbits: int, odd: bool) -> np.ndarray:
-    """Take every second bit (even positions, or odd ones) and pack them."""
-    out = np.zeros_like(mask, dtype=np.uint64)
+def _deinterleave(mask, nbits: int, odd: bool) -> np.ndarray:
+    """Take every second bit (even positions, or odd ones) and pack them; mask is a
+    uint64 array or a list of uint64 words (bit 64w + i in word w)."""
+    words = mask if isinstance(mask, list) else [mask]
+    out = np.zeros_like(words[0], dtype=np.uint64)
     off = 1 if odd else 0
     for p in range(nbits):
-        out |= ((mask >> U64(2 * p + off)) & U64(1)) << U64(p)
+        bit = 2 * p + off
+        out |= ((words[bit // 64] >> U64(bit % 64)) & U64(1)) << U64(p)
     return out
 
 
@@ -95,39 +98,84 @@ def synthetic_integrals(norb: int, seed: int = 0, nchol: int = 24):
 # Jordan-Wigner over interleaved spin orbitals
 # ---------------------------------------------------------------------------
 
-def _ladder_components(modes: np.ndarray, dagger: Sequence[bool]):
+def _ladder_components(modes: np.ndarray, dagger: Sequence[bool], words: int = 1):
     """Pauli expansion of a product of ladder operators, vectorised over rows.
 
     ``modes`` is (n_terms, k) spin-orbital indices; ``dagger[i]`` tells whether
     factor i is a creation operator.  Each factor is
     ``1/2 X_j Z^{below j} (+/-) 1/2 X_j Z^{below j | j}`` (+ for creation).
     Returns (x, z, sign) arrays of shape (n_terms, 2**k); the common factor
-    2**-k is left to the caller.
+    2**-k is left to the caller.  With ``words`` > 1 the masks span
+    64 * words spin orbitals (the reference's UInt128 interleaved masks for
+    more than 32 spatial orbitals) and x, z are lists of per-word arrays,
+    word w holding spin orbitals 64w..64w+63.
     """
     n, k = modes.shape
-    x = np.zeros((n, 1), dtype=np.uint64)
-    z = np.zeros((n, 1), dtype=np.uint64)
+    if words == 1:
+        x = np.zeros((n, 1), dtype=np.uint64)
+        z = np.zeros((n, 1), dtype=np.uint64)
+        s = np.ones((n, 1), dtype=np.int64)
+        for i in range(k):
+            j = modes[:, i].astype(np.uint64)
+            e = (U64(1) << j)[:, None]
+            m = e - U64(1)
+            comps = [(m, 1), (m | e, 1 if dagger[i] else -1)]
+            xs, zs, ss = [], [], []
+            for zc, sc in comps:
+                # (x, z) * (e, zc): sign (-1)^popc(z & e)
+                flip = 1 - 2 * (popcount_u64(z & e) & 1)
+                xs.append(x ^ e)
+                zs.append(z ^ zc)
+                ss.append(s * flip * sc)
+            x = np.concatenate(xs, axis=1)
+            z = np.concatenate(zs, axis=1)
+            s = np.concatenate(ss, axis=1)
+        return x, z, s
+    x = [np.zeros((n, 1), dtype=np.uint64) for _ in range(words)]
+    z = [np.zeros((n, 1), dtype=np.uint64) for _ in range(words)]
     s = np.ones((n, 1), dtype=np.int64)
+    full = U64(0xFFFFFFFFFFFFFFFF)
     for i in range(k):
-        j = modes[:, i].astype(np.uint64)
-        e = (U64(1) << j)[:, None]
-        m = e - U64(1)
-        comps = [(m, 1), (m | e, 1 if dagger[i] else -1)]
-        xs, zs, ss = [], [], []
+        j = modes[:, i].astype(np.int64)
+        wj, bj = j // 64, (j % 64).astype(np.uint64)
+        e = [np.where(wj == w, U64(1) << bj, U64(0))[:, None] for w in range(words)]
+        m = [np.where(w < wj, full, np.where(wj == w, (U64(1) << bj) - U64(1), U64(0)))[:, None]
+             for w in range(words)]
+        comps = [(m, 1), ([m[w] | e[w] for w in range(words)], 1 if dagger[i] else -1)]
+        xs, zs, ss = [[] for _ in range(words)], [[] for _ in range(words)], []
         for zc, sc in comps:
-            # (x, z) * (e, zc): sign (-1)^popc(z & e)
-            flip = 1 - 2 * (popcount_u64(z & e) & 1)
-            xs.append(x ^ e)
-            zs.append(z ^ zc)
+            bit = np.zeros_like(s)
+            for w in range(words):
+                bit = bit + ((z[w] & e[w]) != 0)
+            flip = 1 - 2 * (bit & 1)
+            for w in range(words):
+                xs[w].append(x[w] ^ e[w])
+                zs[w].append(z[w] ^ zc[w])
             ss.append(s * flip * sc)
-        x = np.concatenate(xs, axis=1)
-        z = np.concatenate(zs, axis=1)
+        x = [np.concatenate(xs[w], axis=1) for w in range(words)]
+        z = [np.concatenate(zs[w], axis=1) for w in range(words)]
         s = np.concatenate(ss, axis=1)
     return x, z, s
 
 
 def _combine_terms(x, z, c, tol):
-    """Sum coefficients of equal (x, z) and drop |c| <= tol; sorted by (x, z)."""
+    """Sum coefficients of equal (x, z) and drop |c| <= tol; sorted by (x, z).
+    x, z are uint64 arrays, or lists of per-word arrays (highest word most
+    significant) for masks wider than 64 spin orbitals."""
+    if isinstance(x, list):
+        keys = tuple(z) + tuple(x)          # lexsort: last key primary -> x high word first
+        order = np.lexsort(keys)
+        x = [w[order] for w in x]
+        z = [w[order] for w in z]
+        c = c[order]
+        diff = np.zeros(max(len(c) - 1, 0), dtype=bool)
+        for w in x + z:
+            diff |= np.diff(w) != 0
+        brk = np.flatnonzero(diff) + 1
+        starts = np.r_[0, brk].astype(np.int64)
+        cs = np.add.reduceat(c, starts) if len(c) else c
+        keep = np.abs(cs) > tol
+        return [w[starts][keep] for w in x], [w[starts][keep] for w in z], cs[keep]
     order = np.lexsort((z, x))
     x, z, c = x[order], z[order], c[order]
     brk = np.flatnonzero((np.diff(x) != 0) | (np.diff(z) != 0)) + 1
@@ -141,21 +189,31 @@ def _combine_terms(x, z, c, tol):
 def jw_hamiltonian_terms(h, g, e_nuc: float = 0.0, tol: float = 1e-12):
     """Jordan-Wigner Pauli terms (x, z, c) of the spin-orbital Hamiltonian.
 
-    Spin orbitals are interleaved (alpha p -> 2p, beta p -> 2p+1).  Requires
-    2*norb <= 64.  Terms are summed, filtered at ``tol`` and sorted by
-    (x, z) as the reference does (``ham.hpp:18-31``, stage 4 sort).
+    Spin orbitals are interleaved (alpha p -> 2p, beta p -> 2p+1), restating
+    the operator of the reference's ham.hpp:402-450; terms are summed, filtered
+    at ``tol`` and sorted by (x, z) as the reference does (``ham.hpp:18-31``,
+    stage 4 sort).  Up to 32 spatial orbitals x and z are uint64 arrays; above
+    that (the reference's UInt128 masks, ham_real.cpp:4) they are lists of two
+    uint64 word arrays, and the two-body terms are combined chunk by chunk.
     """
     norb = h.shape[0]
-    if 2 * norb > 64:
-        raise ValueError("jw_hamiltonian_terms supports at most 32 spatial orbitals")
+    if 2 * norb > 128:
+        raise ValueError("jw_hamiltonian_terms supports at most 64 spatial orbitals")
+    words = 1 if 2 * norb <= 64 else 2
     xs, zs, cs = [], [], []
+
+    def add(x, z, c):
+        if words == 1:
+            xs.append(x.ravel()); zs.append(z.ravel()); cs.append(c.ravel())
+        else:   # combine each chunk at once to bound memory
+            cx, cz, cc = _combine_terms([w.ravel() for w in x], [w.ravel() for w in z], c.ravel(), 0.0)
+            xs.append(cx); zs.append(cz); cs.append(cc)
     # one-body: h_pq a+_{p s} a_{q s}
     p, q = np.nonzero(np.abs(h) > tol)
     for sp in (0, 1):
         modes = np.stack([2 * p + sp, 2 * q + sp], axis=1)
-        x, z, s = _ladder_components(modes, (True, False))
-        xs.append(x.ravel()); zs.append(z.ravel())
-        cs.append((s * (h[p, q] * 0.25)[:, None]).ravel())
+        x, z, sgn = _ladder_components(modes, (True, False), words)
+        add(x, z, sgn * (h[p, q] * 0.25)[:, None])
     # two-body: 1/2 g_pqrs a+_{p s} a+_{q t} a_{r t} a_{s s}
     idx = np.nonzero(np.abs(g) > tol)
     vals = g[idx] * 0.5
@@ -165,18 +223,25 @@ def jw_hamiltonian_terms(h, g, e_nuc: float = 0.0, tol: float = 1e-12):
         # chunk to bound memory
         for lo in range(0, len(vals), 1 << 18):
             hi = min(len(vals), lo + (1 << 18))
-            x, z, s = _ladder_components(modes[lo:hi], (True, True, False, False))
-            xs.append(x.ravel()); zs.append(z.ravel())
-            cs.append((s * (vals[lo:hi] * 0.0625)[:, None]).ravel())
+            x, z, sgn = _ladder_components(modes[lo:hi], (True, True, False, False), words)
+            add(x, z, sgn * (vals[lo:hi] * 0.0625)[:, None])
     if abs(e_nuc) > tol:
-        xs.append(np.zeros(1, np.uint64)); zs.append(np.zeros(1, np.uint64))
+        if words == 1:
+            xs.append(np.zeros(1, np.uint64)); zs.append(np.zeros(1, np.uint64))
+        else:
+            xs.append([np.zeros(1, np.uint64)] * 2); zs.append([np.zeros(1, np.uint64)] * 2)
         cs.append(np.array([e_nuc]))
-    x = np.concatenate(xs); z = np.concatenate(zs); c = np.concatenate(cs).astype(np.float64)
-    return _combine_terms(x, z, c, tol)
+    if words == 1:
+        x = np.concatenate(xs); z = np.concatenate(zs); c = np.concatenate(cs).astype(np.float64)
+        return _combine_terms(x, z, c, tol)
+    x = [np.concatenate([t[w] for t in xs]) for w in range(2)]
+    z = [np.concatenate([t[w] for t in zs]) for w in range(2)]
+    return _combine_terms(x, z, np.concatenate(cs).astype(np.float64), tol)
 
 
 def split_aabb(x, z, norb):
-    """De-interleave Pauli masks into alpha and beta halves (``ham.hpp:520-551``)."""
+    """De-interleave Pauli masks into alpha and beta halves (``ham.hpp:520-551``);
+    x, z may be uint64 arrays or lists of words (spin orbital 64w + i in word w)."""
     return (_deinterleave(x, norb, False), _deinterleave(z, norb, False),
             _deinterleave(x, norb, True), _deinterleave(z, norb, True))
 
@@ -238,9 +303,15 @@ def compress_groups(ax, az, bx, bz, c, norb, tol=1e-12, orbsym=None) -> OTFNetwo
     key_change = np.flatnonzero((np.diff(ax) != 0) | (np.diff(bx) != 0)) + 1
     starts = np.r_[0, key_change].astype(np.int64) if n else np.zeros(0, np.int64)
     ends = np.r_[key_change, n].astype(np.int64) if n else np.zeros(0, np.int64)
+    return _compress_runs(ax, az, bx, bz, c, starts, ends, norb, tol, orbsym)
+
+
+def _compress_runs(ax, az, bx, bz, c, starts, ends, norb, tol=1e-12, orbsym=None) -> OTFNetwork:
+    """One group per run [starts[i], ends[i]) of terms: the run's Z coefficient
+    matrix M[za, zb] compressed by SVD (rank = singular values > tol, wa = U sqrt(S),
+    wb = V sqrt(S), entries below 1e-12 zeroed), SVDs batched by matrix shape."""
     ngs = len(starts)
     groups = [None] * ngs
-    # batch SVDs by matrix shape
     shapes = {}
     for gi, (i, j) in enumerate(zip(starts, ends)):
         ua = np.unique(az[i:j]); ub = np.unique(bz[i:j])
@@ -345,18 +416,16 @@ def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None
     Vanishing components (t = t^dagger) are dropped.  A spin-adapted generator
     applies its components in list order with a shared angle.
     """
-    comps = []          # (ax, az, bx, bz, C)
-    comp_index = {}
+    keys = []            # unique (cre, ann) spin-orbital components, first appearance order
+    key_index = {}
     gens, labels = [], []
 
     def comp_id(cre, ann):
         key = (tuple(cre), tuple(ann))
-        if key not in comp_index:
-            c = _component(cre, ann, norb)
-            comp_index[key] = None if c is None else len(comps)
-            if c is not None:
-                comps.append(c)
-        return comp_index[key]
+        if key not in key_index:
+            key_index[key] = len(keys)
+            keys.append(key)
+        return key_index[key]
 
     orbs = range(norb)
     if singles:
@@ -364,10 +433,7 @@ def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None
             for q in orbs:
                 if p <= q:
                     continue
-                ids = [comp_id([2 * p + s], [2 * q + s]) for s in (0, 1)]
-                ids = [i for i in ids if i is not None]
-                if ids:
-                    gens.append(ids); labels.append(("s", p, q))
+                gens.append([comp_id([2 * p + s], [2 * q + s]) for s in (0, 1)]); labels.append(("s", p, q))
     if doubles:
         pairs = [(p, q) for p in orbs for q in orbs if p >= q]
         for (p, q), (r, s_) in itertools.combinations(pairs, 2):
@@ -378,15 +444,32 @@ def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None
                 if a1 == a2 or b1 == b2:
                     continue
                 i = comp_id([a1, a2], [b2, b1])
-                if i is not None and i not in ids:
+                if i not in ids:
                     ids.append(i)
-            if ids:
-                gens.append(ids); labels.append(("d", p, q, r, s_))
+            gens.append(ids); labels.append(("d", p, q, r, s_))
+    # Pauli terms of every component, vectorised over components of one shape
+    terms = [None] * len(keys)
+    by_shape = {}
+    for i, (cr, an) in enumerate(keys):
+        by_shape.setdefault((len(cr), len(an)), []).append(i)
+    for shp, idx in by_shape.items():
+        for lo in range(0, len(idx), 1 << 15):
+            chunk = idx[lo:lo + (1 << 15)]
+            for i, t in zip(chunk, _components_batch([keys[i] for i in chunk], norb)):
+                terms[i] = t
+    # drop vanishing components (t = t^dagger) and renumber
+    new_id = {}
     groups = []
-    for (ax, az, bx, bz, C) in comps:
-        order = np.lexsort((bz, az))
-        ax, az, bx, bz, C = ax[order], az[order], bx[order], bz[order], C[order]
-        groups.append((ax, az, bx, bz, C))
+    for i, t in enumerate(terms):
+        if t is None:
+            continue
+        new_id[i] = len(groups)
+        groups.append(t)
+    gens2, labels2 = [], []
+    for ids, lab in zip(gens, labels):
+        ids = [new_id[i] for i in ids if i in new_id]
+        if ids:
+            gens2.append(ids); labels2.append(lab)
     if not groups:
         raise ValueError("empty pool")
     AX = np.concatenate([g[0] for g in groups]); AZ = np.concatenate([g[1] for g in groups])
@@ -394,29 +477,64 @@ def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None
     CC = np.concatenate([g[4] for g in groups])
     sizes = [len(g[4]) for g in groups]
     net = _compress_each(AX, AZ, BX, BZ, CC, sizes, norb)
-    return Pool(network=net, components=gens, labels=labels)
+    return Pool(network=net, components=gens2, labels=labels2)
 
 
 def _compress_each(ax, az, bx, bz, c, sizes, norb, tol=1e-12) -> OTFNetwork:
     """SVD-compress consecutive runs of given sizes, one group per run
     (``jl/network.jl:248-301``)."""
-    out = []
-    lo = 0
-    for n in sizes:
-        hi = lo + n
-        ua = np.unique(az[lo:hi]); ub = np.unique(bz[lo:hi])
-        M = np.zeros((len(ua), len(ub)))
-        np.add.at(M, (np.searchsorted(ua, az[lo:hi]), np.searchsorted(ub, bz[lo:hi])), c[lo:hi])
-        U, S, Vt = np.linalg.svd(M, full_matrices=False)
-        keep = np.flatnonzero(np.abs(S) > tol)
-        sq = np.sqrt(S[keep])
-        wa = U[:, keep] * sq
-        wb = Vt[keep, :].T * sq
-        wa[np.abs(wa) < 1e-12] = 0.0
-        wb[np.abs(wb) < 1e-12] = 0.0
-        out.append((int(ax[lo]), int(bx[lo]), len(keep), ua, ub, wa, wb))
-        lo = hi
-    return _pack(out, norb)
+    sizes = np.asarray(sizes, np.int64)
+    ends = np.cumsum(sizes)
+    starts = ends - sizes
+    return _compress_runs(ax, az, bx, bz, c, starts, ends, norb, tol)
+
+
+def _components_batch(keys, norb):
+    """Pauli terms of t - t^dagger for many spin-orbital generators at once (all with
+    the same numbers of creators and annihilators), de-interleaved to AABB form.
+
+    Returns, per key, (ax, az, bx, bz, C) term arrays sorted by (x, z) or None when
+    the generator vanishes (the per-generator path of ``_generator_terms``,
+    vectorised over generators)."""
+    words = 1 if 2 * norb <= 64 else 2
+    n = len(keys)
+    kc, ka = len(keys[0][0]), len(keys[0][1])
+    modes = np.array([list(cr) + list(an) for cr, an in keys], dtype=np.int64)
+    modes_d = np.array([list(reversed(an)) + list(reversed(cr)) for cr, an in keys], dtype=np.int64)
+    x, z, sg = _ladder_components(modes, [True] * kc + [False] * ka, words)
+    xd, zd, sd = _ladder_components(modes_d, [True] * ka + [False] * kc, words)
+    scale = 0.5 ** (kc + ka)
+    if words == 1:
+        x, z, xd, zd = [x], [z], [xd], [zd]
+    X = [np.concatenate([x[w], xd[w]], axis=1).ravel() for w in range(words)]
+    Z = [np.concatenate([z[w], zd[w]], axis=1).ravel() for w in range(words)]
+    C = np.concatenate([sg * scale, -sd * scale], axis=1).astype(np.float64).ravel()
+    row = np.repeat(np.arange(n, dtype=np.int64), sg.shape[1] * 2)
+    # sum equal (row, x, z) terms, drop |c| <= 1e-14 (as _combine_terms per generator)
+    order = np.lexsort(tuple(Z) + tuple(X) + (row,))
+    row, C = row[order], C[order]
+    X = [w[order] for w in X]
+    Z = [w[order] for w in Z]
+    diff = np.diff(row) != 0
+    for w in X + Z:
+        diff |= np.diff(w) != 0
+    starts = np.r_[0, np.flatnonzero(diff) + 1].astype(np.int64)
+    cs = np.add.reduceat(C, starts)
+    keep = np.abs(cs) > 1e-14
+    starts = starts[keep]
+    row, cs = row[starts], cs[keep]
+    X = [w[starts] for w in X]
+    Z = [w[starts] for w in Z]
+    ax, az, bx, bz = split_aabb(X if words > 1 else X[0], Z if words > 1 else Z[0], norb)
+    out = [None] * n
+    bnd = np.r_[0, np.flatnonzero(np.diff(row) != 0) + 1, len(row)]
+    for i in range(len(bnd) - 1):
+        lo, hi = bnd[i], bnd[i + 1]
+        r = int(row[lo])
+        if np.any(ax[lo:hi] != ax[lo]) or np.any(bx[lo:hi] != bx[lo]):
+            raise AssertionError("a generator t - t^dagger must have a single X mask")
+        out[r] = (ax[lo:hi], az[lo:hi], bx[lo:hi], bz[lo:hi], cs[lo:hi])
+    return out
 
 
 def draw_generators(pool: Pool, n: int, seed: int = 0, amp_sigma: float = 0.05):

@@ -657,6 +657,165 @@ def gpu_vqe(args):
     return res
 
 
+# ---------------------------------------------------------------------------
+# ADAPT workload: pool-gradient screening on UInt64 strings, plus the adjoint gradient
+# ---------------------------------------------------------------------------
+
+# BASELINE config 4 is 36 orbitals 3a+3b; its 516K Hamiltonian groups and 840K
+# pool components need sparse-regime kernels (the tile kernels visit every
+# (tile, group) pair), so the workload runs the same operator mix at 20 orbitals
+# (--adapt-norb sets it) on UInt64 strings
+ADAPT_CFG = dict(norb=20, na=3, nb=3, seed=0, n_gen=40, amp=0.05, ckpt=8)
+ADAPT_METRIC = "ADAPT pool screening: spin-adapted pool gradients per second (UInt64 strings)"
+
+
+def adapt_problem(cfg):
+    from binsim_b200 import network as nw
+    t0 = time.time()
+    ham = nw.hamiltonian_network(cfg["norb"], seed=cfg["seed"])
+    pool = nw.ucc_pool(cfg["norb"])
+    op_idx, param_idx, th = nw.draw_generators(pool, cfg["n_gen"], seed=cfg["seed"], amp_sigma=cfg["amp"])
+    log(f"adapt problem built in {time.time() - t0:.1f}s: {ham.ngs} Hamiltonian groups, {pool.network.ngs} pool "
+        f"components, {len(pool.components)} generators")
+    return ham, pool, op_idx, param_idx, th
+
+
+def adapt_cfg(args):
+    cfg = dict(ADAPT_CFG)
+    cfg["norb"] = args.adapt_norb
+    return cfg
+
+
+def gpu_adapt(args):
+    """ADAPT-VQE screening (reference ADAPT use of batch_grad: theta = 0, l = psi,
+    r = H psi, op/batchgrad.hpp:529-540): the commutator expectation of every
+    spin-adapted pool generator = sum of its components' gradients; then the
+    adjoint energy gradient of the 40-generator ansatz that made psi."""
+    import torch
+    from binsim_b200 import cuotf
+    cfg = adapt_cfg(args)
+    torch.cuda.set_device(0)
+    ham, pool, op_idx, param_idx, th = adapt_problem(cfg)
+    B = cuotf.CuBasis(cfg["norb"], cfg["na"], cfg["nb"], string_bits=64)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(ham, string_bits=64), cuotf.CuNetwork(pool.network, string_bits=64))
+    dim = B.dim
+    ref_idx, ref_val = np.array([B.hf_index()]), np.array([1.0])
+    psi = torch.empty(dim, dtype=torch.float64, device="cuda")
+    hpsi = torch.empty_like(psi)
+    ngs = pool.network.ngs
+    zeros = torch.zeros(ngs, dtype=torch.float64, device="cuda")
+    grads = torch.empty(ngs, dtype=torch.float64, device="cuda")
+    f.prepare_state(op_idx, param_idx, th, ref_idx, ref_val, psi)
+    # generator gradient = sum over its components (products at theta = 0)
+    comp_gen = np.zeros(ngs, np.int64)
+    for gi, comps in enumerate(pool.components):
+        comp_gen[comps] = gi
+    comp_gen_t = torch.from_numpy(comp_gen).cuda()
+    gen_grads = torch.zeros(len(pool.components), dtype=torch.float64, device="cuda")
+
+    def screen():
+        f.hvec(psi, hpsi)
+        f.batchgrad(psi, hpsi, grads, zeros)
+        gen_grads.zero_().index_add_(0, comp_gen_t, grads)
+    steps, warm = max(1, args.steps), max(3, args.warmup)
+    with Clocks(0) as clk:
+        ms = timed_events(screen, steps, warm)
+        ms_h = timed_events(lambda: f.hvec(psi, hpsi), steps, 1)
+        ms_bg = timed_events(lambda: f.batchgrad(psi, hpsi, grads, zeros), steps, 1)
+    launches = count_launches(screen)
+    g = gen_grads.cpu().numpy()
+    top = np.argsort(-np.abs(g))[:5]
+    # adjoint gradient of the ansatz that made psi
+    lv, rv = torch.empty_like(psi), torch.empty_like(psi)
+    out = {}
+
+    def adjoint():
+        out["a"] = f.energy_grad(op_idx, param_idx, th, ref_idx, ref_val, lv, rv, ckpt_every=cfg["ckpt"])
+    ms_adj = timed_events(adjoint, steps, 1)
+    E, ga, _ = out["a"]
+    res = {
+        "metric": ADAPT_METRIC, "value": len(pool.components) / (ms * 1e-3), "unit": "generators/s", "n_gpus": 1,
+        "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "replicas",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"ADAPT screening: {cfg['norb']} orbitals {cfg['na']}a+{cfg['nb']}b, {dim:,} dets, "
+                               f"UInt64 strings (ranked addressing), {ham.ngs} Hamiltonian groups, pool of "
+                               f"{len(pool.components)} spin-adapted generalised singles/doubles ({ngs} components), "
+                               f"state from {cfg['n_gen']} seeded generators, amplitudes N(0, {cfg['amp']}^2); one "
+                               "step = H psi + every component's gradient at theta = 0 + the per-generator sums",
+                   "dim": dim, "pool_generators": len(pool.components), "pool_components": ngs,
+                   "hamiltonian_groups": int(ham.ngs)},
+        "sigma_ms": ms_h, "batchgrad_ms": ms_bg,
+        "top_generators": [{"label": [str(v) for v in pool.labels[int(i)]], "grad": float(g[int(i)])} for i in top],
+        "adjoint": {"ms": ms_adj, "energy": E, "params": int(len(th)), "max_abs_grad": float(np.abs(ga).max())},
+        "e2e": {"value": len(pool.components) / (ms * 1e-3), "unit": "generators/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(8 * len(pool.components)), "ms_per_step": ms,
+                "note": "psi resident on the device between ADAPT iterations; the generator gradients are read back"},
+        "gpu_launches": launches * steps if launches is not None else None,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        cpu = run_cpu_adapt(args, ham, pool, psi.cpu().numpy(), hpsi.cpu().numpy(), grads.cpu().numpy())
+        if cpu and "seconds" in cpu:
+            res["cpu_baseline"] = {"value": len(pool.components) / cpu["seconds"], "unit": "generators/s",
+                                   "cores": cpu["cores"], "kind": "port", "sample": cpu["sample"]}
+            res["parity_vs_oracle"] = {"max_abs_diff": cpu["max_abs_diff"], "components_checked": cpu["checked"]}
+    return res
+
+
+def cpu_adapt_worker(args):
+    """The oracle (C restatement of op/batchgrad.hpp over UInt64 strings with the
+    reference's sorted-list string search) on a bounded sample of pool components
+    and Hamiltonian groups; also checks the sampled components' GPU gradients."""
+    from oracle.oracle import Oracle
+    import pickle
+    cfg = adapt_cfg(args)
+    with open(args.adapt_state, "rb") as fh:
+        st = pickle.load(fh)
+    ham, pool = st["ham"], st["pool"]
+    O = Oracle()
+    Bo = O.basis(cfg["norb"], cfg["na"], cfg["nb"])
+    psi, hpsi, gpu = st["psi"], st["hpsi"], st["grads"]
+    ngs = pool.network.ngs
+    stride = max(1, ngs // args.adapt_sample)
+    keep = np.arange(0, ngs, stride)
+    sub = subnetwork(pool.network, keep)
+    No = O.network(sub)
+    t0 = time.perf_counter()
+    g = O.batchgrad(Bo, No, np.zeros(len(keep)), psi, hpsi)
+    t_bg = (time.perf_counter() - t0) * ngs / len(keep)
+    hstride = max(1, ham.ngs // args.adapt_sample)
+    hkeep = np.arange(0, ham.ngs, hstride)
+    Ho = O.network(subnetwork(ham, hkeep))
+    t0 = time.perf_counter()
+    O.hvec(Bo, Ho, psi)
+    t_h = (time.perf_counter() - t0) * ham.ngs / len(hkeep)
+    print(json.dumps({"seconds": t_bg + t_h, "max_abs_diff": float(np.abs(g - gpu[keep]).max()),
+                      "checked": int(len(keep)), "bg_sample": int(len(keep)), "h_sample": int(len(hkeep)),
+                      "t_batchgrad": t_bg, "t_hvec": t_h}))
+
+
+def run_cpu_adapt(args, ham, pool, psi, hpsi, grads):
+    import pickle
+    import tempfile
+    with tempfile.NamedTemporaryFile(suffix=".pkl", delete=False) as fh:
+        pickle.dump({"ham": ham, "pool": pool, "psi": psi, "hpsi": hpsi, "grads": grads}, fh)
+        path = fh.name
+    try:
+        out, cores = run_cpu_worker(args, ["--workload", "adapt", "--adapt-state", path,
+                                           "--adapt-sample", str(args.adapt_sample),
+                                           "--adapt-norb", str(args.adapt_norb)])
+    finally:
+        os.unlink(path)
+    if out is None or "seconds" not in out:
+        return out
+    out["cores"] = cores
+    out["sample"] = (f"oracle (C restatement, UInt64 strings, OpenMP) on a stride of the {args.adapt_norb}-orbital pool "
+                     f"giving {out['bg_sample']} components and {out['h_sample']} Hamiltonian "
+                     f"groups, times scaled by the group counts; the reference's basis library is UInt32-only, "
+                     f"so no reference code runs this space; {cpu_model()}")
+    return out
+
+
 def cpu_davidson_worker(args):
     from binsim_b200 import network as nw
     from oracle.oracle import RefLibs, ref_available
@@ -769,7 +928,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="sigma", choices=["sigma", "davidson", "vqe"])
+    ap.add_argument("--workload", default="sigma", choices=["sigma", "davidson", "vqe", "adapt"])
+    ap.add_argument("--adapt-state", default="")
+    ap.add_argument("--adapt-sample", type=int, default=400)
+    ap.add_argument("--adapt-norb", type=int, default=ADAPT_CFG["norb"])
     ap.add_argument("--dav-size", default="12o", choices=sorted(DAV_CFGS))
     ap.add_argument("--sigma-size", default="16o", choices=sorted(SIGMA_CFGS))
     ap.add_argument("--dav-oracle", action="store_true")
@@ -781,7 +943,8 @@ def main():
     args = ap.parse_args()
 
     if args.cpu_worker:
-        {"sigma": cpu_worker, "davidson": cpu_davidson_worker, "vqe": cpu_vqe_worker}[args.workload](args)
+        {"sigma": cpu_worker, "davidson": cpu_davidson_worker, "vqe": cpu_vqe_worker,
+         "adapt": cpu_adapt_worker}[args.workload](args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -798,7 +961,7 @@ def main():
         # Davidson and VQE are single-state solves: one GPU (further ranks would be replicas)
         if rank != 0:
             return
-        result = gpu_davidson(args) if args.workload == "davidson" else gpu_vqe(args)
+        result = {"davidson": gpu_davidson, "vqe": gpu_vqe, "adapt": gpu_adapt}[args.workload](args)
         if args.workload == "vqe" and not args.no_cpu_baseline:
             cpu = run_cpu_vqe(args)
             if cpu and "seconds" in cpu:
@@ -865,6 +1028,12 @@ def reference_arm(args):
                     cpu_baseline={"value": cpu["seconds"], "unit": "s", "cores": cpu["cores"], "kind": "reference",
                                   "sample": cpu["sample"]},
                     e2e={"value": cpu["seconds"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    elif args.workload == "adapt":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's basis library is UInt32-only and its "
+                                                              "dense string map overflows at 36 orbitals "
+                                                              "(basis.hpp:271); the GPU line carries the oracle port "
+                                                              "as cpu_baseline"}))
+        return
     else:
         cpu = run_cpu_vqe(args)
         if not cpu or "seconds" not in cpu:

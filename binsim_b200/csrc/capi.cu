@@ -86,8 +86,6 @@ int check_handles(void *basis, std::initializer_list<void *> nets)
 
 template <typename Ti>
 DevNet<Ti> *net_of(DevBasis<Ti> *, void *n) { return static_cast<DevNet<Ti> *>(n); }
-template <typename Ti>
-constexpr bool is_u32(DevBasis<Ti> *) { return sizeof(Ti) == 4; }
 
 }  // namespace
 
@@ -327,12 +325,10 @@ int bsim_hvec_f32in(void *basis, void *net, const float *src, double *dst, bsim_
 int bsim_hvec_path(void *basis, void *net, char *why, int why_len, int *residual_groups)
 {
     return with_handles(basis, {net}, [&](auto *b) -> int {
-        std::string w = "UInt64 strings: generic tile kernel";
-        int nres = 0, r = 0;
-        if constexpr (is_u32((decltype(b))nullptr)) {
-            r = bsim::fast_sigma_info(b, net_of(b, net), &w, &nres);
-            if (r < 0) return r;
-        }
+        std::string w;
+        int nres = 0;
+        const int r = bsim::fast_sigma_info(b, net_of(b, net), &w, &nres);
+        if (r < 0) return r;
         if (why && why_len > 0) snprintf(why, why_len, "%s", w.c_str());
         if (residual_groups) *residual_groups = nres;
         return r;
@@ -344,11 +340,8 @@ int bsim_hvec_cols(void *basis, void *net, const double *src, double *dst, int64
 {
     if (int st0 = check_handles(basis, {net})) return st0;
     NEED(src); NEED(dst);
-    return with_handles(basis, {net}, [&](auto *b) -> int {
-        if constexpr (is_u32((decltype(b))nullptr))
-            return bsim::sigma_fast_cols(b, net_of(b, net), src, dst, mixed != 0, col_lo, col_hi, stream);
-        bsim::set_error("column-band sigma needs the structured path (UInt32 strings)");
-        return BSIM_ERR_UNSUPPORTED;
+    return with_handles(basis, {net}, [&](auto *b) {
+        return bsim::sigma_fast_cols(b, net_of(b, net), src, dst, mixed != 0, col_lo, col_hi, stream);
     });
 }
 
@@ -357,12 +350,8 @@ int bsim_hvec_stage_times(void *basis, void *net, const double *src, double *dst
 {
     if (int st0 = check_handles(basis, {net})) return st0;
     NEED(src); NEED(dst); NEED(ms_out); NEED(launches_out);
-    return with_handles(basis, {net}, [&](auto *b) -> int {
-        if constexpr (is_u32((decltype(b))nullptr))
-            return bsim::sigma_fast_stages(b, net_of(b, net), src, dst, mixed != 0, stream, ms_out, launches_out,
-                                           nstages);
-        bsim::set_error("stage timing covers the structured path (UInt32 strings)");
-        return BSIM_ERR_UNSUPPORTED;
+    return with_handles(basis, {net}, [&](auto *b) {
+        return bsim::sigma_fast_stages(b, net_of(b, net), src, dst, mixed != 0, stream, ms_out, launches_out, nstages);
     });
 }
 

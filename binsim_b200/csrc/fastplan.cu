@@ -399,7 +399,6 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     }
     P->M = M;
     if (M > 64 && P->nE > 0) { P->why = "more than 64 connected alpha singles per string"; return BSIM_OK; }
-    if (P->nPA > 4096 || P->nPB > 4096) { P->why = "more than 4096 pure groups on one side"; return BSIM_OK; }
 
     P->fits64 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 8) <= 227 * 1024;
     P->fits32 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 4) <= 227 * 1024;
@@ -573,5 +572,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
 }
 
 template int build_fast_plan<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, FastPlan<unsigned> *);
+template int build_fast_plan<unsigned long long>(const DevBasis<unsigned long long> *,
+                                                 const DevNet<unsigned long long> *, FastPlan<unsigned long long> *);
 
 }  // namespace bsim

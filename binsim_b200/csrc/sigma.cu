@@ -221,13 +221,11 @@ int sigma(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *src, const f
         const char *e = getenv("BSIM_SIGMA_GENERIC");
         return e && e[0] == '1';
     }();
-    if constexpr (sizeof(Ti) == 4) {   // the structured path addresses strings of up to 24 orbitals
-        if (!force_generic && B->dim > 0) {
-            bool used = false;
-            int st = sigma_fast(B, N, src, src32, dst, mixed, s, &used);
-            if (st != BSIM_OK) return st;
-            if (used) return BSIM_OK;
-        }
+    if (!force_generic && B->dim > 0) {
+        bool used = false;
+        int st = sigma_fast(B, N, src, src32, dst, mixed, s, &used);
+        if (st != BSIM_OK) return st;
+        if (used) return BSIM_OK;
     }
     return sigma_tiles(B, N, src, src32, dst, mixed, 0, num_tiles(B), s);
 }

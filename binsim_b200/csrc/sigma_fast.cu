@@ -924,4 +924,13 @@ template int sigma_fast_cols<unsigned>(const DevBasis<unsigned> *, const DevNet<
 template int sigma_fast_stages<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *, double *,
                                          bool, cudaStream_t, double *, int *, int);
 
+template int fast_sigma_info<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, std::string *, int *);
+template bool fast_sigma_available<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *);
+template int sigma_fast<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, const double *, const float *,
+                                  double *, bool, cudaStream_t, bool *);
+template int sigma_fast_cols<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, const double *, double *,
+                                       bool, i64, i64, cudaStream_t);
+template int sigma_fast_stages<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, const double *, double *,
+                                         bool, cudaStream_t, double *, int *, int);
+
 }  // namespace bsim

@@ -71,6 +71,11 @@ int batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *thetas, 
               double *grads, cudaStream_t s)
 {
     if (N->ngs == 0) return BSIM_OK;
+    if (B->dim > 0) {   // single-block bases: one launch over the groups' pair lists
+        bool used = false;
+        int st0 = pair_list_batchgrad(B, N, thetas, l, r, grads, s, &used);
+        if (st0 != BSIM_OK || used) return st0;
+    }
     BSIM_CUDA(cudaMemsetAsync(grads, 0, sizeof(double) * N->ngs, s));
     if (B->dim == 0 || N->plan_chunks.empty()) return BSIM_OK;
     Workspace &ws = workspace_for(B);

@@ -85,6 +85,12 @@ inline i64 pair_grid(const DevBasis<Ti> *B) { return (i64)B->max_na * B->num_blo
 struct PairAngles { double c0, c1, c2, c3; };
 enum PairOpKind { kPairExpm = 0, kPairGrad = 1, kPairBackgrad = 2 };
 
+// Gradients of every group of a pool network in one launch over the pair lists
+// (single-block bases, ranks <= 4); *used = false when the tile kernel must run.
+template <typename Ti>
+int pair_list_batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *thetas, const double *l,
+                        const double *r, double *grads, cudaStream_t s, bool *used);
+
 // Pair operator over the precomputed pair lists (single-block bases, rank <= 4).
 // Sets *used = false (and launches nothing) when the row kernel must serve the
 // call.  grad/backgrad write at most max_slots partials before the ticket.

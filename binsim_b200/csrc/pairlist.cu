@@ -29,6 +29,16 @@ constexpr int kListCols = 256;     // beta entries per CTA (one per thread)
 constexpr int kListMaxRank = 4;
 constexpr int kListMaxZ = 64;      // Z masks per spin staged in shared memory
 
+// One group's work for the batched gradient: its pair lists, phase data and
+// tile count (tiles of kBatchRows alpha entries x kListCols beta entries).
+struct BGroup {
+    int aoff, acnt, boff, bcnt;   // list offsets (-1: identity) and lengths
+    int R, nza, nzb, orig;
+    int ntx, pad;
+    i64 za_off, zb_off, wa_off, wb_off;
+};
+constexpr int kBatchRows = 4;
+
 template <typename Ti>
 struct PairPlan {
     const void *basis = nullptr;
@@ -37,7 +47,18 @@ struct PairPlan {
     std::vector<int4> desc;        // per group: {alpha offset or -1, alpha count, beta offset or -1, beta count}
     Arena arena;
     const int2 *d_alist = nullptr, *d_blist = nullptr;
-    ~PairPlan() { arena.release(); }
+    // batched gradient over the whole network (built on first use)
+    int bg_state = 0;              // 0 not built, 1 usable, -1 a group needs the tile kernel
+    i64 bg_tiles = 0;
+    int bg_n = 0;
+    BGroup *d_bg = nullptr;
+    i64 *d_tstart = nullptr;
+    ~PairPlan()
+    {
+        arena.release();
+        if (d_bg) cudaFree(d_bg);
+        if (d_tstart) cudaFree(d_tstart);
+    }
 };
 
 std::mutex g_pair_mu;
@@ -287,6 +308,140 @@ pair_list_kernel(const Ti *__restrict__ astrs, const Ti *__restrict__ bstrs, con
     }
 }
 
+// Gradient of every group of a network at its own angle, one launch: the
+// groups' tiles form one index space (prefix sums tstart); each CTA takes a
+// contiguous range of tiles, so it meets few group boundaries, and adds its
+// partial sum of a group into grads[orig] when it leaves the group.
+template <typename Ti>
+__global__ void __launch_bounds__(kListCols)
+pair_list_batchgrad_kernel(const Ti *__restrict__ astrs, const Ti *__restrict__ bstrs, int nB,
+                           const Ti *__restrict__ zall, const double *__restrict__ wall,
+                           const int2 *__restrict__ alist_all, const int2 *__restrict__ blist_all,
+                           const BGroup *__restrict__ groups, const i64 *__restrict__ tstart, int ngroups, i64 T,
+                           const double *__restrict__ thetas, const double *__restrict__ l,
+                           const double *__restrict__ r, double *__restrict__ grads)
+{
+    __shared__ double spa[kBatchRows][kListMaxRank];
+    __shared__ long long arow[kBatchRows], asrc[kBatchRows];
+    __shared__ double red[kListCols / 32];
+    __shared__ unsigned long long zsa[kListMaxZ], zsb[kListMaxZ];
+    __shared__ double wsa[kListMaxRank * kListMaxZ], wsb[kListMaxRank * kListMaxZ];
+    __shared__ BGroup G;
+    __shared__ double ang0, ang1;
+    __shared__ int gcur;
+    const int t = threadIdx.x;
+    const i64 t0 = (i64)blockIdx.x * T / gridDim.x, t1 = (i64)(blockIdx.x + 1) * T / gridDim.x;
+    if (t0 >= t1) return;
+    if (t == 0) {   // group of the first tile: last g with tstart[g] <= t0
+        int lo = 0, hi = ngroups - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tstart[mid] <= t0) lo = mid; else hi = mid - 1;
+        }
+        gcur = lo;
+    }
+    __syncthreads();
+    int g = -1;
+    double acc = 0.0;
+    auto flush = [&]() {
+        double v = warp_sum(acc);
+        acc = 0.0;
+        __syncthreads();
+        if ((t & 31) == 0) red[t >> 5] = v;
+        __syncthreads();
+        if (t == 0) {
+            double sum = 0.0;
+            for (int i = 0; i < kListCols / 32; ++i) sum += red[i];
+            atomicAdd(grads + G.orig, sum);
+        }
+    };
+    for (i64 tile = t0; tile < t1; ++tile) {
+        if (g < 0 || tile >= tstart[g + 1]) {   // entering a new group (uniform across the CTA)
+            if (g >= 0) flush();
+            __syncthreads();
+            if (t == 0) {
+                int gg = g < 0 ? gcur : g + 1;
+                while (tile >= tstart[gg + 1]) ++gg;
+                gcur = gg;
+                G = groups[gg];
+                const double th = thetas[G.orig];
+                ang0 = -sin(th);   // grad_update, core/math.hpp:148-162
+                ang1 = cos(th);
+            }
+            __syncthreads();
+            g = gcur;
+            for (int i = t; i < G.nza; i += kListCols) zsa[i] = (unsigned long long)zall[G.za_off + i];
+            for (int i = t; i < G.nzb; i += kListCols) zsb[i] = (unsigned long long)zall[G.zb_off + i];
+            for (int i = t; i < G.R * G.nza; i += kListCols) wsa[i] = wall[G.wa_off + i];
+            for (int i = t; i < G.R * G.nzb; i += kListCols) wsb[i] = wall[G.wb_off + i];
+        }
+        const i64 local = tile - tstart[g];
+        const int tx = (int)(local % G.ntx), ty = (int)(local / G.ntx);
+        const int2 *alist = G.aoff >= 0 ? alist_all + G.aoff : nullptr;
+        const int2 *blist = G.boff >= 0 ? blist_all + G.boff : nullptr;
+        const int R = G.R;
+        __syncthreads();   // smem of the previous tile consumed, this group's masks staged
+        if (t < kBatchRows) {
+            const int i = tx * kBatchRows + t;
+            long long ar = -1, as = -1;
+            double p[kListMaxRank] = {0.0, 0.0, 0.0, 0.0};
+            if (i < G.acnt) {
+                const int2 e = alist ? alist[i] : make_int2(i, i);
+                ar = (long long)e.x * nB;
+                as = (long long)e.y * nB;
+                const unsigned long long sv = (unsigned long long)astrs[e.y];
+                for (int q = 0; q < G.nza; ++q) {
+                    const bool odd = par(sv & zsa[q]);
+#pragma unroll
+                    for (int rr = 0; rr < kListMaxRank; ++rr)
+                        if (rr < R) p[rr] += odd ? -wsa[rr * G.nza + q] : wsa[rr * G.nza + q];
+                }
+            }
+            arow[t] = ar;
+            asrc[t] = as;
+#pragma unroll
+            for (int rr = 0; rr < kListMaxRank; ++rr) spa[t][rr] = p[rr];
+        }
+        const int j = ty * kListCols + t;
+        int b = -1, sb = -1;
+        double pb[kListMaxRank] = {0.0, 0.0, 0.0, 0.0};
+        if (j < G.bcnt) {
+            const int2 e = blist ? blist[j] : make_int2(j, j);
+            b = e.x;
+            sb = e.y;
+            const unsigned long long sv = (unsigned long long)bstrs[sb];
+            for (int q = 0; q < G.nzb; ++q) {
+                const bool odd = par(sv & zsb[q]);
+#pragma unroll
+                for (int rr = 0; rr < kListMaxRank; ++rr)
+                    if (rr < R) pb[rr] += odd ? -wsb[rr * G.nzb + q] : wsb[rr * G.nzb + q];
+            }
+        }
+        __syncthreads();
+        if (b >= 0) {
+            double li[kBatchRows], lj[kBatchRows], ri[kBatchRows], rj[kBatchRows];
+#pragma unroll
+            for (int k = 0; k < kBatchRows; ++k) {
+                li[k] = lj[k] = ri[k] = rj[k] = 0.0;
+                if (arow[k] < 0) continue;
+                const i64 di = arow[k] + b, si = asrc[k] + sb;
+                li[k] = __ldg(l + si); lj[k] = __ldg(l + di);
+                ri[k] = __ldg(r + si); rj[k] = __ldg(r + di);
+            }
+#pragma unroll
+            for (int k = 0; k < kBatchRows; ++k) {
+                if (arow[k] < 0) continue;
+                double vt = 0.0;
+#pragma unroll
+                for (int rr = 0; rr < kListMaxRank; ++rr) vt += spa[k][rr] * pb[rr];
+                const double vd = ang0 * (vt * vt), vo = ang1 * vt;
+                acc += li[k] * (ri[k] * vd + rj[k] * vo) + lj[k] * (rj[k] * vd - ri[k] * vo);
+            }
+        }
+    }
+    flush();
+}
+
 }  // namespace
 
 template <typename Ti, int OP>
@@ -320,6 +475,58 @@ int pair_list_launch(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, PairA
     BSIM_CUDA(cudaGetLastError());
     return BSIM_OK;
 }
+
+template <typename Ti>
+int pair_list_batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *thetas, const double *l,
+                        const double *r, double *grads, cudaStream_t s, bool *used)
+{
+    *used = false;
+    PairPlan<Ti> *P = nullptr;
+    int st = get_pair_plan(B, N, &P);
+    if (st != BSIM_OK) return st;
+    if (!P->ok) return BSIM_OK;
+    if (P->bg_state == 0) {
+        std::vector<BGroup> bg;
+        std::vector<i64> ts(1, 0);
+        P->bg_state = 1;
+        for (i64 g = 0; g < N->ngs; ++g) {
+            const GroupDev &Gd = N->groups[g];
+            if (Gd.type == 0) continue;   // diagonal groups contribute zero for real vectors
+            if (Gd.rank > kListMaxRank || Gd.nza > kListMaxZ || Gd.nzb > kListMaxZ) { P->bg_state = -1; break; }
+            const int4 d = P->desc[g];
+            if (d.y == 0 || d.w == 0) continue;
+            BGroup x{d.x, d.y, d.z, d.w, Gd.rank, Gd.nza, Gd.nzb, (int)g, (d.y + kBatchRows - 1) / kBatchRows, 0,
+                     Gd.za_off, Gd.zb_off, Gd.wa_off, Gd.wb_off};
+            bg.push_back(x);
+            ts.push_back(ts.back() + (i64)x.ntx * ((d.w + kListCols - 1) / kListCols));
+        }
+        if (P->bg_state == 1 && !bg.empty()) {
+            ts.push_back(ts.back());   // sentinel: tstart[n + 1] for the last group's boundary test
+            BSIM_CUDA(cudaMalloc(&P->d_bg, bg.size() * sizeof(BGroup)));
+            BSIM_CUDA(cudaMalloc(&P->d_tstart, ts.size() * sizeof(i64)));
+            BSIM_CUDA(cudaMemcpy(P->d_bg, bg.data(), bg.size() * sizeof(BGroup), cudaMemcpyHostToDevice));
+            BSIM_CUDA(cudaMemcpy(P->d_tstart, ts.data(), ts.size() * sizeof(i64), cudaMemcpyHostToDevice));
+            P->bg_n = (int)bg.size();
+            P->bg_tiles = ts[bg.size()];
+        }
+    }
+    if (P->bg_state < 0) return BSIM_OK;
+    *used = true;
+    BSIM_CUDA(cudaMemsetAsync(grads, 0, sizeof(double) * N->ngs, s));
+    if (P->bg_n == 0 || P->bg_tiles == 0) return BSIM_OK;
+    const i64 grid = std::min<i64>(P->bg_tiles, (i64)148 * 32);
+    pair_list_batchgrad_kernel<Ti><<<(unsigned)grid, kListCols, 0, s>>>(
+        B->view.astrs, B->view.bstrs, B->nb[0], N->view.z, N->view.w, P->d_alist, P->d_blist, P->d_bg, P->d_tstart,
+        P->bg_n, P->bg_tiles, thetas, l, r, grads);
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+template int pair_list_batchgrad<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *,
+                                           const double *, const double *, double *, cudaStream_t, bool *);
+template int pair_list_batchgrad<unsigned long long>(const DevBasis<unsigned long long> *,
+                                                     const DevNet<unsigned long long> *, const double *,
+                                                     const double *, const double *, double *, cudaStream_t, bool *);
 
 #define PAIR_LIST_INST(OP)                                                                                   \
     template int pair_list_launch<unsigned, OP>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64,     \

@@ -37,7 +37,7 @@ struct BGroup {
     int ntx, pad;
     i64 za_off, zb_off, wa_off, wb_off;
 };
-constexpr int kBatchRows = 4;
+constexpr int kBatchRows = 16;   // alpha entries per tile of the batched gradient (loads in groups of 4)
 
 template <typename Ti>
 struct PairPlan {
@@ -419,23 +419,28 @@ pair_list_batchgrad_kernel(const Ti *__restrict__ astrs, const Ti *__restrict__ 
         }
         __syncthreads();
         if (b >= 0) {
-            double li[kBatchRows], lj[kBatchRows], ri[kBatchRows], rj[kBatchRows];
 #pragma unroll
-            for (int k = 0; k < kBatchRows; ++k) {
-                li[k] = lj[k] = ri[k] = rj[k] = 0.0;
-                if (arow[k] < 0) continue;
-                const i64 di = arow[k] + b, si = asrc[k] + sb;
-                li[k] = __ldg(l + si); lj[k] = __ldg(l + di);
-                ri[k] = __ldg(r + si); rj[k] = __ldg(r + di);
-            }
+            for (int k0 = 0; k0 < kBatchRows; k0 += 4) {
+                double li[4], lj[4], ri[4], rj[4];
 #pragma unroll
-            for (int k = 0; k < kBatchRows; ++k) {
-                if (arow[k] < 0) continue;
-                double vt = 0.0;
+                for (int kk = 0; kk < 4; ++kk) {
+                    const int k = k0 + kk;
+                    li[kk] = lj[kk] = ri[kk] = rj[kk] = 0.0;
+                    if (arow[k] < 0) continue;
+                    const i64 di = arow[k] + b, si = asrc[k] + sb;
+                    li[kk] = __ldg(l + si); lj[kk] = __ldg(l + di);
+                    ri[kk] = __ldg(r + si); rj[kk] = __ldg(r + di);
+                }
 #pragma unroll
-                for (int rr = 0; rr < kListMaxRank; ++rr) vt += spa[k][rr] * pb[rr];
-                const double vd = ang0 * (vt * vt), vo = ang1 * vt;
-                acc += li[k] * (ri[k] * vd + rj[k] * vo) + lj[k] * (rj[k] * vd - ri[k] * vo);
+                for (int kk = 0; kk < 4; ++kk) {
+                    const int k = k0 + kk;
+                    if (arow[k] < 0) continue;
+                    double vt = 0.0;
+#pragma unroll
+                    for (int rr = 0; rr < kListMaxRank; ++rr) vt += spa[k][rr] * pb[rr];
+                    const double vd = ang0 * (vt * vt), vo = ang1 * vt;
+                    acc += li[kk] * (ri[kk] * vd + rj[kk] * vo) + lj[kk] * (rj[kk] * vd - ri[kk] * vo);
+                }
             }
         }
     }
@@ -463,13 +468,13 @@ int pair_list_launch(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, PairA
     }
     ListArgs A{B->nb[0], d.y, d.w, G.rank, G.nza, G.nzb, d.x >= 0 ? P->d_alist + d.x : nullptr,
                d.z >= 0 ? P->d_blist + d.z : nullptr, G.za_off, G.zb_off, G.wa_off, G.wb_off};
-    // 4 alpha entries per tile, loads of all 4 pairs issued before their stores,
-    // 3 CTAs per SM (a sweep of tile shapes on the VQE workload chose it)
-    constexpr int kRT = 4;
+    // 16 alpha entries per tile (per pair of barriers), the loads of each group
+    // of 4 pairs issued before their stores, 3 CTAs per SM
+    constexpr int kRT = 16;
     const i64 cap = OP == kPairExpm ? (i64)148 * 64 : std::max<i64>(1, max_slots);
     const i64 tiles = (i64)((d.y + kRT - 1) / kRT) * ((d.w + kListCols - 1) / kListCols);
     const unsigned grid = (unsigned)std::min<i64>(tiles, cap);
-    pair_list_kernel<Ti, OP, kRT, kRT, 3><<<grid, kListCols, 0, s>>>(B->view.astrs, B->view.bstrs, N->view.z,
+    pair_list_kernel<Ti, OP, kRT, 4, 3><<<grid, kListCols, 0, s>>>(B->view.astrs, B->view.bstrs, N->view.z,
                                                                       N->view.w, A, ang, l, r, part, ticket, out,
                                                                       accumulate ? 1 : 0);
     BSIM_CUDA(cudaGetLastError());

@@ -49,6 +49,44 @@ u64 comb_count(int n, int k)
     return r;
 }
 
+// String -> index of one spin's list: a dense table up to 24 orbitals, above
+// that the colex rank of the string (Gosper order) indexing a table of
+// C(norb, n) entries; -1 for strings outside the list.
+struct StrIndex {
+    int norb = 0, nel = 0;
+    bool ranked = false;
+    std::vector<int> tab;
+    std::vector<u64> binom;   // [65 x 65]
+    template <typename Ti>
+    void build(int norb_, const std::vector<Ti> &strs)
+    {
+        norb = norb_;
+        nel = strs.empty() ? 0 : popc((u64)strs[0]);
+        ranked = norb > 24;
+        binom.assign(65 * 65, 0);
+        for (int n = 0; n <= 64; ++n) {
+            binom[n * 65] = 1;
+            for (int k = 1; k <= n; ++k) binom[n * 65 + k] = binom[(n - 1) * 65 + k - 1] + (k <= n - 1 ? binom[(n - 1) * 65 + k] : 0);
+        }
+        tab.assign(ranked ? (size_t)binom[norb * 65 + nel] : (size_t)1 << norb, -1);
+        for (size_t i = 0; i < strs.size(); ++i) tab[slot((u64)strs[i])] = (int)i;
+    }
+    size_t slot(u64 s) const
+    {
+        if (!ranked) return (size_t)s;
+        u64 r = 0;
+        int i = 1;
+        for (u64 y = s; y; y &= y - 1, ++i) r += binom[__builtin_ctzll(y) * 65 + i];
+        return (size_t)r;
+    }
+    int operator()(u64 s) const
+    {
+        if (norb < 64 && (s >> norb)) return -1;
+        if (ranked && popc(s) != nel) return -1;
+        return tab[slot(s)];
+    }
+};
+
 }  // namespace
 
 template <typename Ti>
@@ -67,7 +105,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
         P->why = "string lists are not complete (symmetry-restricted)";
         return BSIM_OK;
     }
-    if (norb > 24) { P->why = "norb > 24"; return BSIM_OK; }
+    if (norb > 63) { P->why = "norb > 63"; return BSIM_OK; }
     P->norb = norb; P->nA = nA; P->nB = nB; P->nelA = nelA; P->nelB = nelB;
     P->ldA = (nB + 7) & ~7;
     P->ldB = (nA + 7) & ~7;
@@ -156,9 +194,9 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     };
     add_side(0, pa);
     add_side(1, pb);
-    std::vector<int> amap((size_t)1 << norb, -1), bmap((size_t)1 << norb, -1);
-    for (int a = 0; a < nA; ++a) amap[(size_t)A[a]] = a;
-    for (int b = 0; b < nB; ++b) bmap[(size_t)Bs[b]] = b;
+    StrIndex amap, bmap;
+    amap.build(norb, A);
+    bmap.build(norb, Bs);
     const int nth_host = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
 
     // ---- same-spin doubles through intermediate strings: extract and verify W ----
@@ -185,7 +223,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
         if (nel < 2 || norb - nel < 2 || nU > 64 || npr > 64 || (ri_env && ri_env[0] == '0')) continue;
         Wri[side].assign((size_t)nP * nP, 0.0);
         const auto &rows = side == 0 ? A : Bs;
-        const std::vector<int> &rmap = side == 0 ? amap : bmap;
+        const StrIndex &rmap = side == 0 ? amap : bmap;
         const int nrows = side == 0 ? nA : nB;
         std::vector<int> cand;
         for (int g = 0; g < ng; ++g)
@@ -202,7 +240,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
                     const u64 d = (u64)rows[r];
                     if (popc(d & x) != 2) continue;
                     const u64 sv = d ^ x;
-                    if (rmap[(size_t)sv] < 0) { ok = false; break; }
+                    if (rmap(sv) < 0) { ok = false; break; }
                     double pa[kSideMaxRank] = {0, 0, 0, 0};
                     for (int q = 0; q < nz; ++q) {
                         const bool odd = popc(sv & S.zmask[S.z_off[g] + q]) & 1;
@@ -257,7 +295,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
             if (li == 2 && !ri_on[1]) continue;
             const SideHost &S = sh[side];
             const auto &rows = side == 0 ? A : Bs;
-            const std::vector<int> &rmap = side == 0 ? amap : bmap;
+            const StrIndex &rmap = side == 0 ? amap : bmap;
             const int nrows = side == 0 ? nA : nB;
             const int ng = (int)S.x.size();
             const int nth = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
@@ -280,7 +318,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
                         if (2 * popc(s0 & x) != popc(x)) continue;
                         const u64 sv = s0 ^ x;
                         if (sv >> norb) continue;
-                        const int src = rmap[(size_t)sv];
+                        const int src = rmap(sv);
                         if (src < 0) continue;
                         double pa[kSideMaxRank] = {0, 0, 0, 0};
                         const int R = S.rank[g], nz = S.nz[g];
@@ -382,7 +420,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     }
     P->nE = (int)P->Emask.size();
     P->nF = (int)P->Fmask.size();
-    if (P->nE > 256 || P->nF > 512) {
+    if (P->nE > 4096 || P->nF > 4096) {
         // too many excitations for the shared-memory tiles: everything generic
         for (auto &r : recs) (void)r;
         P->why = "too many single excitations for the structured mixed kernel";
@@ -398,10 +436,10 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
         M = std::max(M, m);
     }
     P->M = M;
-    if (M > 64 && P->nE > 0) { P->why = "more than 64 connected alpha singles per string"; return BSIM_OK; }
+    if (M > kMaxConn && P->nE > 0) { P->why = "more than 128 connected alpha singles per string"; return BSIM_OK; }
 
-    P->fits64 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 8) <= 227 * 1024;
-    P->fits32 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 4) <= 227 * 1024;
+    P->fits64 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 8, mixed_lam_streamed(nB, P->nF, 8)) <= 227 * 1024;
+    P->fits32 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 4, mixed_lam_streamed(nB, P->nF, 4)) <= 227 * 1024;
     if (!P->fits64 && !P->fits32) { P->why = "beta row too long for the mixed kernel's shared memory"; return BSIM_OK; }
 
     // ---- gather-index table of the mixed GEMM: X[F][b] = sB_F(b^F) c~[a', b^F] ------
@@ -433,7 +471,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
         RIHost &H = rih[side];
         const int nel = side == 0 ? nelA : nelB;
         const auto &rows = side == 0 ? A : Bs;
-        const std::vector<int> &rmap = side == 0 ? amap : bmap;
+        const StrIndex &rmap = side == 0 ? amap : bmap;
         const int nrows = side == 0 ? nA : nB;
         H.nU = (int)comb_count(norb - nel + 2, 2);
         H.npr = (int)comb_count(nel, 2);
@@ -461,7 +499,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
                 const int p = __builtin_ctzll(yp);
                 for (u64 yq = yp & (yp - 1); yq; yq &= yq - 1) {
                     const int q = __builtin_ctzll(yq);
-                    const int row = rmap[(size_t)(m | (1ull << p) | (1ull << q))];
+                    const int row = rmap(m | (1ull << p) | (1ull << q));
                     H.src[(size_t)i * H.nU + slot] = (row << 1) | spair(m, p, q);
                     H.pid[(size_t)i * H.nU + slot] = pair_id(p, q);
                     ++slot;

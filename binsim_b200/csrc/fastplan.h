@@ -131,10 +131,18 @@ inline size_t ri_smem_bytes(int nU, size_t elem)
 
 // Shared memory of the mixed GEMM kernel: source row, Lam_conn [K x 64], an
 // X slice [32 x kMixCols] and the connected-excitation lists.
-inline size_t mixed_smem_bytes(int nB, int nF, size_t elem)
+constexpr int kMaxConn = 128;   // connected alpha singles per string: up to two 64-row GEMM passes
+
+// With `stream`, Lam_conn is staged one 32-row F chunk at a time instead of whole.
+inline size_t mixed_smem_bytes(int nB, int nF, size_t elem, bool stream)
 {
-    return (((size_t)nB + 7) & ~size_t(7)) * elem + (((size_t)nF + 3) & ~size_t(3)) * gemm_ls(elem) * elem +
-           32 * gemm_xs(elem) * elem + 128 * 4;
+    const size_t lam_rows = stream ? 32 : (((size_t)nF + 3) & ~size_t(3));
+    return (((size_t)nB + 7) & ~size_t(7)) * elem + lam_rows * gemm_ls(elem) * elem + 32 * gemm_xs(elem) * elem +
+           2 * kMaxConn * 4;
+}
+inline bool mixed_lam_streamed(int nB, int nF, size_t elem)
+{
+    return mixed_smem_bytes(nB, nF, elem, false) > 226 * 1024;
 }
 
 template <typename Ti>

@@ -183,13 +183,13 @@ __device__ __forceinline__ int connected_excitations(const MixedArgs &P, u64 sa,
         for (int w2 = 0; w2 < wid; ++w2) off += wcnt[w2];
         if (ok) {
             const int j = off + __popc(m & ((1u << lane) - 1u));
-            if (j < 64) { conn[j] = e; sgn[j] = (__popcll(sa & P.mA[e]) & 1) ? -1 : 1; }
+            if (j < kMaxConn) { conn[j] = e; sgn[j] = (__popcll(sa & P.mA[e]) & 1) ? -1 : 1; }
         }
         __syncthreads();
         if (threadIdx.x == 0) for (int w2 = 0; w2 < NW; ++w2) *cnt += wcnt[w2];
         __syncthreads();
     }
-    return min(*cnt, 64);
+    return min(*cnt, kMaxConn);
 }
 
 // EPT consecutive Lam_conn values (32 bytes) from shared memory
@@ -367,27 +367,30 @@ struct GemmCore<double, EPT> {
 // kMixCols-column chunk (conflict-free 2-element shared loads).  The X slice for
 // (chunk, 32 F) is filled from the gather-index table, whose next slice is
 // loaded into registers while the current one is multiplied.
-template <typename Ti, typename T, int EPT>
+template <typename Ti, typename T, int EPT, bool STREAM>
 __global__ void __launch_bounds__((64 / EPT) * 32, sizeof(T) == 4 ? 2 : 1)
 mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__restrict__ ct, T *__restrict__ Z,
-                  int z0, int W)
+                  int z0, int W, int jbase)
 {
     constexpr int NT = (64 / EPT) * 32, NW = NT / 32;
     constexpr int ITEMS = 32 * kMixCols / NT;
-    using V2 = typename Vec2<T>::type;
+    constexpr int LITEMS = STREAM ? 32 * 64 / NT : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.nF, M = P.M;
     T *srow = reinterpret_cast<T *>(smem_raw);                    // [ldA]
     constexpr int LS = GemmLayout<T>::LS, XS = GemmLayout<T>::XS;
     const int Kp = (K + 3) & ~3;
-    T *lam = srow + P.ldA;                                         // [Kp][LS], rows >= K zero
-    T *xs = lam + (size_t)Kp * LS;                                 // [32][XS]
-    int *conn = reinterpret_cast<int *>(xs + 32 * XS);             // [64]
-    int *sgn = conn + 64;                                          // [64]
+    T *lam = srow + P.ldA;                                         // [Kp or 32][LS], rows past K zero
+    T *xs = lam + (size_t)(STREAM ? 32 : Kp) * LS;                 // [32][XS]
+    int *conn = reinterpret_cast<int *>(xs + 32 * XS);             // [kMaxConn]
+    int *sgn = conn + kMaxConn;                                    // [kMaxConn]
     __shared__ int wcnt[NW], cnt;
     const int a = blockIdx.x;
     const int m = connected_excitations<NT>(P, (u64)astr[a], conn, sgn, wcnt, &cnt);
-    // stage the source row (16-byte copies) and Lam restricted to the connected excitations
+    const int jm = min(64, m - jbase);   // output rows of this pass
+    if (jm <= 0) return;                 // uniform across the CTA
+    // stage the source row (16-byte copies) and, when it fits, Lam restricted to
+    // this pass's connected excitations
     {
         const int4 *src = reinterpret_cast<const int4 *>(ct + (i64)a * P.ldA);
         int4 *dst = reinterpret_cast<int4 *>(srow);
@@ -395,16 +398,18 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
         for (int i = threadIdx.x; i < n16; i += NT) dst[i] = __ldg(src + i);
     }
     const T *Lam = static_cast<const T *>(P.Lam);
-    for (int i = threadIdx.x; i < Kp * LS; i += NT) {
-        const int f = i / LS, j = i % LS;
-        lam[i] = (j < m && f < K) ? (T)sgn[j] * Lam[(i64)conn[j] * K + f] : T(0);
-    }
+    if (!STREAM)
+        for (int i = threadIdx.x; i < Kp * LS; i += NT) {
+            const int f = i / LS, j = i % LS;
+            lam[i] = (j < jm && f < K) ? (T)sgn[jbase + j] * Lam[(i64)conn[jbase + j] * K + f] : T(0);
+        }
     const int zend = min(P.cend, z0 + W);
     const int ncb = (zend - z0 + kMixCols - 1) / kMixCols;
     const int nfc = (K + 31) / 32;
     const int nsteps = ncb * nfc;
-    const bool active = GemmCore<T, EPT>::active(m);
+    const bool active = GemmCore<T, EPT>::active(jm);
     int gpre[ITEMS];
+    T lpre[LITEMS];
     auto load_g = [&](int step) {
         const int cb = z0 + (step / nfc) * kMixCols, f0 = (step % nfc) * 32;
 #pragma unroll
@@ -412,6 +417,15 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
             const int i = threadIdx.x + it * NT;
             const int f = i / kMixCols, cl = i % kMixCols;
             gpre[it] = f0 + f < K ? __ldg(P.gidx + (i64)(f0 + f) * P.ldG + cb + cl) : -1;
+        }
+        if (STREAM) {
+#pragma unroll
+            for (int it = 0; it < LITEMS; ++it) {
+                const int i = threadIdx.x + it * NT;
+                const int f = i >> 6, j = i & 63;
+                lpre[it] = (j < jm && f0 + f < K) ? (T)sgn[jbase + j] * __ldg(Lam + (i64)conn[jbase + j] * K + f0 + f)
+                                                  : T(0);
+            }
         }
     };
     GemmCore<T, EPT> acc;
@@ -432,11 +446,18 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
             const int i = threadIdx.x + it * NT;
             xs[(i / kMixCols) * XS + i % kMixCols] = x;
         }
+        if (STREAM) {
+#pragma unroll
+            for (int it = 0; it < LITEMS; ++it) {
+                const int i = threadIdx.x + it * NT;
+                lam[(i >> 6) * LS + (i & 63)] = lpre[it];
+            }
+        }
         __syncthreads();
         if (step + 1 < nsteps) load_g(step + 1);
-        if (active) acc.step(lam, xs, f0, nf);
+        if (active) acc.step(lam, xs, STREAM ? 0 : f0, nf);
         if (fci == nfc - 1) {
-            if (active) acc.store(Z + (i64)a * M * W + cbi * kMixCols, W, m);
+            if (active) acc.store(Z + ((i64)a * M + jbase) * W + cbi * kMixCols, W, jm);
             acc.zero();
         }
     }
@@ -445,13 +466,13 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
 // ---- 4b. gather of the mixed contributions ------------------------------------------------
 template <typename Ti, typename T>
 __global__ void __launch_bounds__(256)
-mixed_gather_kernel(const MixedArgs P, const Ti *__restrict__ astr, const int *__restrict__ amap,
-                    const T *__restrict__ Z, double *__restrict__ sig, int z0, int W)
+mixed_gather_kernel(const MixedArgs P, const BasisView<Ti> BV, const T *__restrict__ Z, double *__restrict__ sig,
+                    int z0, int W)
 {
-    __shared__ int esrc[64], ej[64];
+    __shared__ int esrc[kMaxConn], ej[kMaxConn];
     __shared__ int wcnt[8], cnt;
     const int a = blockIdx.x;
-    const u64 s0 = (u64)astr[a];
+    const u64 s0 = (u64)BV.astrs[a];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (threadIdx.x == 0) cnt = 0;
     __syncthreads();
@@ -461,9 +482,9 @@ mixed_gather_kernel(const MixedArgs P, const Ti *__restrict__ astr, const int *_
         int src = -1, j = 0;
         if (e < P.nE && __popcll(s0 & P.Emask[e]) == 1) {
             const u64 s = s0 ^ P.Emask[e];
-            src = amap[s];
+            src = string_index(BV, BV.amap, BV.nel_a, (Ti)s);
             for (int e2 = 0; e2 < e; ++e2) j += __popcll(s & P.Emask[e2]) == 1;
-            ok = src >= 0 && j < 64;
+            ok = src >= 0 && j < kMaxConn;
         }
         const unsigned m = __ballot_sync(0xffffffffu, ok);
         if (lane == 0) wcnt[wid] = __popc(m);
@@ -472,13 +493,13 @@ mixed_gather_kernel(const MixedArgs P, const Ti *__restrict__ astr, const int *_
         for (int w2 = 0; w2 < wid; ++w2) off += wcnt[w2];
         if (ok) {
             const int p = off + __popc(m & ((1u << lane) - 1u));
-            if (p < 64) { esrc[p] = src; ej[p] = j; }
+            if (p < kMaxConn) { esrc[p] = src; ej[p] = j; }
         }
         __syncthreads();
         if (threadIdx.x == 0) for (int w2 = 0; w2 < 8; ++w2) cnt += wcnt[w2];
         __syncthreads();
     }
-    const int n = min(cnt, 64);
+    const int n = min(cnt, kMaxConn);
     const int zend = min(P.cend, z0 + W);
     for (int b = z0 + blockIdx.y * kRowChunk + threadIdx.x; b < min(zend, z0 + (blockIdx.y + 1) * kRowChunk);
          b += blockDim.x) {
@@ -744,15 +765,18 @@ static int launch_mixed(const DevBasis<Ti> *B, FastPlan<Ti> &P, FastScratch<Ti> 
     if ((rc = ensure(&S.Z, &S.z_n, per_col * Wz)) != BSIM_OK) return rc;
     MixedArgs ma{nA, nB, P.nE, P.nF, P.M, P.ldA, P.ldG, c1, P.d_Emask, P.d_mA,
                  sizeof(T) == 8 ? (const void *)P.d_Lam : (const void *)P.d_Lam32, P.d_gidx};
-    const size_t smem = mixed_smem_bytes(nB, P.nF, sizeof(T));
+    const bool stream = mixed_lam_streamed(nB, P.nF, sizeof(T));
+    const size_t smem = mixed_smem_bytes(nB, P.nF, sizeof(T), stream);
     if (smem > 227 * 1024) { set_error("mixed kernel needs %zu bytes of shared memory", smem); return BSIM_ERR_UNSUPPORTED; }
-    BSIM_CUDA(cudaFuncSetAttribute(mixed_gemm_kernel<Ti, T, EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
+    auto kern = stream ? mixed_gemm_kernel<Ti, T, EPT, true> : mixed_gemm_kernel<Ti, T, EPT, false>;
+    BSIM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     T *Z = static_cast<T *>(S.Z);
+    const int passes = (P.M + 63) / 64;   // 64 connected excitations per GEMM pass
     for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
-        STAGE(tm, 3, s, (mixed_gemm_kernel<Ti, T, EPT><<<nA, NT, smem, s>>>(ma, P.d_astr, ct, Z, z0, (int)Wz)));
+        for (int pass = 0; pass < passes; ++pass)
+            STAGE(tm, 3, s, (kern<<<nA, NT, smem, s>>>(ma, P.d_astr, ct, Z, z0, (int)Wz, 64 * pass)));
         dim3 g(nA, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
-        STAGE(tm, 4, s, (mixed_gather_kernel<Ti, T><<<g, 256, 0, s>>>(ma, P.d_astr, B->view.amap, Z, dst, z0, (int)Wz)));
+        STAGE(tm, 4, s, (mixed_gather_kernel<Ti, T><<<g, 256, 0, s>>>(ma, B->view, Z, dst, z0, (int)Wz)));
     }
     return BSIM_OK;
 }

@@ -144,3 +144,45 @@ def test_column_bands_reassemble_sigma(cuda, mixed):
     # misaligned band start is an argument error
     with pytest.raises(cuotf.CuOTFError):
         f.hvec_cols(x, y, 5, 40)
+
+
+def sparse_hamiltonian_network(norb, seed, nquads=1500):
+    """Jordan-Wigner network of a Hamiltonian with a random symmetric one-body part and
+    a few random 8-fold-symmetric two-body integrals (quick to build at any norb)."""
+    from binsim_b200 import network as nw
+    rng = np.random.default_rng(seed)
+    h = rng.normal(scale=0.1, size=(norb, norb))
+    h = h + h.T
+    g = np.zeros((norb,) * 4)
+    for _ in range(nquads):
+        p, q, r, s = rng.integers(0, norb, size=4)
+        v = rng.normal(scale=0.05)
+        for (a, b, c, d) in ((p, q, r, s), (q, p, s, r), (r, s, p, q), (s, r, q, p),
+                             (q, p, r, s), (p, q, s, r), (s, r, p, q), (r, s, q, p)):
+            g[a, b, c, d] = v   # (pq|rs) symmetric under the chemist's 8-fold permutations
+    eri = np.einsum("psqr->pqrs", g)   # passed as g[p,q,r,s] = (ps|qr)
+    x, z, c = nw.jw_hamiltonian_terms(h, eri, 0.0)
+    ax, az, bx, bz = nw.split_aabb(x, z, norb)
+    return nw.compress_groups(ax, az, bx, bz, c, norb)
+
+
+@pytest.mark.parametrize("norb,na,nb,bits", [(18, 5, 2, 32), (28, 3, 1, 32), (28, 3, 1, 64)])
+def test_structured_sigma_two_passes_and_streamed_lam(cuda, norb, na, nb, bits):
+    """More than 64 connected alpha singles per string (two GEMM passes), and at 28
+    orbitals a Lam too large for shared memory (streamed per F chunk) with ranked string
+    addressing, against the generic tile kernel (itself oracle-tested)."""
+    from binsim_b200 import cuotf
+    net = sparse_hamiltonian_network(norb, seed=norb + na)
+    B = cuotf.CuBasis(norb, na, nb, string_bits=bits)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net, string_bits=bits))
+    path = f.sigma_path()
+    assert path[0] == 1, path
+    x = dev(cuda, np.random.default_rng(2).normal(size=B.dim))
+    y = cuda.empty_like(x)
+    y_ref = cuda.empty_like(x)
+    f.hvec(x, y)
+    f.hvec_tiles(x, y_ref, 0, f.num_tiles())
+    scale = float(y_ref.abs().max())
+    assert float((y - y_ref).abs().max()) <= 1e-12 * scale
+    f.hvec_mixed(x, y)
+    assert float((y - y_ref).abs().max()) <= 2e-6 * scale

@@ -661,11 +661,9 @@ def gpu_vqe(args):
 # ADAPT workload: pool-gradient screening on UInt64 strings, plus the adjoint gradient
 # ---------------------------------------------------------------------------
 
-# BASELINE config 4 is 36 orbitals 3a+3b; its 516K Hamiltonian groups and 840K
-# pool components need sparse-regime kernels (the tile kernels visit every
-# (tile, group) pair), so the workload runs the same operator mix at 20 orbitals
-# (--adapt-norb sets it) on UInt64 strings
-ADAPT_CFG = dict(norb=20, na=3, nb=3, seed=0, n_gen=40, amp=0.05, ckpt=8)
+# 36 orbitals 3a+3b (7140^2 determinants): 516K Hamiltonian groups, 840K pool
+# components; --adapt-norb 20 gives a quick case of the same operator mix
+ADAPT_CFG = dict(norb=36, na=3, nb=3, seed=0, n_gen=40, amp=0.05, ckpt=8)
 ADAPT_METRIC = "ADAPT pool screening: spin-adapted pool gradients per second (UInt64 strings)"
 
 

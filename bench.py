@@ -556,6 +556,119 @@ def gpu_davidson(args):
 
 
 # ---------------------------------------------------------------------------
+# Block Davidson workload: lowest 2 roots, FP32 subspace + FP64 refinement
+# ---------------------------------------------------------------------------
+
+BLOCK_CFGS = {
+    # 18 orbitals 8a+8b (1.91e9 dets): 6 FP32 subspace vectors (7.66 GB each) plus their
+    # sigmas, FP64 roots; FP64 block Davidson with 6 kept vectors does not fit in HBM
+    "18o": dict(norb=18, na=8, nb=8, seed=0, nroots=2, maxspace=6, ncv=2, modes=("mixed",), scratch_gb=4.0,
+                maxiter=160),
+    # the same solver at 16 orbitals, where both precisions fit: the FP64/mixed comparison
+    "16o": dict(norb=16, na=8, nb=8, seed=0, nroots=2, maxspace=6, ncv=2, modes=("fp64", "mixed"), scratch_gb=24.0,
+                maxiter=400),
+}
+BLOCK_TOL = 1e-5
+BLOCK_METRIC = "FCI block Davidson time to the lowest 2 roots (FP64 residual norms < 1e-5)"
+
+
+def gpu_block_davidson(args):
+    import torch
+    from binsim_b200 import cuotf, network as nw
+    cfg = BLOCK_CFGS[args.block_size]
+    os.environ["BSIM_SIGMA_SCRATCH_GB"] = str(cfg["scratch_gb"])
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    net = nw.hamiltonian_network(cfg["norb"], seed=cfg["seed"])
+    B = cuotf.CuBasis(cfg["norb"], cfg["na"], cfg["nb"])
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    dim, k = B.dim, cfg["nroots"]
+    log(f"block davidson: network {net.ngs} groups, dim {dim:,}, setup {time.time() - t0:.1f}s")
+    X = torch.zeros((k, dim), dtype=torch.float64, device="cuda")
+    f.get_diags(X[0])                      # FP64 diagonal, kept in FP32 for the preconditioner
+    d32 = X[0].float()
+    X[0].zero_()
+    starts, saved = [], []
+    for _ in range(k):                     # the k lowest-diagonal determinants
+        i = int(torch.argmin(d32))
+        starts.append(i)
+        saved.append(float(d32[i]))
+        d32[i] = float("inf")
+    for i, v in zip(starts, saved):
+        d32[i] = v
+
+    def reset():
+        X.zero_()
+        for j, i in enumerate(starts):
+            X[j, i] = 1.0
+    # warm-up: plan build and both sigma precisions (the scratch reaches its FP64 size)
+    reset()
+    t1 = time.time()
+    for _ in range(max(1, args.warmup)):
+        f.hvec(X[0], X[1])
+        f.hvec_mixed(X[0], X[1])
+    torch.cuda.synchronize()
+    log(f"sigma path {f.sigma_path()}, warm-up {time.time() - t1:.1f}s")
+    # full-size checks on random vectors u, v: <v|H u> = <u|H v> (FP64), and the
+    # FP32-bulk sigma against the FP64 one
+    g = torch.Generator(device="cuda").manual_seed(1)
+    X[0].normal_(generator=g)
+    X[0] /= X[0].norm()
+    v = torch.empty(dim, dtype=torch.float64, device="cuda").normal_(generator=g)
+    v /= v.norm()
+    y = torch.empty_like(v)
+    f.hvec(X[0], X[1])
+    f.hvec(v, y)
+    a, b = float(torch.dot(v, X[1])), float(torch.dot(X[0], y))
+    f.hvec_mixed(X[0], y)
+    checks = {"symmetry_rel": abs(a - b) / abs(a),
+              "fp32_bulk_vs_fp64_rel": float((y - X[1]).abs().max() / X[1].abs().max())}
+    del v, y
+    torch.cuda.empty_cache()
+    log(f"full-size checks {checks}")
+    stages = {}
+    for mixed in (False, True):
+        reset()
+        tm = f.sigma_stage_times(X[0], X[1], mixed=mixed)
+        stages["fp32" if mixed else "fp64"] = {"total_ms": float(sum(v[0] for v in tm.values())),
+                                               "stages_ms": {kk: round(v[0], 3) for kk, v in tm.items()}}
+    out = {}
+    for mode in cfg["modes"]:
+        reset()
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = f.davidson_block(X, d32, k, tol=BLOCK_TOL, maxiter=cfg["maxiter"], ncv=cfg["ncv"],
+                              maxspace=cfg["maxspace"], mixed=(mode == "mixed"), verbose=args.verbose)
+        e1.record()
+        torch.cuda.synchronize()
+        st["seconds"] = e0.elapsed_time(e1) * 1e-3
+        st["free_gb_before"] = free0 / 1e9
+        out[mode] = st
+        log(f"{mode}: {st}")
+    main = out["mixed"]
+    res = {
+        "metric": BLOCK_METRIC, "value": main["seconds"], "unit": "s", "n_gpus": 1, "steps": 1,
+        "warmup": f"{max(1, args.warmup)} sigma applications per precision (one solve takes minutes)",
+        "ms_per_step": main["seconds"] * 1e3, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32 subspace / f64 refinement", "data": "synthetic",
+        "config": {"workload": f"mixed-precision block Davidson, lowest {k} roots, {cfg['norb']} orbitals "
+                               f"{cfg['na']}a+{cfg['nb']}b, {dim:,} dets, UInt32 strings, seeded synthetic "
+                               f"integrals (seed {cfg['seed']}), start: the {k} lowest-diagonal determinants, "
+                               f"{cfg['maxspace']} FP32 subspace vectors kept, restart to {cfg['ncv']}, FP32 "
+                               f"diagonal preconditioner, FP64 residual tol {BLOCK_TOL}",
+                   "dim": dim, "l2": "vectors larger than L2"},
+        "sigma_ms": stages, "sigma_checks": checks, "solves": out,
+    }
+    if "fp64" in out:
+        res["fp64_vs_mixed"] = {"speedup": out["fp64"]["seconds"] / main["seconds"],
+                                "max_abs_energy_diff": max(abs(a - b) for a, b in
+                                                           zip(out["fp64"]["energies"], main["energies"]))}
+    return res
+
+
+# ---------------------------------------------------------------------------
 # VQE workload: energy + full gradient by the adjoint sweep
 # ---------------------------------------------------------------------------
 
@@ -926,7 +1039,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="sigma", choices=["sigma", "davidson", "vqe", "adapt"])
+    ap.add_argument("--workload", default="sigma", choices=["sigma", "davidson", "vqe", "adapt", "block"])
+    ap.add_argument("--block-size", default="16o", choices=sorted(BLOCK_CFGS))
+    ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--adapt-state", default="")
     ap.add_argument("--adapt-sample", type=int, default=400)
     ap.add_argument("--adapt-norb", type=int, default=ADAPT_CFG["norb"])
@@ -959,7 +1074,8 @@ def main():
         # Davidson and VQE are single-state solves: one GPU (further ranks would be replicas)
         if rank != 0:
             return
-        result = {"davidson": gpu_davidson, "vqe": gpu_vqe, "adapt": gpu_adapt}[args.workload](args)
+        result = {"davidson": gpu_davidson, "vqe": gpu_vqe, "adapt": gpu_adapt,
+                  "block": gpu_block_davidson}[args.workload](args)
         if args.workload == "vqe" and not args.no_cpu_baseline:
             cpu = run_cpu_vqe(args)
             if cpu and "seconds" in cpu:

@@ -498,6 +498,31 @@ int bsim_davidson(void *basis, void *net, double *v0, const double *diags, doubl
     return rc;
 }
 
+int bsim_davidson_block(void *basis, void *net, int nroots, double *X, const void *diags, int diag_fp32, double tol,
+                        int maxiter, int ncv, int maxspace, int mixed, double *energies, double *residuals,
+                        int *iterations, int *sigma_fp64, int *sigma_fp32, int verbose, bsim_stream_t stream)
+{
+    if (int st0 = check_handles(basis, {net})) return st0;
+    NEED(X); NEED(diags);
+    bsim::DavBlockStats st{};
+    int rc = with_handles(basis, {net}, [&](auto *b) {
+        return bsim::davidson_block(b, net_of(b, net), nroots, X, diags, diag_fp32 != 0, tol, maxiter, ncv, maxspace,
+                                    mixed != 0, &st, verbose, stream);
+    });
+    if (rc == BSIM_OK) {
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) rc = bsim::cuda_status(e, "davidson_block");
+    }
+    for (int i = 0; i < nroots && i < bsim::kMaxRoots; ++i) {
+        if (energies) energies[i] = st.energy[i];
+        if (residuals) residuals[i] = st.residual[i];
+    }
+    if (iterations) *iterations = st.iterations;
+    if (sigma_fp64) *sigma_fp64 = st.sigma_fp64;
+    if (sigma_fp32) *sigma_fp32 = st.sigma_fp32;
+    return rc;
+}
+
 // ============================== Part 3 ======================================
 static double fetch1(const double *dev)
 {

@@ -23,6 +23,8 @@ template <typename TV, typename TX>
 int dav_combine(i64 n, int k, const double *coeffs, const TV *const *V, TX *x, cudaStream_t s);
 int dav_precondition(DavScratch &S, i64 n, double *r, const double *d, double e, double shift, double *norm_dev,
                      cudaStream_t s);
+int dav_precondition(DavScratch &S, i64 n, double *r, const float *d, double e, double shift, double *norm_dev,
+                     cudaStream_t s);
 template <typename TV>
 int dav_mgs(DavScratch &S, i64 n, int k, const TV *const *V, double *v, double *norm_dev, cudaStream_t s);
 int dav_normalize(DavScratch &S, i64 n, double *v, double *norm_dev, cudaStream_t s);
@@ -55,5 +57,22 @@ int davidson_fp64(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const 
 template <typename Ti>
 int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const double *diags, double tol,
                    int maxiter, int maxspace, double *x_out, DavStats *stats, int verbose, cudaStream_t s);
+
+// Lowest nroots eigenpairs by block Davidson (the reference driver,
+// jl/davidson.jl:1-185, generalised to a block of roots; the reference has a
+// single-root driver only).  X (device, nroots x dim, root-major) holds the
+// start vectors on entry and the Ritz vectors on exit; diag is FP64 or FP32.
+constexpr int kMaxRoots = 8;
+struct DavBlockStats {
+    double energy[kMaxRoots];
+    double residual[kMaxRoots];   // FP64 residual norms at exit
+    int iterations;               // expansion steps (FP32 phase + refinement)
+    int sigma_fp64, sigma_fp32;
+    int converged;
+};
+template <typename Ti>
+int davidson_block(const DevBasis<Ti> *B, const DevNet<Ti> *N, int nroots, double *X, const void *diag,
+                   bool diag32, double tol, int maxiter, int ncv, int maxspace, bool mixed, DavBlockStats *stats,
+                   int verbose, cudaStream_t s);
 
 }  // namespace bsim

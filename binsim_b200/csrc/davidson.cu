@@ -83,15 +83,17 @@ __global__ void combine_kernel(i64 n, int k, Coeffs c, Ptrs<TV> V, TX *__restric
     }
 }
 
-// r_i /= (d_i - e), denominator clamped to +-|shift|  (davidson.hpp:97-117)
-__global__ void precondition_kernel(i64 n, double *__restrict__ r, const double *__restrict__ d, double e,
+// r_i /= (d_i - e), denominator clamped to +-|shift|  (davidson.hpp:97-117); the
+// diagonal may be stored in FP32 (the preconditioner only needs it approximately)
+template <typename TD>
+__global__ void precondition_kernel(i64 n, double *__restrict__ r, const TD *__restrict__ d, double e,
                                     double shift, double *__restrict__ part)
 {
     __shared__ double red[32];
     const double as = fabs(shift);
     double s = 0.0;
     for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
-        double diff = d[i] - e;
+        double diff = (double)d[i] - e;
         if (fabs(diff) < as) diff = (diff >= 0) ? as : -as;
         const double v = r[i] / diff;
         r[i] = v;
@@ -208,16 +210,29 @@ int dav_combine(i64 n, int k, const double *coeffs, const TV *const *V, TX *x, c
     return BSIM_OK;
 }
 
-int dav_precondition(DavScratch &S, i64 n, double *r, const double *d, double e, double shift, double *norm_dev,
-                     cudaStream_t s)
+template <typename TD>
+static int precondition_impl(DavScratch &S, i64 n, double *r, const TD *d, double e, double shift,
+                             double *norm_dev, cudaStream_t s)
 {
     int st = S.ensure();
     if (st) return st;
     const int g = grid_for(n);
-    precondition_kernel<<<g, kRedThreads, 0, s>>>(n, r, d, e, shift, norm_dev ? S.part : nullptr);
+    precondition_kernel<TD><<<g, kRedThreads, 0, s>>>(n, r, d, e, shift, norm_dev ? S.part : nullptr);
     if (norm_dev) finish_kernel<<<1, 1024, 0, s>>>(S.part, g, 1, norm_dev, 1);
     BSIM_CUDA(cudaGetLastError());
     return BSIM_OK;
+}
+
+int dav_precondition(DavScratch &S, i64 n, double *r, const double *d, double e, double shift, double *norm_dev,
+                     cudaStream_t s)
+{
+    return precondition_impl(S, n, r, d, e, shift, norm_dev, s);
+}
+
+int dav_precondition(DavScratch &S, i64 n, double *r, const float *d, double e, double shift, double *norm_dev,
+                     cudaStream_t s)
+{
+    return precondition_impl(S, n, r, d, e, shift, norm_dev, s);
 }
 
 template <typename TV>

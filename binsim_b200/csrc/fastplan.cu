@@ -220,7 +220,7 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
         const int nU = (int)comb_count(norb - nel + 2, 2), npr = (int)comb_count(nel, 2);
         ri_grp[side].assign(ng, 0);
         const char *ri_env = getenv("BSIM_SIGMA_RI");   // BSIM_SIGMA_RI=0 keeps these groups in the row lists
-        if (nel < 2 || norb - nel < 2 || nU > 64 || npr > 64 || (ri_env && ri_env[0] == '0')) continue;
+        if (nel < 2 || norb - nel < 2 || nU > kRiMaxU || npr > 64 || (ri_env && ri_env[0] == '0')) continue;
         Wri[side].assign((size_t)nP * nP, 0.0);
         const auto &rows = side == 0 ? A : Bs;
         const StrIndex &rmap = side == 0 ? amap : bmap;
@@ -438,9 +438,8 @@ int build_fast_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastPlan<Ti> *P)
     P->M = M;
     if (M > kMaxConn && P->nE > 0) { P->why = "more than 128 connected alpha singles per string"; return BSIM_OK; }
 
-    P->fits64 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 8, mixed_lam_streamed(nB, P->nF, 8)) <= 227 * 1024;
-    P->fits32 = P->nE == 0 || mixed_smem_bytes(nB, P->nF, 4, mixed_lam_streamed(nB, P->nF, 4)) <= 227 * 1024;
-    if (!P->fits64 && !P->fits32) { P->why = "beta row too long for the mixed kernel's shared memory"; return BSIM_OK; }
+    P->row64 = P->nE == 0 || !mixed_shape(nB, P->nF, 8, kSmemMax).grow;
+    P->row32 = P->nE == 0 || !mixed_shape(nB, P->nF, 4, kSmemMax).grow;
 
     // ---- gather-index table of the mixed GEMM: X[F][b] = sB_F(b^F) c~[a', b^F] ------
     std::vector<int> gidx((size_t)P->nF * P->ldG, -1);

@@ -96,7 +96,7 @@ struct FastPlan {
     std::vector<double> Lam;           // [nE x nF]
     std::vector<int> residual;         // original group ids for the generic kernel
     i64 mixed_pairs = 0;
-    bool fits64 = false, fits32 = false;   // mixed GEMM shared memory fits (FP64 / FP32 rows)
+    bool row64 = false, row32 = false;     // the mixed GEMM stages the source row in shared memory (FP64 / FP32)
     // device
     Arena arena;
     const Ti *d_astr = nullptr, *d_bstr = nullptr;
@@ -119,30 +119,49 @@ struct FastPlan {
 
 constexpr int kMixCols = 128;                             // columns per GEMM chunk
 
-// Shared memory of the intermediate-string GEMM: W_m [nU x 64] and an X slice.
-// (Row strides: 68 / kMixCols + 4 elements for FP64, 64 / kMixCols for FP32;
-// rows rounded up to a multiple of 4.)
+// Shared memory of the intermediate-string GEMM: W_m [nU x ri_ls] and an X slice.
+// Output rows past 64 (up to kRiMaxU) are computed by all threads with scalar
+// FMAs next to the 64-row register tiles, so W_m rows are 8 elements wider
+// than the mixed GEMM's Lam_conn rows (72 / 76 elements: 4 mod 16 doubles for
+// the FP64 fragments' banks).
+constexpr int kRiMaxU = 72;
 inline size_t gemm_ls(size_t elem) { return elem == 8 ? 68 : 64; }
 inline size_t gemm_xs(size_t elem) { return elem == 8 ? kMixCols + 4 : kMixCols; }
+inline size_t ri_ls(size_t elem) { return gemm_ls(elem) + 8; }
 inline size_t ri_smem_bytes(int nU, size_t elem)
 {
-    return (((size_t)nU + 3) & ~size_t(3)) * gemm_ls(elem) * elem + 32 * gemm_xs(elem) * elem + 64 * 8;
+    return (((size_t)nU + 3) & ~size_t(3)) * ri_ls(elem) * elem + 32 * gemm_xs(elem) * elem + kRiMaxU * 8;
 }
 
-// Shared memory of the mixed GEMM kernel: source row, Lam_conn [K x 64], an
-// X slice [32 x kMixCols] and the connected-excitation lists.
+// Shared memory of the mixed GEMM kernel: source row (unless it is read from
+// global memory), Lam_conn [K x 64] (or one 32-row F chunk of it), an X slice
+// [32 x kMixCols] and the connected-excitation lists.
 constexpr int kMaxConn = 128;   // connected alpha singles per string: up to two 64-row GEMM passes
+constexpr size_t kSmemMax = 227 * 1024;
 
-// With `stream`, Lam_conn is staged one 32-row F chunk at a time instead of whole.
-inline size_t mixed_smem_bytes(int nB, int nF, size_t elem, bool stream)
+inline size_t mixed_smem_bytes(int nB, int nF, size_t elem, bool stream, bool grow)
 {
     const size_t lam_rows = stream ? 32 : (((size_t)nF + 3) & ~size_t(3));
-    return (((size_t)nB + 7) & ~size_t(7)) * elem + lam_rows * gemm_ls(elem) * elem + 32 * gemm_xs(elem) * elem +
-           2 * kMaxConn * 4;
+    return (grow ? 0 : (((size_t)nB + 7) & ~size_t(7)) * elem) + lam_rows * gemm_ls(elem) * elem +
+           32 * gemm_xs(elem) * elem + 2 * kMaxConn * 4;
 }
-inline bool mixed_lam_streamed(int nB, int nF, size_t elem)
+
+// Kernel shape of the mixed GEMM: the source row is staged in shared memory
+// when it fits under row_limit (Lam_conn streamed per F chunk if needed), else
+// the X gather reads it from global memory (an 18-orbital FP64 row is 350 KB).
+struct MixedShape {
+    bool stream, grow;
+    size_t smem;
+};
+inline MixedShape mixed_shape(int nB, int nF, size_t elem, size_t row_limit)
 {
-    return mixed_smem_bytes(nB, nF, elem, false) > 226 * 1024;
+    const size_t lim = row_limit < kSmemMax ? row_limit : kSmemMax;
+    for (int grow = 0; grow < 2; ++grow)
+        for (int stream = 0; stream < 2; ++stream) {
+            const size_t b = mixed_smem_bytes(nB, nF, elem, stream, grow);
+            if (b <= (grow ? kSmemMax : lim)) return MixedShape{stream != 0, grow != 0, b};
+        }
+    return MixedShape{true, true, mixed_smem_bytes(nB, nF, elem, true, true)};
 }
 
 template <typename Ti>

@@ -1,17 +1,20 @@
 // Structured sigma (single-block bases): see fastplan.h for the frame.
 //
 // Per sigma application, with c~ = eps * c:
-//   1. frame_transpose : c~ (row-major, rows padded to ldA) and c~^T (rows
-//                        padded to ldB)                                  [HBM streaming]
+//   1. frame       : c~ (row-major, rows padded to ldA)               [HBM streaming]
 //   2. pure_rows(alpha): s~ = D * c~ + sum_pure-alpha PA(a') PB(b) c~[a', b]
-//   3. pure_rows(beta) : t  = same on c~^T with the pure-beta groups
-//   4. per column tile of the intermediate Z:
+//   3. per column tile of the intermediate Z:
 //        mixed_gemm   : for every source row a', X[F][b] = sB_F c~[a', b^F] is
 //                       gathered once (through the precomputed index table
 //                       gidx[F][b]) and Y = Lam_conn(a') X is a register-blocked
 //                       GEMM; Z[a'][j][b] = sA_E(a') Y[j][b]
 //        mixed_gather : s~[a, b] += sum_E Z[a^E][j(E)][b]               [coalesced]
-//   5. final: sigma = eps * (s~ + t^T)
+//   4. transpose   : c~^T (rows padded to ldB) into the buffer c~ held
+//   5. pure_rows(beta) : t  = same as 2 on c~^T with the pure-beta groups
+//   6. final: sigma = eps * (s~ + t^T)
+// The alpha side runs first so that c~ and c~^T share one buffer and t's buffer
+// holds the alpha side's intermediate Z: the scratch of one sigma is one input
+// copy in the bulk precision plus one FP64 vector (and a bounded Z).
 // Steps 2/3 read source rows with 16-byte vector loads; the grid runs
 // column-chunk-major so the chunk of every source row stays in L2 while all
 // destination rows use it.
@@ -61,9 +64,10 @@ __global__ void frame_transpose_kernel(int nA, int nB, int ldA, int ldB, const T
             v = (T)c[(i64)a * nB + b];
             if (par((u64)bstr[b] & Ka[a])) v = -v;
         }
-        if (a < nA && b < ldA) ct[(i64)a * ldA + b] = v;
+        if (ct && a < nA && b < ldA) ct[(i64)a * ldA + b] = v;
         tile[i][tx] = v;
     }
+    if (!ctT) return;   // uniform across the CTA
     __syncthreads();
     for (int i = ty; i < 32; i += blockDim.y) {
         const int b = b0 + i, a = a0 + tx;
@@ -296,9 +300,10 @@ struct GemmCore {
     GemmTile<T, EPT> acc;
     __device__ __forceinline__ void zero() { acc.zero(); }
     __device__ __forceinline__ static bool active(int rows) { return (int)(threadIdx.x >> 5) * EPT < rows; }
+    template <int LS = GemmLayout<T>::LS>
     __device__ __forceinline__ void step(const T *lam, const T *xs, int f0, int nf)
     {
-        constexpr int LS = GemmLayout<T>::LS, XS = GemmLayout<T>::XS;
+        constexpr int XS = GemmLayout<T>::XS;
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll 4
         for (int f = 0; f < nf; ++f) {
@@ -334,9 +339,10 @@ struct GemmCore<double, EPT> {
         for (int k = 0; k < 8; ++k) c[k][0] = c[k][1] = 0.0;
     }
     __device__ __forceinline__ static bool active(int rows) { return (int)(threadIdx.x >> 6) * 8 < rows; }
+    template <int LS = GemmLayout<double>::LS>
     __device__ __forceinline__ void step(const double *lam, const double *xs, int f0, int nf)
     {
-        constexpr int LS = GemmLayout<double>::LS, XS = GemmLayout<double>::XS;
+        constexpr int XS = GemmLayout<double>::XS;
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
         const int g = lane >> 2, t = lane & 3, rb = wid >> 1, ch = wid & 1;
         const double *la = lam + (size_t)(f0 + t) * LS + rb * 8 + g;
@@ -366,8 +372,10 @@ struct GemmCore<double, EPT> {
 // the row's connected list; lane l owns columns {2l, 2l+1, 64+2l, 64+2l+1} of a
 // kMixCols-column chunk (conflict-free 2-element shared loads).  The X slice for
 // (chunk, 32 F) is filled from the gather-index table, whose next slice is
-// loaded into registers while the current one is multiplied.
-template <typename Ti, typename T, int EPT, bool STREAM>
+// loaded into registers while the current one is multiplied.  With GROW the
+// source row stays in global memory (L2) and the next slice's values, not only
+// their indices, are prefetched.
+template <typename Ti, typename T, int EPT, bool STREAM, bool GROW>
 __global__ void __launch_bounds__((64 / EPT) * 32, sizeof(T) == 4 ? 2 : 1)
 mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__restrict__ ct, T *__restrict__ Z,
                   int z0, int W, int jbase)
@@ -377,10 +385,10 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
     constexpr int LITEMS = STREAM ? 32 * 64 / NT : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.nF, M = P.M;
-    T *srow = reinterpret_cast<T *>(smem_raw);                    // [ldA]
+    T *srow = reinterpret_cast<T *>(smem_raw);                    // [ldA] unless GROW
     constexpr int LS = GemmLayout<T>::LS, XS = GemmLayout<T>::XS;
     const int Kp = (K + 3) & ~3;
-    T *lam = srow + P.ldA;                                         // [Kp or 32][LS], rows past K zero
+    T *lam = srow + (GROW ? 0 : P.ldA);                            // [Kp or 32][LS], rows past K zero
     T *xs = lam + (size_t)(STREAM ? 32 : Kp) * LS;                 // [32][XS]
     int *conn = reinterpret_cast<int *>(xs + 32 * XS);             // [kMaxConn]
     int *sgn = conn + kMaxConn;                                    // [kMaxConn]
@@ -389,10 +397,11 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
     const int m = connected_excitations<NT>(P, (u64)astr[a], conn, sgn, wcnt, &cnt);
     const int jm = min(64, m - jbase);   // output rows of this pass
     if (jm <= 0) return;                 // uniform across the CTA
+    const T *grow = ct + (i64)a * P.ldA;
     // stage the source row (16-byte copies) and, when it fits, Lam restricted to
     // this pass's connected excitations
-    {
-        const int4 *src = reinterpret_cast<const int4 *>(ct + (i64)a * P.ldA);
+    if (!GROW) {
+        const int4 *src = reinterpret_cast<const int4 *>(grow);
         int4 *dst = reinterpret_cast<int4 *>(srow);
         const int n16 = (int)((size_t)P.ldA * sizeof(T) / 16);
         for (int i = threadIdx.x; i < n16; i += NT) dst[i] = __ldg(src + i);
@@ -408,7 +417,8 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
     const int nfc = (K + 31) / 32;
     const int nsteps = ncb * nfc;
     const bool active = GemmCore<T, EPT>::active(jm);
-    int gpre[ITEMS];
+    int gpre[GROW ? 1 : ITEMS];
+    T gval[GROW ? ITEMS : 1];
     T lpre[LITEMS];
     auto load_g = [&](int step) {
         const int cb = z0 + (step / nfc) * kMixCols, f0 = (step % nfc) * 32;
@@ -416,7 +426,17 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
         for (int it = 0; it < ITEMS; ++it) {
             const int i = threadIdx.x + it * NT;
             const int f = i / kMixCols, cl = i % kMixCols;
-            gpre[it] = f0 + f < K ? __ldg(P.gidx + (i64)(f0 + f) * P.ldG + cb + cl) : -1;
+            const int g = f0 + f < K ? __ldg(P.gidx + (i64)(f0 + f) * P.ldG + cb + cl) : -1;
+            if constexpr (GROW) {
+                T x = T(0);
+                if (g >= 0) {
+                    x = __ldg(grow + (g >> 1));
+                    if (g & 1) x = -x;
+                }
+                gval[it] = x;
+            } else {
+                gpre[it] = g;
+            }
         }
         if (STREAM) {
 #pragma unroll
@@ -437,11 +457,16 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
         __syncthreads();   // the previous slice is consumed (and srow/lam are staged)
 #pragma unroll
         for (int it = 0; it < ITEMS; ++it) {
-            const int g = gpre[it];
-            T x = T(0);
-            if (g >= 0) {
-                x = srow[g >> 1];
-                if (g & 1) x = -x;
+            T x;
+            if constexpr (GROW) {
+                x = gval[it];
+            } else {
+                const int g = gpre[it];
+                x = T(0);
+                if (g >= 0) {
+                    x = srow[g >> 1];
+                    if (g & 1) x = -x;
+                }
             }
             const int i = threadIdx.x + it * NT;
             xs[(i / kMixCols) * XS + i % kMixCols] = x;
@@ -520,24 +545,26 @@ struct RIArgs {
 // nU pairs outside m (coalesced row segments, the next slice prefetched into
 // registers), Z[m][j][col] = sum_k W[pair_j][pair_k] X[k][col].  Same tiling as
 // the mixed GEMM: warp w owns output rows w*EPT.., lane l owns columns
-// {2l, 2l+1, 64+2l, 64+2l+1} of a kMixCols chunk.
+// {2l, 2l+1, 64+2l, 64+2l+1} of a kMixCols chunk.  Rows 64 .. nU-1 (at most
+// kRiMaxU - 64; 66 pairs at 18 orbitals and 8 electrons) are computed by every
+// thread with scalar FMAs, one (row, column) output per thread and pass.
 template <typename T, int EPT>
 __global__ void __launch_bounds__((64 / EPT) * 32, sizeof(T) == 4 ? 2 : 1)
 ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int z0, int W)
 {
     constexpr int NT = (64 / EPT) * 32;
     constexpr int ITEMS = 32 * kMixCols / NT;
-    using V2 = typename Vec2<T>::type;
+    constexpr int TQ = ((kRiMaxU - 64) * kMixCols + NT - 1) / NT;   // tail outputs per thread
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.nU;
-    constexpr int LS = GemmLayout<T>::LS, XS = GemmLayout<T>::XS;
+    constexpr int LS = GemmLayout<T>::LS + 8, XS = GemmLayout<T>::XS;
     const int Kp = (K + 3) & ~3;
     T *wm = reinterpret_cast<T *>(smem_raw);                          // [Kp][LS], rows >= K zero
     T *xs = wm + (size_t)Kp * LS;                                      // [32][XS]
-    long long *soff = reinterpret_cast<long long *>(xs + 32 * XS);     // [64]
+    long long *soff = reinterpret_cast<long long *>(xs + 32 * XS);     // [kRiMaxU]
     const int m = blockIdx.x;
     const int *srcm = P.src + (i64)m * K, *pidm = P.pid + (i64)m * K;
-    for (int i = threadIdx.x; i < 64; i += NT) {
+    for (int i = threadIdx.x; i < kRiMaxU; i += NT) {
         long long o = 0;
         if (i < K) {
             const int v = srcm[i];
@@ -556,6 +583,7 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
     const int nfc = (K + 31) / 32;
     const int nsteps = ncb * nfc;
     const bool active = GemmCore<T, EPT>::active(K);
+    const int ntail = K > 64 ? (K - 64) * kMixCols : 0;
     T gpre[ITEMS];
     auto load_x = [&](int step) {
         const int cb = z0 + (step / nfc) * kMixCols, f0 = (step % nfc) * 32;
@@ -574,6 +602,9 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
     };
     GemmCore<T, EPT> acc;
     acc.zero();
+    T tacc[TQ];
+#pragma unroll
+    for (int q = 0; q < TQ; ++q) tacc[q] = T(0);
     if (nsteps > 0) load_x(0);
     for (int step = 0; step < nsteps; ++step) {
         const int cbi = step / nfc, fci = step % nfc;
@@ -586,10 +617,26 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
         }
         __syncthreads();
         if (step + 1 < nsteps) load_x(step + 1);
-        if (active) acc.step(wm, xs, f0, nf);
+        if (active) acc.template step<LS>(wm, xs, f0, nf);
+#pragma unroll
+        for (int q = 0; q < TQ; ++q) {
+            const int o = threadIdx.x + q * NT;
+            if (o < ntail) {
+                const int row = 64 + o / kMixCols, col = o % kMixCols;
+                T t = tacc[q];
+                for (int f = 0; f < nf; ++f) t += wm[(f0 + f) * LS + row] * xs[f * XS + col];
+                tacc[q] = t;
+            }
+        }
         if (fci == nfc - 1) {
             if (active) acc.store(Z + (i64)m * K * W + cbi * kMixCols, W, K);
             acc.zero();
+#pragma unroll
+            for (int q = 0; q < TQ; ++q) {
+                const int o = threadIdx.x + q * NT;
+                if (o < ntail) Z[((i64)m * K + 64 + o / kMixCols) * W + cbi * kMixCols + o % kMixCols] = tacc[q];
+                tacc[q] = T(0);
+            }
         }
     }
 }
@@ -645,12 +692,15 @@ __global__ void final_kernel(int nA, int nB, int ldB, int col_begin, int col_end
 }
 
 // ---- host ------------------------------------------------------------------------------------
+// in: c~ (alpha side), then c~^T (beta side); tT: the alpha side's Z, then the
+// beta-side result t; Z: the beta side's Z, and the alpha side's when the
+// scratch budget allows a wider chunk than tT holds.
 template <typename Ti>
 struct FastScratch {
-    void *ct = nullptr, *ctT = nullptr, *Z = nullptr, *tT = nullptr;
-    size_t ct_n = 0, ctT_n = 0, z_n = 0, tT_n = 0;
+    void *in = nullptr, *tT = nullptr, *Z = nullptr;
+    size_t in_n = 0, tT_n = 0, z_n = 0;
     ~FastScratch() {
-        for (void *p : {ct, ctT, Z, tT})
+        for (void *p : {in, tT, Z})
             if (p) cudaFree(p);
     }
 };
@@ -696,6 +746,35 @@ static int ensure(void **p, size_t *have, size_t bytes)
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) { *p = nullptr; return cuda_status(e, "sigma scratch"); }
     *have = bytes;
+    return BSIM_OK;
+}
+
+// Largest shared-memory footprint for which the mixed GEMM keeps the source row
+// on chip (BSIM_MIXED_ROW_SMEM bytes lowers it, which moves the row to global
+// memory at small sizes too).
+static size_t mixed_row_limit()
+{
+    const char *e = getenv("BSIM_MIXED_ROW_SMEM");
+    return e ? (size_t)atoll(e) : kSmemMax;
+}
+
+// Intermediate Z of one stage: chunk width (columns, a multiple of kMixCols) and
+// buffer.  A buffer that is free during the stage (spare) is used when it holds
+// at least the width the scratch budget would give; otherwise the Z scratch
+// grows to the budget.
+struct ZSlot {
+    void *p;
+    size_t w;
+};
+static int z_slot(void **zbuf, size_t *zhave, void *spare, size_t spare_n, size_t per_col, int ncols, ZSlot *out)
+{
+    const size_t need = ((size_t)ncols + kMixCols - 1) / kMixCols * kMixCols;
+    const size_t wb = std::min(need, std::max<size_t>(kMixCols, (scratch_budget() / per_col) / kMixCols * kMixCols));
+    const size_t ws = spare ? std::min(need, (spare_n / per_col) / kMixCols * kMixCols) : 0;
+    if (ws >= wb) { *out = ZSlot{spare, ws}; return BSIM_OK; }
+    const int rc = ensure(zbuf, zhave, per_col * wb);
+    if (rc != BSIM_OK) return rc;
+    *out = ZSlot{*zbuf, wb};
     return BSIM_OK;
 }
 
@@ -752,53 +831,61 @@ struct StageTimer {
         if (tm) { int rc__ = (tm)->end(s); if (rc__) return rc__; } \
     } while (0)
 
+template <typename Ti, typename T, int EPT, bool STREAM, bool GROW>
+static int launch_mixed_shape(const DevBasis<Ti> *B, FastPlan<Ti> &P, const MixedArgs &ma, const T *ct, T *Z,
+                              double *dst, int c0, int c1, size_t Wz, size_t smem, cudaStream_t s, StageTimer *tm)
+{
+    constexpr int NT = (64 / EPT) * 32;
+    auto kern = mixed_gemm_kernel<Ti, T, EPT, STREAM, GROW>;
+    BSIM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int passes = (P.M + 63) / 64;   // 64 connected excitations per GEMM pass
+    for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
+        for (int pass = 0; pass < passes; ++pass)
+            STAGE(tm, 3, s, (kern<<<P.nA, NT, smem, s>>>(ma, P.d_astr, ct, Z, z0, (int)Wz, 64 * pass)));
+        dim3 g(P.nA, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
+        STAGE(tm, 4, s, (mixed_gather_kernel<Ti, T><<<g, 256, 0, s>>>(ma, B->view, Z, dst, z0, (int)Wz)));
+    }
+    return BSIM_OK;
+}
+
 template <typename Ti, typename T, int EPT>
 static int launch_mixed(const DevBasis<Ti> *B, FastPlan<Ti> &P, FastScratch<Ti> &S, const T *ct, double *dst,
                         int c0, int c1, cudaStream_t s, StageTimer *tm)
 {
-    constexpr int NT = (64 / EPT) * 32;
-    const int nA = P.nA, nB = P.nB;
-    const size_t per_col = (size_t)nA * P.M * sizeof(T);
-    size_t Wz = std::max<size_t>(kMixCols, (scratch_budget() / per_col) / kMixCols * kMixCols);
-    Wz = std::min<size_t>(Wz, ((size_t)(c1 - c0) + kMixCols - 1) / kMixCols * kMixCols);
-    int rc;
-    if ((rc = ensure(&S.Z, &S.z_n, per_col * Wz)) != BSIM_OK) return rc;
-    MixedArgs ma{nA, nB, P.nE, P.nF, P.M, P.ldA, P.ldG, c1, P.d_Emask, P.d_mA,
+    const size_t per_col = (size_t)P.nA * P.M * sizeof(T);
+    ZSlot z;
+    int rc = z_slot(&S.Z, &S.z_n, S.tT, S.tT_n, per_col, c1 - c0, &z);
+    if (rc != BSIM_OK) return rc;
+    MixedArgs ma{P.nA, P.nB, P.nE, P.nF, P.M, P.ldA, P.ldG, c1, P.d_Emask, P.d_mA,
                  sizeof(T) == 8 ? (const void *)P.d_Lam : (const void *)P.d_Lam32, P.d_gidx};
-    const bool stream = mixed_lam_streamed(nB, P.nF, sizeof(T));
-    const size_t smem = mixed_smem_bytes(nB, P.nF, sizeof(T), stream);
-    if (smem > 227 * 1024) { set_error("mixed kernel needs %zu bytes of shared memory", smem); return BSIM_ERR_UNSUPPORTED; }
-    auto kern = stream ? mixed_gemm_kernel<Ti, T, EPT, true> : mixed_gemm_kernel<Ti, T, EPT, false>;
-    BSIM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    T *Z = static_cast<T *>(S.Z);
-    const int passes = (P.M + 63) / 64;   // 64 connected excitations per GEMM pass
-    for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
-        for (int pass = 0; pass < passes; ++pass)
-            STAGE(tm, 3, s, (kern<<<nA, NT, smem, s>>>(ma, P.d_astr, ct, Z, z0, (int)Wz, 64 * pass)));
-        dim3 g(nA, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
-        STAGE(tm, 4, s, (mixed_gather_kernel<Ti, T><<<g, 256, 0, s>>>(ma, B->view, Z, dst, z0, (int)Wz)));
-    }
-    return BSIM_OK;
+    const MixedShape sh = mixed_shape(P.nB, P.nF, sizeof(T), mixed_row_limit());
+    if (sh.smem > kSmemMax) { set_error("mixed kernel needs %zu bytes of shared memory", sh.smem); return BSIM_ERR_UNSUPPORTED; }
+    T *Z = static_cast<T *>(z.p);
+    if (sh.grow)
+        return sh.stream ? launch_mixed_shape<Ti, T, EPT, true, true>(B, P, ma, ct, Z, dst, c0, c1, z.w, sh.smem, s, tm)
+                         : launch_mixed_shape<Ti, T, EPT, false, true>(B, P, ma, ct, Z, dst, c0, c1, z.w, sh.smem, s, tm);
+    return sh.stream ? launch_mixed_shape<Ti, T, EPT, true, false>(B, P, ma, ct, Z, dst, c0, c1, z.w, sh.smem, s, tm)
+                     : launch_mixed_shape<Ti, T, EPT, false, false>(B, P, ma, ct, Z, dst, c0, c1, z.w, sh.smem, s, tm);
 }
 
 // Same-spin doubles of one side through the intermediate strings, columns [c0, c1)
 // of the side's rows (all rows), accumulated into out.
 template <typename T, int EPT>
 static int launch_ri(const RISide &R, const T *in, int ld_in, double *out, int ld_out, int nrows, int c0, int c1,
-                     void **zbuf, size_t *zhave, cudaStream_t s, StageTimer *tm)
+                     void **zbuf, size_t *zhave, void *spare, size_t spare_n, cudaStream_t s, StageTimer *tm)
 {
     constexpr int NT = (64 / EPT) * 32;
     if (c1 <= c0) return BSIM_OK;
     const size_t per_col = (size_t)R.nM * R.nU * sizeof(T);
-    size_t Wz = std::max<size_t>(kMixCols, (scratch_budget() / per_col) / kMixCols * kMixCols);
-    Wz = std::min<size_t>(Wz, ((size_t)(c1 - c0) + kMixCols - 1) / kMixCols * kMixCols);
-    int rc;
-    if ((rc = ensure(zbuf, zhave, per_col * Wz)) != BSIM_OK) return rc;
+    ZSlot z;
+    int rc = z_slot(zbuf, zhave, spare, spare_n, per_col, c1 - c0, &z);
+    if (rc != BSIM_OK) return rc;
+    const size_t Wz = z.w;
     RIArgs ra{R.nM, R.nU, R.npr, R.nP, ld_in, c1, R.src, R.pid,
               sizeof(T) == 8 ? (const void *)R.W : (const void *)R.W32};
     const size_t smem = ri_smem_bytes(R.nU, sizeof(T));
     BSIM_CUDA(cudaFuncSetAttribute(ri_gemm_kernel<T, EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    T *Z = static_cast<T *>(*zbuf);
+    T *Z = static_cast<T *>(z.p);
     for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
         STAGE(tm, 7, s, (ri_gemm_kernel<T, EPT><<<R.nM, NT, smem, s>>>(ra, in, Z, z0, (int)Wz)));
         dim3 g(nrows, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
@@ -815,50 +902,51 @@ static int run_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastState<Ti> *s
     FastScratch<Ti> &S = st->scratch;
     const int nA = P.nA, nB = P.nB;
     int rc;
-    if ((rc = ensure(&S.ct, &S.ct_n, (size_t)nA * P.ldA * sizeof(T))) != BSIM_OK) return rc;
-    if ((rc = ensure(&S.ctT, &S.ctT_n, (size_t)nB * P.ldB * sizeof(T))) != BSIM_OK) return rc;
+    const size_t in_bytes = std::max((size_t)nA * P.ldA, (size_t)nB * P.ldB) * sizeof(T);
+    if ((rc = ensure(&S.in, &S.in_n, in_bytes)) != BSIM_OK) return rc;
     if ((rc = ensure(&S.tT, &S.tT_n, (size_t)nB * P.ldB * sizeof(double))) != BSIM_OK) return rc;
-    T *ct = static_cast<T *>(S.ct), *ctT = static_cast<T *>(S.ctT);
+    T *in = static_cast<T *>(S.in);
     double *tT = static_cast<double *>(S.tT);
-    // 1. frame + transpose (grid covers the padded strides)
     dim3 tgrid((nB + 31) / 32, (nA + 31) / 32), tblk(32, 8);
-    if (src32)
-        STAGE(tm, 0, s, (frame_transpose_kernel<Ti, float, T><<<tgrid, tblk, 0, s>>>(nA, nB, P.ldA, P.ldB, P.d_bstr,
-                                                                                   P.d_Ka, src32, ct, ctT)));
-    else
-        STAGE(tm, 0, s, (frame_transpose_kernel<Ti, double, T><<<tgrid, tblk, 0, s>>>(nA, nB, P.ldA, P.ldB, P.d_bstr,
-                                                                                    P.d_Ka, src, ct, ctT)));
-    // 2. pure alpha + diagonal -> dst (the frame's s~)
-    {
-        dim3 g(nA, (c1 - c0 + kRowChunk - 1) / kRowChunk);
-        STAGE(tm, 1, s, (pure_rows_kernel<T><<<g, 256, 0, s>>>(0, c0, c1, P.ldA, P.csrA, ct, dst, nB,
-                                                               P.rank_d ? P.d_PAd : nullptr, P.d_PBdT, P.rank_d)));
-    }
+    auto frame = [&](T *ct, T *ctT) {
+        if (src32)
+            frame_transpose_kernel<Ti, float, T><<<tgrid, tblk, 0, s>>>(nA, nB, P.ldA, P.ldB, P.d_bstr, P.d_Ka, src32,
+                                                                         ct, ctT);
+        else
+            frame_transpose_kernel<Ti, double, T><<<tgrid, tblk, 0, s>>>(nA, nB, P.ldA, P.ldB, P.d_bstr, P.d_Ka, src,
+                                                                          ct, ctT);
+    };
     // FP64: 16 warps of DMMA 8x8 tiles; FP32: 8 warps of 8 x 4 f32x2 register tiles
     constexpr int kEPT = sizeof(T) == 8 ? 4 : 8;
-    // 2b. same-spin alpha doubles through intermediate strings -> dst
-    if (P.riA.on) {
-        rc = launch_ri<T, kEPT>(P.riA, ct, P.ldA, dst, nB, nA, c0, c1, &S.Z, &S.z_n, s, tm);
+    // ---- alpha side: c~ in `in`, results into dst; tT's buffer is free for Z ----
+    STAGE(tm, 0, s, frame(in, nullptr));
+    {   // pure alpha + diagonal -> dst (the frame's s~)
+        dim3 g(nA, (c1 - c0 + kRowChunk - 1) / kRowChunk);
+        STAGE(tm, 1, s, (pure_rows_kernel<T><<<g, 256, 0, s>>>(0, c0, c1, P.ldA, P.csrA, in, dst, nB,
+                                                               P.rank_d ? P.d_PAd : nullptr, P.d_PBdT, P.rank_d)));
+    }
+    if (P.riA.on) {   // same-spin alpha doubles through intermediate strings -> dst
+        rc = launch_ri<T, kEPT>(P.riA, in, P.ldA, dst, nB, nA, c0, c1, &S.Z, &S.z_n, S.tT, S.tT_n, s, tm);
         if (rc != BSIM_OK) return rc;
     }
-    // 3. pure beta on the transposed vector -> tT (the beta doubles through
-    //    intermediates when the whole sigma is computed, else through the rows)
+    if (P.nE > 0 && P.nF > 0 && P.M > 0) {
+        rc = launch_mixed<Ti, T, kEPT>(B, P, S, in, dst, c0, c1, s, tm);
+        if (rc != BSIM_OK) return rc;
+    }
+    // ---- beta side: c~^T in `in`, result t^T in tT (the beta doubles through
+    //      intermediates when the whole sigma is computed, else through the rows) ----
+    STAGE(tm, 0, s, frame(nullptr, in));
     const bool ri_b = P.riB.on && c0 == 0 && c1 == nB;
     {
         dim3 g(c1 - c0, (nA + kRowChunk - 1) / kRowChunk);
-        STAGE(tm, 2, s, (pure_rows_kernel<T><<<g, 256, 0, s>>>(c0, 0, nA, P.ldB, ri_b ? P.csrBri : P.csrB, ctT, tT,
+        STAGE(tm, 2, s, (pure_rows_kernel<T><<<g, 256, 0, s>>>(c0, 0, nA, P.ldB, ri_b ? P.csrBri : P.csrB, in, tT,
                                                                P.ldB, nullptr, nullptr, 0)));
     }
     if (ri_b) {
-        rc = launch_ri<T, kEPT>(P.riB, ctT, P.ldB, tT, P.ldB, nB, 0, nA, &S.Z, &S.z_n, s, tm);
+        rc = launch_ri<T, kEPT>(P.riB, in, P.ldB, tT, P.ldB, nB, 0, nA, &S.Z, &S.z_n, nullptr, 0, s, tm);
         if (rc != BSIM_OK) return rc;
     }
-    // 4. mixed
-    if (P.nE > 0 && P.nF > 0 && P.M > 0) {
-        rc = launch_mixed<Ti, T, kEPT>(B, P, S, ct, dst, c0, c1, s, tm);
-        if (rc != BSIM_OK) return rc;
-    }
-    // 5. final combine
+    // ---- final combine ----
     dim3 fgrid((c1 - c0 + 31) / 32, (nA + 31) / 32);
     STAGE(tm, 5, s, (final_kernel<Ti><<<fgrid, tblk, 0, s>>>(nA, nB, P.ldB, c0, c1, P.d_bstr, P.d_Ka, tT, dst)));
     BSIM_CUDA(cudaGetLastError());
@@ -873,7 +961,7 @@ static int sigma_fast_impl(const DevBasis<Ti> *B, const DevNet<Ti> *N, const dou
     FastState<Ti> *st = nullptr;
     int rc = get_fast(B, N, &st);
     if (rc != BSIM_OK) return rc;
-    if (!st->plan.ok || (mixed ? !st->plan.fits32 : !st->plan.fits64)) return BSIM_OK;
+    if (!st->plan.ok) return BSIM_OK;
     rc = mixed ? run_fast<Ti, float>(B, N, st, src, src32, dst, 0, st->plan.nB, s, tm)
                : run_fast<Ti, double>(B, N, st, src, nullptr, dst, 0, st->plan.nB, s, tm);
     if (rc != BSIM_OK) return rc;
@@ -901,9 +989,9 @@ int sigma_fast_cols(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *sr
     int rc = get_fast(B, N, &st);
     if (rc != BSIM_OK) return rc;
     const FastPlan<Ti> &P = st->plan;
-    if (!P.ok || (mixed ? !P.fits32 : !P.fits64) || !P.residual.empty()) {
+    if (!P.ok || !P.residual.empty()) {
         set_error("column-band sigma needs the structured path with no residual groups (%s)",
-                  P.ok ? "residual groups or shared memory" : P.why.c_str());
+                  P.ok ? "residual groups" : P.why.c_str());
         return BSIM_ERR_UNSUPPORTED;
     }
     if (col_lo < 0 || col_hi > P.nB || col_lo > col_hi || (col_lo % kMixCols) != 0) {
@@ -934,9 +1022,11 @@ int fast_sigma_info(const DevBasis<Ti> *B, const DevNet<Ti> *N, std::string *why
     FastState<Ti> *st = nullptr;
     int rc = get_fast(B, N, &st);
     if (rc != BSIM_OK) return rc;
-    *why = st->plan.ok ? "structured" : st->plan.why;
+    *why = st->plan.ok ? std::string("structured") + (st->plan.riA.on ? " ri-alpha" : "") +
+                             (st->plan.riB.on ? " ri-beta" : "")
+                       : st->plan.why;
     *nresid = (int)st->plan.residual.size();
-    return st->plan.ok ? (st->plan.fits64 ? 1 : 2) : 0;
+    return st->plan.ok ? (st->plan.row64 ? 1 : 2) : 0;
 }
 
 template int fast_sigma_info<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, std::string *, int *);

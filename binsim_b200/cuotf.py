@@ -86,6 +86,7 @@ def lib() -> C.CDLL:
         "bsim_prepare_state": (ci, [vp, vp, i64, vp, vp, vp, vp, vp, i64, vp, vp]),
         "bsim_vqe_energy_grad": (ci, [vp, vp, vp, i64, vp, vp, i64, vp, vp, vp, i64, i64, vp, vp, vp, vp, vp, vp]),
         "bsim_davidson": (ci, [vp, vp, vp, vp, dbl, ci, ci, ci, ci, vp, vp, vp, vp, vp, vp, ci, vp]),
+        "bsim_davidson_block": (ci, [vp, vp, ci, vp, vp, ci, dbl, ci, ci, ci, ci, vp, vp, vp, vp, vp, ci, vp]),
         # part 3
         "build_ritz_and_residual_cuda": (dbl, [i64, ci, vp, dbl, vp, vp, vp]),
         "build_ritz_vector_cuda": (None, [i64, ci, vp, vp, vp]),
@@ -246,7 +247,8 @@ class CuOTFFunctions:
                                      1 if mixed else 0, _stream(stream)), "hvec_tiles")
 
     def sigma_path(self):
-        """(path, reason, residual groups): path 1 structured, 2 structured FP32 only, 0 generic."""
+        """(path, reason, residual groups): path 1 structured, 2 structured with the FP64
+        source row in global memory, 0 generic."""
         buf = C.create_string_buffer(256)
         nres = C.c_int()
         r = lib().bsim_hvec_path(self.basis.h, self.ham.h, buf, 256, C.byref(nres))
@@ -331,3 +333,19 @@ class CuOTFFunctions:
                                    C.byref(s64), C.byref(s32), 1 if verbose else 0, _stream(stream)), "davidson")
         return dict(energy=e.value, residual=r.value, iterations=it.value, sigma_fp64=s64.value,
                     sigma_fp32=s32.value)
+
+    def davidson_block(self, X, diags, nroots, tol=1e-5, maxiter=200, ncv=None, maxspace=None, mixed=False,
+                       verbose=False, stream=None):
+        """Lowest ``nroots`` eigenpairs by block Davidson.  X (device, nroots x dim FP64):
+        start vectors in, Ritz vectors out; diags FP64 or FP32 (device).  Returns a
+        stats dict with per-root energies and FP64 residual norms."""
+        ncv = nroots if ncv is None else ncv
+        maxspace = ncv + 2 * nroots if maxspace is None else maxspace
+        d32 = 1 if str(diags.dtype).endswith("float32") else 0
+        en, rs = (C.c_double * nroots)(), (C.c_double * nroots)()
+        it, s64, s32 = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().bsim_davidson_block(self.basis.h, self.ham.h, nroots, _ptr(X), _ptr(diags), d32, tol, maxiter,
+                                         ncv, maxspace, 1 if mixed else 0, en, rs, C.byref(it), C.byref(s64),
+                                         C.byref(s32), 1 if verbose else 0, _stream(stream)), "davidson_block")
+        return dict(energies=list(en), residuals=list(rs), iterations=it.value, sigma_fp64=s64.value,
+                    sigma_fp32=s32.value, converged=all(r < tol for r in rs))

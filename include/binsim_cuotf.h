@@ -131,8 +131,10 @@ int bsim_hvec_mixed(void *basis, void *net, const double *src, double *dst, bsim
 /* As bsim_hvec_mixed with an FP32 input vector. */
 int bsim_hvec_f32in(void *basis, void *net, const float *src, double *dst, bsim_stream_t stream);
 /* Which sigma kernel bsim_hvec uses for this (basis, network) pair: 1 the
- * structured path (FP64 and FP32-bulk), 2 structured for FP32 bulk only, 0 the
- * generic tile kernel; negative on error.  why receives the reason, and
+ * structured path with the mixed GEMM's source row in shared memory, 2 the
+ * structured path with the FP64 source row read from global memory (beta rows
+ * longer than shared memory, e.g. 18 orbitals 8 electrons), 0 the generic tile
+ * kernel; negative on error.  why receives the reason, and
  * residual_groups the number of groups the structured path leaves to the
  * generic kernel.  Builds (and caches) the plan on first use. */
 int bsim_hvec_path(void *basis, void *net, char *why, int why_len, int *residual_groups);
@@ -214,6 +216,23 @@ int bsim_vqe_energy_grad(void *basis, void *ham, void *pool, int64_t n_ops, cons
 int bsim_davidson(void *basis, void *net, double *v0, const double *diags, double tol, int maxiter, int ncv,
                   int maxspace, int mixed, double *x_out, double *energy, double *residual, int *iterations,
                   int *sigma_fp64, int *sigma_fp32, int verbose, bsim_stream_t stream);
+/* Lowest nroots (1..8) eigenpairs by block Davidson on device: the steps of
+ * jl/davidson.jl:1-185 (Ritz residual, clamped preconditioner, MGS, restart to
+ * ncv Ritz vectors) applied to every unconverged root of the block; the
+ * reference driver follows one root only.  X (device, nroots x dim, FP64,
+ * root-major): start vectors on entry (orthonormalised in place), Ritz vectors
+ * on exit.  diags: the Hamiltonian diagonal, FP64 (diag_fp32 = 0) or FP32 (1).
+ * nroots <= ncv <= 8, ncv + nroots <= maxspace <= 64.  mixed = 0: FP64
+ * subspace (the first nroots subspace vectors are X itself) and FP64 sigma.
+ * mixed = 1: FP32 subspace storage and FP32-bulk sigma until the FP32
+ * residuals reach tol or stall, then FP64 refinement of the block (FP64 sigma
+ * and Rayleigh-Ritz among the roots, FP32 corrections coupled through the FP64
+ * sigmas) until every FP64 residual norm is below tol.  energies, residuals
+ * (host, nroots): Ritz values and FP64 residual norms at exit; convergence is
+ * residuals[i] < tol for all i.  Outputs may be NULL. */
+int bsim_davidson_block(void *basis, void *net, int nroots, double *X, const void *diags, int diag_fp32, double tol,
+                        int maxiter, int ncv, int maxspace, int mixed, double *energies, double *residuals,
+                        int *iterations, int *sigma_fp64, int *sigma_fp32, int verbose, bsim_stream_t stream);
 
 /* ========================================================================
  * Part 3: libdiag's Davidson helpers (diag/declare.hpp:4-75) on device

@@ -83,3 +83,50 @@ def test_davidson_fp64_and_mixed(cuda, oracle):
     sm = f.davidson(v0.clone(), diags, xm, tol=1e-6, maxiter=300, maxspace=12, mixed=True)
     assert abs(sm["energy"] - e_ref) < 1e-8, (sm, e_ref)
     assert sm["sigma_fp32"] > 0 and sm["residual"] < 1e-6
+
+
+@pytest.mark.parametrize("mixed,diag32", [(False, False), (True, False), (True, True)])
+def test_block_davidson_lowest_two_roots(cuda, oracle, mixed, diag32):
+    """Block Davidson for 2 roots (FP64, and FP32 storage with FP64 refinement, with an
+    FP64 or FP32 diagonal) against the oracle's two lowest eigenvalues (scipy eigsh over
+    the oracle sigma): energies within 1e-9, H x_i = E_i x_i, orthonormal Ritz vectors."""
+    from binsim_b200 import cuotf, network as nw
+    norb, na, nb = 9, 4, 4
+    net = nw.hamiltonian_network(norb, seed=21)
+    Bo, No = oracle.basis(norb, na, nb), oracle.network(net)
+    e_ref = _lowest(oracle, Bo, No, k=2)
+    B = cuotf.CuBasis(norb, na, nb)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    diags = cuda.zeros(B.dim, dtype=cuda.float64, device="cuda")
+    f.get_diags(diags)
+    X = cuda.zeros((2, B.dim), dtype=cuda.float64, device="cuda")
+    low = cuda.argsort(diags)[:2]
+    X[0, low[0]] = 1.0
+    X[1, low[1]] = 1.0
+    d = diags.float() if diag32 else diags
+    st = f.davidson_block(X, d, 2, tol=1e-6, maxiter=400, ncv=2, maxspace=8, mixed=mixed)
+    assert st["converged"], st
+    np.testing.assert_allclose(st["energies"], e_ref, rtol=0, atol=1e-9)
+    if mixed:
+        assert st["sigma_fp32"] > st["sigma_fp64"] > 0
+    else:
+        assert st["sigma_fp32"] == 0
+    G = (X @ X.T).cpu().numpy()
+    np.testing.assert_allclose(G, np.eye(2), atol=1e-10)
+    for i in range(2):
+        hx = cuda.empty_like(diags)
+        f.hvec(X[i].contiguous(), hx)
+        r = float((hx - st["energies"][i] * X[i]).norm())
+        assert r < 2e-6, (i, r)
+
+
+def test_block_davidson_rejects_bad_shapes(cuda):
+    from binsim_b200 import cuotf, network as nw
+    B = cuotf.CuBasis(6, 3, 3)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(nw.hamiltonian_network(6, seed=1)))
+    d = cuda.ones(B.dim, dtype=cuda.float64, device="cuda")
+    X = cuda.zeros((2, B.dim), dtype=cuda.float64, device="cuda")
+    with pytest.raises(cuotf.CuOTFError):   # maxspace < ncv + nroots
+        f.davidson_block(X, d, 2, ncv=2, maxspace=3)
+    with pytest.raises(cuotf.CuOTFError):   # linearly dependent start vectors
+        f.davidson_block(X, d, 2)

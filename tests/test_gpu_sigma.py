@@ -186,3 +186,51 @@ def test_structured_sigma_two_passes_and_streamed_lam(cuda, norb, na, nb, bits):
     assert float((y - y_ref).abs().max()) <= 1e-12 * scale
     f.hvec_mixed(x, y)
     assert float((y - y_ref).abs().max()) <= 2e-6 * scale
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_mixed_gemm_source_row_in_global_memory(cuda, oracle, monkeypatch, mixed):
+    """The mixed GEMM reading its source row from global memory (the kernel shape used
+    when a beta row exceeds shared memory: FP64 at 18 orbitals, 8 electrons) gives the
+    same bits as the row staged on chip, and the oracle's sigma."""
+    from binsim_b200 import cuotf, network as nw
+    norb, na, nb = 11, 5, 5
+    net = nw.hamiltonian_network(norb, seed=5)
+    B = cuotf.CuBasis(norb, na, nb)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    assert f.sigma_path()[0] == 1
+    xh = np.random.default_rng(3).normal(size=B.dim)
+    x = dev(cuda, xh)
+    y_chip, y_glob = cuda.empty_like(x), cuda.empty_like(x)
+    run = f.hvec_mixed if mixed else f.hvec
+    run(x, y_chip)
+    monkeypatch.setenv("BSIM_MIXED_ROW_SMEM", "1")
+    run(x, y_glob)
+    monkeypatch.delenv("BSIM_MIXED_ROW_SMEM")
+    assert cuda.equal(y_chip, y_glob)
+    ref = oracle.hvec(oracle.basis(norb, na, nb), oracle.network(net), xh)
+    tol = 2e-6 if mixed else 1e-12
+    assert np.abs(y_glob.cpu().numpy() - ref).max() <= tol * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("norb,na,nb", [(13, 3, 3), (13, 3, 4), (14, 4, 4)])
+def test_intermediate_string_gemm_beyond_64_pairs(cuda, oracle, norb, na, nb):
+    """66 pairs outside each (n-2)-electron intermediate string (the count at 18 orbitals,
+    8 electrons): rows 64-65 of the intermediate-string GEMM come from the tail FMAs.
+    Against the oracle, and against the same sigma with those doubles in the row lists."""
+    from binsim_b200 import cuotf, network as nw
+    net = nw.hamiltonian_network(norb, seed=norb + nb)
+    B = cuotf.CuBasis(norb, na, nb)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    path, why, _ = f.sigma_path()
+    assert path == 1 and "ri-alpha" in why and "ri-beta" in why, why
+    xh = np.random.default_rng(norb).normal(size=B.dim)
+    x = dev(cuda, xh)
+    y = cuda.empty_like(x)
+    f.hvec(x, y)
+    ref = oracle.hvec(oracle.basis(norb, na, nb), oracle.network(net), xh)
+    scale = np.abs(ref).max()
+    np.testing.assert_allclose(y.cpu().numpy(), ref, rtol=0, atol=1e-12 * scale)
+    ym = cuda.empty_like(x)
+    f.hvec_mixed(x, ym)
+    assert np.abs(ym.cpu().numpy() - ref).max() <= 2e-6 * scale

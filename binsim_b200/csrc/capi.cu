@@ -171,6 +171,26 @@ void batchgrad_cuda(void *basis, void *net, const double *thetas, const double *
     report(bsim_batchgrad(basis, net, thetas, l, r, grads, nullptr), "batchgrad_cuda");
 }
 
+void tvec_cuda(void *basis, void *net, int64_t idx, const double *src, double *dst)
+{
+    report(bsim_tvec(basis, net, idx, src, dst, nullptr), "tvec_cuda");
+}
+
+void backtran_cuda(void *basis, void *net, int64_t idx, double theta, double *l, double *r, double *b)
+{
+    report(bsim_backtran(basis, net, idx, theta, l, r, b, nullptr), "backtran_cuda");
+}
+
+void batchexpm_cuda(void *basis, void *net, int64_t idx, double theta, double *matrix, int ld, int num_vecs)
+{
+    report(bsim_batchexpm(basis, net, idx, theta, matrix, ld, num_vecs, nullptr), "batchexpm_cuda");
+}
+
+void batchtran_cuda(void *basis, void *net, const double *l, const double *r, double *trans)
+{
+    report(bsim_batchtran(basis, net, l, r, trans, nullptr), "batchtran_cuda");
+}
+
 void expm_cuda_2d(void *basis, void *net, int64_t idx, double theta, double *vec)
 {
     expm_cuda(basis, net, idx, theta, vec);
@@ -435,6 +455,40 @@ int bsim_batchgrad(void *basis, void *net, const double *thetas, const double *l
     return with_handles(basis, {net}, [&](auto *b) {
         return bsim::batchgrad(b, net_of(b, net), thetas, l, r, grads, stream);
     });
+}
+
+int bsim_tvec(void *basis, void *net, int64_t idx, const double *src, double *dst, bsim_stream_t stream)
+{
+    if (int st0 = check_handles(basis, {net})) return st0;
+    NEED(src); NEED(dst);
+    return with_handles(basis, {net}, [&](auto *b) { return bsim::tvec(b, net_of(b, net), idx, src, dst, stream); });
+}
+
+int bsim_backtran(void *basis, void *net, int64_t idx, double theta, double *l, double *r, double *bvec,
+                  bsim_stream_t stream)
+{
+    if (int st0 = check_handles(basis, {net})) return st0;
+    NEED(l); NEED(r); NEED(bvec);
+    return with_handles(basis, {net}, [&](auto *b) {
+        return bsim::backtran(b, net_of(b, net), idx, theta, l, r, bvec, stream);
+    });
+}
+
+int bsim_batchexpm(void *basis, void *net, int64_t idx, double theta, double *matrix, int ld, int num_vecs,
+                   bsim_stream_t stream)
+{
+    if (int st0 = check_handles(basis, {net})) return st0;
+    NEED(matrix);
+    return with_handles(basis, {net}, [&](auto *b) {
+        return bsim::batchexpm(b, net_of(b, net), idx, theta, matrix, ld, num_vecs, stream);
+    });
+}
+
+int bsim_batchtran(void *basis, void *net, const double *l, const double *r, double *trans, bsim_stream_t stream)
+{
+    if (int st0 = check_handles(basis, {net})) return st0;
+    NEED(l); NEED(r); NEED(trans);
+    return with_handles(basis, {net}, [&](auto *b) { return bsim::batchtran(b, net_of(b, net), l, r, trans, stream); });
 }
 
 int bsim_prepare_state(void *basis, void *pool, int64_t n_ops, const int64_t *op_idx, const int64_t *param_idx,

@@ -73,6 +73,21 @@ int backgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta,
              double *out_dev, bool accumulate, cudaStream_t s);
 
 // Pool gradient: grads[orig] = grad of every group at thetas[orig] (device arrays).
+// Single-group operators of the reference CPU library without a GPU
+// counterpart there (op/tvec.hpp, op/backtran.hpp, op/batchexpm.hpp,
+// op/batchtran.hpp): dst = T src; l, r <- e^{theta T}; b = T l; e^{theta T} on
+// nv columns of a row-major dim x ld matrix; <l|T_g|r> for every group.
+template <typename Ti>
+int tvec(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, const double *src, double *dst, cudaStream_t s);
+template <typename Ti>
+int backtran(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta, double *l, double *r, double *b,
+             cudaStream_t s);
+template <typename Ti>
+int batchexpm(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta, double *matrix, int ld, int nv,
+              cudaStream_t s);
+template <typename Ti>
+int batchtran(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *l, const double *r, double *trans,
+              cudaStream_t s);
 template <typename Ti>
 int batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *thetas, const double *l,
               const double *r, double *grads, cudaStream_t s);
@@ -83,7 +98,8 @@ inline i64 pair_grid(const DevBasis<Ti> *B) { return (i64)B->max_na * B->num_blo
 
 // Angle terms of the pair updates (core/math.hpp:132-215).
 struct PairAngles { double c0, c1, c2, c3; };
-enum PairOpKind { kPairExpm = 0, kPairGrad = 1, kPairBackgrad = 2 };
+enum PairOpKind { kPairExpm = 0, kPairGrad = 1, kPairBackgrad = 2, kPairTvec = 3, kPairBacktran = 4, kPairTran = 5,
+                  kPairBatchExpm = 6 };
 
 // Gradients of every group of a pool network in one launch over the pair lists
 // (single-block bases, ranks <= 4); *used = false when the tile kernel must run.

@@ -1,7 +1,10 @@
 // Single-generator pair operators: expm, grad, backgrad
 // (reference op/expm.hpp:374-438, op/grad.hpp:397-465, op/backgrad.hpp:406-474,
 //  update rules core/math.hpp:132-215; GPU counterparts cuda/expm.cuh,
-//  cuda/grad.cuh, cuda/backgrad.cuh).
+//  cuda/grad.cuh, cuda/backgrad.cuh), and the operators the reference has on
+// the CPU only: tvec (op/tvec.hpp), backtran (op/backtran.hpp), batchexpm
+// (op/batchexpm.hpp) and the per-group transition <l|T|r> of batchtran
+// (op/batchtran.hpp), with the update rules of core/math.hpp:165-252.
 //
 // Launch shape: one CTA per destination alpha row of every block
 // (grid = max_na x num_blocks).  A CTA whose row is connected to a source row
@@ -21,13 +24,23 @@ namespace bsim {
 constexpr int kPairThreads = 256;
 constexpr int kExpm = kPairExpm, kGrad = kPairGrad, kBackgrad = kPairBackgrad;
 
+// third vector (backtran's b) and the matrix shape of batchexpm
+struct PairExtra {
+    double *b;
+    int ld, nv;
+};
+// operators that act on diagonal groups too (the others skip them: real vectors)
+__host__ __device__ constexpr bool pair_diag_op(int op) { return op == kPairTvec || op == kPairBacktran || op == kPairTran; }
+// operators with a scalar result (deterministic last-CTA reduction)
+__host__ __device__ constexpr bool pair_reduces(int op) { return op == kPairGrad || op == kPairBackgrad || op == kPairTran; }
+
 // Ticket counters for the last-CTA reduction live with the partials: the
 // scratch buffer holds [nslots partials][1 counter as unsigned long long].
 template <typename Ti, int OP>
 __global__ void __launch_bounds__(kPairThreads)
 pair_row_kernel(const BasisView<Ti> B, const NetView<Ti> N, int gid, PairAngles ang, double *__restrict__ l,
                 double *__restrict__ r, double *__restrict__ partials, unsigned long long *__restrict__ ticket,
-                double *__restrict__ out, int accumulate)
+                double *__restrict__ out, int accumulate, PairExtra X)
 {
     __shared__ double spa[kMaxRank];
     __shared__ double red[32];
@@ -35,7 +48,7 @@ pair_row_kernel(const BasisView<Ti> B, const NetView<Ti> N, int gid, PairAngles 
     const int kd = blockIdx.y, a = blockIdx.x;
     const GroupDev g = N.g[gid];
     const int nirr = B.num_irreps;
-    bool active = (g.type != 0) && a < B.blk_na[kd];
+    bool active = (g.type != 0 || pair_diag_op(OP)) && a < B.blk_na[kd];
     int ks = -1, sa = -1;
     Ti s_a = 0;
     if (active) {
@@ -92,6 +105,38 @@ pair_row_kernel(const BasisView<Ti> B, const NetView<Ti> N, int gid, PairAngles 
                 const double vd = ang.c0 * (vt * vt), vo = ang.c1 * vt;
                 const double rvi = r[si], rvj = r[di];
                 acc += l[si] * (rvi * vd + rvj * vo) + l[di] * (rvj * vd - rvi * vo);
+            } else if (OP == kPairTvec) {
+                // tvec_update, core/math.hpp:165-170: l = src, r = dst; a diagonal
+                // group has si == di and the second store leaves dst = src * vt
+                const double ss = l[si], sd = l[di];
+                r[si] = sd * (-vt);
+                r[di] = ss * vt;
+            } else if (OP == kPairBacktran) {
+                if (g.type == 0) {   // op/backtran.hpp:7-70: the diagonal exponential is 1
+                    X.b[di] = l[di] * vt;
+                } else {             // backtran_update, core/math.hpp:217-226
+                    const double vd = 1.0 + ang.c0 * (vt * vt), vo = ang.c1 * vt;
+                    const double li = l[si], lj = l[di], ri = r[si], rj = r[di];
+                    const double ls = li * vd - lj * vo, ld = lj * vd + li * vo;
+                    l[si] = ls;
+                    l[di] = ld;
+                    r[si] = ri * vd - rj * vo;
+                    r[di] = rj * vd + ri * vo;
+                    X.b[si] = ld * (-vt);
+                    X.b[di] = ls * vt;
+                }
+            } else if (OP == kPairTran) {
+                // tran_update, core/math.hpp:180-184; diagonal groups l_i vt r_i (op/batchtran.hpp:7-81)
+                acc += g.type == 0 ? l[di] * vt * r[di] : l[si] * vt * r[di] - l[di] * vt * r[si];
+            } else if (OP == kPairBatchExpm) {
+                // expm_batch_update_matrix, core/math.hpp:228-252: the first nv entries of rows si, di
+                const double vd = 1.0 + ang.c0 * (vt * vt), vo = ang.c1 * vt;
+                double *sp = l + si * X.ld, *dp = l + di * X.ld;
+                for (int k = 0; k < X.nv; ++k) {
+                    const double vi = sp[k], vj = dp[k];
+                    sp[k] = vi * vd - vj * vo;
+                    dp[k] = vj * vd + vi * vo;
+                }
             } else {
                 // backgrad_update, core/math.hpp:187-215
                 const double evd = 1.0 + ang.c0 * (vt * vt), evo = ang.c1 * vt;
@@ -107,7 +152,7 @@ pair_row_kernel(const BasisView<Ti> B, const NetView<Ti> N, int gid, PairAngles 
             }
         }
     }
-    if (OP == kExpm) return;
+    if (!pair_reduces(OP)) return;
     // ---- deterministic reduction --------------------------------------------
     acc = warp_sum(acc);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -167,17 +212,18 @@ static int pair_scratch(const DevBasis<Ti> *B, double **part, unsigned long long
 
 template <typename Ti, int OP>
 static int launch_pair(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, PairAngles ang, double *l, double *r,
-                       double *out, bool accumulate, cudaStream_t s, double *ext_part, size_t ext_n)
+                       double *out, bool accumulate, cudaStream_t s, double *ext_part, size_t ext_n,
+                       PairExtra X = PairExtra{nullptr, 0, 0})
 {
     int st = check_group(N, gidx);
     if (st != BSIM_OK) return st;
     if (B->num_blocks == 0 || B->max_na == 0) {
-        if (OP != kExpm && !accumulate) BSIM_CUDA(cudaMemsetAsync(out, 0, sizeof(double), s));
+        if (pair_reduces(OP) && !accumulate) BSIM_CUDA(cudaMemsetAsync(out, 0, sizeof(double), s));
         return BSIM_OK;
     }
     double *part = nullptr;
     unsigned long long *ticket = nullptr;
-    if (OP != kExpm) {
+    if (pair_reduces(OP)) {
         if (ext_part) {
             if (ext_n < (size_t)pair_grid(B) + 1) { set_error("scratch too small"); return BSIM_ERR_TOO_LARGE; }
             part = ext_part;
@@ -187,12 +233,14 @@ static int launch_pair(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, Pai
             if (st != BSIM_OK) return st;
         }
     }
-    bool used = false;
-    st = pair_list_launch<Ti, OP>(B, N, gidx, ang, l, r, part, ticket, pair_grid(B), out, accumulate, s, &used);
-    if (st != BSIM_OK || used) return st;
+    if constexpr (OP <= kPairBackgrad) {   // the pair-list kernels serve expm, grad, backgrad
+        bool used = false;
+        st = pair_list_launch<Ti, OP>(B, N, gidx, ang, l, r, part, ticket, pair_grid(B), out, accumulate, s, &used);
+        if (st != BSIM_OK || used) return st;
+    }
     dim3 grid(B->max_na, B->num_blocks);
     pair_row_kernel<Ti, OP><<<grid, kPairThreads, 0, s>>>(B->view, N->view, (int)gidx, ang, l, r, part, ticket, out,
-                                                         accumulate ? 1 : 0);
+                                                         accumulate ? 1 : 0, X);
     BSIM_CUDA(cudaGetLastError());
     return BSIM_OK;
 }
@@ -221,6 +269,80 @@ int backgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta,
     PairAngles a{cos(theta) - 1.0, -sin(theta), -sin(theta), cos(theta)};
     return launch_pair<Ti, kBackgrad>(B, N, gidx, a, l, r, out_dev, accumulate, s, nullptr, 0);
 }
+
+template <typename Ti>
+int tvec(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, const double *src, double *dst, cudaStream_t s)
+{
+    if (B->dim > 0) BSIM_CUDA(cudaMemsetAsync(dst, 0, sizeof(double) * B->dim, s));   // op/tvec.hpp: dst zeroed
+    return launch_pair<Ti, kPairTvec>(B, N, gidx, PairAngles{0, 0, 0, 0}, const_cast<double *>(src), dst, nullptr,
+                                      false, s, nullptr, 0);
+}
+
+template <typename Ti>
+int backtran(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta, double *l, double *r, double *b,
+             cudaStream_t s)
+{
+    if (B->dim > 0) BSIM_CUDA(cudaMemsetAsync(b, 0, sizeof(double) * B->dim, s));     // op/backtran.hpp: b zeroed
+    PairAngles a{cos(theta) - 1.0, sin(theta), 0.0, 0.0};                            // backtran.hpp:75-76
+    return launch_pair<Ti, kPairBacktran>(B, N, gidx, a, l, r, nullptr, false, s, nullptr, 0, PairExtra{b, 0, 0});
+}
+
+template <typename Ti>
+int batchexpm(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, double theta, double *matrix, int ld, int nv,
+              cudaStream_t s)
+{
+    if (nv < 0 || ld < nv) { set_error("batchexpm needs 0 <= num_vecs <= ld (got %d, %d)", nv, ld); return BSIM_ERR_ARG; }
+    int st = check_group(N, gidx);
+    if (st != BSIM_OK) return st;
+    if (nv == 0 || N->groups[gidx].type == 0) return BSIM_OK;   // diagonal groups: identity for real vectors
+    PairAngles a{cos(theta) - 1.0, sin(theta), 0.0, 0.0};
+    return launch_pair<Ti, kPairBatchExpm>(B, N, gidx, a, matrix, nullptr, nullptr, false, s, nullptr, 0,
+                                           PairExtra{nullptr, ld, nv});
+}
+
+// trans[orig] = <l|T_g|r> for every group (op/batchtran.hpp:514-528): the
+// off-diagonal groups through the pool-gradient kernels at theta = 0 (the
+// update rules coincide there), the diagonal groups through the row kernel.
+template <typename Ti>
+int batchtran(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *l, const double *r, double *trans,
+              cudaStream_t s)
+{
+    if (N->ngs == 0) return BSIM_OK;
+    double *zeros = nullptr;
+    BSIM_CUDA(cudaMallocAsync(&zeros, sizeof(double) * N->ngs, s));
+    cudaError_t e = cudaMemsetAsync(zeros, 0, sizeof(double) * N->ngs, s);
+    int st = e == cudaSuccess ? BSIM_OK : cuda_status(e, "batchtran");
+    if (st == BSIM_OK) e = cudaMemsetAsync(trans, 0, sizeof(double) * N->ngs, s);
+    if (st == BSIM_OK && e != cudaSuccess) st = cuda_status(e, "batchtran");
+    if (st == BSIM_OK) st = batchgrad(B, N, zeros, l, r, trans, s);
+    cudaFreeAsync(zeros, s);
+    if (st != BSIM_OK) return st;
+    for (i64 g = 0; g < N->ngs; ++g) {
+        const GroupDev &G = N->groups[g];
+        if (G.type != 0) continue;
+        st = launch_pair<Ti, kPairTran>(B, N, g, PairAngles{0, 0, 0, 0}, const_cast<double *>(l),
+                                        const_cast<double *>(r), trans + G.orig, true, s, nullptr, 0);
+        if (st != BSIM_OK) return st;
+    }
+    return BSIM_OK;
+}
+
+template int tvec<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, const double *, double *,
+                            cudaStream_t);
+template int backtran<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, double, double *, double *,
+                                double *, cudaStream_t);
+template int batchexpm<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, double, double *, int,
+                                 int, cudaStream_t);
+template int batchtran<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *, const double *,
+                                 double *, cudaStream_t);
+template int tvec<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *, i64,
+                                      const double *, double *, cudaStream_t);
+template int backtran<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *,
+                                          i64, double, double *, double *, double *, cudaStream_t);
+template int batchexpm<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *,
+                                           i64, double, double *, int, int, cudaStream_t);
+template int batchtran<unsigned long long>(const DevBasis<unsigned long long> *, const DevNet<unsigned long long> *,
+                                           const double *, const double *, double *, cudaStream_t);
 
 template int expm<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, double, double *, cudaStream_t);
 template int grad<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64, double, const double *,

@@ -83,6 +83,14 @@ def lib() -> C.CDLL:
         "bsim_backgrad": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_grad_noalloc": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_batchgrad": (ci, [vp, vp, vp, vp, vp, vp, vp]),
+        "bsim_tvec": (ci, [vp, vp, i64, vp, vp, vp]),
+        "bsim_backtran": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
+        "bsim_batchexpm": (ci, [vp, vp, i64, dbl, vp, ci, ci, vp]),
+        "bsim_batchtran": (ci, [vp, vp, vp, vp, vp, vp]),
+        "tvec_cuda": (None, [vp, vp, i64, vp, vp]),
+        "backtran_cuda": (None, [vp, vp, i64, dbl, vp, vp, vp]),
+        "batchexpm_cuda": (None, [vp, vp, i64, dbl, vp, ci, ci]),
+        "batchtran_cuda": (None, [vp, vp, vp, vp, vp]),
         "bsim_prepare_state": (ci, [vp, vp, i64, vp, vp, vp, vp, vp, i64, vp, vp]),
         "bsim_vqe_energy_grad": (ci, [vp, vp, vp, i64, vp, vp, i64, vp, vp, vp, i64, i64, vp, vp, vp, vp, vp, vp]),
         "bsim_davidson": (ci, [vp, vp, vp, vp, dbl, ci, ci, ci, ci, vp, vp, vp, vp, vp, vp, ci, vp]),
@@ -294,6 +302,27 @@ class CuOTFFunctions:
     def batchgrad(self, lv, rv, grads, x, stream=None):
         _check(lib().bsim_batchgrad(self.basis.h, self.pool.h, _ptr(x), _ptr(lv), _ptr(rv), _ptr(grads),
                                     _stream(stream)), "batchgrad")
+
+    # the CPU-only operators of the reference (jl/network.jl:451-466)
+    def tvec(self, idx: int, lv, rv, stream=None):
+        """|rv> = T_idx |lv> (1-based idx)."""
+        _check(lib().bsim_tvec(self.basis.h, self.pool.h, idx - 1, _ptr(lv), _ptr(rv), _stream(stream)), "tvec")
+
+    def backtran(self, idx: int, theta: float, lv, rv, tlv, stream=None):
+        """lv, rv <- exp(theta T_idx) lv, rv; tlv = T_idx lv (rotated)."""
+        _check(lib().bsim_backtran(self.basis.h, self.pool.h, idx - 1, theta, _ptr(lv), _ptr(rv), _ptr(tlv),
+                                   _stream(stream)), "backtran")
+
+    def batchexpm(self, idx: int, theta: float, mat, N: int, j: int, stream=None):
+        """exp(theta T_idx) on the first j of the N entries each determinant holds in mat
+        (Julia's N x dim column-major matrix, i.e. a row-major dim x N array)."""
+        _check(lib().bsim_batchexpm(self.basis.h, self.pool.h, idx - 1, theta, _ptr(mat), N, j, _stream(stream)),
+               "batchexpm")
+
+    def batchtran(self, lv, rv, trans, stream=None):
+        """trans[g] = <lv|T_g|rv> for every pool group."""
+        _check(lib().bsim_batchtran(self.basis.h, self.pool.h, _ptr(lv), _ptr(rv), _ptr(trans), _stream(stream)),
+               "batchtran")
 
     # -- sequence-level entry points ------------------------------------------
     def expm_seq(self, idxs: Sequence[int], thetas: Sequence[float], v, stream=None):

@@ -67,6 +67,19 @@ void batchgrad_cuda(void *basis, void *net, const double *thetas, const double *
 void expm_cuda_2d(void *basis, void *net, int64_t idx, double theta, double *vec);
 double grad_cuda_2d(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r);
 double backgrad_cuda_2d(void *basis, void *net, int64_t idx, double theta, double *l, double *r);
+/* GPU counterparts of the reference CPU library's tvec_contract_otf,
+ * backtran_contract_otf, batch_expm_contract_otf and batch_tran_contract_otf
+ * (op/declare.hpp:76-123), which jl/cuda/cunetwork.jl:78-84 leaves as no-ops
+ * (f_tvec, f_backtran, f_batchexpm, f_batchtran); same arguments on device
+ * pointers, idx 0-based.  tvec: dst = T_idx src (dst overwritten).  backtran:
+ * l, r <- e^{theta T} l, r and b = T l of the rotated l (b overwritten).
+ * batchexpm: e^{theta T} on the first num_vecs columns of the row-major
+ * dim x ld matrix.  batchtran: trans[g] = <l|T_g|r> for every group
+ * (original order, overwritten). */
+void tvec_cuda(void *basis, void *net, int64_t idx, const double *src, double *dst);
+void backtran_cuda(void *basis, void *net, int64_t idx, double theta, double *l, double *r, double *b);
+void batchexpm_cuda(void *basis, void *net, int64_t idx, double theta, double *matrix, int ld, int num_vecs);
+void batchtran_cuda(void *basis, void *net, const double *l, const double *r, double *trans);
 
 /* ========================================================================
  * Part 2: status-returning API.  Every function returns 0 on success or a
@@ -194,6 +207,15 @@ int bsim_backgrad(void *basis, void *net, int64_t idx, double theta, double *l, 
 /* Pool gradient (thetas, grads: device, original group order). */
 int bsim_batchgrad(void *basis, void *net, const double *thetas, const double *l, const double *r,
                    double *grads, bsim_stream_t stream);
+/* Status-returning forms of tvec_cuda, backtran_cuda, batchexpm_cuda and
+ * batchtran_cuda (same semantics; every group type and symmetry-block layout;
+ * batchexpm needs 0 <= num_vecs <= ld). */
+int bsim_tvec(void *basis, void *net, int64_t idx, const double *src, double *dst, bsim_stream_t stream);
+int bsim_backtran(void *basis, void *net, int64_t idx, double theta, double *l, double *r, double *b,
+                  bsim_stream_t stream);
+int bsim_batchexpm(void *basis, void *net, int64_t idx, double theta, double *matrix, int ld, int num_vecs,
+                   bsim_stream_t stream);
+int bsim_batchtran(void *basis, void *net, const double *l, const double *r, double *trans, bsim_stream_t stream);
 /* vec <- prod_i exp(thetas[param_idx[i]] G_{op_idx[i]}) |ref>, |ref> = sum_j ref_val[j] e_{ref_idx[j]};
  * all index/angle arrays are host arrays. */
 int bsim_prepare_state(void *basis, void *pool, int64_t n_ops, const int64_t *op_idx, const int64_t *param_idx,

@@ -71,6 +71,10 @@ class Oracle:
         lib.oracle_backgrad.restype = dbl
         lib.oracle_backgrad.argtypes = [vp, vp, i64, dbl, vp, vp]
         lib.oracle_batchgrad.argtypes = [vp, vp, vp, vp, vp, vp]
+        lib.oracle_tvec.argtypes = [vp, vp, i64, vp, vp]
+        lib.oracle_backtran.argtypes = [vp, vp, i64, dbl, vp, vp, vp]
+        lib.oracle_batchexpm.argtypes = [vp, vp, i64, dbl, vp, C.c_int, C.c_int]
+        lib.oracle_batchtran.argtypes = [vp, vp, vp, vp, vp]
         lib.oracle_ritz_residual.restype = dbl
         lib.oracle_ritz_residual.argtypes = [i64, C.c_int, vp, dbl, vp, vp, vp]
         lib.oracle_ritz_vector.argtypes = [i64, C.c_int, vp, vp, vp]
@@ -134,6 +138,31 @@ class Oracle:
         g = np.zeros(N.ngs)
         self.lib.oracle_batchgrad(B.h, N.h, P(thetas), P(l), P(r), P(g))
         return g
+
+    def tvec(self, B, N, idx, src):
+        src = np.ascontiguousarray(src, np.float64)
+        dst = np.zeros(B.dim)
+        self.lib.oracle_tvec(B.h, N.h, idx, P(src), P(dst))
+        return dst
+
+    def backtran(self, B, N, idx, theta, l, r):
+        """Returns (l_new, r_new, b); inputs are not modified."""
+        l = np.array(l, np.float64, copy=True); r = np.array(r, np.float64, copy=True)
+        b = np.zeros(B.dim)
+        self.lib.oracle_backtran(B.h, N.h, idx, theta, P(l), P(r), P(b))
+        return l, r, b
+
+    def batchexpm(self, B, N, idx, theta, M, nv):
+        """M: (dim, ld) row-major; the first nv columns are rotated (a copy is returned)."""
+        M = np.array(M, np.float64, copy=True, order="C")
+        self.lib.oracle_batchexpm(B.h, N.h, idx, theta, P(M), M.shape[1], nv)
+        return M
+
+    def batchtran(self, B, N, l, r):
+        l = np.ascontiguousarray(l, np.float64); r = np.ascontiguousarray(r, np.float64)
+        t = np.zeros(N.ngs)
+        self.lib.oracle_batchtran(B.h, N.h, P(l), P(r), P(t))
+        return t
 
     # -- Davidson helpers -------------------------------------------------
     def ritz_residual(self, coeffs, e, V, AV):
@@ -258,6 +287,10 @@ class RefLibs:
         self.otf.backgrad_contract_otf_f64.restype = dbl
         self.otf.backgrad_contract_otf_f64.argtypes = [vp, vp, i64, dbl, vp, vp]
         self.otf.batch_grad_contract_otf_f64.argtypes = [vp, vp, vp, vp, vp, vp]
+        self.otf.tvec_contract_otf_f64.argtypes = [vp, vp, i64, vp, vp]
+        self.otf.backtran_contract_otf_f64.argtypes = [vp, vp, i64, dbl, vp, vp, vp]
+        self.otf.batch_expm_contract_otf_f64.argtypes = [vp, vp, i64, dbl, vp, C.c_int, C.c_int]
+        self.otf.batch_tran_contract_otf_f64.argtypes = [vp, vp, vp, vp, vp]
         self.bas.create_basis_manager.restype = vp
         self.bas.create_basis_manager.argtypes = [i64, i64, i64, i64, vp, i64]
         self.bas.get_subspace_dim.restype = i64
@@ -334,6 +367,27 @@ class RefLibs:
         self.otf.batch_grad_contract_otf_f64(b, n, P(np.ascontiguousarray(thetas, np.float64)),
                                              P(np.ascontiguousarray(l)), P(np.ascontiguousarray(r)), P(g))
         return g
+
+    def tvec(self, b, n, idx, src, dim):
+        dst = np.zeros(dim)
+        self.otf.tvec_contract_otf_f64(b, n, idx, P(np.ascontiguousarray(src, np.float64)), P(dst))
+        return dst
+
+    def backtran(self, b, n, idx, theta, l, r, dim):
+        l = np.array(l, np.float64, copy=True); r = np.array(r, np.float64, copy=True)
+        bv = np.zeros(dim)
+        self.otf.backtran_contract_otf_f64(b, n, idx, theta, P(l), P(r), P(bv))
+        return l, r, bv
+
+    def batchexpm(self, b, n, idx, theta, M, nv):
+        M = np.array(M, np.float64, copy=True, order="C")
+        self.otf.batch_expm_contract_otf_f64(b, n, idx, theta, P(M), M.shape[1], nv)
+        return M
+
+    def batchtran(self, b, n, l, r, ngs):
+        t = np.zeros(ngs)
+        self.otf.batch_tran_contract_otf_f64(b, n, P(np.ascontiguousarray(l)), P(np.ascontiguousarray(r)), P(t))
+        return t
 
     def det_index(self, b, astr, bstr, dim):
         v = np.zeros(dim)

@@ -485,6 +485,134 @@ void oracle_batchgrad(void *bp, void *np, const double *thetas,
         grads[g] = oracle_grad(bp, np, g, thetas[g], l, r);
 }
 
+/* ---------------- tvec / backtran / batchexpm / batchtran ---------------- */
+
+typedef struct { const double *src; double *dst; } TvecCtx;
+
+/* tvec_update, core/math.hpp:165-170 (real Tv): ds = sd * (-vt), dd = ss * vt.
+ * A diagonal group visits si == di, where the second store leaves
+ * dst = src * vt, the diagonal rule of op/tvec.hpp:7-60. */
+static void tvec_pair(i64 di, i64 si, double vt, void *ctx, double *acc)
+{
+    (void)acc;
+    TvecCtx *c = (TvecCtx *)ctx;
+    double ss = c->src[si], sd = c->src[di];
+    c->dst[si] = sd * (-vt);
+    c->dst[di] = ss * vt;
+}
+
+/* dst = T_idx src for one group, op/tvec.hpp (tvec_svd_network_otf):
+ * dst is zeroed first. */
+void oracle_tvec(void *bp, void *np, i64 idx, const double *src, double *dst)
+{
+    OBasis *B = (OBasis *)bp;
+    ONet *N = (ONet *)np;
+    memset(dst, 0, sizeof(double) * B->dim);
+    TvecCtx c = {src, dst};
+    visit_pairs(B, N, &N->g[idx], 1, tvec_pair, &c);
+}
+
+typedef struct { double *l, *r, *b; double cd, co; } BacktranCtx;
+
+/* backtran_update, core/math.hpp:217-226 (real Tv): expm_update on l and on r,
+ * then tvec_update from the rotated l into b. */
+static void backtran_pair(i64 di, i64 si, double vt, void *ctx, double *acc)
+{
+    (void)acc;
+    BacktranCtx *c = (BacktranCtx *)ctx;
+    double vd = 1.0 + c->cd * (vt * vt), vo = c->co * vt;
+    double li = c->l[si], lj = c->l[di], ri = c->r[si], rj = c->r[di];
+    double ls = li * vd - lj * vo, ld = lj * vd + li * vo;
+    c->l[si] = ls;
+    c->l[di] = ld;
+    c->r[si] = ri * vd - rj * vo;
+    c->r[di] = rj * vd + ri * vo;
+    c->b[si] = ld * (-vt);
+    c->b[di] = ls * vt;
+}
+
+/* Diagonal group of backtran, op/backtran.hpp:7-70 (real Tv: the diagonal
+ * exponential is 1): b = l * vt. */
+static void backtran_diag(i64 di, i64 si, double vt, void *ctx, double *acc)
+{
+    (void)acc;
+    (void)si;
+    BacktranCtx *c = (BacktranCtx *)ctx;
+    c->b[di] = c->l[di] * vt;
+}
+
+/* l <- e^{theta T} l, r <- e^{theta T} r, b = T l (rotated l); b zeroed first,
+ * op/backtran.hpp (backtran_svd_network_otf, angles at :75-76). */
+void oracle_backtran(void *bp, void *np, i64 idx, double theta, double *l, double *r, double *b)
+{
+    OBasis *B = (OBasis *)bp;
+    ONet *N = (ONet *)np;
+    const OGroup *G = &N->g[idx];
+    memset(b, 0, sizeof(double) * B->dim);
+    BacktranCtx c = {l, r, b, cos(theta) - 1.0, sin(theta)};
+    visit_pairs(B, N, G, 1, G->type == 0 ? backtran_diag : backtran_pair, &c);
+}
+
+typedef struct { double *m; int ld, nv; double cd, co; } BatchExpmCtx;
+
+/* expm_batch_update_matrix, core/math.hpp:228-252: expm_update on the first nv
+ * entries of the rows si and di of a row-major matrix with row stride ld. */
+static void batchexpm_pair(i64 di, i64 si, double vt, void *ctx, double *acc)
+{
+    (void)acc;
+    BatchExpmCtx *c = (BatchExpmCtx *)ctx;
+    double vd = 1.0 + c->cd * (vt * vt), vo = c->co * vt;
+    double *sp = c->m + si * c->ld, *dp = c->m + di * c->ld;
+    for (int k = 0; k < c->nv; ++k) {
+        double vi = sp[k], vj = dp[k];
+        sp[k] = vi * vd - vj * vo;
+        dp[k] = vj * vd + vi * vo;
+    }
+}
+
+/* e^{theta T_idx} on nv vectors stored as the columns of a dim x ld row-major
+ * matrix, op/batchexpm.hpp (expm_svd_batched_network_otf); diagonal groups are
+ * the identity for real vectors. */
+void oracle_batchexpm(void *bp, void *np, i64 idx, double theta, double *matrix, int ld, int nv)
+{
+    OBasis *B = (OBasis *)bp;
+    ONet *N = (ONet *)np;
+    const OGroup *G = &N->g[idx];
+    if (G->type == 0) return;
+    BatchExpmCtx c = {matrix, ld, nv, cos(theta) - 1.0, sin(theta)};
+    visit_pairs(B, N, G, 1, batchexpm_pair, &c);
+}
+
+typedef struct { const double *l, *r; } TranCtx;
+
+/* tran_update, core/math.hpp:180-184 (real Tv): vt (l_s r_d - l_d r_s). */
+static void tran_pair(i64 di, i64 si, double vt, void *ctx, double *acc)
+{
+    TranCtx *c = (TranCtx *)ctx;
+    *acc += c->l[si] * vt * c->r[di] - c->l[di] * vt * c->r[si];
+}
+
+/* Diagonal group of batchtran, op/batchtran.hpp:7-81: l_i vt r_i. */
+static void tran_diag(i64 di, i64 si, double vt, void *ctx, double *acc)
+{
+    (void)si;
+    TranCtx *c = (TranCtx *)ctx;
+    *acc += c->l[di] * vt * c->r[di];
+}
+
+/* trans[orig] = <l| T_g |r> for every group, op/batchtran.hpp:514-528
+ * (tran_pool_network_batched_otf); trans is overwritten. */
+void oracle_batchtran(void *bp, void *np, const double *l, const double *r, double *trans)
+{
+    OBasis *B = (OBasis *)bp;
+    ONet *N = (ONet *)np;
+    TranCtx c = {l, r};
+    for (i64 g = 0; g < N->ngs; ++g) {
+        const OGroup *G = &N->g[g];
+        trans[g] = visit_pairs(B, N, G, 1, G->type == 0 ? tran_diag : tran_pair, &c);
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* Davidson vector helpers: diag/davidson.hpp:31-272 (real)            */
 /* ------------------------------------------------------------------ */

@@ -4,7 +4,8 @@ libraries (oracle/_ref, compiled from the reference sources by oracle/Makefile).
 Each fixture stores the inputs (the OTF network as flat arrays, basis
 parameters, seeded vectors, angles) and the reference outputs of
 hvec_gather_contract_otf_f64, get_diags_elements_f64, expm/grad/backgrad/
-batch_grad_contract_otf_f64 and a few libdiag helpers.  Run:
+batch_grad_contract_otf_f64, tvec/backtran/batch_expm/batch_tran_contract_otf_f64
+and a few libdiag helpers.  Run:
 
     python tests/golden/gen_golden.py
 
@@ -62,12 +63,28 @@ def main():
         bth = rng.normal(0, 0.3, size=pool.ngs)
         batch = ref.batchgrad(rb, rp, bth, x, sigma, pool.ngs)
         hf = ref.det_index(rb, (1 << na) - 1, (1 << nb) - 1, dim)
+        # tvec / backtran / batch_expm / batch_tran (drawn after the arrays above,
+        # so those stay as they were): pool generators and the diagonal group 0
+        # of the Hamiltonian
+        top = ops[:4]
+        tvec = np.stack([ref.tvec(rb, rp, int(i), x, dim) for i in top])
+        tvec_ham0 = ref.tvec(rb, rh, 0, x, dim)
+        bt = [ref.backtran(rb, rp, int(i), t, x, y, dim) for i, t in zip(top, thetas[:4])]
+        bt_ham0 = ref.backtran(rb, rh, 0, 0.4, x, y, dim)
+        bem = rng.normal(size=(dim, 3))
+        bexp = ref.batchexpm(rb, rp, int(ops[0]), float(thetas[0]), bem, 2)
+        trans_pool = ref.batchtran(rb, rp, x, y, pool.ngs)
+        trans_ham = ref.batchtran(rb, rh, x, y, ham.ngs)
         np.savez_compressed(
             os.path.join(OUT, f"{name}.npz"),
             norb=norb, na=na, nb=nb, orbsym=osym, total_sym=tsym, num_irreps=nirr, dim=dim, hf=hf,
             x=x, y=y, sigma=sigma, diag=diag, ops=ops, thetas=thetas, expm=expm, grad=grad,
             backgrad=np.array([b[0] for b in bg]), backgrad_l=np.stack([b[1] for b in bg]),
             backgrad_r=np.stack([b[2] for b in bg]), batch_thetas=bth, batchgrad=batch,
+            tvec=tvec, tvec_ham0=tvec_ham0, backtran_l=np.stack([b[0] for b in bt]),
+            backtran_r=np.stack([b[1] for b in bt]), backtran_b=np.stack([b[2] for b in bt]),
+            backtran_ham0=np.stack(bt_ham0), batchexpm_in=bem, batchexpm=bexp, trans_pool=trans_pool,
+            trans_ham=trans_ham,
             **net_arrays("ham", ham), **net_arrays("pool", pool))
         print(name, "dim", dim, "ham groups", ham.ngs, "pool groups", pool.ngs)
 

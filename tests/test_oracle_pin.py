@@ -94,3 +94,60 @@ def test_oracle_davidson_helpers_match_libdiag(oracle, reflibs):
     col = np.zeros(k)
     reflibs.diag.compute_heff_col_f64(n, k, arr(V), AV[0].ctypes.data, col.ctypes.data)
     np.testing.assert_allclose(oracle.heff_col(V, AV[0]), col, rtol=1e-12)
+
+
+@pytest.mark.parametrize("norb,na,nb,orbsym,tsym", [
+    (6, 3, 2, None, 0),
+    (7, 3, 3, [0, 1, 2, 3, 0, 1, 2], 2),
+])
+def test_oracle_tvec_backtran_batch_ops_match_reference_libs(oracle, reflibs, norb, na, nb, orbsym, tsym):
+    """tvec, backtran, batch_expm and batch_tran (the reference CPU library's
+    tvec_contract_otf, backtran_contract_otf, batch_expm_contract_otf and
+    batch_tran_contract_otf) against the C restatement, on Hamiltonian groups
+    (including the diagonal group) and on pool generators."""
+    from binsim_b200 import network as nw
+    osym = np.zeros(norb, np.int64) if orbsym is None else np.asarray(orbsym, np.int64)
+    ham = nw.hamiltonian_network(norb, seed=norb * 3 + 2)
+    pool = nw.ucc_pool(norb).network
+    ham.orbsym = osym; pool.orbsym = osym
+    rb, dim = reflibs.basis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
+    B = oracle.basis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
+    rng = np.random.default_rng(norb + 100)
+    x, y = rng.normal(size=dim), rng.normal(size=dim)
+    for net in (ham, pool):
+        rn, N = reflibs.network(net), oracle.network(net)
+        for i in sorted(set([0] + list(rng.choice(net.ngs, 12, replace=False)))):
+            i = int(i)
+            np.testing.assert_allclose(oracle.tvec(B, N, i, x), reflibs.tvec(rb, rn, i, x, dim), rtol=0, atol=1e-13)
+            t = rng.normal()
+            for a, b in zip(oracle.backtran(B, N, i, t, x, y), reflibs.backtran(rb, rn, i, t, x, y, dim)):
+                np.testing.assert_allclose(a, b, rtol=0, atol=1e-13)
+            M = rng.normal(size=(dim, 4))
+            np.testing.assert_allclose(oracle.batchexpm(B, N, i, t, M, 3), reflibs.batchexpm(rb, rn, i, t, M, 3),
+                                       rtol=0, atol=1e-13)
+        tr = reflibs.batchtran(rb, rn, x, y, net.ngs)
+        np.testing.assert_allclose(oracle.batchtran(B, N, x, y), tr, rtol=0, atol=1e-11 * max(1.0, np.abs(tr).max()))
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_tvec_backtran_batch_ops_match_golden(oracle, name):
+    """The restated tvec / backtran / batch_expm / batch_tran against the reference's
+    outputs stored in the golden fixtures."""
+    z, ham, pool = load_golden(name)
+    B = _basis(oracle, z)
+    H, P = oracle.network(ham), oracle.network(pool)
+    x, y = z["x"], z["y"]
+    for k, i in enumerate(z["ops"][:4]):
+        np.testing.assert_allclose(oracle.tvec(B, P, int(i), x), z["tvec"][k], rtol=0, atol=1e-14)
+        l2, r2, b2 = oracle.backtran(B, P, int(i), z["thetas"][k], x, y)
+        np.testing.assert_allclose(l2, z["backtran_l"][k], rtol=0, atol=1e-14)
+        np.testing.assert_allclose(r2, z["backtran_r"][k], rtol=0, atol=1e-14)
+        np.testing.assert_allclose(b2, z["backtran_b"][k], rtol=0, atol=1e-14)
+    np.testing.assert_allclose(oracle.tvec(B, H, 0, x), z["tvec_ham0"], rtol=0, atol=1e-13)
+    for a, b in zip(oracle.backtran(B, H, 0, 0.4, x, y), z["backtran_ham0"]):
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-13)
+    np.testing.assert_allclose(oracle.batchexpm(B, P, int(z["ops"][0]), z["thetas"][0], z["batchexpm_in"], 2),
+                               z["batchexpm"], rtol=0, atol=1e-14)
+    np.testing.assert_allclose(oracle.batchtran(B, P, x, y), z["trans_pool"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(oracle.batchtran(B, H, x, y), z["trans_ham"], rtol=0,
+                               atol=1e-12 * max(1.0, np.abs(z["trans_ham"]).max()))

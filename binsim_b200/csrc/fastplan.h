@@ -119,7 +119,8 @@ struct FastPlan {
 
 constexpr int kMixCols = 128;                             // columns per GEMM chunk
 
-// Shared memory of the intermediate-string GEMM: W_m [nU x ri_ls] and an X slice.
+// Shared memory of the intermediate-string GEMM: W_m [nU x ri_ls] and a ring of
+// X slices.
 // Output rows past 64 (up to kRiMaxU) are computed by all threads with scalar
 // FMAs next to the 64-row register tiles, so W_m rows are 8 elements wider
 // than the mixed GEMM's Lam_conn rows (72 / 76 elements: 4 mod 16 doubles for
@@ -128,9 +129,11 @@ constexpr int kRiMaxU = 72;
 inline size_t gemm_ls(size_t elem) { return elem == 8 ? 68 : 64; }
 inline size_t gemm_xs(size_t elem) { return elem == 8 ? kMixCols + 4 : kMixCols; }
 inline size_t ri_ls(size_t elem) { return gemm_ls(elem) + 8; }
+constexpr int kRiStagesHost = 3;   // X slices in the cp.async ring of the intermediate-string GEMM
 inline size_t ri_smem_bytes(int nU, size_t elem)
 {
-    return (((size_t)nU + 3) & ~size_t(3)) * ri_ls(elem) * elem + 32 * gemm_xs(elem) * elem + kRiMaxU * 8;
+    return (((size_t)nU + 3) & ~size_t(3)) * ri_ls(elem) * elem + kRiStagesHost * 32 * gemm_xs(elem) * elem +
+           kRiMaxU * 8;
 }
 
 // Shared memory of the mixed GEMM kernel: source row (unless it is read from

@@ -541,10 +541,25 @@ struct RIArgs {
     const void *W;          // T [nP x nP]
 };
 
-// One CTA per intermediate m: X[k][col] = s(m, pair_k) c~[m + pair_k][col] for the
-// nU pairs outside m (coalesced row segments, the next slice prefetched into
-// registers), Z[m][j][col] = sum_k W[pair_j][pair_k] X[k][col].  Same tiling as
-// the mixed GEMM: warp w owns output rows w*EPT.., lane l owns columns
+// 16-byte asynchronous copy global -> shared (cp.async, L2 only); src_bytes 0
+// writes zeros without reading.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+constexpr int kRiStages = kRiStagesHost;   // X slices in flight in the intermediate-string GEMM
+
+// One CTA per intermediate m: X[k][col] = c~[m + pair_k][col] for the nU pairs
+// outside m, Z[m][j][col] = sum_k W[pair_j][pair_k] s(m, pair_k) X[k][col] (the
+// sign of each source row is folded into W_m's column, so X rows are copied
+// verbatim).  The X slices (32 rows x kMixCols columns) stream through a
+// kRiStages-deep cp.async ring in shared memory.  Same tiling as the mixed
+// GEMM: warp w owns output rows w*EPT.., lane l owns columns
 // {2l, 2l+1, 64+2l, 64+2l+1} of a kMixCols chunk.  Rows 64 .. nU-1 (at most
 // kRiMaxU - 64; 66 pairs at 18 orbitals and 8 electrons) are computed by every
 // thread with scalar FMAs, one (row, column) output per thread and pass.
@@ -553,15 +568,16 @@ __global__ void __launch_bounds__((64 / EPT) * 32, sizeof(T) == 4 ? 2 : 1)
 ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int z0, int W)
 {
     constexpr int NT = (64 / EPT) * 32;
-    constexpr int ITEMS = 32 * kMixCols / NT;
     constexpr int TQ = ((kRiMaxU - 64) * kMixCols + NT - 1) / NT;   // tail outputs per thread
+    constexpr int CH = 16 / (int)sizeof(T);                          // elements per 16-byte copy
+    constexpr int CPR = kMixCols / CH;                               // copies per slice row
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.nU;
     constexpr int LS = GemmLayout<T>::LS + 8, XS = GemmLayout<T>::XS;
     const int Kp = (K + 3) & ~3;
     T *wm = reinterpret_cast<T *>(smem_raw);                          // [Kp][LS], rows >= K zero
-    T *xs = wm + (size_t)Kp * LS;                                      // [32][XS]
-    long long *soff = reinterpret_cast<long long *>(xs + 32 * XS);     // [kRiMaxU]
+    T *xs = wm + (size_t)Kp * LS;                                      // [kRiStages][32][XS]
+    long long *soff = reinterpret_cast<long long *>(xs + kRiStages * 32 * XS);   // [kRiMaxU]
     const int m = blockIdx.x;
     const int *srcm = P.src + (i64)m * K, *pidm = P.pid + (i64)m * K;
     for (int i = threadIdx.x; i < kRiMaxU; i += NT) {
@@ -575,7 +591,12 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
     const T *Wt = static_cast<const T *>(P.W);
     for (int i = threadIdx.x; i < Kp * LS; i += NT) {
         const int k = i / LS, j = i % LS;
-        wm[i] = (j < K && k < K) ? Wt[(i64)pidm[j] * P.nP + pidm[k]] : T(0);
+        T w = T(0);
+        if (j < K && k < K) {
+            w = Wt[(i64)pidm[j] * P.nP + pidm[k]];
+            if (srcm[k] & 1) w = -w;
+        }
+        wm[i] = w;
     }
     __syncthreads();
     const int zend = min(P.cend, z0 + W);
@@ -584,47 +605,45 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
     const int nsteps = ncb * nfc;
     const bool active = GemmCore<T, EPT>::active(K);
     const int ntail = K > 64 ? (K - 64) * kMixCols : 0;
-    T gpre[ITEMS];
-    auto load_x = [&](int step) {
-        const int cb = z0 + (step / nfc) * kMixCols, f0 = (step % nfc) * 32;
-#pragma unroll
-        for (int it = 0; it < ITEMS; ++it) {
-            const int i = threadIdx.x + it * NT;
-            const int k = f0 + i / kMixCols, col = cb + i % kMixCols;
-            T v = T(0);
-            if (k < K && col < zend) {
-                const long long o = soff[k];
-                v = __ldg(in + (o >> 1) + col);
-                if (o & 1) v = -v;
+    // copies of slice `step` into ring slot step % kRiStages (rows past K and
+    // columns past the padded row length are zero-filled); one commit group per
+    // call, empty past the last step, so the wait counts stay uniform
+    auto issue = [&](int step) {
+        if (step < nsteps) {
+            const int cb = z0 + (step / nfc) * kMixCols, f0 = (step % nfc) * 32;
+            T *dst = xs + (step % kRiStages) * 32 * XS;
+            for (int i = threadIdx.x; i < 32 * CPR; i += NT) {
+                const int k = i / CPR, c = (i % CPR) * CH;
+                const int row = f0 + k, col = cb + c;
+                const bool ok = row < K && col < P.ld_in;
+                cp_async16(dst + k * XS + c, ok ? (const void *)(in + (soff[row] >> 1) + col) : (const void *)in,
+                           ok ? 16 : 0);
             }
-            gpre[it] = v;
         }
+        cp_async_commit();
     };
     GemmCore<T, EPT> acc;
     acc.zero();
     T tacc[TQ];
 #pragma unroll
     for (int q = 0; q < TQ; ++q) tacc[q] = T(0);
-    if (nsteps > 0) load_x(0);
+#pragma unroll
+    for (int st = 0; st < kRiStages - 1; ++st) issue(st);
     for (int step = 0; step < nsteps; ++step) {
         const int cbi = step / nfc, fci = step % nfc;
         const int f0 = fci * 32, nf = min(32, K - f0);
-        __syncthreads();
-#pragma unroll
-        for (int it = 0; it < ITEMS; ++it) {
-            const int i = threadIdx.x + it * NT;
-            xs[(i / kMixCols) * XS + i % kMixCols] = gpre[it];
-        }
-        __syncthreads();
-        if (step + 1 < nsteps) load_x(step + 1);
-        if (active) acc.template step<LS>(wm, xs, f0, nf);
+        cp_async_wait<kRiStages - 2>();   // this thread's copies of slice `step` landed
+        __syncthreads();                  // everyone's did; the slot refilled below is consumed
+        issue(step + kRiStages - 1);
+        const T *xcur = xs + (step % kRiStages) * 32 * XS;
+        if (active) acc.template step<LS>(wm, xcur, f0, nf);
 #pragma unroll
         for (int q = 0; q < TQ; ++q) {
             const int o = threadIdx.x + q * NT;
             if (o < ntail) {
                 const int row = 64 + o / kMixCols, col = o % kMixCols;
                 T t = tacc[q];
-                for (int f = 0; f < nf; ++f) t += wm[(f0 + f) * LS + row] * xs[f * XS + col];
+                for (int f = 0; f < nf; ++f) t += wm[(f0 + f) * LS + row] * xcur[f * XS + col];
                 tacc[q] = t;
             }
         }
@@ -639,6 +658,7 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
             }
         }
     }
+    cp_async_wait<0>();
 }
 
 // out[row][b] += sum over the pairs pq in the row's string of s(m, pq) Z[m][slot(pq)][b]

@@ -378,7 +378,24 @@ def gpu_sigma(args, rank, world, local_rank):
         x.copy_(xpin, non_blocking=True)
         step(False)
         ypin.copy_(y, non_blocking=True)
-    ms_e2e = timed(e2e_step, max(1, args.steps // 2), 1)
+    ms_e2e_serial = timed(e2e_step, max(1, args.steps // 2), 1)
+    # the public host-vector call: every step copies its input in and its result
+    # out, the copies of neighbouring steps overlapped with the sigma between them
+    ms_e2e = None
+    if world == 1:
+        ksteps = max(1, args.steps)
+        f.hvec_host([xpin], [ypin])   # warm-up (device buffers of the pipeline)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        f.hvec_host([xpin] * ksteps, [ypin] * ksteps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = e0.elapsed_time(e1) / ksteps
+        host_err = float(np.abs(ypin.numpy() - y.cpu().numpy()).max() / np.abs(y.cpu().numpy()).max())
+    else:
+        ms_e2e = ms_e2e_serial
+        host_err = None
 
     result = None
     if rank == 0:
@@ -403,7 +420,12 @@ def gpu_sigma(args, rank, world, local_rank):
                                     f"({shard.exchange_bytes() / 1e9:.2f} GB received per rank per step)")
                        if world > 1 else "single GPU"},
             "e2e": {"value": 1000.0 / ms_e2e, "unit": UNIT, "h2d_bytes_per_step": dim * 8,
-                    "d2h_bytes_per_step": dim * 8, "ms_per_step": ms_e2e},
+                    "d2h_bytes_per_step": dim * 8, "ms_per_step": ms_e2e,
+                    "path": "bsim_hvec_host over pinned host vectors: per step H2D of c, sigma, D2H of sigma; "
+                            "copies of neighbouring steps overlap the sigma between them" if world == 1 else
+                            "H2D, sharded sigma, D2H in sequence",
+                    "serial_ms_per_step": ms_e2e_serial,
+                    "max_rel_diff_host_vs_device_result": host_err},
             "mixed": {"value": 1000.0 / ms_mixed, "unit": UNIT, "ms_per_step": ms_mixed,
                       "dtype": "f32 bulk, f64 accumulate", "max_rel_err_vs_fp64": err_mixed,
                       "speedup_vs_fp64": ms / ms_mixed},

@@ -5,6 +5,7 @@
 
 #include <cstdio>
 #include <initializer_list>
+#include <memory>
 #include <mutex>
 
 using bsim::DevBasis;
@@ -326,6 +327,93 @@ int bsim_hvec(void *basis, void *net, const double *src, double *dst, bsim_strea
     if (int st0 = check_handles(basis, {net})) return st0;
     NEED(src); NEED(dst);
     return with_handles(basis, {net}, [&](auto *b) { return bsim::sigma(b, net_of(b, net), src, nullptr, dst, false, stream); });
+}
+
+namespace {
+
+// Device side of bsim_hvec_host: two input and two output vectors, a copy
+// stream per direction and the events that order them.
+struct HostPipe {
+    double *in[2] = {nullptr, nullptr}, *out[2] = {nullptr, nullptr};
+    cudaStream_t cin = nullptr, cout = nullptr;
+    cudaEvent_t in_ready[2] = {}, done[2] = {}, out_read[2] = {};
+    ~HostPipe()
+    {
+        for (int i = 0; i < 2; ++i) {
+            if (in[i]) cudaFree(in[i]);
+            if (out[i]) cudaFree(out[i]);
+            for (cudaEvent_t e : {in_ready[i], done[i], out_read[i]})
+                if (e) cudaEventDestroy(e);
+        }
+        if (cin) cudaStreamDestroy(cin);
+        if (cout) cudaStreamDestroy(cout);
+    }
+    int init(int64_t dim)
+    {
+        for (int i = 0; i < 2; ++i) {
+            BSIM_CUDA(cudaMalloc(&in[i], sizeof(double) * std::max<int64_t>(dim, 1)));
+            BSIM_CUDA(cudaMalloc(&out[i], sizeof(double) * std::max<int64_t>(dim, 1)));
+            BSIM_CUDA(cudaEventCreateWithFlags(&in_ready[i], cudaEventDisableTiming));
+            BSIM_CUDA(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming));
+            BSIM_CUDA(cudaEventCreateWithFlags(&out_read[i], cudaEventDisableTiming));
+        }
+        BSIM_CUDA(cudaStreamCreateWithFlags(&cin, cudaStreamNonBlocking));
+        BSIM_CUDA(cudaStreamCreateWithFlags(&cout, cudaStreamNonBlocking));
+        return BSIM_OK;
+    }
+};
+
+}  // namespace
+
+int bsim_hvec_host(void *basis, void *net, int64_t nvec, const double *const *src_host, double *const *dst_host,
+                   int mixed, bsim_stream_t stream)
+{
+    if (int st0 = check_handles(basis, {net})) return st0;
+    if (nvec < 0) { bsim::set_error("nvec = %lld", (long long)nvec); return BSIM_ERR_ARG; }
+    if (nvec == 0) return BSIM_OK;
+    NEED(src_host); NEED(dst_host);
+    for (int64_t k = 0; k < nvec; ++k) { NEED(src_host[k]); NEED(dst_host[k]); }
+    return with_handles(basis, {net}, [&](auto *b) -> int {
+        const int64_t dim = b->dim;
+        const size_t bytes = sizeof(double) * (size_t)dim;
+        // one pipe per process, kept between calls and regrown for a larger basis
+        static std::mutex mu;
+        static std::unique_ptr<HostPipe> pipe;
+        static int64_t pipe_dim = -1;
+        std::lock_guard<std::mutex> lk(mu);
+        int st = BSIM_OK;
+        if (!pipe || pipe_dim < dim) {
+            pipe.reset();
+            pipe_dim = -1;
+            auto np = std::make_unique<HostPipe>();
+            if ((st = np->init(dim)) != BSIM_OK) return st;
+            pipe = std::move(np);
+            pipe_dim = dim;
+        }
+        HostPipe &P = *pipe;
+        // step k: H2D on cin into in[k%2] (after sigma k-2 read it), sigma on the
+        // caller's stream into out[k%2] (after the D2H of step k-2 read it), D2H
+        // on cout; the copies of neighbouring steps overlap the sigma between them
+        for (int64_t k = 0; k < nvec; ++k) {
+            const int sl = (int)(k & 1);
+            if (k >= 2) BSIM_CUDA(cudaStreamWaitEvent(P.cin, P.done[sl], 0));
+            BSIM_CUDA(cudaMemcpyAsync(P.in[sl], src_host[k], bytes, cudaMemcpyHostToDevice, P.cin));
+            BSIM_CUDA(cudaEventRecord(P.in_ready[sl], P.cin));
+            BSIM_CUDA(cudaStreamWaitEvent(stream, P.in_ready[sl], 0));
+            if (k >= 2) BSIM_CUDA(cudaStreamWaitEvent(stream, P.out_read[sl], 0));
+            st = bsim::sigma(b, net_of(b, net), P.in[sl], nullptr, P.out[sl], mixed != 0, stream);
+            if (st != BSIM_OK) break;
+            BSIM_CUDA(cudaEventRecord(P.done[sl], stream));
+            BSIM_CUDA(cudaStreamWaitEvent(P.cout, P.done[sl], 0));
+            BSIM_CUDA(cudaMemcpyAsync(dst_host[k], P.out[sl], bytes, cudaMemcpyDeviceToHost, P.cout));
+            BSIM_CUDA(cudaEventRecord(P.out_read[sl], P.cout));
+        }
+        cudaError_t e1 = cudaStreamSynchronize(P.cout), e2 = cudaStreamSynchronize(stream);
+        if (st != BSIM_OK) return st;
+        if (e1 != cudaSuccess) return bsim::cuda_status(e1, "hvec_host");
+        if (e2 != cudaSuccess) return bsim::cuda_status(e2, "hvec_host");
+        return (int)BSIM_OK;
+    });
 }
 
 int bsim_hvec_mixed(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream)

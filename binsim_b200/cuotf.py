@@ -83,6 +83,7 @@ def lib() -> C.CDLL:
         "bsim_backgrad": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_grad_noalloc": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_batchgrad": (ci, [vp, vp, vp, vp, vp, vp, vp]),
+        "bsim_hvec_host": (ci, [vp, vp, i64, vp, vp, ci, vp]),
         "bsim_tvec": (ci, [vp, vp, i64, vp, vp, vp]),
         "bsim_backtran": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_batchexpm": (ci, [vp, vp, i64, dbl, vp, ci, ci, vp]),
@@ -263,6 +264,17 @@ class CuOTFFunctions:
         if r < 0:
             _check(r, "hvec_path")
         return r, buf.value.decode(), nres.value
+
+    def hvec_host(self, srcs, dsts, mixed=False, stream=None):
+        """dsts[k] = H srcs[k] for host tensors/arrays (dim float64 each), the copies of
+        neighbouring steps overlapped with sigma; pinned host memory lets them overlap."""
+        n = len(srcs)
+        if len(dsts) != n:
+            raise ValueError("srcs and dsts differ in length")
+        sp = (C.c_void_p * max(n, 1))(*[_ptr(x) for x in srcs])
+        dp = (C.c_void_p * max(n, 1))(*[_ptr(x) for x in dsts])
+        _check(lib().bsim_hvec_host(self.basis.h, self.ham.h, n, sp, dp, 1 if mixed else 0, _stream(stream)),
+               "hvec_host")
 
     def hvec_cols(self, v, Hv, col_lo: int, col_hi: int, mixed=False, stream=None):
         """sigma on beta columns [col_lo, col_hi) only (column-band sharding)."""

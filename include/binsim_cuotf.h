@@ -137,6 +137,15 @@ int64_t bsim_network_ngs(void *net);
 
 /* dst = H src, FP64. */
 int bsim_hvec(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream);
+/* sigma of nvec HOST vectors: dst_host[k] = H src_host[k] (dim doubles each;
+ * the same host buffer may appear in several slots).  The library holds two
+ * device input and two output vectors and orders, per step, the host-to-device
+ * copy (its own copy stream), sigma (on `stream`) and the device-to-host copy
+ * (a second copy stream), so the copies of neighbouring steps overlap the sigma
+ * between them; returns when the last result is on the host.  Page-locked host
+ * buffers let the copies run asynchronously.  mixed selects the FP32-bulk sigma. */
+int bsim_hvec_host(void *basis, void *net, int64_t nvec, const double *const *src_host, double *const *dst_host,
+                   int mixed, bsim_stream_t stream);
 /* dst = H src with FP32 bulk (FP32 phases, weights and gathered source,
  * products summed in FP32 per chunk of <= 64 group-ranks) and FP64
  * accumulation across chunks. */

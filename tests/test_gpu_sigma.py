@@ -234,3 +234,26 @@ def test_intermediate_string_gemm_beyond_64_pairs(cuda, oracle, norb, na, nb):
     ym = cuda.empty_like(x)
     f.hvec_mixed(x, ym)
     assert np.abs(ym.cpu().numpy() - ref).max() <= 2e-6 * scale
+
+
+def test_hvec_host_pipeline(cuda):
+    """bsim_hvec_host over several distinct host vectors (pinned and pageable, the same
+    output buffer twice) gives the device sigma of each, bit for bit."""
+    from binsim_b200 import cuotf, network as nw
+    norb, na, nb = 10, 5, 4
+    B = cuotf.CuBasis(norb, na, nb)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(nw.hamiltonian_network(norb, seed=3)))
+    rng = np.random.default_rng(0)
+    xs = [rng.normal(size=B.dim) for _ in range(5)]
+    srcs = [cuda.from_numpy(xs[0]).pin_memory(), cuda.from_numpy(xs[1]).pin_memory(), xs[2], xs[3],
+            cuda.from_numpy(xs[4]).pin_memory()]
+    outs = [cuda.empty(B.dim, dtype=cuda.float64).pin_memory() for _ in range(3)] + [np.zeros(B.dim)]
+    dsts = [outs[0], outs[1], outs[2], outs[3], outs[0]]   # slot 0 is written twice, last by step 4
+    for mixed in (False, True):
+        f.hvec_host(srcs, dsts, mixed=mixed)
+        for k in (1, 2, 3, 4):
+            y = cuda.empty(B.dim, dtype=cuda.float64, device="cuda")
+            (f.hvec_mixed if mixed else f.hvec)(dev(cuda, xs[k]), y)
+            got = dsts[k].numpy() if hasattr(dsts[k], "numpy") else dsts[k]
+            assert np.array_equal(got, y.cpu().numpy()), (mixed, k)
+    f.hvec_host([], [])

@@ -142,10 +142,13 @@ inline size_t ri_smem_bytes(int nU, size_t elem)
 constexpr int kMaxConn = 128;   // connected alpha singles per string: up to two 64-row GEMM passes
 constexpr size_t kSmemMax = 227 * 1024;
 
-inline size_t mixed_smem_bytes(int nB, int nF, size_t elem, bool stream, bool grow)
+// rows: connected excitations per GEMM pass (64, or 80 for the FP32 80-row tile,
+// whose Lam_conn rows are 80 elements long)
+inline size_t mixed_smem_bytes(int nB, int nF, size_t elem, bool stream, bool grow, int rows = 64)
 {
     const size_t lam_rows = stream ? 32 : (((size_t)nF + 3) & ~size_t(3));
-    return (grow ? 0 : (((size_t)nB + 7) & ~size_t(7)) * elem) + lam_rows * gemm_ls(elem) * elem +
+    const size_t ls = rows > 64 ? (size_t)rows : gemm_ls(elem);
+    return (grow ? 0 : (((size_t)nB + 7) & ~size_t(7)) * elem) + lam_rows * ls * elem +
            32 * gemm_xs(elem) * elem + 2 * kMaxConn * 4;
 }
 
@@ -156,15 +159,15 @@ struct MixedShape {
     bool stream, grow;
     size_t smem;
 };
-inline MixedShape mixed_shape(int nB, int nF, size_t elem, size_t row_limit)
+inline MixedShape mixed_shape(int nB, int nF, size_t elem, size_t row_limit, int rows = 64)
 {
     const size_t lim = row_limit < kSmemMax ? row_limit : kSmemMax;
     for (int grow = 0; grow < 2; ++grow)
         for (int stream = 0; stream < 2; ++stream) {
-            const size_t b = mixed_smem_bytes(nB, nF, elem, stream, grow);
+            const size_t b = mixed_smem_bytes(nB, nF, elem, stream, grow, rows);
             if (b <= (grow ? kSmemMax : lim)) return MixedShape{stream != 0, grow != 0, b};
         }
-    return MixedShape{true, true, mixed_smem_bytes(nB, nF, elem, true, true)};
+    return MixedShape{true, true, mixed_smem_bytes(nB, nF, elem, true, true, rows)};
 }
 
 template <typename Ti>

@@ -211,10 +211,19 @@ __device__ __forceinline__ void load_lam(const double *p, double l[EPT])
 template <int EPT>
 __device__ __forceinline__ void load_lam(const float *p, float l[EPT])
 {
-    static_assert(EPT == 8, "FP32 GEMM uses 8 excitations per thread");
-    const float4 q0 = reinterpret_cast<const float4 *>(p)[0], q1 = reinterpret_cast<const float4 *>(p)[1];
-    l[0] = q0.x; l[1] = q0.y; l[2] = q0.z; l[3] = q0.w;
-    l[4] = q1.x; l[5] = q1.y; l[6] = q1.z; l[7] = q1.w;
+    static_assert(EPT == 8 || EPT == 10, "FP32 GEMM uses 8 (64-row tile) or 10 (80-row tile) excitations per thread");
+    if constexpr (EPT == 8) {   // 32-byte aligned: two 16-byte loads
+        const float4 q0 = reinterpret_cast<const float4 *>(p)[0], q1 = reinterpret_cast<const float4 *>(p)[1];
+        l[0] = q0.x; l[1] = q0.y; l[2] = q0.z; l[3] = q0.w;
+        l[4] = q1.x; l[5] = q1.y; l[6] = q1.z; l[7] = q1.w;
+    } else {                    // 40-byte runs, 8-byte aligned
+#pragma unroll
+        for (int i = 0; i < EPT / 2; ++i) {
+            const float2 q = reinterpret_cast<const float2 *>(p)[i];
+            l[2 * i] = q.x;
+            l[2 * i + 1] = q.y;
+        }
+    }
 }
 
 // Register tile of the two GEMMs: EPT output rows x the lane's 4 columns
@@ -374,19 +383,23 @@ struct GemmCore<double, EPT> {
 // (chunk, 32 F) is filled from the gather-index table, whose next slice is
 // loaded into registers while the current one is multiplied.  With GROW the
 // source row stays in global memory (L2) and the next slice's values, not only
-// their indices, are prefetched.
+// their indices, are prefetched.  A pass covers ROWS connected excitations: 64
+// (FP64: 16 warps of 8x8 DMMA tiles; FP32: 8 warps x 8 rows), or 80 for FP32
+// with 10 rows per warp (18 orbitals, 8 electrons: 80 connected singles in one
+// pass instead of a 64-row and a 16-row pass).
 template <typename Ti, typename T, int EPT, bool STREAM, bool GROW>
-__global__ void __launch_bounds__((64 / EPT) * 32, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(sizeof(T) == 8 ? 512 : 256, (sizeof(T) == 4 && EPT == 8) ? 2 : 1)
 mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__restrict__ ct, T *__restrict__ Z,
                   int z0, int W, int jbase)
 {
-    constexpr int NT = (64 / EPT) * 32, NW = NT / 32;
+    constexpr int NT = sizeof(T) == 8 ? 512 : 256, NW = NT / 32;
+    constexpr int ROWS = sizeof(T) == 8 ? 64 : NW * EPT;
     constexpr int ITEMS = 32 * kMixCols / NT;
-    constexpr int LITEMS = STREAM ? 32 * 64 / NT : 1;
+    constexpr int LITEMS = STREAM ? 32 * ROWS / NT : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.nF, M = P.M;
     T *srow = reinterpret_cast<T *>(smem_raw);                    // [ldA] unless GROW
-    constexpr int LS = GemmLayout<T>::LS, XS = GemmLayout<T>::XS;
+    constexpr int LS = ROWS > 64 ? ROWS : GemmLayout<T>::LS, XS = GemmLayout<T>::XS;
     const int Kp = (K + 3) & ~3;
     T *lam = srow + (GROW ? 0 : P.ldA);                            // [Kp or 32][LS], rows past K zero
     T *xs = lam + (size_t)(STREAM ? 32 : Kp) * LS;                 // [32][XS]
@@ -395,8 +408,8 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
     __shared__ int wcnt[NW], cnt;
     const int a = blockIdx.x;
     const int m = connected_excitations<NT>(P, (u64)astr[a], conn, sgn, wcnt, &cnt);
-    const int jm = min(64, m - jbase);   // output rows of this pass
-    if (jm <= 0) return;                 // uniform across the CTA
+    const int jm = min(ROWS, m - jbase);   // output rows of this pass
+    if (jm <= 0) return;                   // uniform across the CTA
     const T *grow = ct + (i64)a * P.ldA;
     // stage the source row (16-byte copies) and, when it fits, Lam restricted to
     // this pass's connected excitations
@@ -442,7 +455,7 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
 #pragma unroll
             for (int it = 0; it < LITEMS; ++it) {
                 const int i = threadIdx.x + it * NT;
-                const int f = i >> 6, j = i & 63;
+                const int f = i / ROWS, j = i % ROWS;
                 lpre[it] = (j < jm && f0 + f < K) ? (T)sgn[jbase + j] * __ldg(Lam + (i64)conn[jbase + j] * K + f0 + f)
                                                   : T(0);
             }
@@ -475,12 +488,12 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
 #pragma unroll
             for (int it = 0; it < LITEMS; ++it) {
                 const int i = threadIdx.x + it * NT;
-                lam[(i >> 6) * LS + (i & 63)] = lpre[it];
+                lam[(i / ROWS) * LS + i % ROWS] = lpre[it];
             }
         }
         __syncthreads();
         if (step + 1 < nsteps) load_g(step + 1);
-        if (active) acc.step(lam, xs, STREAM ? 0 : f0, nf);
+        if (active) acc.template step<LS>(lam, xs, STREAM ? 0 : f0, nf);
         if (fci == nfc - 1) {
             if (active) acc.store(Z + ((i64)a * M + jbase) * W + cbi * kMixCols, W, jm);
             acc.zero();
@@ -769,6 +782,14 @@ static int ensure(void **p, size_t *have, size_t bytes)
     return BSIM_OK;
 }
 
+// BSIM_MIXED_ROWS80=0 keeps the 64-row FP32 mixed GEMM passes for 65..80
+// connected singles (comparison and tests).
+static bool mixed_rows80_off()
+{
+    const char *e = getenv("BSIM_MIXED_ROWS80");
+    return e && e[0] == '0';
+}
+
 // Largest shared-memory footprint for which the mixed GEMM keeps the source row
 // on chip (BSIM_MIXED_ROW_SMEM bytes lowers it, which moves the row to global
 // memory at small sizes too).
@@ -855,13 +876,14 @@ template <typename Ti, typename T, int EPT, bool STREAM, bool GROW>
 static int launch_mixed_shape(const DevBasis<Ti> *B, FastPlan<Ti> &P, const MixedArgs &ma, const T *ct, T *Z,
                               double *dst, int c0, int c1, size_t Wz, size_t smem, cudaStream_t s, StageTimer *tm)
 {
-    constexpr int NT = (64 / EPT) * 32;
+    constexpr int NT = sizeof(T) == 8 ? 512 : 256;
+    constexpr int ROWS = sizeof(T) == 8 ? 64 : (NT / 32) * EPT;
     auto kern = mixed_gemm_kernel<Ti, T, EPT, STREAM, GROW>;
     BSIM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int passes = (P.M + 63) / 64;   // 64 connected excitations per GEMM pass
+    const int passes = (P.M + ROWS - 1) / ROWS;   // ROWS connected excitations per GEMM pass
     for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
         for (int pass = 0; pass < passes; ++pass)
-            STAGE(tm, 3, s, (kern<<<P.nA, NT, smem, s>>>(ma, P.d_astr, ct, Z, z0, (int)Wz, 64 * pass)));
+            STAGE(tm, 3, s, (kern<<<P.nA, NT, smem, s>>>(ma, P.d_astr, ct, Z, z0, (int)Wz, ROWS * pass)));
         dim3 g(P.nA, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
         STAGE(tm, 4, s, (mixed_gather_kernel<Ti, T><<<g, 256, 0, s>>>(ma, B->view, Z, dst, z0, (int)Wz)));
     }
@@ -878,7 +900,8 @@ static int launch_mixed(const DevBasis<Ti> *B, FastPlan<Ti> &P, FastScratch<Ti> 
     if (rc != BSIM_OK) return rc;
     MixedArgs ma{P.nA, P.nB, P.nE, P.nF, P.M, P.ldA, P.ldG, c1, P.d_Emask, P.d_mA,
                  sizeof(T) == 8 ? (const void *)P.d_Lam : (const void *)P.d_Lam32, P.d_gidx};
-    const MixedShape sh = mixed_shape(P.nB, P.nF, sizeof(T), mixed_row_limit());
+    const int rows = (sizeof(T) == 4 && EPT == 10) ? 80 : 64;
+    const MixedShape sh = mixed_shape(P.nB, P.nF, sizeof(T), mixed_row_limit(), rows);
     if (sh.smem > kSmemMax) { set_error("mixed kernel needs %zu bytes of shared memory", sh.smem); return BSIM_ERR_UNSUPPORTED; }
     T *Z = static_cast<T *>(z.p);
     if (sh.grow)
@@ -950,7 +973,15 @@ static int run_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastState<Ti> *s
         if (rc != BSIM_OK) return rc;
     }
     if (P.nE > 0 && P.nF > 0 && P.M > 0) {
-        rc = launch_mixed<Ti, T, kEPT>(B, P, S, in, dst, c0, c1, s, tm);
+        // FP32 with 65..80 connected singles: one 80-row pass instead of 64 + 16 rows
+        bool done = false;
+        if constexpr (sizeof(T) == 4) {
+            if (P.M > 64 && P.M <= 80 && !mixed_rows80_off()) {
+                rc = launch_mixed<Ti, T, 10>(B, P, S, in, dst, c0, c1, s, tm);
+                done = true;
+            }
+        }
+        if (!done) rc = launch_mixed<Ti, T, kEPT>(B, P, S, in, dst, c0, c1, s, tm);
         if (rc != BSIM_OK) return rc;
     }
     // ---- beta side: c~^T in `in`, result t^T in tT (the beta doubles through

@@ -257,3 +257,21 @@ def test_hvec_host_pipeline(cuda):
             got = dsts[k].numpy() if hasattr(dsts[k], "numpy") else dsts[k]
             assert np.array_equal(got, y.cpu().numpy()), (mixed, k)
     f.hvec_host([], [])
+
+
+def test_fp32_mixed_gemm_80_row_tile_matches_64_row_passes(cuda, monkeypatch):
+    """65..80 connected alpha singles (18 orbitals, 5 alpha electrons: 65): the FP32 80-row
+    tile gives the same bits as a 64-row and a 16-row pass (each output accumulates the
+    same FMAs in the same order)."""
+    from binsim_b200 import cuotf
+    net = sparse_hamiltonian_network(18, seed=23)
+    B = cuotf.CuBasis(18, 5, 2)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    assert f.sigma_path()[0] == 1
+    x = dev(cuda, np.random.default_rng(4).normal(size=B.dim))
+    y80, y64 = cuda.empty_like(x), cuda.empty_like(x)
+    f.hvec_mixed(x, y80)
+    monkeypatch.setenv("BSIM_MIXED_ROWS80", "0")
+    f.hvec_mixed(x, y64)
+    monkeypatch.delenv("BSIM_MIXED_ROWS80")
+    assert cuda.equal(y80, y64)

@@ -305,6 +305,13 @@ int bsim_network_create_u64(const int64_t *orbsym, int64_t norb, int64_t ngs, co
 
 int bsim_network_destroy(void *net)
 {
+    if (bsim::is_c64_net(net)) {
+        if (*static_cast<const unsigned *>(net) == bsim::HandleMagic<unsigned long long>::net_c64)
+            delete static_cast<DevNet<unsigned long long> *>(net);
+        else
+            delete static_cast<DevNet<unsigned> *>(net);
+        return BSIM_OK;
+    }
     if (bsim::is_u64_net(net)) {
         delete static_cast<DevNet<unsigned long long> *>(net);
         return BSIM_OK;
@@ -316,6 +323,11 @@ int bsim_network_destroy(void *net)
 
 int64_t bsim_network_ngs(void *net)
 {
+    if (bsim::is_c64_net(net)) {
+        if (*static_cast<const unsigned *>(net) == bsim::HandleMagic<unsigned long long>::net_c64)
+            return static_cast<DevNet<unsigned long long> *>(net)->ngs;
+        return static_cast<DevNet<unsigned> *>(net)->ngs;
+    }
     if (bsim::is_u64_net(net)) return static_cast<DevNet<unsigned long long> *>(net)->ngs;
     return bsim::valid(N(net)) ? N(net)->ngs : -1;
 }

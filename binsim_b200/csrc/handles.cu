@@ -294,7 +294,7 @@ template <typename Ti>
 int make_network(const i64 *orbsym, i64 norb, i64 ngs, const Ti *axs, const Ti *bxs,
                  const i64 *ranks, const i64 *nzas, const i64 *nzbs, const Ti *flat_za,
                  const Ti *flat_zb, const double *flat_wa, const double *flat_wb,
-                 DevNet<Ti> **out)
+                 DevNet<Ti> **out, bool wcomplex)
 {
     if (!out) { set_error("null out"); return BSIM_ERR_NULL; }
     *out = nullptr;
@@ -325,11 +325,16 @@ int make_network(const i64 *orbsym, i64 norb, i64 ngs, const Ti *axs, const Ti *
         return BSIM_ERR_NULL;
     }
     N->z.resize(tza + tzb);
-    N->w.resize(twa + twb);
+    const i64 wm = wcomplex ? 2 : 1;   // doubles per weight
+    N->w.resize(wm * (twa + twb));
     if (tza) memcpy(N->z.data(), flat_za, tza * sizeof(Ti));
     if (tzb) memcpy(N->z.data() + tza, flat_zb, tzb * sizeof(Ti));
-    if (twa) memcpy(N->w.data(), flat_wa, twa * sizeof(double));
-    if (twb) memcpy(N->w.data() + twa, flat_wb, twb * sizeof(double));
+    if (twa) memcpy(N->w.data(), flat_wa, wm * twa * sizeof(double));
+    if (twb) memcpy(N->w.data() + wm * twa, flat_wb, wm * twb * sizeof(double));
+    if (wcomplex) {
+        N->cplx = 1;
+        N->magic = HandleMagic<Ti>::net_c64;
+    }
     N->groups.resize(ngs);
     for (i64 g = 0; g < ngs; ++g) {
         GroupDev &G = N->groups[g];
@@ -505,14 +510,14 @@ int network_from_ref_handle(const void *host_net, DevNet<unsigned> **out)
 template int make_basis<unsigned>(i64, i64, i64, i64, const i64 *, i64, DevBasis<unsigned> **);
 template int make_network<unsigned>(const i64 *, i64, i64, const unsigned *, const unsigned *, const i64 *,
                                     const i64 *, const i64 *, const unsigned *, const unsigned *,
-                                    const double *, const double *, DevNet<unsigned> **);
+                                    const double *, const double *, DevNet<unsigned> **, bool);
 template struct DevBasis<unsigned>;
 template struct DevNet<unsigned>;
 template int make_basis<unsigned long long>(i64, i64, i64, i64, const i64 *, i64, DevBasis<unsigned long long> **);
 template int make_network<unsigned long long>(const i64 *, i64, i64, const unsigned long long *,
                                               const unsigned long long *, const i64 *, const i64 *, const i64 *,
                                               const unsigned long long *, const unsigned long long *, const double *,
-                                              const double *, DevNet<unsigned long long> **);
+                                              const double *, DevNet<unsigned long long> **, bool);
 template struct DevBasis<unsigned long long>;
 template struct DevNet<unsigned long long>;
 

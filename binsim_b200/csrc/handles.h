@@ -11,11 +11,13 @@ namespace bsim {
 // Magic words per string type: UInt32 handles (the reference's GPU library's
 // type) and UInt64 handles (up to 63 spatial orbitals).
 template <typename Ti> struct HandleMagic;
+// Complex (c64) networks carry their own magic words, so the real operators
+// reject them and the c64 operators reject real networks.
 template <> struct HandleMagic<unsigned> {
-    static constexpr unsigned basis = 0xB5B1A515u, net = 0xB5B1E7A1u;
+    static constexpr unsigned basis = 0xB5B1A515u, net = 0xB5B1E7A1u, net_c64 = 0xB5B1C632u;
 };
 template <> struct HandleMagic<unsigned long long> {
-    static constexpr unsigned basis = 0xB5B1A564u, net = 0xB5B1E764u;
+    static constexpr unsigned basis = 0xB5B1A564u, net = 0xB5B1E764u, net_c64 = 0xB5B1C664u;
 };
 constexpr unsigned kBasisMagic = HandleMagic<unsigned>::basis;
 constexpr unsigned kNetMagic = HandleMagic<unsigned>::net;
@@ -84,7 +86,8 @@ struct DevNet {
     i64 ngs = 0;
     std::vector<GroupDev> groups;        // original order
     std::vector<Ti> z;
-    std::vector<double> w;
+    std::vector<double> w;               // complex networks: interleaved (re, im), offsets in complex units
+    int cplx = 0;                        // 1: complex weights (the reference's Tv = complex<double>)
     std::vector<i64> orbsym;
     // reference-style bookkeeping (ham/otf.hpp:329-344)
     std::vector<int> excit_type;         // [ngs] original index -> type
@@ -123,11 +126,13 @@ template <typename Ti>
 int make_basis(i64 norb, i64 na, i64 nb, i64 total_sym, const i64 *orbsym, i64 num_irreps,
                DevBasis<Ti> **out);
 
+// wcomplex: flat_wa / flat_wb hold interleaved complex weights (twice the
+// doubles), the network gets the c64 magic word.
 template <typename Ti>
 int make_network(const i64 *orbsym, i64 norb, i64 ngs, const Ti *axs, const Ti *bxs,
                  const i64 *ranks, const i64 *nzas, const i64 *nzbs, const Ti *flat_za,
                  const Ti *flat_zb, const double *flat_wa, const double *flat_wb,
-                 DevNet<Ti> **out);
+                 DevNet<Ti> **out, bool wcomplex = false);
 
 // From the reference's own host handles (layout mirrors in refmirror.h).
 int basis_from_ref_handle(const void *host_basis, DevBasis<unsigned> **out);
@@ -137,8 +142,16 @@ template <typename Ti>
 inline bool valid(const DevBasis<Ti> *b) { return b && b->magic == HandleMagic<Ti>::basis; }
 template <typename Ti>
 inline bool valid(const DevNet<Ti> *n) { return n && n->magic == HandleMagic<Ti>::net; }
+template <typename Ti>
+inline bool valid_c64(const DevNet<Ti> *n) { return n && n->magic == HandleMagic<Ti>::net_c64; }
 // The first word of a handle tells its string type.
 inline bool is_u64_basis(const void *h) { return h && *static_cast<const unsigned *>(h) == HandleMagic<unsigned long long>::basis; }
 inline bool is_u64_net(const void *h) { return h && *static_cast<const unsigned *>(h) == HandleMagic<unsigned long long>::net; }
+inline bool is_c64_net(const void *h)
+{
+    if (!h) return false;
+    const unsigned m = *static_cast<const unsigned *>(h);
+    return m == HandleMagic<unsigned>::net_c64 || m == HandleMagic<unsigned long long>::net_c64;
+}
 
 }  // namespace bsim

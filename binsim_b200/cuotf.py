@@ -84,6 +84,18 @@ def lib() -> C.CDLL:
         "bsim_grad_noalloc": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_batchgrad": (ci, [vp, vp, vp, vp, vp, vp, vp]),
         "bsim_hvec_host": (ci, [vp, vp, i64, vp, vp, ci, vp]),
+        "bsim_network_create_c64": (ci, [vp, i64, i64] + [vp] * 10),
+        "bsim_network_create_c64_u64": (ci, [vp, i64, i64] + [vp] * 10),
+        "bsim_hvec_c64": (ci, [vp, vp, vp, vp, vp]),
+        "bsim_diag_c64": (ci, [vp, vp, vp, vp]),
+        "bsim_expm_c64": (ci, [vp, vp, i64, dbl, vp, vp]),
+        "bsim_grad_c64": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
+        "bsim_backgrad_c64": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
+        "bsim_tvec_c64": (ci, [vp, vp, i64, vp, vp, vp]),
+        "bsim_backtran_c64": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
+        "bsim_batchexpm_c64": (ci, [vp, vp, i64, dbl, vp, ci, ci, vp]),
+        "bsim_batchgrad_c64": (ci, [vp, vp, vp, vp, vp, vp, vp]),
+        "bsim_batchtran_c64": (ci, [vp, vp, vp, vp, vp, vp]),
         "bsim_tvec": (ci, [vp, vp, i64, vp, vp, vp]),
         "bsim_backtran": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_batchexpm": (ci, [vp, vp, i64, dbl, vp, ci, ci, vp]),
@@ -229,6 +241,82 @@ class CuNetwork:
             self.close()
         except Exception:
             pass
+
+
+class CuNetworkC64:
+    """Device OTF network with complex weights (the reference's _c64 networks):
+    ``wa``, ``wb`` are complex128 arrays in the order of ``net.flat_wa`` /
+    ``net.flat_wb`` (the real ``net`` supplies masks, ranks and counts)."""
+
+    def __init__(self, net: nw.OTFNetwork, wa, wb, string_bits: Optional[int] = None):
+        L = lib()
+        out = vp()
+        bits = string_bits or (32 if net.norb <= 32 else 64)
+        if bits == 32:
+            a = net.as_uint32()
+        else:
+            a = {k: _host(getattr(net, k), np.uint64) for k in ("axs", "bxs", "flat_zas", "flat_zbs")}
+        self._keep = [
+            _host(net.orbsym, np.int64), a["axs"], a["bxs"], _host(net.ranks, np.int64),
+            _host(net.num_zas, np.int64), _host(net.num_zbs, np.int64), a["flat_zas"], a["flat_zbs"],
+            np.ascontiguousarray(wa, np.complex128), np.ascontiguousarray(wb, np.complex128)]
+        k = self._keep
+        create = L.bsim_network_create_c64 if bits == 32 else L.bsim_network_create_c64_u64
+        _check(create(k[0].ctypes.data, net.norb, net.ngs, *[x.ctypes.data for x in k[1:]], C.byref(out)),
+               "bsim_network_create_c64")
+        self.h = out.value
+        self.ngs = L.bsim_network_ngs(self.h)
+
+    close = CuNetwork.close
+    __del__ = CuNetwork.__del__
+
+
+class CuOTFC64:
+    """Complex operators on complex128 torch tensors (the reference CPU library's
+    _c64 interface, jl/network.jl:516-556, on the GPU); group indices 0-based."""
+
+    def __init__(self, basis: "CuBasis", net: CuNetworkC64):
+        self.basis, self.net = basis, net
+        import torch
+        self._slot = torch.zeros(2, dtype=torch.float64, device="cuda")
+
+    def _c(self, name, *args):
+        _check(getattr(lib(), name)(self.basis.h, self.net.h, *args), name)
+
+    def hvec(self, src, dst, stream=None):
+        self._c("bsim_hvec_c64", _ptr(src), _ptr(dst), _stream(stream))
+
+    def get_diags(self, d, stream=None):
+        self._c("bsim_diag_c64", _ptr(d), _stream(stream))
+
+    def expm(self, idx: int, theta: float, v, stream=None):
+        self._c("bsim_expm_c64", idx, theta, _ptr(v), _stream(stream))
+
+    def grad(self, idx: int, theta: float, l, r, stream=None) -> complex:
+        self._c("bsim_grad_c64", idx, theta, _ptr(l), _ptr(r), _ptr(self._slot), _stream(stream))
+        re, im = self._slot.tolist()
+        return complex(re, im)
+
+    def backgrad(self, idx: int, theta: float, l, r, stream=None) -> complex:
+        self._c("bsim_backgrad_c64", idx, theta, _ptr(l), _ptr(r), _ptr(self._slot), _stream(stream))
+        re, im = self._slot.tolist()
+        return complex(re, im)
+
+    def tvec(self, idx: int, src, dst, stream=None):
+        self._c("bsim_tvec_c64", idx, _ptr(src), _ptr(dst), _stream(stream))
+
+    def backtran(self, idx: int, theta: float, l, r, b, stream=None):
+        self._c("bsim_backtran_c64", idx, theta, _ptr(l), _ptr(r), _ptr(b), _stream(stream))
+
+    def batchexpm(self, idx: int, theta: float, mat, ld: int, nv: int, stream=None):
+        self._c("bsim_batchexpm_c64", idx, theta, _ptr(mat), ld, nv, _stream(stream))
+
+    def batchgrad(self, thetas, l, r, grads, stream=None):
+        th = _host(thetas, np.float64)
+        self._c("bsim_batchgrad_c64", th.ctypes.data, _ptr(l), _ptr(r), _ptr(grads), _stream(stream))
+
+    def batchtran(self, l, r, trans, stream=None):
+        self._c("bsim_batchtran_c64", _ptr(l), _ptr(r), _ptr(trans), _stream(stream))
 
 
 class CuOTFFunctions:

@@ -216,6 +216,47 @@ int bsim_backgrad(void *basis, void *net, int64_t idx, double theta, double *l, 
 /* Pool gradient (thetas, grads: device, original group order). */
 int bsim_batchgrad(void *basis, void *net, const double *thetas, const double *l, const double *r,
                    double *grads, bsim_stream_t stream);
+/* ------------------------------------------------------------------------
+ * Complex (c64) networks and operators: the reference CPU library's _c64
+ * exports (src/extern/otf_native.cpp:4,6; Tv = complex<double>) on device
+ * vectors of interleaved (re, im) doubles, dim complex entries each.  The
+ * reference has no GPU counterpart.  flat_wa / flat_wb hold interleaved complex
+ * weights (2 doubles per weight, the layout of ComplexF64 arrays); the other
+ * arguments are those of bsim_network_create_u32 / _u64.  A c64 network works
+ * only with the _c64 calls (and bsim_network_destroy), and any basis handle.
+ * Semantics per call as the real ones, with the complex rules of
+ * core/math.hpp:7-252 (diagonal groups: exp(i theta Im vt) factors):
+ *   hvec: dst = H src (overwritten); diag: diag += diagonal (accumulates);
+ *   expm: vec <- e^{theta G} vec; grad / backgrad: *out_dev (2 doubles, device)
+ *   = the complex gradient term; tvec: dst = T src (overwritten); backtran:
+ *   l, r <- e^{theta T} l, r and b = T l (overwritten); batchexpm on num_vecs
+ *   entries of ld per determinant; batchgrad: grads[g] at thetas_host[g] (host
+ *   angles, device complex grads); batchtran: trans[g] = <l|T_g|r>.
+ * ------------------------------------------------------------------------ */
+int bsim_network_create_c64(const int64_t *orbsym, int64_t norb, int64_t ngs, const uint32_t *axs,
+                            const uint32_t *bxs, const int64_t *ranks, const int64_t *num_zas,
+                            const int64_t *num_zbs, const uint32_t *flat_zas, const uint32_t *flat_zbs,
+                            const double *flat_wa, const double *flat_wb, void **out);
+int bsim_network_create_c64_u64(const int64_t *orbsym, int64_t norb, int64_t ngs, const uint64_t *axs,
+                                const uint64_t *bxs, const int64_t *ranks, const int64_t *num_zas,
+                                const int64_t *num_zbs, const uint64_t *flat_zas, const uint64_t *flat_zbs,
+                                const double *flat_wa, const double *flat_wb, void **out);
+int bsim_hvec_c64(void *basis, void *net, const double *src, double *dst, bsim_stream_t stream);
+int bsim_diag_c64(void *basis, void *net, double *diag, bsim_stream_t stream);
+int bsim_expm_c64(void *basis, void *net, int64_t idx, double theta, double *vec, bsim_stream_t stream);
+int bsim_grad_c64(void *basis, void *net, int64_t idx, double theta, const double *l, const double *r,
+                  double *out_dev, bsim_stream_t stream);
+int bsim_backgrad_c64(void *basis, void *net, int64_t idx, double theta, double *l, double *r, double *out_dev,
+                      bsim_stream_t stream);
+int bsim_tvec_c64(void *basis, void *net, int64_t idx, const double *src, double *dst, bsim_stream_t stream);
+int bsim_backtran_c64(void *basis, void *net, int64_t idx, double theta, double *l, double *r, double *b,
+                      bsim_stream_t stream);
+int bsim_batchexpm_c64(void *basis, void *net, int64_t idx, double theta, double *matrix, int ld, int num_vecs,
+                       bsim_stream_t stream);
+int bsim_batchgrad_c64(void *basis, void *net, const double *thetas_host, const double *l, const double *r,
+                       double *grads, bsim_stream_t stream);
+int bsim_batchtran_c64(void *basis, void *net, const double *l, const double *r, double *trans, bsim_stream_t stream);
+
 /* Status-returning forms of tvec_cuda, backtran_cuda, batchexpm_cuda and
  * batchtran_cuda (same semantics; every group type and symmetry-block layout;
  * batchexpm needs 0 <= num_vecs <= ld). */

@@ -72,6 +72,18 @@ class Oracle:
         lib.oracle_backgrad.argtypes = [vp, vp, i64, dbl, vp, vp]
         lib.oracle_batchgrad.argtypes = [vp, vp, vp, vp, vp, vp]
         lib.oracle_tvec.argtypes = [vp, vp, i64, vp, vp]
+        lib.oracle_net_create_c64.restype = vp
+        lib.oracle_net_create_c64.argtypes = [vp, i64, i64] + [vp] * 9
+        for name, args in (("oracle_hvec_c64", [vp, vp, vp, vp]), ("oracle_diag_c64", [vp, vp, vp]),
+                           ("oracle_expm_c64", [vp, vp, i64, dbl, vp]),
+                           ("oracle_grad_c64", [vp, vp, i64, dbl, vp, vp, vp]),
+                           ("oracle_backgrad_c64", [vp, vp, i64, dbl, vp, vp, vp]),
+                           ("oracle_tvec_c64", [vp, vp, i64, vp, vp]),
+                           ("oracle_backtran_c64", [vp, vp, i64, dbl, vp, vp, vp]),
+                           ("oracle_batchexpm_c64", [vp, vp, i64, dbl, vp, C.c_int, C.c_int]),
+                           ("oracle_batchgrad_c64", [vp, vp, vp, vp, vp, vp]),
+                           ("oracle_batchtran_c64", [vp, vp, vp, vp, vp])):
+            getattr(lib, name).argtypes = args
         lib.oracle_backtran.argtypes = [vp, vp, i64, dbl, vp, vp, vp]
         lib.oracle_batchexpm.argtypes = [vp, vp, i64, dbl, vp, C.c_int, C.c_int]
         lib.oracle_batchtran.argtypes = [vp, vp, vp, vp, vp]
@@ -104,6 +116,77 @@ class Oracle:
         h = self.lib.oracle_net_create(P(a["orbsym"]), net.norb, net.ngs, P(a["axs"]), P(a["bxs"]), P(a["ranks"]),
                                        P(a["nza"]), P(a["nzb"]), P(a["za"]), P(a["zb"]), P(a["wa"]), P(a["wb"]))
         return OracleNet(self, h, net.ngs, a)
+
+    def network_c64(self, net, wa, wb):
+        """Complex-weight network (the reference's Tv = complex<double>): wa, wb are
+        complex128 arrays in the order of net.flat_wa / net.flat_wb."""
+        a = dict(orbsym=np.ascontiguousarray(net.orbsym, np.int64),
+                 axs=np.ascontiguousarray(net.axs, np.uint64), bxs=np.ascontiguousarray(net.bxs, np.uint64),
+                 ranks=np.ascontiguousarray(net.ranks, np.int64),
+                 nza=np.ascontiguousarray(net.num_zas, np.int64), nzb=np.ascontiguousarray(net.num_zbs, np.int64),
+                 za=np.ascontiguousarray(net.flat_zas, np.uint64), zb=np.ascontiguousarray(net.flat_zbs, np.uint64),
+                 wa=np.ascontiguousarray(wa, np.complex128), wb=np.ascontiguousarray(wb, np.complex128))
+        h = self.lib.oracle_net_create_c64(P(a["orbsym"]), net.norb, net.ngs, P(a["axs"]), P(a["bxs"]),
+                                           P(a["ranks"]), P(a["nza"]), P(a["nzb"]), P(a["za"]), P(a["zb"]),
+                                           P(a["wa"]), P(a["wb"]))
+        return OracleNet(self, h, net.ngs, a)
+
+    # complex operators on complex128 arrays
+    def hvec_c64(self, B, N, x):
+        x = np.ascontiguousarray(x, np.complex128); y = np.zeros(B.dim, np.complex128)
+        self.lib.oracle_hvec_c64(B.h, N.h, P(x), P(y))
+        return y
+
+    def diag_c64(self, B, N):
+        d = np.zeros(B.dim, np.complex128)
+        self.lib.oracle_diag_c64(B.h, N.h, P(d))
+        return d
+
+    def expm_c64(self, B, N, idx, theta, v):
+        v = np.array(v, np.complex128, copy=True)
+        self.lib.oracle_expm_c64(B.h, N.h, idx, theta, P(v))
+        return v
+
+    def grad_c64(self, B, N, idx, theta, l, r):
+        out = np.zeros(2)
+        self.lib.oracle_grad_c64(B.h, N.h, idx, theta, P(np.ascontiguousarray(l, np.complex128)),
+                                 P(np.ascontiguousarray(r, np.complex128)), P(out))
+        return complex(out[0], out[1])
+
+    def backgrad_c64(self, B, N, idx, theta, l, r):
+        l = np.array(l, np.complex128, copy=True); r = np.array(r, np.complex128, copy=True)
+        out = np.zeros(2)
+        self.lib.oracle_backgrad_c64(B.h, N.h, idx, theta, P(l), P(r), P(out))
+        return complex(out[0], out[1]), l, r
+
+    def tvec_c64(self, B, N, idx, src):
+        dst = np.zeros(B.dim, np.complex128)
+        self.lib.oracle_tvec_c64(B.h, N.h, idx, P(np.ascontiguousarray(src, np.complex128)), P(dst))
+        return dst
+
+    def backtran_c64(self, B, N, idx, theta, l, r):
+        l = np.array(l, np.complex128, copy=True); r = np.array(r, np.complex128, copy=True)
+        b = np.zeros(B.dim, np.complex128)
+        self.lib.oracle_backtran_c64(B.h, N.h, idx, theta, P(l), P(r), P(b))
+        return l, r, b
+
+    def batchexpm_c64(self, B, N, idx, theta, M, nv):
+        M = np.array(M, np.complex128, copy=True, order="C")
+        self.lib.oracle_batchexpm_c64(B.h, N.h, idx, theta, P(M), M.shape[1], nv)
+        return M
+
+    def batchgrad_c64(self, B, N, thetas, l, r):
+        g = np.zeros(N.ngs, np.complex128)
+        self.lib.oracle_batchgrad_c64(B.h, N.h, P(np.ascontiguousarray(thetas, np.float64)),
+                                      P(np.ascontiguousarray(l, np.complex128)),
+                                      P(np.ascontiguousarray(r, np.complex128)), P(g))
+        return g
+
+    def batchtran_c64(self, B, N, l, r):
+        t = np.zeros(N.ngs, np.complex128)
+        self.lib.oracle_batchtran_c64(B.h, N.h, P(np.ascontiguousarray(l, np.complex128)),
+                                      P(np.ascontiguousarray(r, np.complex128)), P(t))
+        return t
 
     # -- operators --------------------------------------------------------
     def hvec(self, B, N, x):
@@ -264,6 +347,11 @@ def build_ref() -> bool:
     return ref_available()
 
 
+class Cplx(C.Structure):
+    """std::complex<double> returned by value (two doubles)."""
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
 class RefLibs:
     """ctypes access to the reference's compiled CPU libraries (uint32 strings)."""
 
@@ -291,6 +379,22 @@ class RefLibs:
         self.otf.backtran_contract_otf_f64.argtypes = [vp, vp, i64, dbl, vp, vp, vp]
         self.otf.batch_expm_contract_otf_f64.argtypes = [vp, vp, i64, dbl, vp, C.c_int, C.c_int]
         self.otf.batch_tran_contract_otf_f64.argtypes = [vp, vp, vp, vp, vp]
+        # complex interface (Tv = complex<double>, otf_native.cpp:4): complex results
+        # come back as two doubles (the layout of std::complex<double>)
+        self.otf.build_network_otf_c64.restype = vp
+        self.otf.build_network_otf_c64.argtypes = [vp, i64, i64] + [vp] * 9
+        self.otf.hvec_gather_contract_otf_c64.argtypes = [vp, vp, vp, vp]
+        self.otf.get_diags_elements_c64.argtypes = [vp, vp, vp]
+        self.otf.expm_contract_otf_c64.argtypes = [vp, vp, i64, dbl, vp]
+        self.otf.grad_contract_otf_c64.restype = Cplx
+        self.otf.grad_contract_otf_c64.argtypes = [vp, vp, i64, dbl, vp, vp]
+        self.otf.backgrad_contract_otf_c64.restype = Cplx
+        self.otf.backgrad_contract_otf_c64.argtypes = [vp, vp, i64, dbl, vp, vp]
+        self.otf.tvec_contract_otf_c64.argtypes = [vp, vp, i64, vp, vp]
+        self.otf.backtran_contract_otf_c64.argtypes = [vp, vp, i64, dbl, vp, vp, vp]
+        self.otf.batch_expm_contract_otf_c64.argtypes = [vp, vp, i64, dbl, vp, C.c_int, C.c_int]
+        self.otf.batch_grad_contract_otf_c64.argtypes = [vp, vp, vp, vp, vp, vp]
+        self.otf.batch_tran_contract_otf_c64.argtypes = [vp, vp, vp, vp, vp]
         self.bas.create_basis_manager.restype = vp
         self.bas.create_basis_manager.argtypes = [i64, i64, i64, i64, vp, i64]
         self.bas.get_subspace_dim.restype = i64
@@ -387,6 +491,71 @@ class RefLibs:
     def batchtran(self, b, n, l, r, ngs):
         t = np.zeros(ngs)
         self.otf.batch_tran_contract_otf_f64(b, n, P(np.ascontiguousarray(l)), P(np.ascontiguousarray(r)), P(t))
+        return t
+
+    def network_c64(self, net, wa, wb):
+        a = [np.ascontiguousarray(net.orbsym, np.int64)]
+        arrs = [np.ascontiguousarray(net.axs, np.uint32), np.ascontiguousarray(net.bxs, np.uint32),
+                np.ascontiguousarray(net.ranks, np.int64), np.ascontiguousarray(net.num_zas, np.int64),
+                np.ascontiguousarray(net.num_zbs, np.int64), np.ascontiguousarray(net.flat_zas, np.uint32),
+                np.ascontiguousarray(net.flat_zbs, np.uint32), np.ascontiguousarray(wa, np.complex128),
+                np.ascontiguousarray(wb, np.complex128)]
+        h = self.otf.build_network_otf_c64(P(a[0]), net.norb, net.ngs, *[P(x) for x in arrs])
+        self._keep.append((a, arrs))
+        return h
+
+    def hvec_c64(self, b, n, x, dim):
+        x = np.ascontiguousarray(x, np.complex128); y = np.zeros(dim, np.complex128)
+        self.otf.hvec_gather_contract_otf_c64(b, n, P(x), P(y))
+        return y
+
+    def diag_c64(self, b, n, dim):
+        d = np.zeros(dim, np.complex128)
+        self.otf.get_diags_elements_c64(b, n, P(d))
+        return d
+
+    def expm_c64(self, b, n, idx, theta, v):
+        v = np.array(v, np.complex128, copy=True)
+        self.otf.expm_contract_otf_c64(b, n, idx, theta, P(v))
+        return v
+
+    def grad_c64(self, b, n, idx, theta, l, r):
+        z = self.otf.grad_contract_otf_c64(b, n, idx, theta, P(np.ascontiguousarray(l, np.complex128)),
+                                           P(np.ascontiguousarray(r, np.complex128)))
+        return complex(z.re, z.im)
+
+    def backgrad_c64(self, b, n, idx, theta, l, r):
+        l = np.array(l, np.complex128, copy=True); r = np.array(r, np.complex128, copy=True)
+        z = self.otf.backgrad_contract_otf_c64(b, n, idx, theta, P(l), P(r))
+        return complex(z.re, z.im), l, r
+
+    def tvec_c64(self, b, n, idx, src, dim):
+        dst = np.zeros(dim, np.complex128)
+        self.otf.tvec_contract_otf_c64(b, n, idx, P(np.ascontiguousarray(src, np.complex128)), P(dst))
+        return dst
+
+    def backtran_c64(self, b, n, idx, theta, l, r, dim):
+        l = np.array(l, np.complex128, copy=True); r = np.array(r, np.complex128, copy=True)
+        bv = np.zeros(dim, np.complex128)
+        self.otf.backtran_contract_otf_c64(b, n, idx, theta, P(l), P(r), P(bv))
+        return l, r, bv
+
+    def batchexpm_c64(self, b, n, idx, theta, M, nv):
+        M = np.array(M, np.complex128, copy=True, order="C")
+        self.otf.batch_expm_contract_otf_c64(b, n, idx, theta, P(M), M.shape[1], nv)
+        return M
+
+    def batchgrad_c64(self, b, n, thetas, l, r, ngs):
+        g = np.zeros(ngs, np.complex128)
+        self.otf.batch_grad_contract_otf_c64(b, n, P(np.ascontiguousarray(thetas, np.float64)),
+                                             P(np.ascontiguousarray(l, np.complex128)),
+                                             P(np.ascontiguousarray(r, np.complex128)), P(g))
+        return g
+
+    def batchtran_c64(self, b, n, l, r, ngs):
+        t = np.zeros(ngs, np.complex128)
+        self.otf.batch_tran_contract_otf_c64(b, n, P(np.ascontiguousarray(l, np.complex128)),
+                                             P(np.ascontiguousarray(r, np.complex128)), P(t))
         return t
 
     def det_index(self, b, astr, bstr, dim):

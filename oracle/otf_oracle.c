@@ -213,11 +213,12 @@ typedef struct {
     OGroup *g;        /* in original order */
 } ONet;
 
-void *oracle_net_create(const i64 *orbsym, i64 norb, i64 ngs,
+/* wm: doubles per weight (1 real, 2 complex (re, im) as ComplexF64 arrays) */
+static void *net_create(const i64 *orbsym, i64 norb, i64 ngs,
                         const u64 *axs, const u64 *bxs, const i64 *ranks,
                         const i64 *nzas, const i64 *nzbs,
                         const u64 *flat_za, const u64 *flat_zb,
-                        const double *flat_wa, const double *flat_wb)
+                        const double *flat_wa, const double *flat_wb, int wm)
 {
     ONet *N = (ONet *)calloc(1, sizeof(ONet));
     N->ngs = ngs;
@@ -242,13 +243,33 @@ void *oracle_net_create(const i64 *orbsym, i64 norb, i64 ngs,
         G->zb = (u64 *)malloc(sizeof(u64) * (G->nzb + 1));
         memcpy(G->za, flat_za + oza, sizeof(u64) * G->nza); oza += G->nza;
         memcpy(G->zb, flat_zb + ozb, sizeof(u64) * G->nzb); ozb += G->nzb;
-        i64 swa = (i64)G->nza * G->rank, swb = (i64)G->nzb * G->rank;
-        G->wa = (double *)malloc(sizeof(double) * (swa + 1));
-        G->wb = (double *)malloc(sizeof(double) * (swb + 1));
+        i64 swa = (i64)G->nza * G->rank * wm, swb = (i64)G->nzb * G->rank * wm;
+        G->wa = (double *)malloc(sizeof(double) * (swa + 2));
+        G->wb = (double *)malloc(sizeof(double) * (swb + 2));
         memcpy(G->wa, flat_wa + owa, sizeof(double) * swa); owa += swa;
         memcpy(G->wb, flat_wb + owb, sizeof(double) * swb); owb += swb;
     }
     return N;
+}
+
+void *oracle_net_create(const i64 *orbsym, i64 norb, i64 ngs,
+                        const u64 *axs, const u64 *bxs, const i64 *ranks,
+                        const i64 *nzas, const i64 *nzbs,
+                        const u64 *flat_za, const u64 *flat_zb,
+                        const double *flat_wa, const double *flat_wb)
+{
+    return net_create(orbsym, norb, ngs, axs, bxs, ranks, nzas, nzbs, flat_za, flat_zb, flat_wa, flat_wb, 1);
+}
+
+/* A network of the complex (Tv = complex<double>) interface, otf_native.cpp:4,6:
+ * the weights are interleaved (re, im) pairs. */
+void *oracle_net_create_c64(const i64 *orbsym, i64 norb, i64 ngs,
+                            const u64 *axs, const u64 *bxs, const i64 *ranks,
+                            const i64 *nzas, const i64 *nzbs,
+                            const u64 *flat_za, const u64 *flat_zb,
+                            const double *flat_wa, const double *flat_wb)
+{
+    return net_create(orbsym, norb, ngs, axs, bxs, ranks, nzas, nzbs, flat_za, flat_zb, flat_wa, flat_wb, 2);
 }
 
 void oracle_net_destroy(void *p)
@@ -699,4 +720,288 @@ double oracle_dot(i64 n, const double *a, const double *b)
 void oracle_heff_col(i64 n, int dim, const double *const *V, const double *av, double *out)
 {
     for (int j = 0; j < dim; ++j) out[j] = oracle_dot(n, V[j], av);
+}
+
+/* ------------------------------------------------------------------ */
+/* Complex (c64) operators: the Tv = complex<double> instantiation of  */
+/* op/*.hpp with the rules of core/math.hpp:7-252 (conjugates, and the */
+/* diagonal factors fast_diag_exp / fast_diag_grad).  Vectors are      */
+/* interleaved (re, im) doubles.                                       */
+/* ------------------------------------------------------------------ */
+#include <complex.h>
+
+typedef double complex zc;
+
+static void phase_c(u64 s, const u64 *z, int nz, const zc *w, int rank, zc *p)
+{
+    for (int r = 0; r < rank; ++r) {
+        const zc *wr = w + (i64)r * nz;
+        zc v = 0.0;
+        for (int k = 0; k < nz; ++k) v += parity64(s & z[k]) ? -wr[k] : wr[k];
+        p[r] = v;
+    }
+}
+
+typedef void (*pair_fn_c)(i64 di, i64 si, zc vt, int diag, void *ctx, zc *acc);
+
+/* visit_pairs with complex phases; `diag` tells the visitor a diagonal group. */
+static zc visit_pairs_c(const OBasis *B, const ONet *N, const OGroup *G, int once, pair_fn_c fn, void *ctx)
+{
+    double tre = 0.0, tim = 0.0;
+    const zc *wa = (const zc *)G->wa, *wb = (const zc *)G->wb;
+    for (i64 kd = 0; kd < B->num_blocks; ++kd) {
+        i64 sa_sym = B->blk_asym[kd] ^ G->asym;
+        i64 sb_sym = B->blk_bsym[kd] ^ G->bsym;
+        if (sa_sym >= B->num_irreps || sb_sym >= B->num_irreps) continue;
+        i64 ks = B->block_map[sa_sym * B->num_irreps + sb_sym];
+        if (ks < 0) continue;
+        if (once && G->type != 0 && ks < kd) continue;
+        const int same = (ks == kd);
+        const i64 na = B->blk_na[kd], nb = B->blk_nb[kd];
+        const i64 nbs = B->blk_nb[ks];
+        const u64 *as = B->blk_astrs[kd], *bs = B->blk_bstrs[kd];
+        i64 *sbi = (i64 *)malloc(sizeof(i64) * (nb + 1));
+        zc *pb = (zc *)malloc(sizeof(zc) * (nb + 1) * (G->rank + 1));
+        for (i64 b = 0; b < nb; ++b) {
+            u64 s = bs[b] ^ G->bx;
+            sbi[b] = (G->bx == 0) ? b : str_index(B, 1, s, N->orbsym);
+            if (sbi[b] >= 0) phase_c(s, G->zb, G->nzb, wb, G->rank, pb + b * G->rank);
+        }
+        double are = 0.0, aim = 0.0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : are, aim)
+        for (i64 a = 0; a < na; ++a) {
+            u64 s = as[a] ^ G->ax;
+            i64 sa = (G->ax == 0) ? a : str_index(B, 0, s, N->orbsym);
+            if (sa < 0) continue;
+            if (once && same && G->type != 2 && G->type != 0 && sa < a) continue;
+            zc pa[MAXR];
+            phase_c(s, G->za, G->nza, wa, G->rank, pa);
+            zc local = 0.0;
+            for (i64 b = 0; b < nb; ++b) {
+                i64 sb = sbi[b];
+                if (sb < 0) continue;
+                if (once && same && G->type == 2 && sb < b) continue;
+                zc vt = 0.0;
+                for (int r = 0; r < G->rank; ++r) vt += pa[r] * pb[b * G->rank + r];
+                i64 di = B->blk_off[kd] + a * nb + b;
+                i64 si = B->blk_off[ks] + sa * nbs + sb;
+                fn(di, si, vt, G->type == 0, ctx, &local);
+            }
+            are += creal(local);
+            aim += cimag(local);
+        }
+        tre += are;
+        tim += aim;
+        free(sbi);
+        free(pb);
+    }
+    return tre + I * tim;
+}
+
+typedef struct { const zc *src; zc *dst; } HvecCtxC;
+
+static void hvec_pair_c(i64 di, i64 si, zc vt, int diag, void *ctx, zc *acc)
+{
+    (void)diag; (void)acc;
+    HvecCtxC *c = (HvecCtxC *)ctx;
+    c->dst[di] += c->src[si] * vt;   /* hvec_update, core/math.hpp:126-130 */
+}
+
+/* dst = H src (op/hvec.hpp:481-496); dst zeroed first. */
+void oracle_hvec_c64(void *bp, void *np, const double *src, double *dst)
+{
+    OBasis *B = (OBasis *)bp;
+    ONet *N = (ONet *)np;
+    memset(dst, 0, sizeof(zc) * B->dim);
+    HvecCtxC c = {(const zc *)src, (zc *)dst};
+    for (i64 g = 0; g < N->ngs; ++g) visit_pairs_c(B, N, &N->g[g], 0, hvec_pair_c, &c);
+}
+
+static void diag_pair_c(i64 di, i64 si, zc vt, int diag, void *ctx, zc *acc)
+{
+    (void)si; (void)diag; (void)acc;
+    ((zc *)ctx)[di] += vt;
+}
+
+/* diag += the first diagonal group's values (op/hvec.hpp:498-554). */
+void oracle_diag_c64(void *bp, void *np, double *diag)
+{
+    ONet *N = (ONet *)np;
+    for (i64 g = 0; g < N->ngs; ++g)
+        if (N->g[g].type == 0) { visit_pairs_c((OBasis *)bp, N, &N->g[g], 1, diag_pair_c, diag); return; }
+}
+
+typedef struct { zc *l, *r, *b; double cd, co, gcd, gco, th_e, th_g; int ld, nv; } OpCtxC;
+
+static zc diag_exp(zc vt, double t) { return cexp(I * (cimag(vt) * t)); }      /* fast_diag_exp */
+static zc diag_grad(zc vt, double t) { return vt * cexp(I * (cimag(vt) * t)); } /* fast_diag_grad */
+
+static void expm_pair_c(i64 di, i64 si, zc vt, int diag, void *ctx, zc *acc)
+{
+    (void)acc;
+    OpCtxC *c = (OpCtxC *)ctx;
+    if (diag) { c->l[di] *= diag_exp(vt, c->th_e); return; }
+    /* expm_update, core/math.hpp:132-146 */
+    double vd = 1.0 + c->cd * creal(vt * conj(vt));
+    zc vf = c->co * vt, vr = c->co * conj(vt);
+    zc vi = c->l[si], vj = c->l[di];
+    c->l[si] = vi * vd - vj * vr;
+    c->l[di] = vj * vd + vi * vf;
+}
+
+void oracle_expm_c64(void *bp, void *np, i64 idx, double theta, double *vec)
+{
+    OpCtxC c = {(zc *)vec, 0, 0, cos(theta) - 1.0, sin(theta), 0, 0, theta, 0, 0, 0};
+    visit_pairs_c((OBasis *)bp, (ONet *)np, &((ONet *)np)->g[idx], 1, expm_pair_c, &c);
+}
+
+static void grad_pair_c(i64 di, i64 si, zc vt, int diag, void *ctx, zc *acc)
+{
+    OpCtxC *c = (OpCtxC *)ctx;
+    if (diag) { *acc += conj(c->l[di] * diag_grad(vt, c->th_g)) * c->r[di]; return; }
+    /* grad_update, core/math.hpp:148-162 */
+    double vd = c->cd * creal(vt * conj(vt));
+    zc vf = c->co * vt, vr = c->co * conj(vt);
+    zc rvi = c->r[si], rvj = c->r[di];
+    *acc += conj(c->l[si]) * (rvi * vd + rvj * vr) + conj(c->l[di]) * (rvj * vd - rvi * vf);
+}
+
+/* <l| G e^{theta G} |r> (op/grad.hpp:397-465), written to out[0..1]. */
+void oracle_grad_c64(void *bp, void *np, i64 idx, double theta, const double *l, const double *r, double *out)
+{
+    OpCtxC c = {(zc *)l, (zc *)r, 0, -sin(theta), cos(theta), 0, 0, 0, theta, 0, 0};
+    zc g = visit_pairs_c((OBasis *)bp, (ONet *)np, &((ONet *)np)->g[idx], 1, grad_pair_c, &c);
+    out[0] = creal(g);
+    out[1] = cimag(g);
+}
+
+static void back_pair_c(i64 di, i64 si, zc vt, int diag, void *ctx, zc *acc)
+{
+    OpCtxC *c = (OpCtxC *)ctx;
+    if (diag) {   /* op/backgrad.hpp:52-70 */
+        zc u = diag_exp(vt, c->th_e);
+        c->l[di] *= u;
+        *acc += conj(c->l[di] * diag_grad(vt, c->th_g)) * c->r[di];
+        c->r[di] *= u;
+        return;
+    }
+    /* backgrad_update, core/math.hpp:187-215 */
+    double n2 = creal(vt * conj(vt));
+    double evd = 1.0 + c->cd * n2, gvd = c->gcd * n2;
+    zc ef = c->co * vt, er = c->co * conj(vt), gf = c->gco * vt, gr = c->gco * conj(vt);
+    zc lvi = c->l[si], lvj = c->l[di], rvi = c->r[si], rvj = c->r[di];
+    zc els = lvi * evd - lvj * er, eld = lvj * evd + lvi * ef;
+    *acc += conj(els) * (rvi * gvd + rvj * gr) + conj(eld) * (rvj * gvd - rvi * gf);
+    c->l[si] = els;
+    c->l[di] = eld;
+    c->r[si] = rvi * evd - rvj * er;
+    c->r[di] = rvj * evd + rvi * ef;
+}
+
+/* Fused adjoint step (op/backgrad.hpp:406-474, angles :81-84). */
+void oracle_backgrad_c64(void *bp, void *np, i64 idx, double theta, double *l, double *r, double *out)
+{
+    OpCtxC c = {(zc *)l, (zc *)r, 0, cos(theta) - 1.0, -sin(theta), -sin(theta), cos(theta), -theta, theta, 0, 0};
+    zc g = visit_pairs_c((OBasis *)bp, (ONet *)np, &((ONet *)np)->g[idx], 1, back_pair_c, &c);
+    out[0] = creal(g);
+    out[1] = cimag(g);
+}
+
+static void tvec_pair_c(i64 di, i64 si, zc vt, int diag, void *ctx, zc *acc)
+{
+    (void)acc;
+    OpCtxC *c = (OpCtxC *)ctx;   /* l = src, r = dst */
+    if (diag) { c->r[di] = c->l[di] * vt; return; }
+    zc ss = c->l[si], sd = c->l[di];   /* tvec_update, core/math.hpp:165-170 */
+    c->r[si] = sd * (-conj(vt));
+    c->r[di] = ss * vt;
+}
+
+void oracle_tvec_c64(void *bp, void *np, i64 idx, const double *src, double *dst)
+{
+    memset(dst, 0, sizeof(zc) * ((OBasis *)bp)->dim);
+    OpCtxC c = {(zc *)src, (zc *)dst, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    visit_pairs_c((OBasis *)bp, (ONet *)np, &((ONet *)np)->g[idx], 1, tvec_pair_c, &c);
+}
+
+static void backtran_pair_c(i64 di, i64 si, zc vt, int diag, void *ctx, zc *acc)
+{
+    (void)acc;
+    OpCtxC *c = (OpCtxC *)ctx;
+    if (diag) {   /* op/backtran.hpp:7-70 */
+        zc u = diag_exp(vt, c->th_e);
+        c->l[di] *= u;
+        c->r[di] *= u;
+        c->b[di] = c->l[di] * vt;
+        return;
+    }
+    /* backtran_update, core/math.hpp:217-226 */
+    double vd = 1.0 + c->cd * creal(vt * conj(vt));
+    zc vf = c->co * vt, vr = c->co * conj(vt);
+    zc li = c->l[si], lj = c->l[di], ri = c->r[si], rj = c->r[di];
+    zc ls = li * vd - lj * vr, ld = lj * vd + li * vf;
+    c->l[si] = ls;
+    c->l[di] = ld;
+    c->r[si] = ri * vd - rj * vr;
+    c->r[di] = rj * vd + ri * vf;
+    c->b[si] = ld * (-conj(vt));
+    c->b[di] = ls * vt;
+}
+
+void oracle_backtran_c64(void *bp, void *np, i64 idx, double theta, double *l, double *r, double *b)
+{
+    memset(b, 0, sizeof(zc) * ((OBasis *)bp)->dim);
+    OpCtxC c = {(zc *)l, (zc *)r, (zc *)b, cos(theta) - 1.0, sin(theta), 0, 0, theta, 0, 0, 0};
+    visit_pairs_c((OBasis *)bp, (ONet *)np, &((ONet *)np)->g[idx], 1, backtran_pair_c, &c);
+}
+
+static void batchexpm_pair_c(i64 di, i64 si, zc vt, int diag, void *ctx, zc *acc)
+{
+    (void)acc;
+    OpCtxC *c = (OpCtxC *)ctx;
+    zc *sp = c->l + si * c->ld, *dp = c->l + di * c->ld;
+    if (diag) {   /* expm_batch_update_diag */
+        zc u = diag_exp(vt, c->th_e);
+        for (int k = 0; k < c->nv; ++k) dp[k] *= u;
+        return;
+    }
+    double vd = 1.0 + c->cd * creal(vt * conj(vt));   /* expm_batch_update_matrix, :228-252 */
+    zc vf = c->co * vt, vr = c->co * conj(vt);
+    for (int k = 0; k < c->nv; ++k) {
+        zc vi = sp[k], vj = dp[k];
+        sp[k] = vi * vd - vj * vr;
+        dp[k] = vj * vd + vi * vf;
+    }
+}
+
+void oracle_batchexpm_c64(void *bp, void *np, i64 idx, double theta, double *matrix, int ld, int nv)
+{
+    OpCtxC c = {(zc *)matrix, 0, 0, cos(theta) - 1.0, sin(theta), 0, 0, theta, 0, ld, nv};
+    visit_pairs_c((OBasis *)bp, (ONet *)np, &((ONet *)np)->g[idx], 1, batchexpm_pair_c, &c);
+}
+
+/* grads[orig] = grad at thetas[orig] for every group (op/batchgrad.hpp:529-540). */
+void oracle_batchgrad_c64(void *bp, void *np, const double *thetas, const double *l, const double *r, double *grads)
+{
+    ONet *N = (ONet *)np;
+    for (i64 g = 0; g < N->ngs; ++g) oracle_grad_c64(bp, np, g, thetas[g], l, r, grads + 2 * g);
+}
+
+static void tran_pair_c(i64 di, i64 si, zc vt, int diag, void *ctx, zc *acc)
+{
+    OpCtxC *c = (OpCtxC *)ctx;
+    if (diag) { *acc += conj(c->l[di] * vt) * c->r[di]; return; }   /* op/batchtran.hpp:7-81 */
+    *acc += conj(c->l[si] * vt) * c->r[di] - conj(c->l[di]) * vt * c->r[si];   /* tran_update */
+}
+
+/* trans[orig] = <l|T_g|r> for every group (op/batchtran.hpp:514-528). */
+void oracle_batchtran_c64(void *bp, void *np, const double *l, const double *r, double *trans)
+{
+    ONet *N = (ONet *)np;
+    OpCtxC c = {(zc *)l, (zc *)r, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (i64 g = 0; g < N->ngs; ++g) {
+        zc t = visit_pairs_c((OBasis *)bp, N, &N->g[g], 1, tran_pair_c, &c);
+        trans[2 * g] = creal(t);
+        trans[2 * g + 1] = cimag(t);
+    }
 }

@@ -151,3 +151,59 @@ def test_oracle_tvec_backtran_batch_ops_match_golden(oracle, name):
     np.testing.assert_allclose(oracle.batchtran(B, P, x, y), z["trans_pool"], rtol=0, atol=1e-13)
     np.testing.assert_allclose(oracle.batchtran(B, H, x, y), z["trans_ham"], rtol=0,
                                atol=1e-12 * max(1.0, np.abs(z["trans_ham"]).max()))
+
+
+def complex_weights(net, seed):
+    """Complex weights for a real network's groups: each real weight times a seeded
+    phase and modulus (the networks of the reference's complex interface)."""
+    rng = np.random.default_rng(seed)
+    wa = np.asarray(net.flat_wa) * rng.uniform(0.5, 1.5, len(net.flat_wa)) * np.exp(1j * rng.uniform(0, 6.3, len(net.flat_wa)))
+    wb = np.asarray(net.flat_wb) * rng.uniform(0.5, 1.5, len(net.flat_wb)) * np.exp(1j * rng.uniform(0, 6.3, len(net.flat_wb)))
+    return wa, wb
+
+
+@pytest.mark.parametrize("norb,na,nb,orbsym,tsym", [
+    (6, 3, 2, None, 0),
+    (7, 3, 3, [0, 1, 2, 3, 0, 1, 2], 2),
+])
+def test_oracle_c64_ops_match_reference_libs(oracle, reflibs, norb, na, nb, orbsym, tsym):
+    """The complex restatement against the reference CPU library's _c64 entry points:
+    sigma, diagonal, expm, grad, backgrad, tvec, backtran, batch_expm, batch_grad and
+    batch_tran, on a Hamiltonian with complex weights (diagonal group included) and on
+    pool generators with complex weights."""
+    from binsim_b200 import network as nw
+    osym = np.zeros(norb, np.int64) if orbsym is None else np.asarray(orbsym, np.int64)
+    ham = nw.hamiltonian_network(norb, seed=norb + 40)
+    pool = nw.ucc_pool(norb).network
+    ham.orbsym = osym; pool.orbsym = osym
+    rb, dim = reflibs.basis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
+    B = oracle.basis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
+    rng = np.random.default_rng(norb + 7)
+    x = rng.normal(size=dim) + 1j * rng.normal(size=dim)
+    y = rng.normal(size=dim) + 1j * rng.normal(size=dim)
+    for k, net in enumerate((ham, pool)):
+        wa, wb = complex_weights(net, seed=norb + k)
+        rn, N = reflibs.network_c64(net, wa, wb), oracle.network_c64(net, wa, wb)
+        if k == 0:
+            s = reflibs.hvec_c64(rb, rn, x, dim)
+            np.testing.assert_allclose(oracle.hvec_c64(B, N, x), s, rtol=0, atol=1e-12 * np.abs(s).max())
+            np.testing.assert_allclose(oracle.diag_c64(B, N), reflibs.diag_c64(rb, rn, dim), rtol=0, atol=1e-12)
+        for i in sorted(set([0] + list(rng.choice(net.ngs, 8, replace=False)))):
+            i, t = int(i), float(rng.normal())
+            np.testing.assert_allclose(oracle.expm_c64(B, N, i, t, x), reflibs.expm_c64(rb, rn, i, t, x), atol=1e-13)
+            assert abs(oracle.grad_c64(B, N, i, t, x, y) - reflibs.grad_c64(rb, rn, i, t, x, y)) < 1e-11
+            g0, l0, r0 = reflibs.backgrad_c64(rb, rn, i, t, x, y)
+            g1, l1, r1 = oracle.backgrad_c64(B, N, i, t, x, y)
+            assert abs(g0 - g1) < 1e-11
+            np.testing.assert_allclose(l1, l0, atol=1e-13); np.testing.assert_allclose(r1, r0, atol=1e-13)
+            np.testing.assert_allclose(oracle.tvec_c64(B, N, i, x), reflibs.tvec_c64(rb, rn, i, x, dim), atol=1e-13)
+            for a, b in zip(oracle.backtran_c64(B, N, i, t, x, y), reflibs.backtran_c64(rb, rn, i, t, x, y, dim)):
+                np.testing.assert_allclose(a, b, atol=1e-13)
+            M = rng.normal(size=(dim, 3)) + 1j * rng.normal(size=(dim, 3))
+            np.testing.assert_allclose(oracle.batchexpm_c64(B, N, i, t, M, 2), reflibs.batchexpm_c64(rb, rn, i, t, M, 2),
+                                       atol=1e-13)
+        th = rng.normal(size=net.ngs)
+        gr = reflibs.batchgrad_c64(rb, rn, th, x, y, net.ngs)
+        np.testing.assert_allclose(oracle.batchgrad_c64(B, N, th, x, y), gr, atol=1e-10 * max(1.0, np.abs(gr).max()))
+        tr = reflibs.batchtran_c64(rb, rn, x, y, net.ngs)
+        np.testing.assert_allclose(oracle.batchtran_c64(B, N, x, y), tr, atol=1e-10 * max(1.0, np.abs(tr).max()))

@@ -1164,6 +1164,12 @@ def reference_arm(args):
                     cpu_baseline={"value": cpu["seconds"], "unit": "s", "cores": cpu["cores"], "kind": "reference",
                                   "sample": cpu["sample"]},
                     e2e={"value": cpu["seconds"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    elif args.workload == "block":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's Davidson driver (jl/davidson.jl) follows "
+                                                              "one root; it has no block solver for the lowest 2 roots, "
+                                                              "and one reference sigma at 18 orbitals takes ~2,900 s on "
+                                                              "the host cores"}))
+        return
     elif args.workload == "adapt":
         print(json.dumps({"impl": "reference", "unavailable": "the reference's basis library is UInt32-only and its "
                                                               "dense string map overflows at 36 orbitals "

@@ -274,9 +274,14 @@ template <typename Ti>
 int c64_scratch(const DevBasis<Ti> *B, double **part, unsigned long long **ticket, cudaStream_t s)
 {
     const size_t nslots = (size_t)pair_grid(B);
-    // [2 * nslots partials][ticket]; the ticket is cleared before every launch
-    int st = B->ws.partials(2 * nslots + 2, part);
+    // The basis workspace starts with the real operators' [nslots partials][ticket]
+    // [result slot], whose ticket word must stay zero between their launches; the
+    // complex partials [2 * nslots][ticket] follow it.  The ticket is cleared
+    // before every launch.
+    double *base = nullptr;
+    int st = B->ws.partials(3 * nslots + 3, &base);
     if (st != BSIM_OK) return st;
+    *part = base + nslots + 2;
     *ticket = reinterpret_cast<unsigned long long *>(*part + 2 * nslots);
     BSIM_CUDA(cudaMemsetAsync(*ticket, 0, sizeof(unsigned long long), s));
     return BSIM_OK;

@@ -117,3 +117,25 @@ def test_c64_sigma_and_pool_ops_match_oracle(cuda, oracle):
     with pytest.raises(cuotf.CuOTFError):
         cuotf.CuOTFFunctions(B, fh.net).hvec(cuda.zeros(B.dim, dtype=cuda.float64, device="cuda"),
                                               cuda.zeros(B.dim, dtype=cuda.float64, device="cuda"))
+
+
+def test_real_and_complex_reductions_share_a_basis(cuda, oracle):
+    """Real grad after complex grads on the same basis handle (they share its reduction
+    scratch): both keep their own partial slots and ticket words."""
+    from binsim_b200 import cuotf, network as nw
+    from test_oracle_pin import complex_weights
+    norb, na, nb = 7, 3, 3
+    pool = nw.ucc_pool(norb).network
+    B = cuotf.CuBasis(norb, na, nb)
+    Bo, Po = oracle.basis(norb, na, nb), oracle.network(pool)
+    fr = cuotf.CuOTFFunctions(B, None, cuotf.CuNetwork(pool))
+    fc = cuotf.CuOTFC64(B, cuotf.CuNetworkC64(pool, *complex_weights(pool, 9)))
+    rng = np.random.default_rng(2)
+    x, y = rng.normal(size=B.dim), rng.normal(size=B.dim)
+    xc, yc = cdev(cuda, x + 1j * y), cdev(cuda, y - 0.5j * x)
+    xd, yd = cuda.as_tensor(x, device="cuda"), cuda.as_tensor(y, device="cuda")
+    for i in (3, 11, 40):
+        fc.grad(i, 0.3, xc, yc)
+        g = fr.grad(i + 1, 0.3, xd, yd)
+        assert abs(g - oracle.grad(Bo, Po, i, 0.3, x, y)) < 1e-11
+        fc.backgrad(i, 0.2, xc.clone(), yc.clone())

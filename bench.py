@@ -238,7 +238,7 @@ def profile_traffic(name):
         return None
 
 
-def sigma_roofline(net, pairs, cfg, dim, stages, hbm, fp64_peak, world, ms):
+def sigma_roofline(net, pairs, cfg, dim, stages, hbm, fp64_peak, world, ms, dmma_peak=None):
     """Roofline of the dominant kernel of the structured sigma, from the per-stage
     CUDA-event times measured in this run.  Returns (roofline dict, launches per sigma)."""
     if not stages:
@@ -262,6 +262,9 @@ def sigma_roofline(net, pairs, cfg, dim, stages, hbm, fp64_peak, world, ms):
         M = cfg["na"] * (cfg["norb"] - cfg["na"])
         bytes_total = dim * 8.0 + nA * M * nB * 8.0
         flops_total = float(np.sum(pairs[types == 3] * (2 * net.ranks[types == 3] + 1)))
+        # the GEMMs as executed: 64-row passes x every F excitation x every column
+        nF = math.comb(cfg["norb"], 2)
+        dense_total = 2.0 * nA * (64 * math.ceil(M / 64)) * nF * nB
     elif top == "pure_rows":
         # per launch (one spin side) the compulsory HBM bytes are one read of the
         # input (c~ or its transpose) and one write of the result; the source-row
@@ -272,6 +275,8 @@ def sigma_roofline(net, pairs, cfg, dim, stages, hbm, fp64_peak, world, ms):
     else:
         bytes_total = dim * 16.0
         flops_total = 0.0
+    if top != "mixed_gemm":
+        dense_total = None
     achieved = bytes_total / max(1, n_launch) / per_launch_s / 1e9
     prof = profile_traffic(f"sigma_{top}_15o7a8b")
     traffic = None
@@ -284,6 +289,9 @@ def sigma_roofline(net, pairs, cfg, dim, stages, hbm, fp64_peak, world, ms):
             "launches_per_sigma": n_launch, "ms_per_launch": per_launch_s * 1e3,
             "fp64_tflops": flops_total / max(1, n_launch) / per_launch_s / 1e12,
             "fp64_frac_of_measured_fma_peak": flops_total / max(1, n_launch) / per_launch_s / 1e12 / fp64_peak,
+            "fp64_dense_gemm_tflops": (dense_total / max(1, n_launch) / per_launch_s / 1e12) if dense_total else None,
+            "dense_frac_of_measured_dmma_peak": (dense_total / max(1, n_launch) / per_launch_s / 1e12 / dmma_peak)
+            if dense_total and dmma_peak else None,
             "note": "dominant kernel of the structured sigma, timed live per launch with CUDA events; achieved = "
                     "its compulsory HBM bytes per launch / launch time, of the measured HBM copy peak; the kernel "
                     "is bound by FP64 issue and shared-memory gathers, see fp64_frac_of_measured_fma_peak; traffic "
@@ -369,6 +377,7 @@ def gpu_sigma(args, rank, world, local_rank):
         stages32 = {k: (float(np.median([r[k][0] for r in runs])), runs[0][k][1]) for k in runs[0]}
     fp64_peak = cuotf.fma_peak(True)
     fp32_peak = cuotf.fma_peak(False)
+    dmma_peak = cuotf.fma_peak(dmma=True)
 
     # e2e through the public API with host buffers: H2D c, sigma, D2H sigma
     xpin = torch.from_numpy(xh).pin_memory()
@@ -402,7 +411,7 @@ def gpu_sigma(args, rank, world, local_rank):
         pk = peaks()
         hbm = pk.get("hbm_gbs")
         tflops = flops / world / (ms * 1e-3) / 1e12
-        roof, launches = sigma_roofline(net, pairs, cfg, dim, stages, hbm, fp64_peak, world, ms)
+        roof, launches = sigma_roofline(net, pairs, cfg, dim, stages, hbm, fp64_peak, world, ms, dmma_peak)
         if launches is None:
             launches = count_launches(step)
         result = {
@@ -438,6 +447,7 @@ def gpu_sigma(args, rank, world, local_rank):
             "stages_ms": {k: round(v[0], 3) for k, v in stages.items()} if stages else None,
             "stages_ms_fp32_bulk": {k: round(v[0], 3) for k, v in stages32.items()} if stages32 else None,
             "fp32_fma_peak_tflops": fp32_peak,
+            "fp64_dmma_peak_tflops": dmma_peak,
             "pair_updates_per_s": float(pairs.sum()) / (ms * 1e-3),
             "sigma_path": {"path": path[0], "reason": path[1], "residual_groups": path[2]},
             "gpu_launches": launches * args.steps if launches else None,

@@ -478,7 +478,7 @@ int bsim_hvec_stage_times(void *basis, void *net, const double *src, double *dst
 int bsim_fma_peak(int fp64, double *tflops_out, bsim_stream_t stream)
 {
     NEED(tflops_out);
-    return bsim::fma_peak(fp64 != 0, tflops_out, stream);
+    return bsim::fma_peak(fp64 == 2 ? 2 : (fp64 != 0 ? 1 : 0), tflops_out, stream);
 }
 
 int64_t bsim_hvec_num_tiles(void *basis)

@@ -1,6 +1,6 @@
-// Measurement helpers: the CUDA-core FMA peak that the sigma kernels' compute
-// roofline is quoted against (the driver-measured peaks cover HBM and bf16
-// tensor throughput only).
+// Measurement helpers: the CUDA-core FMA peaks and the FP64 tensor-core (DMMA)
+// peak that the sigma kernels' compute rooflines are quoted against (the
+// driver-measured peaks cover HBM and bf16 tensor throughput only).
 #include "ops.h"
 
 #include <algorithm>
@@ -25,9 +25,30 @@ __global__ void __launch_bounds__(256) fma_chain_kernel(T *__restrict__ out, int
     if (s == (T)-12345.0) out[blockIdx.x] = s;   // keeps the chains live; never true for these inputs
 }
 
+// FP64 tensor-core (DMMA) chains: 8 independent m8n8k4 accumulators per warp
+__global__ void __launch_bounds__(256) dmma_chain_kernel(double *__restrict__ out, int iters, double a0, double b0)
+{
+    double c[8][2];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) c[k][0] = c[k][1] = 0.0;
+    const double a = a0 + 1e-9 * (threadIdx.x & 31), b = b0;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                         : "+d"(c[k][0]), "+d"(c[k][1])
+                         : "d"(a), "d"(b));
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += c[k][0] + c[k][1];
+    if (s == -12345.0) out[blockIdx.x] = s;   // keeps the chains live; never true for these inputs
+}
+
 }  // namespace
 
-int fma_peak(bool fp64, double *tflops, cudaStream_t s)
+// mode 0: FP32 FMA chains, 1: FP64 FMA chains, 2: FP64 tensor-core (DMMA m8n8k4) chains
+int fma_peak(int mode, double *tflops, cudaStream_t s)
 {
     int dev = 0, sms = 0;
     BSIM_CUDA(cudaGetDevice(&dev));
@@ -41,7 +62,8 @@ int fma_peak(bool fp64, double *tflops, cudaStream_t s)
     float best = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
         BSIM_CUDA(cudaEventRecord(e0, s));
-        if (fp64) fma_chain_kernel<double><<<blocks, threads, 0, s>>>((double *)out, iters, 0.9999999, 1e-7);
+        if (mode == 2) dmma_chain_kernel<<<blocks, threads, 0, s>>>((double *)out, iters / 4, 1e-3, 1e-3);
+        else if (mode == 1) fma_chain_kernel<double><<<blocks, threads, 0, s>>>((double *)out, iters, 0.9999999, 1e-7);
         else fma_chain_kernel<float><<<blocks, threads, 0, s>>>((float *)out, iters, 0.9999999f, 1e-7f);
         BSIM_CUDA(cudaEventRecord(e1, s));
         BSIM_CUDA(cudaEventSynchronize(e1));
@@ -52,7 +74,9 @@ int fma_peak(bool fp64, double *tflops, cudaStream_t s)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     BSIM_CUDA(cudaFreeAsync(out, s));
-    const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
+    // per instruction: one FMA per thread (2 flops), or one 8x8x4 DMMA per warp (512 flops)
+    const double flops = mode == 2 ? 512.0 * 8.0 * (iters / 4) * (double)blocks * (threads / 32)
+                                   : 2.0 * 8.0 * iters * (double)blocks * threads;
     *tflops = flops / (best * 1e-3) / 1e12;
     return BSIM_OK;
 }

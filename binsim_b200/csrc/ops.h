@@ -40,7 +40,7 @@ int sigma_fast_stages(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *
                       cudaStream_t s, double *ms, int *launches, int nstages);
 
 // Arithmetic peak of the CUDA cores (FMA chains), TFLOP/s, FP64 or FP32.
-int fma_peak(bool fp64, double *tflops, cudaStream_t s);
+int fma_peak(int mode, double *tflops, cudaStream_t s);   // 0 FP32 FMA, 1 FP64 FMA, 2 FP64 DMMA
 
 template <typename Ti>
 int fast_sigma_info(const DevBasis<Ti> *B, const DevNet<Ti> *N, std::string *why, int *nresid);

@@ -151,10 +151,11 @@ def _host(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
-def fma_peak(fp64: bool = True, stream=None) -> float:
-    """CUDA-core FMA throughput of the current GPU, TFLOP/s."""
+def fma_peak(fp64: bool = True, stream=None, dmma: bool = False) -> float:
+    """CUDA-core FMA throughput of the current GPU (FP64 or FP32), or with dmma the
+    FP64 tensor-core MMA throughput, TFLOP/s."""
     t = C.c_double()
-    _check(lib().bsim_fma_peak(1 if fp64 else 0, C.byref(t), _stream(stream)), "fma_peak")
+    _check(lib().bsim_fma_peak(2 if dmma else (1 if fp64 else 0), C.byref(t), _stream(stream)), "fma_peak")
     return t.value
 
 

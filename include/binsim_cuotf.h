@@ -177,8 +177,9 @@ int bsim_hvec_cols(void *basis, void *net, const double *src, double *dst, int64
  * BSIM_ERR_UNSUPPORTED when the structured path is off. */
 int bsim_hvec_stage_times(void *basis, void *net, const double *src, double *dst, int mixed, double *ms_out,
                           int *launches_out, int nstages, bsim_stream_t stream);
-/* Measurement: CUDA-core FMA throughput of this GPU in TFLOP/s (fp64 != 0:
- * FP64, else FP32), from chains of dependent FMAs on every SM. */
+/* Measurement: throughput of this GPU in TFLOP/s from chains of dependent
+ * operations on every SM: fp64 = 0 FP32 FMA, 1 FP64 FMA, 2 FP64 tensor-core
+ * MMA (m8n8k4, the DMMA path the FP64 sigma GEMMs use). */
 int bsim_fma_peak(int fp64, double *tflops_out, bsim_stream_t stream);
 /* Number of 32 x 32 destination tiles of sigma (block-major, then row-major). */
 int64_t bsim_hvec_num_tiles(void *basis);

@@ -1,0 +1,250 @@
+// Native OTF network construction (host): the grouping and SVD compression of
+// jl/network.jl:158-246 (compress_by_svd) for a list of aabb Pauli terms
+// (ax, az, bx, bz, c), in C++ instead of the host scripting language.
+//
+// Terms with equal (ax, bx) form a group (groups in order of first appearance);
+// the group's coefficient matrix M[za, zb] (distinct za and zb sorted
+// ascending) is factorised by a one-sided Jacobi SVD; singular values above
+// tol are kept (rank), wa = U sqrt(S), wb = V sqrt(S), entries below 1e-12 are
+// zeroed, and the weights are stored column-major [num_z x rank] as the
+// reference's build_network_otf expects (otf.hpp:84-85).  Groups are
+// independent and compressed on all host threads.  No device code: the result
+// feeds bsim_network_create_u32 / _u64.
+#include "../../include/binsim_cuotf.h"
+#include "common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace bsim {
+
+namespace {
+
+struct BuiltGroup {
+    u64 ax, bx;
+    std::vector<u64> za, zb;
+    int rank = 0;
+    std::vector<double> wa, wb;   // column-major [nza x rank], [nzb x rank]
+};
+
+struct NetBuild {
+    unsigned magic = 0xB5B1B11Du;
+    std::vector<BuiltGroup> g;
+};
+
+// One-sided Jacobi SVD of A (m x n, column-major, m >= n): on return A's
+// columns are U * S, V (n x n, column-major) the right singular vectors, in
+// the order of the columns (unsorted).
+void jacobi_svd(int m, int n, std::vector<double> &A, std::vector<double> &V)
+{
+    V.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        double off = 0.0;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                double *ap = &A[(size_t)p * m], *aq = &A[(size_t)q * m];
+                double alpha = 0.0, beta = 0.0, gamma = 0.0;
+                for (int i = 0; i < m; ++i) {
+                    alpha += ap[i] * ap[i];
+                    beta += aq[i] * aq[i];
+                    gamma += ap[i] * aq[i];
+                }
+                if (std::fabs(gamma) <= 1e-300) continue;
+                const double scale = std::sqrt(alpha * beta);
+                if (scale <= 0.0) continue;
+                off = std::max(off, std::fabs(gamma) / scale);
+                if (std::fabs(gamma) <= 1e-15 * scale) continue;
+                const double zeta = (beta - alpha) / (2.0 * gamma);
+                const double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+                const double c = 1.0 / std::sqrt(1.0 + t * t), s = c * t;
+                for (int i = 0; i < m; ++i) {
+                    const double x = ap[i], y = aq[i];
+                    ap[i] = c * x - s * y;
+                    aq[i] = s * x + c * y;
+                }
+                double *vp = &V[(size_t)p * n], *vq = &V[(size_t)q * n];
+                for (int i = 0; i < n; ++i) {
+                    const double x = vp[i], y = vq[i];
+                    vp[i] = c * x - s * y;
+                    vq[i] = s * x + c * y;
+                }
+            }
+        if (off <= 1e-15) break;
+    }
+}
+
+// M (m x n, column-major) -> rank, wa (m x rank), wb (n x rank), column-major
+void compress(int m, int n, const std::vector<double> &M, double tol, BuiltGroup &G)
+{
+    const bool tr = m < n;   // factor the transpose when it is the taller one
+    const int mm = tr ? n : m, nn = tr ? m : n;
+    std::vector<double> A((size_t)mm * nn), V;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) {
+            const double v = M[(size_t)j * m + i];
+            if (tr) A[(size_t)i * mm + j] = v;   // A = M^T
+            else A[(size_t)j * mm + i] = v;
+        }
+    jacobi_svd(mm, nn, A, V);
+    std::vector<double> sv(nn);
+    for (int k = 0; k < nn; ++k) {
+        double s = 0.0;
+        for (int i = 0; i < mm; ++i) s += A[(size_t)k * mm + i] * A[(size_t)k * mm + i];
+        sv[k] = std::sqrt(s);
+    }
+    std::vector<int> order(nn);
+    for (int k = 0; k < nn; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sv[a] > sv[b]; });
+    std::vector<int> keep;
+    for (int k : order)
+        if (sv[k] > tol) keep.push_back(k);
+    const int r = (int)keep.size();
+    // A's column k is sv_k u_k (left vectors of the factored matrix), V's column k is v_k
+    std::vector<double> L((size_t)mm * r), R((size_t)nn * r);
+    for (int t = 0; t < r; ++t) {
+        const int k = keep[t];
+        const double sq = std::sqrt(sv[k]);
+        for (int i = 0; i < mm; ++i) L[(size_t)t * mm + i] = A[(size_t)k * mm + i] / sv[k] * sq;
+        for (int i = 0; i < nn; ++i) R[(size_t)t * nn + i] = V[(size_t)k * nn + i] * sq;
+    }
+    // M = L R^T when not transposed; M^T = L R^T (so M = R L^T) when transposed
+    G.rank = r;
+    G.wa = tr ? R : L;
+    G.wb = tr ? L : R;
+    for (double &x : G.wa)
+        if (std::fabs(x) < 1e-12) x = 0.0;
+    for (double &x : G.wb)
+        if (std::fabs(x) < 1e-12) x = 0.0;
+}
+
+NetBuild *nb_of(void *h)
+{
+    auto *p = static_cast<NetBuild *>(h);
+    return (p && p->magic == 0xB5B1B11Du) ? p : nullptr;
+}
+
+}  // namespace
+}  // namespace bsim
+
+extern "C" {
+
+int bsim_netbuild_compress(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx,
+                           const uint64_t *bz, const double *coef, double tol, void **out)
+{
+    using bsim::u64;
+    if (!out) { bsim::set_error("null out"); return BSIM_ERR_NULL; }
+    *out = nullptr;
+    if (nterms < 0) { bsim::set_error("nterms = %lld", (long long)nterms); return BSIM_ERR_ARG; }
+    if (nterms > 0 && (!ax || !az || !bx || !bz || !coef)) { bsim::set_error("null term array"); return BSIM_ERR_NULL; }
+    auto *B = new bsim::NetBuild();
+    // groups in order of first appearance of (ax, bx)
+    struct KeyHash {
+        size_t operator()(const std::pair<u64, u64> &k) const { return std::hash<u64>()(k.first * 0x9E3779B97F4A7C15ull ^ k.second); }
+    };
+    std::unordered_map<std::pair<u64, u64>, int, KeyHash> gid;
+    std::vector<std::vector<int64_t>> members;
+    for (int64_t t = 0; t < nterms; ++t) {
+        const auto key = std::make_pair((u64)ax[t], (u64)bx[t]);
+        auto it = gid.find(key);
+        int g;
+        if (it == gid.end()) {
+            g = (int)members.size();
+            gid.emplace(key, g);
+            members.emplace_back();
+            B->g.emplace_back();
+            B->g.back().ax = key.first;
+            B->g.back().bx = key.second;
+        } else g = it->second;
+        members[g].push_back(t);
+    }
+    const int ng = (int)members.size();
+    const int nth = std::max(1, std::min(32, (int)std::thread::hardware_concurrency()));
+    auto work = [&](int w) {
+        for (int g = w; g < ng; g += nth) {
+            bsim::BuiltGroup &G = B->g[g];
+            for (int64_t t : members[g]) { G.za.push_back((u64)az[t]); G.zb.push_back((u64)bz[t]); }
+            std::sort(G.za.begin(), G.za.end());
+            G.za.erase(std::unique(G.za.begin(), G.za.end()), G.za.end());
+            std::sort(G.zb.begin(), G.zb.end());
+            G.zb.erase(std::unique(G.zb.begin(), G.zb.end()), G.zb.end());
+            const int m = (int)G.za.size(), n = (int)G.zb.size();
+            std::vector<double> M((size_t)m * n, 0.0);
+            for (int64_t t : members[g]) {
+                const int i = (int)(std::lower_bound(G.za.begin(), G.za.end(), (u64)az[t]) - G.za.begin());
+                const int j = (int)(std::lower_bound(G.zb.begin(), G.zb.end(), (u64)bz[t]) - G.zb.begin());
+                M[(size_t)j * m + i] += coef[t];
+            }
+            bsim::compress(m, n, M, tol, G);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int w = 1; w < nth; ++w) th.emplace_back(work, w);
+    work(0);
+    for (auto &x : th) x.join();
+    *out = B;
+    return BSIM_OK;
+}
+
+int bsim_netbuild_sizes(void *h, int64_t *ngs, int64_t *nza_total, int64_t *nzb_total, int64_t *nwa_total,
+                        int64_t *nwb_total)
+{
+    bsim::NetBuild *B = bsim::nb_of(h);
+    if (!B) { bsim::set_error("invalid network builder handle"); return BSIM_ERR_ARG; }
+    int64_t a = 0, b = 0, wa = 0, wb = 0;
+    for (auto &G : B->g) {
+        a += (int64_t)G.za.size();
+        b += (int64_t)G.zb.size();
+        wa += (int64_t)G.wa.size();
+        wb += (int64_t)G.wb.size();
+    }
+    if (ngs) *ngs = (int64_t)B->g.size();
+    if (nza_total) *nza_total = a;
+    if (nzb_total) *nzb_total = b;
+    if (nwa_total) *nwa_total = wa;
+    if (nwb_total) *nwb_total = wb;
+    return BSIM_OK;
+}
+
+int bsim_netbuild_export(void *h, uint64_t *axs, uint64_t *bxs, int64_t *ranks, int64_t *num_zas, int64_t *num_zbs,
+                         uint64_t *flat_zas, uint64_t *flat_zbs, double *flat_wa, double *flat_wb)
+{
+    bsim::NetBuild *B = bsim::nb_of(h);
+    if (!B) { bsim::set_error("invalid network builder handle"); return BSIM_ERR_ARG; }
+    if (!B->g.empty() && (!axs || !bxs || !ranks || !num_zas || !num_zbs)) {
+        bsim::set_error("null output array");
+        return BSIM_ERR_NULL;
+    }
+    int64_t oa = 0, ob = 0, owa = 0, owb = 0;
+    for (size_t i = 0; i < B->g.size(); ++i) {
+        const auto &G = B->g[i];
+        axs[i] = G.ax;
+        bxs[i] = G.bx;
+        ranks[i] = G.rank;
+        num_zas[i] = (int64_t)G.za.size();
+        num_zbs[i] = (int64_t)G.zb.size();
+        if (flat_zas) std::copy(G.za.begin(), G.za.end(), flat_zas + oa);
+        if (flat_zbs) std::copy(G.zb.begin(), G.zb.end(), flat_zbs + ob);
+        if (flat_wa) std::copy(G.wa.begin(), G.wa.end(), flat_wa + owa);
+        if (flat_wb) std::copy(G.wb.begin(), G.wb.end(), flat_wb + owb);
+        oa += (int64_t)G.za.size();
+        ob += (int64_t)G.zb.size();
+        owa += (int64_t)G.wa.size();
+        owb += (int64_t)G.wb.size();
+    }
+    return BSIM_OK;
+}
+
+int bsim_netbuild_destroy(void *h)
+{
+    bsim::NetBuild *B = bsim::nb_of(h);
+    if (!B) { bsim::set_error("invalid network builder handle"); return BSIM_ERR_ARG; }
+    B->magic = 0;
+    delete B;
+    return BSIM_OK;
+}
+
+}  // extern "C"

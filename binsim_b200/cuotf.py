@@ -84,6 +84,10 @@ def lib() -> C.CDLL:
         "bsim_grad_noalloc": (ci, [vp, vp, i64, dbl, vp, vp, vp, vp]),
         "bsim_batchgrad": (ci, [vp, vp, vp, vp, vp, vp, vp]),
         "bsim_hvec_host": (ci, [vp, vp, i64, vp, vp, ci, vp]),
+        "bsim_netbuild_compress": (ci, [i64, vp, vp, vp, vp, vp, dbl, vp]),
+        "bsim_netbuild_sizes": (ci, [vp, vp, vp, vp, vp, vp]),
+        "bsim_netbuild_export": (ci, [vp] * 10),
+        "bsim_netbuild_destroy": (ci, [vp]),
         "bsim_network_create_c64": (ci, [vp, i64, i64] + [vp] * 10),
         "bsim_network_create_c64_u64": (ci, [vp, i64, i64] + [vp] * 10),
         "bsim_hvec_c64": (ci, [vp, vp, vp, vp, vp]),
@@ -149,6 +153,32 @@ def _stream(stream=None):
 
 def _host(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
+
+
+def compress_groups_native(ax, az, bx, bz, c, norb: int, tol: float = 1e-12, orbsym=None) -> nw.OTFNetwork:
+    """The grouping and SVD compression of network.compress_groups (jl/network.jl:158-246)
+    in the library's native builder (host threads); groups in order of first appearance."""
+    L = lib()
+    arrs = [_host(ax, np.uint64), _host(az, np.uint64), _host(bx, np.uint64), _host(bz, np.uint64),
+            _host(c, np.float64)]
+    h = vp()
+    _check(L.bsim_netbuild_compress(len(arrs[4]), *[a.ctypes.data for a in arrs], tol, C.byref(h)),
+           "bsim_netbuild_compress")
+    try:
+        n = [C.c_int64() for _ in range(5)]
+        _check(L.bsim_netbuild_sizes(h, *[C.byref(x) for x in n]), "bsim_netbuild_sizes")
+        ngs, tza, tzb, twa, twb = [x.value for x in n]
+        out = dict(axs=np.zeros(ngs, np.uint64), bxs=np.zeros(ngs, np.uint64), ranks=np.zeros(ngs, np.int64),
+                   num_zas=np.zeros(ngs, np.int64), num_zbs=np.zeros(ngs, np.int64),
+                   flat_zas=np.zeros(tza, np.uint64), flat_zbs=np.zeros(tzb, np.uint64),
+                   flat_wa=np.zeros(twa, np.float64), flat_wb=np.zeros(twb, np.float64))
+        _check(L.bsim_netbuild_export(h, *[out[k].ctypes.data for k in
+                                           ("axs", "bxs", "ranks", "num_zas", "num_zbs", "flat_zas", "flat_zbs",
+                                            "flat_wa", "flat_wb")]), "bsim_netbuild_export")
+    finally:
+        L.bsim_netbuild_destroy(h)
+    osym = np.zeros(norb, np.int64) if orbsym is None else np.asarray(orbsym, np.int64)
+    return nw.OTFNetwork(norb=norb, orbsym=osym, **out)
 
 
 def fma_peak(fp64: bool = True, stream=None, dmma: bool = False) -> float:

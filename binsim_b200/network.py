@@ -349,11 +349,15 @@ def _pack(groups, norb, orbsym=None) -> OTFNetwork:
     )
 
 
-def hamiltonian_network(norb: int, seed: int = 0, tol: float = 1e-12, e_nuc=None) -> OTFNetwork:
-    """OTF network of the seeded synthetic Hamiltonian on ``norb`` orbitals."""
+def hamiltonian_network(norb: int, seed: int = 0, tol: float = 1e-12, e_nuc=None, native: bool = False) -> OTFNetwork:
+    """OTF network of the seeded synthetic Hamiltonian on ``norb`` orbitals.  native:
+    group and compress with the library's builder (bsim_netbuild_*, host threads)."""
     h, g, e0 = synthetic_integrals(norb, seed)
     x, z, c = jw_hamiltonian_terms(h, g, e0 if e_nuc is None else e_nuc, tol)
     ax, az, bx, bz = split_aabb(x, z, norb)
+    if native:
+        from binsim_b200 import cuotf
+        return cuotf.compress_groups_native(ax, az, bx, bz, c, norb, tol)
     return compress_groups(ax, az, bx, bz, c, norb, tol)
 
 

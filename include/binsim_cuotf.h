@@ -218,6 +218,25 @@ int bsim_backgrad(void *basis, void *net, int64_t idx, double theta, double *l, 
 int bsim_batchgrad(void *basis, void *net, const double *thetas, const double *l, const double *r,
                    double *grads, bsim_stream_t stream);
 /* ------------------------------------------------------------------------
+ * Native network construction (host code, no device work): the grouping and
+ * SVD compression of jl/network.jl:158-246 for nterms aabb Pauli terms
+ * (per-spin X / Z masks and real coefficients).  Terms with equal (ax, bx)
+ * form a group (groups in order of first appearance); each group's matrix
+ * M[za, zb] (distinct za, zb ascending) is factorised by a one-sided Jacobi
+ * SVD, singular values above tol kept, wa = U sqrt(S), wb = V sqrt(S) with
+ * entries below 1e-12 zeroed.  bsim_netbuild_sizes gives the array lengths of
+ * bsim_netbuild_export, whose outputs are the bsim_network_create_* arguments
+ * (flat_* may be NULL to skip them).
+ * ------------------------------------------------------------------------ */
+int bsim_netbuild_compress(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx,
+                           const uint64_t *bz, const double *coef, double tol, void **out);
+int bsim_netbuild_sizes(void *h, int64_t *ngs, int64_t *nza_total, int64_t *nzb_total, int64_t *nwa_total,
+                        int64_t *nwb_total);
+int bsim_netbuild_export(void *h, uint64_t *axs, uint64_t *bxs, int64_t *ranks, int64_t *num_zas, int64_t *num_zbs,
+                         uint64_t *flat_zas, uint64_t *flat_zbs, double *flat_wa, double *flat_wb);
+int bsim_netbuild_destroy(void *h);
+
+/* ------------------------------------------------------------------------
  * Complex (c64) networks and operators: the reference CPU library's _c64
  * exports (src/extern/otf_native.cpp:4,6; Tv = complex<double>) on device
  * vectors of interleaved (re, im) doubles, dim complex entries each.  The

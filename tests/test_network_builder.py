@@ -96,3 +96,49 @@ def test_draw_generators_is_seeded():
         np.testing.assert_array_equal(x, y)
     op_idx, param_idx, th = a
     assert len(th) == 20 and param_idx.max() == 19 and np.all(np.diff(param_idx) >= 0)
+
+
+@pytest.mark.parametrize("norb", [6, 8])
+def test_native_builder_matches_numpy_grouping_and_sigma(oracle, norb):
+    """The library's native grouping + Jacobi-SVD compression (bsim_netbuild_*) gives the
+    numpy builder's groups, Z lists and ranks, the same group matrices M = wa wb^T, and
+    the same oracle sigma."""
+    from binsim_b200 import cuotf, network as nw
+    h, g, e = nw.synthetic_integrals(norb, 3)
+    x, z, c = nw.jw_hamiltonian_terms(h, g, e)
+    ax, az, bx, bz = nw.split_aabb(x, z, norb)
+    a = nw.compress_groups(ax, az, bx, bz, c, norb)
+    b = cuotf.compress_groups_native(ax, az, bx, bz, c, norb)
+    for k in ("axs", "bxs", "ranks", "num_zas", "num_zbs", "flat_zas", "flat_zbs"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    oa = ob = 0
+    for gi in range(a.ngs):
+        na, nb, r = int(a.num_zas[gi]), int(a.num_zbs[gi]), int(a.ranks[gi])
+        Ma = a.flat_wa[oa:oa + na * r].reshape(r, na).T @ a.flat_wb[ob:ob + nb * r].reshape(r, nb)
+        Mb = b.flat_wa[oa:oa + na * r].reshape(r, na).T @ b.flat_wb[ob:ob + nb * r].reshape(r, nb)
+        assert np.abs(Ma - Mb).max() < 1e-12, gi
+        oa += na * r; ob += nb * r
+    B = oracle.basis(norb, norb // 2, norb // 2)
+    v = np.random.default_rng(0).normal(size=B.dim)
+    sa, sb = oracle.hvec(B, oracle.network(a), v), oracle.hvec(B, oracle.network(b), v)
+    assert np.abs(sa - sb).max() <= 1e-13 * np.abs(sa).max()
+
+
+def test_native_builder_rank_and_errors():
+    """Exact rank of a planted rank-1 group (outer product of two vectors) and the
+    builder's argument checks."""
+    import ctypes as C
+    from binsim_b200 import cuotf
+    za, zb = np.array([1, 2, 4], np.uint64), np.array([1, 8], np.uint64)
+    u, w = np.array([0.3, -1.2, 0.5]), np.array([2.0, -0.7])
+    AZ, BZ = np.meshgrid(za, zb, indexing="ij")
+    coef = np.outer(u, w).ravel()
+    n = coef.size
+    net = cuotf.compress_groups_native(np.full(n, 3, np.uint64), AZ.ravel(), np.full(n, 5, np.uint64), BZ.ravel(),
+                                       coef, 4)
+    assert net.ngs == 1 and int(net.ranks[0]) == 1
+    M = net.flat_wa.reshape(1, 3).T @ net.flat_wb.reshape(1, 2)
+    np.testing.assert_allclose(M, np.outer(u, w), atol=1e-14)
+    L = cuotf.lib()
+    assert L.bsim_netbuild_destroy(None) == -2
+    assert L.bsim_netbuild_compress(1, None, None, None, None, None, 1e-12, C.byref(C.c_void_p())) == -1

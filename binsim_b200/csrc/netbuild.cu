@@ -130,37 +130,56 @@ NetBuild *nb_of(void *h)
 }  // namespace
 }  // namespace bsim
 
-extern "C" {
-
-int bsim_netbuild_compress(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx,
-                           const uint64_t *bz, const double *coef, double tol, void **out)
+static int netbuild(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx, const uint64_t *bz,
+                    const double *coef, double tol, int64_t nruns, const int64_t *run_sizes, void **out)
 {
     using bsim::u64;
     if (!out) { bsim::set_error("null out"); return BSIM_ERR_NULL; }
     *out = nullptr;
     if (nterms < 0) { bsim::set_error("nterms = %lld", (long long)nterms); return BSIM_ERR_ARG; }
     if (nterms > 0 && (!ax || !az || !bx || !bz || !coef)) { bsim::set_error("null term array"); return BSIM_ERR_NULL; }
-    auto *B = new bsim::NetBuild();
-    // groups in order of first appearance of (ax, bx)
-    struct KeyHash {
-        size_t operator()(const std::pair<u64, u64> &k) const { return std::hash<u64>()(k.first * 0x9E3779B97F4A7C15ull ^ k.second); }
-    };
-    std::unordered_map<std::pair<u64, u64>, int, KeyHash> gid;
     std::vector<std::vector<int64_t>> members;
-    for (int64_t t = 0; t < nterms; ++t) {
-        const auto key = std::make_pair((u64)ax[t], (u64)bx[t]);
-        auto it = gid.find(key);
-        int g;
-        if (it == gid.end()) {
-            g = (int)members.size();
-            gid.emplace(key, g);
+    std::vector<std::pair<u64, u64>> keys;
+    if (run_sizes) {
+        // one group per run of consecutive terms (one X group per generator, network.jl:248-301)
+        int64_t t0 = 0;
+        for (int64_t r = 0; r < nruns; ++r) {
+            const int64_t n = run_sizes[r];
+            if (n <= 0 || t0 + n > nterms) { bsim::set_error("run %lld of size %lld exceeds the terms", (long long)r, (long long)n); return BSIM_ERR_ARG; }
             members.emplace_back();
-            B->g.emplace_back();
-            B->g.back().ax = key.first;
-            B->g.back().bx = key.second;
-        } else g = it->second;
-        members[g].push_back(t);
+            keys.emplace_back((u64)ax[t0], (u64)bx[t0]);
+            for (int64_t t = t0; t < t0 + n; ++t) {
+                if ((u64)ax[t] != keys.back().first || (u64)bx[t] != keys.back().second) {
+                    bsim::set_error("run %lld mixes X masks", (long long)r);
+                    return BSIM_ERR_ARG;
+                }
+                members.back().push_back(t);
+            }
+            t0 += n;
+        }
+        if (t0 != nterms) { bsim::set_error("runs cover %lld of %lld terms", (long long)t0, (long long)nterms); return BSIM_ERR_ARG; }
+    } else {
+        // groups in order of first appearance of (ax, bx)
+        struct KeyHash {
+            size_t operator()(const std::pair<u64, u64> &k) const { return std::hash<u64>()(k.first * 0x9E3779B97F4A7C15ull ^ k.second); }
+        };
+        std::unordered_map<std::pair<u64, u64>, int, KeyHash> gid;
+        for (int64_t t = 0; t < nterms; ++t) {
+            const auto key = std::make_pair((u64)ax[t], (u64)bx[t]);
+            auto it = gid.find(key);
+            int g;
+            if (it == gid.end()) {
+                g = (int)members.size();
+                gid.emplace(key, g);
+                members.emplace_back();
+                keys.push_back(key);
+            } else g = it->second;
+            members[g].push_back(t);
+        }
     }
+    auto *B = new bsim::NetBuild();
+    B->g.resize(members.size());
+    for (size_t g = 0; g < members.size(); ++g) { B->g[g].ax = keys[g].first; B->g[g].bx = keys[g].second; }
     const int ng = (int)members.size();
     const int nth = std::max(1, std::min(32, (int)std::thread::hardware_concurrency()));
     auto work = [&](int w) {
@@ -187,6 +206,24 @@ int bsim_netbuild_compress(int64_t nterms, const uint64_t *ax, const uint64_t *a
     for (auto &x : th) x.join();
     *out = B;
     return BSIM_OK;
+}
+
+extern "C" {
+
+int bsim_netbuild_compress(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx,
+                           const uint64_t *bz, const double *coef, double tol, void **out)
+{
+    return netbuild(nterms, ax, az, bx, bz, coef, tol, 0, nullptr, out);
+}
+
+int bsim_netbuild_compress_runs(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx,
+                                const uint64_t *bz, const double *coef, double tol, int64_t nruns,
+                                const int64_t *run_sizes, void **out)
+{
+    if (nruns > 0 && !run_sizes) { bsim::set_error("null run_sizes"); return BSIM_ERR_NULL; }
+    if (nruns < 0) { bsim::set_error("nruns = %lld", (long long)nruns); return BSIM_ERR_ARG; }
+    static const int64_t none = 0;
+    return netbuild(nterms, ax, az, bx, bz, coef, tol, nruns, nruns > 0 ? run_sizes : &none, out);
 }
 
 int bsim_netbuild_sizes(void *h, int64_t *ngs, int64_t *nza_total, int64_t *nzb_total, int64_t *nwa_total,

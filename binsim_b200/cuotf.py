@@ -85,6 +85,7 @@ def lib() -> C.CDLL:
         "bsim_batchgrad": (ci, [vp, vp, vp, vp, vp, vp, vp]),
         "bsim_hvec_host": (ci, [vp, vp, i64, vp, vp, ci, vp]),
         "bsim_netbuild_compress": (ci, [i64, vp, vp, vp, vp, vp, dbl, vp]),
+        "bsim_netbuild_compress_runs": (ci, [i64, vp, vp, vp, vp, vp, dbl, i64, vp, vp]),
         "bsim_netbuild_sizes": (ci, [vp, vp, vp, vp, vp, vp]),
         "bsim_netbuild_export": (ci, [vp] * 10),
         "bsim_netbuild_destroy": (ci, [vp]),
@@ -155,15 +156,22 @@ def _host(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
-def compress_groups_native(ax, az, bx, bz, c, norb: int, tol: float = 1e-12, orbsym=None) -> nw.OTFNetwork:
+def compress_groups_native(ax, az, bx, bz, c, norb: int, tol: float = 1e-12, orbsym=None,
+                           run_sizes=None) -> nw.OTFNetwork:
     """The grouping and SVD compression of network.compress_groups (jl/network.jl:158-246)
-    in the library's native builder (host threads); groups in order of first appearance."""
+    in the library's native builder (host threads); groups in order of first appearance,
+    or with run_sizes one group per run of consecutive terms (the pool form)."""
     L = lib()
     arrs = [_host(ax, np.uint64), _host(az, np.uint64), _host(bx, np.uint64), _host(bz, np.uint64),
             _host(c, np.float64)]
     h = vp()
-    _check(L.bsim_netbuild_compress(len(arrs[4]), *[a.ctypes.data for a in arrs], tol, C.byref(h)),
-           "bsim_netbuild_compress")
+    if run_sizes is None:
+        _check(L.bsim_netbuild_compress(len(arrs[4]), *[a.ctypes.data for a in arrs], tol, C.byref(h)),
+               "bsim_netbuild_compress")
+    else:
+        rs = _host(run_sizes, np.int64)
+        _check(L.bsim_netbuild_compress_runs(len(arrs[4]), *[a.ctypes.data for a in arrs], tol, len(rs),
+                                             rs.ctypes.data, C.byref(h)), "bsim_netbuild_compress_runs")
     try:
         n = [C.c_int64() for _ in range(5)]
         _check(L.bsim_netbuild_sizes(h, *[C.byref(x) for x in n]), "bsim_netbuild_sizes")

@@ -408,7 +408,7 @@ def _component(cre, ann, norb):
     return ax, az, bx, bz, C
 
 
-def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None) -> Pool:
+def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None, native: bool = False) -> Pool:
     """Spin-adapted generalised singles and doubles as ordered products of
     spin-orbital generators (alpha = 2p, beta = 2p+1).
 
@@ -480,7 +480,11 @@ def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None
     BX = np.concatenate([g[2] for g in groups]); BZ = np.concatenate([g[3] for g in groups])
     CC = np.concatenate([g[4] for g in groups])
     sizes = [len(g[4]) for g in groups]
-    net = _compress_each(AX, AZ, BX, BZ, CC, sizes, norb)
+    if native:   # the library's builder, one group per component run (bsim_netbuild_compress_runs)
+        from binsim_b200 import cuotf
+        net = cuotf.compress_groups_native(AX, AZ, BX, BZ, CC, norb, run_sizes=sizes)
+    else:
+        net = _compress_each(AX, AZ, BX, BZ, CC, sizes, norb)
     return Pool(network=net, components=gens2, labels=labels2)
 
 

@@ -230,6 +230,12 @@ int bsim_batchgrad(void *basis, void *net, const double *thetas, const double *l
  * ------------------------------------------------------------------------ */
 int bsim_netbuild_compress(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx,
                            const uint64_t *bz, const double *coef, double tol, void **out);
+/* As bsim_netbuild_compress with one group per run of run_sizes[r] consecutive
+ * terms (the pool form, one X group per generator: jl/network.jl:248-301); every
+ * term of a run must share its (ax, bx). */
+int bsim_netbuild_compress_runs(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx,
+                                const uint64_t *bz, const double *coef, double tol, int64_t nruns,
+                                const int64_t *run_sizes, void **out);
 int bsim_netbuild_sizes(void *h, int64_t *ngs, int64_t *nza_total, int64_t *nzb_total, int64_t *nwa_total,
                         int64_t *nwb_total);
 int bsim_netbuild_export(void *h, uint64_t *axs, uint64_t *bxs, int64_t *ranks, int64_t *num_zas, int64_t *num_zbs,

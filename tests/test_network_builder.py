@@ -142,3 +142,27 @@ def test_native_builder_rank_and_errors():
     L = cuotf.lib()
     assert L.bsim_netbuild_destroy(None) == -2
     assert L.bsim_netbuild_compress(1, None, None, None, None, None, 1e-12, C.byref(C.c_void_p())) == -1
+
+
+def test_native_pool_builder_matches_numpy(oracle):
+    """ucc_pool(native=True): one group per generator component through
+    bsim_netbuild_compress_runs; same groups, Z lists and ranks as the numpy builder, the
+    same group matrices (the rank-2 factors may rotate inside degenerate singular pairs)
+    and the same oracle expm for every group checked."""
+    from binsim_b200 import network as nw
+    norb = 7
+    a, b = nw.ucc_pool(norb).network, nw.ucc_pool(norb, native=True).network
+    for k in ("axs", "bxs", "ranks", "num_zas", "num_zbs", "flat_zas", "flat_zbs"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    oa = ob = 0
+    for gi in range(a.ngs):
+        na, nb, r = int(a.num_zas[gi]), int(a.num_zbs[gi]), int(a.ranks[gi])
+        Ma = a.flat_wa[oa:oa + na * r].reshape(r, na).T @ a.flat_wb[ob:ob + nb * r].reshape(r, nb)
+        Mb = b.flat_wa[oa:oa + na * r].reshape(r, na).T @ b.flat_wb[ob:ob + nb * r].reshape(r, nb)
+        assert np.abs(Ma - Mb).max() < 1e-12, gi
+        oa += na * r; ob += nb * r
+    B = oracle.basis(norb, 3, 3)
+    Na, Nb = oracle.network(a), oracle.network(b)
+    v = np.random.default_rng(1).normal(size=B.dim)
+    for gi in range(0, a.ngs, 97):
+        np.testing.assert_allclose(oracle.expm(B, Na, gi, 0.4, v), oracle.expm(B, Nb, gi, 0.4, v), rtol=0, atol=1e-14)

@@ -349,6 +349,24 @@ def _pack(groups, norb, orbsym=None) -> OTFNetwork:
     )
 
 
+def group_range(net: OTFNetwork, lo: int, hi: int) -> OTFNetwork:
+    """The network's groups [lo, hi) as a network of their own (the flat arrays sliced;
+    a rank's share of a pool when the pool gradient is split over ranks)."""
+    if not 0 <= lo <= hi <= net.ngs:
+        raise ValueError(f"group range [{lo}, {hi}) outside [0, {net.ngs})")
+    nza, nzb = np.asarray(net.num_zas, np.int64), np.asarray(net.num_zbs, np.int64)
+    rk = np.asarray(net.ranks, np.int64)
+    za0, zb0 = int(nza[:lo].sum()), int(nzb[:lo].sum())
+    za1, zb1 = int(nza[:hi].sum()), int(nzb[:hi].sum())
+    wa0, wb0 = int((nza[:lo] * rk[:lo]).sum()), int((nzb[:lo] * rk[:lo]).sum())
+    wa1, wb1 = int((nza[:hi] * rk[:hi]).sum()), int((nzb[:hi] * rk[:hi]).sum())
+    c = lambda a: np.ascontiguousarray(a)
+    return OTFNetwork(norb=net.norb, orbsym=c(net.orbsym), axs=c(net.axs[lo:hi]), bxs=c(net.bxs[lo:hi]),
+                      ranks=c(rk[lo:hi]), num_zas=c(nza[lo:hi]), num_zbs=c(nzb[lo:hi]),
+                      flat_zas=c(net.flat_zas[za0:za1]), flat_zbs=c(net.flat_zbs[zb0:zb1]),
+                      flat_wa=c(net.flat_wa[wa0:wa1]), flat_wb=c(net.flat_wb[wb0:wb1]))
+
+
 def hamiltonian_network(norb: int, seed: int = 0, tol: float = 1e-12, e_nuc=None, native: bool = False) -> OTFNetwork:
     """OTF network of the seeded synthetic Hamiltonian on ``norb`` orbitals.  native:
     group and compress with the library's builder (bsim_netbuild_*, host threads)."""

@@ -79,3 +79,76 @@ def test_sharded_sigma_gloo_matches_oracle(tmp_path, world):
         assert ok == 1.0, f"rank {r}: gathered sigma differs from the oracle"
         assert band_only == 1.0, f"rank {r}: computed outside its band"
         assert nbytes > 0
+
+
+def test_group_ranges_cover_once_and_balance():
+    from binsim_b200.shard import group_ranges
+    rng = np.random.default_rng(0)
+    for n in (0, 1, 7, 100, 1001):
+        for world in (1, 2, 3, 8):
+            costs = rng.integers(1, 50, size=n)
+            rs = group_ranges(costs, world)
+            assert len(rs) == world and rs[0][0] == 0 and rs[-1][1] == n
+            assert all(rs[i][1] == rs[i + 1][0] for i in range(world - 1))
+            if n >= world:
+                loads = [costs[lo:hi].sum() for lo, hi in rs]
+                assert max(loads) - min(loads) <= 2 * costs.max()
+
+
+def test_group_range_subnetwork_acts_like_the_slice(oracle):
+    from binsim_b200 import network as nw
+    norb = 6
+    pool = nw.ucc_pool(norb).network
+    B = oracle.basis(norb, 3, 3)
+    N = oracle.network(pool)
+    lo, hi = 101, 173
+    S = oracle.network(nw.group_range(pool, lo, hi))
+    v = np.random.default_rng(2).normal(size=B.dim)
+    for g in (0, 17, hi - lo - 1):
+        assert np.array_equal(oracle.expm(B, S, g, 0.3, v), oracle.expm(B, N, lo + g, 0.3, v))
+
+
+def _pool_worker(rank, world, port, norb, na, nb, outdir):
+    import torch
+    import torch.distributed as dist
+    from binsim_b200 import network as nw
+    from binsim_b200.shard import PoolShardedGradient
+    from oracle.oracle import Oracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        O = Oracle()
+        Bo = O.basis(norb, na, nb)
+        pool = nw.ucc_pool(norb).network
+        rng = np.random.default_rng(4)
+        psi, hpsi = rng.normal(size=Bo.dim), rng.normal(size=Bo.dim)   # the same state on every rank
+        ref = O.batchgrad(Bo, O.network(pool), np.zeros(pool.ngs), psi, hpsi)
+        calls = []
+
+        def compute(lo, hi, out):
+            calls.append((lo, hi))
+            sub = O.network(nw.group_range(pool, lo, hi))
+            out.copy_(torch.from_numpy(O.batchgrad(Bo, sub, np.zeros(hi - lo), psi, hpsi)))
+        costs = np.asarray(pool.num_zas) + np.asarray(pool.num_zbs)   # any positive work estimate
+        S = PoolShardedGradient(compute, pool.ngs, costs=costs)
+        g = torch.full((pool.ngs,), float("nan"), dtype=torch.float64)
+        S(g)
+        # the oracle's OpenMP reductions round in thread order: equal to 1e-12 relative
+        ok = bool(np.abs(g.numpy() - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()))
+        np.save(os.path.join(outdir, f"pool{rank}.npy"),
+                np.array([ok, calls == [S.range] if S.range[1] > S.range[0] else calls == []], dtype=np.float64))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_pool_gradient_gloo_matches_oracle(tmp_path, world):
+    """The pool gradient split by ranges of pool groups over world ranks (gloo), every
+    rank ending with the whole gradient vector, equal to the unsplit oracle."""
+    import torch.multiprocessing as mp
+    mp.spawn(_pool_worker, args=(world, _free_port(), 6, 3, 3, str(tmp_path)), nprocs=world, join=True)
+    for r in range(world):
+        ok, own_only = np.load(tmp_path / f"pool{r}.npy")
+        assert ok == 1.0, f"rank {r}: gathered pool gradient differs from the oracle"
+        assert own_only == 1.0, f"rank {r}: computed outside its range"

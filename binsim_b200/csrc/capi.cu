@@ -421,6 +421,12 @@ int bsim_hvec_host(void *basis, void *net, int64_t nvec, const double *const *sr
             BSIM_CUDA(cudaEventRecord(P.out_read[sl], P.cout));
         }
         cudaError_t e1 = cudaStreamSynchronize(P.cout), e2 = cudaStreamSynchronize(stream);
+        // keep the pipeline's four vectors between calls only while they are small
+        // (8 GB in all); larger ones are released with the call
+        if (4.0 * (double)bytes > 8e9) {
+            pipe.reset();
+            pipe_dim = -1;
+        }
         if (st != BSIM_OK) return st;
         if (e1 != cudaSuccess) return bsim::cuda_status(e1, "hvec_host");
         if (e2 != cudaSuccess) return bsim::cuda_status(e2, "hvec_host");

@@ -143,7 +143,9 @@ int bsim_hvec(void *basis, void *net, const double *src, double *dst, bsim_strea
  * copy (its own copy stream), sigma (on `stream`) and the device-to-host copy
  * (a second copy stream), so the copies of neighbouring steps overlap the sigma
  * between them; returns when the last result is on the host.  Page-locked host
- * buffers let the copies run asynchronously.  mixed selects the FP32-bulk sigma. */
+ * buffers let the copies run asynchronously.  mixed selects the FP32-bulk sigma.
+ * The four device vectors stay allocated for the next call while they total at
+ * most 8 GB, and are released at the end of the call otherwise. */
 int bsim_hvec_host(void *basis, void *net, int64_t nvec, const double *const *src_host, double *const *dst_host,
                    int mixed, bsim_stream_t stream);
 /* dst = H src with FP32 bulk (FP32 phases, weights and gathered source,

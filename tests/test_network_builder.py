@@ -166,3 +166,41 @@ def test_native_pool_builder_matches_numpy(oracle):
     v = np.random.default_rng(1).normal(size=B.dim)
     for gi in range(0, a.ngs, 97):
         np.testing.assert_allclose(oracle.expm(B, Na, gi, 0.4, v), oracle.expm(B, Nb, gi, 0.4, v), rtol=0, atol=1e-14)
+
+
+def _dense_pauli(x, z, c, ns):
+    """sum_k c_k P(x_k, z_k) on ns qubits, P(x, z)|s> = (-1)^popc(s & z) |s ^ x>, with
+    qubit k the k-th Kronecker factor (the most significant bit of the index first)."""
+    dim = 1 << ns
+    idx = lambda s: sum(((s >> k) & 1) << (ns - 1 - k) for k in range(ns))
+    M = np.zeros((dim, dim))
+    for xi, zi, ci in zip(np.asarray(x, np.uint64).tolist(), np.asarray(z, np.uint64).tolist(), np.asarray(c).tolist()):
+        for s in range(dim):
+            M[idx(s ^ xi), idx(s)] += ci * (-1) ** bin(s & zi).count("1")
+    return M
+
+
+@pytest.mark.parametrize("cre,ann", [((3,), (0,)), ((1,), (4,)), ((5, 2), (0, 3)), ((4, 1), (3, 0)),
+                                     ((2, 5), (1, 4)), ((0, 3), (5, 2))])
+def test_generator_pauli_terms_match_dense_fermion_operators(cre, ann):
+    """The Pauli expansion of a generator t - t^dagger (t = a+_cre... a_ann..., spin
+    orbitals, Jordan-Wigner with Z on the lower modes) equals the same operator built
+    from dense Fock-space ladder matrices."""
+    ns = 6
+    I2, Z, a1 = np.eye(2), np.diag([1.0, -1.0]), np.array([[0, 1], [0, 0.0]])
+
+    def op(j):
+        m = np.array([[1.0]])
+        for k in range(ns):
+            m = np.kron(m, Z if k < j else (a1 if k == j else I2))
+        return m
+    an = [op(j) for j in range(ns)]
+    cr = [x.T for x in an]
+    t = np.eye(1 << ns)
+    for j in cre:
+        t = t @ cr[j]
+    for j in ann:
+        t = t @ an[j]
+    terms = nw._generator_terms(cre, ann)
+    assert terms is not None
+    np.testing.assert_allclose(_dense_pauli(*terms, ns), t - t.T, atol=1e-14)

@@ -89,6 +89,7 @@ def lib() -> C.CDLL:
         "bsim_netbuild_sizes": (ci, [vp, vp, vp, vp, vp, vp]),
         "bsim_netbuild_export": (ci, [vp] * 10),
         "bsim_netbuild_destroy": (ci, [vp]),
+        "bsim_poolplan_classify": (ci, [i64, i64] + [vp] * 12),
         "bsim_network_create_c64": (ci, [vp, i64, i64] + [vp] * 10),
         "bsim_network_create_c64_u64": (ci, [vp, i64, i64] + [vp] * 10),
         "bsim_hvec_c64": (ci, [vp, vp, vp, vp, vp]),
@@ -187,6 +188,28 @@ def compress_groups_native(ax, az, bx, bz, c, norb: int, tol: float = 1e-12, orb
         L.bsim_netbuild_destroy(h)
     osym = np.zeros(norb, np.int64) if orbsym is None else np.asarray(orbsym, np.int64)
     return nw.OTFNetwork(norb=norb, orbsym=osym, **out)
+
+
+POOL_KINDS = {"general": -1, "zero": 0, "d1a": 1, "d1b": 2, "tab": 3, "gaa": 4, "gbb": 5}
+
+
+def pool_plan(net: nw.OTFNetwork):
+    """Per group of a generator network: (kind, idx[ngs, 4], coef) from the library's
+    pool-gradient plan (bsim_poolplan_classify, host code): group g is
+    coef[g] / (alpha-first reordering sign) * (t - t^dagger) for the excitation whose
+    transition-density entry idx[g] of table kind[g] it names; kind -1 matches no
+    excitation, 0 has a zero gradient for real vectors."""
+    L = lib()
+    n = net.ngs
+    arrs = [_host(net.axs, np.uint64), _host(net.bxs, np.uint64), _host(net.ranks, np.int64),
+            _host(net.num_zas, np.int64), _host(net.num_zbs, np.int64), _host(net.flat_zas, np.uint64),
+            _host(net.flat_zbs, np.uint64), _host(net.flat_wa, np.float64), _host(net.flat_wb, np.float64)]
+    kind = np.zeros(n, np.int32)
+    idx = np.zeros((n, 4), np.int32)
+    coef = np.zeros(n, np.float64)
+    _check(L.bsim_poolplan_classify(net.norb, n, *[a.ctypes.data for a in arrs], kind.ctypes.data,
+                                    idx.ctypes.data, coef.ctypes.data), "bsim_poolplan_classify")
+    return kind, idx, coef
 
 
 def fma_peak(fp64: bool = True, stream=None, dmma: bool = False) -> float:

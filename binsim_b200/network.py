@@ -410,11 +410,14 @@ class Pool:
 
     ``network`` holds one group per spin-orbital component (original index =
     component index).  ``components[i]`` lists the component indices whose
-    ordered product, sharing one angle, forms spin-adapted generator ``i``."""
+    ordered product, sharing one angle, forms spin-adapted generator ``i``.
+    ``excitations[g]`` is the (creators, annihilators) spin-orbital tuple of
+    group g: the group is t - t^dagger with t = a+_{cre...} a_{ann...}."""
 
     network: OTFNetwork
     components: List[List[int]]
     labels: List[Tuple]
+    excitations: List[Tuple[Tuple[int, ...], Tuple[int, ...]]] = dataclasses.field(default_factory=list)
 
 
 def _component(cre, ann, norb):
@@ -481,12 +484,13 @@ def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None
                 terms[i] = t
     # drop vanishing components (t = t^dagger) and renumber
     new_id = {}
-    groups = []
+    groups, excitations = [], []
     for i, t in enumerate(terms):
         if t is None:
             continue
         new_id[i] = len(groups)
         groups.append(t)
+        excitations.append(keys[i])
     gens2, labels2 = [], []
     for ids, lab in zip(gens, labels):
         ids = [new_id[i] for i in ids if i in new_id]
@@ -503,7 +507,7 @@ def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None
         net = cuotf.compress_groups_native(AX, AZ, BX, BZ, CC, norb, run_sizes=sizes)
     else:
         net = _compress_each(AX, AZ, BX, BZ, CC, sizes, norb)
-    return Pool(network=net, components=gens2, labels=labels2)
+    return Pool(network=net, components=gens2, labels=labels2, excitations=excitations)
 
 
 def _compress_each(ax, az, bx, bz, c, sizes, norb, tol=1e-12) -> OTFNetwork:

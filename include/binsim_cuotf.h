@@ -245,6 +245,42 @@ int bsim_netbuild_export(void *h, uint64_t *axs, uint64_t *bxs, int64_t *ranks, 
 int bsim_netbuild_destroy(void *h);
 
 /* ------------------------------------------------------------------------
+ * Pool-gradient plan (host code, no device work).  Recognises each group of a
+ * generator network (the bsim_network_create_* arrays) as
+ * lam * (t - t^dagger), t a spin-orbital excitation with at most two creators
+ * and two annihilators (the pool components of jl/adapt.jl, one group per
+ * component as jl/network.jl:248-301 builds them).  For such groups the pool
+ * gradient at theta = 0 (batch_grad_contract_otf, op/batchgrad.hpp:529-540)
+ * is grad_g = coef[g] * (X[dagger(i)] - X[i]), i = idx[4g..4g+3] and X one of
+ * the transition densities of l~ = eps l, r~ = eps r (eps(a, b) =
+ * (-1)^popc(b & K(a)), K(a) = XOR over alpha electrons i of (1 << i) - 1)
+ * chosen by kind[g]:
+ *   BSIM_POOL_D1A  X[p][q]       = <l~| a+_p a_q |r~> (alpha),  dagger(p,q) = (q,p)
+ *   BSIM_POOL_D1B  the same for beta
+ *   BSIM_POOL_TAB  X[p][q][r][s] = <l~| a+_p a_q (alpha) a+_r a_s (beta) |r~>,
+ *                  dagger(p,q,r,s) = (q,p,s,r)
+ *   BSIM_POOL_GAA  X[p][q][r][s] = <l~| a+_p a+_q a_r a_s |r~> (alpha),
+ *                  dagger(p,q,r,s) = (s,r,q,p)
+ *   BSIM_POOL_GBB  the same for beta
+ * BSIM_POOL_ZERO marks groups whose gradient is zero for real vectors
+ * (diagonal or empty groups); BSIM_POOL_GENERAL groups match no excitation and
+ * keep the pair-list gradient.  norb <= 64.
+ * ------------------------------------------------------------------------ */
+enum {
+    BSIM_POOL_GENERAL = -1,
+    BSIM_POOL_ZERO = 0,
+    BSIM_POOL_D1A = 1,
+    BSIM_POOL_D1B = 2,
+    BSIM_POOL_TAB = 3,
+    BSIM_POOL_GAA = 4,
+    BSIM_POOL_GBB = 5
+};
+int bsim_poolplan_classify(int64_t norb, int64_t ngs, const uint64_t *axs, const uint64_t *bxs,
+                           const int64_t *ranks, const int64_t *num_zas, const int64_t *num_zbs,
+                           const uint64_t *flat_zas, const uint64_t *flat_zbs, const double *flat_wa,
+                           const double *flat_wb, int32_t *kind, int32_t *idx, double *coef);
+
+/* ------------------------------------------------------------------------
  * Complex (c64) networks and operators: the reference CPU library's _c64
  * exports (src/extern/otf_native.cpp:4,6; Tv = complex<double>) on device
  * vectors of interleaved (re, im) doubles, dim complex entries each.  The

@@ -1,0 +1,118 @@
+"""CPU statement (numpy, test infrastructure) of the pool gradient at theta = 0 through
+transition densities, the computation bsim_poolplan_classify plans for.
+
+With l~ = eps l and r~ = eps r (eps(a, b) = (-1)^popc(b & K(a)), K(a) = XOR over alpha
+electrons i of (1 << i) - 1: the interleaved -> alpha-first determinant sign) every pool
+component's gradient <r| G |l> (op/batchgrad.hpp:529-540 at theta = 0) is a difference of
+two entries of five tables, each a GEMM over strings with holes:
+
+  D1a[p][q]       = sum_{k (n-1 electrons), b} (k+p | b)  (k+q | b)
+  Tab[p][q][r][s] = sum_{kA, kB (n-1 each)}   (kA+p | kB+r) (kA+q | kB+s)
+  Gaa[p][q][r][s] = sum_{k (n-2 electrons), b} (k+p+q | b) (k+s+r | b)   (a+_p a+_q a_r a_s)
+
+where (k+p | b) is the l~ (left factor) or r~ (right factor) element of the string
+a+_p |k> with that creation sign; D1b and Gbb are the same on the beta strings.
+Single symmetry block only.
+"""
+import itertools
+
+import numpy as np
+
+
+def _popc(x):
+    return bin(int(x)).count("1")
+
+
+def eps_frame(astr, bstr):
+    """eps[a, b] = (-1)^popc(b & K(a)) over the strings of one block."""
+    K = []
+    for a in astr:
+        k = 0
+        for i in range(64):
+            if (int(a) >> i) & 1:
+                k ^= (1 << i) - 1
+        K.append(k)
+    return np.array([[1.0 - 2.0 * (_popc(int(b) & k) & 1) for b in bstr] for k in K])
+
+
+def _create(s, orbs):
+    """(sign, string) of a+_{orbs[0]} a+_{orbs[1]} ... |s> (rightmost applied first), or (0, None)."""
+    sg = 1
+    for o in reversed(orbs):
+        if (s >> o) & 1:
+            return 0, None
+        if _popc(s & ((1 << o) - 1)) & 1:
+            sg = -sg
+        s |= 1 << o
+    return sg, s
+
+
+def hole_table(strs, k, norb):
+    """For the strings with k holes (k electrons removed from any string of strs):
+    idx[h, t] (string index of a+_{t0} .. a+_{t(k-1)} |h>, 0 where it vanishes) and
+    sgn[h, t] (its sign, 0 where it vanishes), t over ordered k-tuples of orbitals."""
+    where = {int(s): i for i, s in enumerate(strs)}
+    holes = sorted({int(s) ^ sum(1 << o for o in c) for s in strs
+                    for c in itertools.combinations([o for o in range(norb) if (int(s) >> o) & 1], k)})
+    tups = list(itertools.product(range(norb), repeat=k))
+    idx = np.zeros((len(holes), len(tups)), np.int64)
+    sgn = np.zeros((len(holes), len(tups)))
+    for h, hs in enumerate(holes):
+        for t, tup in enumerate(tups):
+            sg, s = _create(hs, list(tup))
+            if sg and s in where:
+                idx[h, t], sgn[h, t] = where[s], sg
+    return idx, sgn
+
+
+def tables(astr, bstr, l, r, norb):
+    """The five transition-density tables of l and r (interleaved-frame vectors of one
+    block, alpha-major), as dense numpy arrays indexed by orbitals."""
+    n = norb
+    E = eps_frame(astr, bstr)
+    L = E * np.asarray(l, float).reshape(len(astr), len(bstr))
+    R = E * np.asarray(r, float).reshape(len(astr), len(bstr))
+    out = {}
+    # one hole: D1 (rows (hole, other-spin string), columns p) and Tab
+    ia, sa = hole_table(astr, 1, n)
+    ib, sb = hole_table(bstr, 1, n)
+
+    def one(M, i1, s1):              # [(h, col), p]
+        return (s1[:, :, None] * M[i1]).transpose(0, 2, 1).reshape(-1, n)
+    out["d1a"] = one(L, ia, sa).T @ one(R, ia, sa)
+    out["d1b"] = one(L.T, ib, sb).T @ one(R.T, ib, sb)
+
+    def two(M):                      # [(hA, hB), (p, r)]
+        g = M[ia[:, None, :, None], ib[None, :, None, :]] * (sa[:, None, :, None] * sb[None, :, None, :])
+        return g.reshape(-1, n * n)
+    T = (two(L).T @ two(R)).reshape(n, n, n, n)          # [p, r, q, s]
+    out["tab"] = T.transpose(0, 2, 1, 3)                 # [p, q, r, s]
+    # two holes, same spin
+    for key, M, N, strs in (("gaa", L, R, astr), ("gbb", L.T, R.T, bstr)):
+        i2, s2 = hole_table(strs, 2, n)
+        lg = (s2[:, :, None] * M[i2]).transpose(0, 2, 1).reshape(-1, n * n)
+        rg = (s2[:, :, None] * N[i2]).transpose(0, 2, 1).reshape(-1, n * n)
+        # <a'| a+_p a+_q |h> <h| a_r a_s |a> with <h| a_r a_s |a> = <a| a+_s a+_r |h>
+        G = (lg.T @ rg).reshape(n, n, n, n)              # [p, q, s, r]
+        out[key] = G.transpose(0, 1, 3, 2)
+    return out
+
+
+_DAGGER = {1: (1, 0), 2: (1, 0), 3: (1, 0, 3, 2), 4: (3, 2, 1, 0), 5: (3, 2, 1, 0)}
+_NAME = {1: "d1a", 2: "d1b", 3: "tab", 4: "gaa", 5: "gbb"}
+
+
+def grads_from_plan(tab, kind, idx, coef):
+    """grad_g = coef_g (X[dagger(idx_g)] - X[idx_g]) for every planned group (kind >= 1),
+    0 for kind 0, NaN for kind -1 (general groups)."""
+    g = np.full(len(kind), np.nan)
+    for i, (k, ix, c) in enumerate(zip(kind, idx, coef)):
+        if k == 0:
+            g[i] = 0.0
+        elif k > 0:
+            X = tab[_NAME[int(k)]]
+            m = len(_DAGGER[int(k)])
+            fwd = tuple(int(v) for v in ix[:m])
+            dag = tuple(fwd[j] for j in _DAGGER[int(k)])
+            g[i] = c * (X[dag] - X[fwd])
+    return g

@@ -1,0 +1,138 @@
+"""Pool-gradient plan (bsim_poolplan_classify, host code): every pool group recognised as
+coef * (t - t^dagger) for one spin-orbital excitation, and the pool gradient at theta = 0
+rebuilt from five transition-density tables (tests/_tdm_ref.py) against the reference's
+batch_tran outputs (golden) and the oracle's batch_grad."""
+import numpy as np
+import pytest
+
+from binsim_b200 import cuotf, network as nw
+from conftest import load_golden
+
+import _tdm_ref as tdm
+
+
+def _normal_form(cre, ann):
+    """(kind, idx, sign) of t = a+_{cre..} a_{ann..} in alpha-first order (spin orbital
+    2p + s), written independently of the library."""
+    ops = [(m, True) for m in cre] + [(m, False) for m in ann]
+    inv = sum(1 for i in range(len(ops)) for j in range(i + 1, len(ops)) if ops[i][0] % 2 and not ops[j][0] % 2)
+    oa = [m // 2 for m, _ in ops if m % 2 == 0]
+    ob = [m // 2 for m, _ in ops if m % 2 == 1]
+    kind = {(2, 0): 1, (0, 2): 2, (2, 2): 3, (4, 0): 4, (0, 4): 5}[(len(oa), len(ob))]
+    idx = (oa + ob + [0, 0, 0, 0])[:4]
+    return kind, idx, (-1.0) ** inv
+
+
+_DAG = {1: (1, 0, 2, 3), 2: (1, 0, 2, 3), 3: (1, 0, 3, 2), 4: (3, 2, 1, 0), 5: (3, 2, 1, 0)}
+
+
+def _canon(kind, idx, coef):
+    """Same-spin doubles are antisymmetric in (p, q) and in (r, s): order each pair
+    descending, with the sign."""
+    idx = [int(v) for v in idx]
+    if kind in (4, 5):
+        if idx[0] < idx[1]:
+            idx[0], idx[1], coef = idx[1], idx[0], -coef
+        if idx[2] < idx[3]:
+            idx[2], idx[3], coef = idx[3], idx[2], -coef
+    return idx, coef
+
+
+def _same_generator(kind, idx, coef, want):
+    """Plan entry equals (kind, idx, sign) up to orientation: coef (X[dag] - X[idx]) is
+    unchanged when idx and its dagger swap and coef changes sign."""
+    k, ix, s = want
+    if kind != k:
+        return False
+    got, c = _canon(k, idx, coef)
+    fwd, sf = _canon(k, ix, s)
+    dag, sd = _canon(k, [ix[j] for j in _DAG[k]], s)
+    return (got == fwd and abs(c - sf) < 1e-12) or (got == dag and abs(c + sd) < 1e-12)
+
+
+@pytest.mark.parametrize("norb", [4, 7])
+def test_plan_recovers_every_pool_excitation(norb):
+    pool = nw.ucc_pool(norb)
+    kind, idx, coef = cuotf.pool_plan(pool.network)
+    assert len(pool.excitations) == pool.network.ngs
+    for g, (cre, ann) in enumerate(pool.excitations):
+        assert _same_generator(kind[g], idx[g], coef[g], _normal_form(cre, ann)), (g, cre, ann)
+
+
+@pytest.mark.parametrize("case", ["h6_3a3b", "h8_4a4b"])
+def test_density_gradient_matches_reference_batch_tran(case):
+    """Golden trans_pool = the reference library's batch_tran_contract_otf(x, y), which is
+    the theta = 0 pool gradient for groups without a diagonal part."""
+    z, _, pool = load_golden(case)
+    from oracle.oracle import Oracle
+    B = Oracle().basis(int(z["norb"]), int(z["na"]), int(z["nb"]))
+    assert B.num_blocks == 1 and B.dim == int(z["dim"])
+    kind, idx, coef = cuotf.pool_plan(pool)
+    assert np.all(kind > 0)
+    tb = tdm.tables(B.strings(0, 0), B.strings(0, 1), z["x"], z["y"], pool.norb)
+    g = tdm.grads_from_plan(tb, kind, idx, coef)
+    ref = z["trans_pool"]
+    assert np.abs(g - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("norb,na,nb", [(5, 2, 3), (6, 3, 2)])
+def test_density_gradient_matches_oracle_batchgrad(oracle, norb, na, nb):
+    pool = nw.ucc_pool(norb)
+    net = pool.network
+    rng = np.random.default_rng(norb + na)
+    scale = rng.uniform(-2.0, 2.0, net.ngs)            # group g becomes scale_g * (t - t^dagger)
+    wa = net.flat_wa.copy()
+    off = 0
+    for g in range(net.ngs):
+        n = int(net.num_zas[g] * net.ranks[g])
+        wa[off:off + n] *= scale[g]
+        off += n
+    net2 = nw.OTFNetwork(**{**net.__dict__, "flat_wa": wa})
+    kind, idx, coef = cuotf.pool_plan(net2)
+    assert np.all(kind > 0)
+    for g, (cre, ann) in enumerate(pool.excitations):
+        k, ix, sg = _normal_form(cre, ann)
+        assert _same_generator(kind[g], idx[g], coef[g] / scale[g], (k, ix, sg)), g
+    B = oracle.basis(norb, na, nb)
+    l, r = rng.normal(size=B.dim), rng.normal(size=B.dim)
+    ref = oracle.batchgrad(B, oracle.network(net2), np.zeros(net2.ngs), l, r)
+    g = tdm.grads_from_plan(tdm.tables(B.strings(0, 0), B.strings(0, 1), l, r, norb), kind, idx, coef)
+    assert np.abs(g - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_hamiltonian_groups_are_not_excitations():
+    """Hermitian groups (t + t^dagger, many-term sums) match no generator: general or zero."""
+    kind, _, _ = cuotf.pool_plan(nw.hamiltonian_network(6, seed=2))
+    assert set(np.unique(kind)) <= {-1, 0} and (kind == 0).sum() == 1
+
+
+def test_plan_beyond_32_orbitals():
+    """Masks past spin orbital 63 (the two-word interleaved form): 40 orbitals."""
+    norb = 40
+    keys = [((2 * 39, 2 * 3 + 1), (2 * 20 + 1, 2 * 0)), ((2 * 38 + 1,), (2 * 31 + 1,)),
+            ((2 * 35, 2 * 33), (2 * 34, 2 * 1)), ((2 * 36 + 1, 2 * 2 + 1), (2 * 2 + 1, 2 * 30 + 1))]
+    ax, az, bx, bz, cc, sizes = [], [], [], [], [], []
+    by_shape = {}
+    for i, (cr, an) in enumerate(keys):
+        by_shape.setdefault((len(cr), len(an)), []).append(i)
+    terms = [None] * len(keys)
+    for _, ids in by_shape.items():
+        for i, t in zip(ids, nw._components_batch([keys[i] for i in ids], norb)):
+            terms[i] = t
+    for t in terms:
+        ax.append(t[0]); az.append(t[1]); bx.append(t[2]); bz.append(t[3]); cc.append(t[4]); sizes.append(len(t[4]))
+    net = nw._compress_each(*[np.concatenate(v) for v in (ax, az, bx, bz, cc)], sizes, norb)
+    kind, idx, coef = cuotf.pool_plan(net)
+    for g, (cre, ann) in enumerate(keys):
+        assert _same_generator(kind[g], idx[g], coef[g], _normal_form(cre, ann)), g
+
+
+def test_plan_argument_checks():
+    import ctypes as C
+    L = cuotf.lib()
+    z = np.zeros(4, np.int64)
+    assert L.bsim_poolplan_classify(4, 0, *([None] * 12)) == 0
+    assert L.bsim_poolplan_classify(4, 1, *([None] * 12)) == -1
+    assert L.bsim_poolplan_classify(65, 1, *([z.ctypes.data] * 12)) == -2
+    assert L.bsim_poolplan_classify(4, -1, *([z.ctypes.data] * 12)) == -2
+    del C

@@ -90,6 +90,10 @@ def lib() -> C.CDLL:
         "bsim_netbuild_export": (ci, [vp] * 10),
         "bsim_netbuild_destroy": (ci, [vp]),
         "bsim_poolplan_classify": (ci, [i64, i64] + [vp] * 12),
+        "bsim_pooldensity_hole_table": (ci, [i64, i64, i64, vp, vp, vp]),
+        "bsim_pooldensity_create": (ci, [vp, i64, vp, vp, vp, vp]),
+        "bsim_pooldensity_grad": (ci, [vp, vp, vp, vp, vp]),
+        "bsim_pooldensity_destroy": (ci, [vp]),
         "bsim_network_create_c64": (ci, [vp, i64, i64] + [vp] * 10),
         "bsim_network_create_c64_u64": (ci, [vp, i64, i64] + [vp] * 10),
         "bsim_hvec_c64": (ci, [vp, vp, vp, vp, vp]),
@@ -210,6 +214,42 @@ def pool_plan(net: nw.OTFNetwork):
     _check(L.bsim_poolplan_classify(net.norb, n, *[a.ctypes.data for a in arrs], kind.ctypes.data,
                                     idx.ctypes.data, coef.ctypes.data), "bsim_poolplan_classify")
     return kind, idx, coef
+
+
+def hole_table(strs, norb: int, holes: int):
+    """(number of hole strings, table[nh, norb or norb (norb - 1) / 2]) of
+    bsim_pooldensity_hole_table (host code): entries (index << 1) | sign or -1."""
+    L = lib()
+    s = _host(strs, np.uint64)
+    nh = C.c_int64()
+    _check(L.bsim_pooldensity_hole_table(norb, holes, len(s), s.ctypes.data, C.byref(nh), None),
+           "bsim_pooldensity_hole_table")
+    w = norb if holes == 1 else norb * (norb - 1) // 2
+    tab = np.zeros((nh.value, w), np.int32)
+    _check(L.bsim_pooldensity_hole_table(norb, holes, len(s), s.ctypes.data, C.byref(nh), tab.ctypes.data),
+           "bsim_pooldensity_hole_table")
+    return nh.value, tab
+
+
+class PoolDensity:
+    """Pool gradient at theta = 0 through transition densities on the GPU
+    (bsim_pooldensity_*): plan from pool_plan(net), device vectors l, r."""
+
+    def __init__(self, basis: "CuBasis", net: nw.OTFNetwork):
+        self.kind, self.idx, self.coef = pool_plan(net)
+        self.ngs = net.ngs
+        self._h = vp()
+        _check(lib().bsim_pooldensity_create(basis.h, self.ngs, self.kind.ctypes.data, self.idx.ctypes.data,
+                                             self.coef.ctypes.data, C.byref(self._h)), "bsim_pooldensity_create")
+
+    def grad(self, l, r, grads, stream=None):
+        _check(lib().bsim_pooldensity_grad(self._h, _ptr(l), _ptr(r), _ptr(grads), _stream(stream)),
+               "bsim_pooldensity_grad")
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().bsim_pooldensity_destroy(self._h)
+            self._h = vp()
 
 
 def fma_peak(fp64: bool = True, stream=None, dmma: bool = False) -> float:

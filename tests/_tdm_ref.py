@@ -116,3 +116,73 @@ def grads_from_plan(tab, kind, idx, coef):
             dag = tuple(fwd[j] for j in _DAGGER[int(k)])
             g[i] = c * (X[dag] - X[fwd])
     return g
+
+
+def emulate_device(astr, bstr, l, r, norb, kind, idx, coef, hole_table):
+    """The arithmetic of the library's density kernels (pooldensity.cu), restated in numpy
+    on the library's own hole tables (hole_table(strs, norb, holes) -> (nh, table) with
+    entries (index << 1) | sign or -1): Tab as C[p n + r][q n + s], the same-spin tables
+    as C2[pq][rs] = <a+_p a+_q a_s a_r> (p > q, r > s), D1 from Tab's traces, then
+    grads = coef (X[dagger] - X[idx]) with 0 for kind 0 and NaN for kind -1."""
+    n = norb
+    nA, nB = len(astr), len(bstr)
+    E = eps_frame(astr, bstr)
+    lt = E * np.asarray(l, float).reshape(nA, nB)
+    rt = E * np.asarray(r, float).reshape(nA, nB)
+    _, tA = hole_table(astr, n, 1)
+    _, tB = hole_table(bstr, n, 1)
+
+    def dec(t):
+        return np.where(t >= 0, t >> 1, 0), np.where(t >= 0, 1.0 - 2.0 * (t & 1), 0.0)
+    ia, sa = dec(tA)
+    ib, sb = dec(tB)
+
+    def gat(M):   # [(hA, hB), (p, r)]
+        g = M[ia[:, None, :, None], ib[None, :, None, :]] * (sa[:, None, :, None] * sb[None, :, None, :])
+        return g.reshape(-1, n * n)
+    C = gat(lt).T @ gat(rt)
+    npair = n * (n - 1) // 2
+    C2 = {}
+    for spin, (strs, Ml, Mr) in enumerate(((astr, lt, rt), (bstr, lt.T, rt.T))):
+        nel = bin(int(strs[0])).count("1")
+        if nel < 2:
+            C2[spin] = None
+            continue
+        _, t2 = hole_table(strs, n, 2)
+        i2, s2 = dec(t2)
+        A = (s2[:, :, None] * Ml[i2]).transpose(0, 2, 1).reshape(-1, npair)
+        B = (s2[:, :, None] * Mr[i2]).transpose(0, 2, 1).reshape(-1, npair)
+        C2[spin] = A.T @ B
+    na_el, nb_el = bin(int(astr[0])).count("1"), bin(int(bstr[0])).count("1")
+    D1a = np.array([[sum(C[x * n + k, y * n + k] for k in range(n)) / nb_el for y in range(n)] for x in range(n)])
+    D1b = np.array([[sum(C[k * n + x, k * n + y] for k in range(n)) / na_el for y in range(n)] for x in range(n)])
+
+    def g2(M, p, q, r_, s):
+        if M is None or p == q or r_ == s:
+            return 0.0
+        sg = -1.0
+        if p < q:
+            p, q, sg = q, p, -sg
+        if r_ < s:
+            r_, s, sg = s, r_, -sg
+        return sg * M[p * (p - 1) // 2 + q, r_ * (r_ - 1) // 2 + s]
+
+    def at(k, i0, i1, i2, i3):
+        if k == 1:
+            return D1a[i0, i1]
+        if k == 2:
+            return D1b[i0, i1]
+        if k == 3:
+            return C[i0 * n + i2, i1 * n + i3]
+        return g2(C2[0] if k == 4 else C2[1], i0, i1, i2, i3)
+    out = np.empty(len(kind))
+    for g, (k, i, c) in enumerate(zip(kind, idx, coef)):
+        k = int(k)
+        if k <= 0:
+            out[g] = 0.0 if k == 0 else np.nan
+            continue
+        i0, i1, i2, i3 = (int(v) for v in i)
+        fwd = at(k, i0, i1, i2, i3)
+        dag = at(k, i1, i0, 0, 0) if k in (1, 2) else (at(k, i1, i0, i3, i2) if k == 3 else at(k, i3, i2, i1, i0))
+        out[g] = c * (dag - fwd)
+    return out

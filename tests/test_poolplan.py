@@ -136,3 +136,55 @@ def test_plan_argument_checks():
     assert L.bsim_poolplan_classify(65, 1, *([z.ctypes.data] * 12)) == -2
     assert L.bsim_poolplan_classify(4, -1, *([z.ctypes.data] * 12)) == -2
     del C
+
+
+@pytest.mark.parametrize("norb,ne,holes", [(6, 3, 1), (6, 3, 2), (7, 2, 2), (9, 4, 1), (40, 3, 2)])
+def test_library_hole_tables(norb, ne, holes):
+    """bsim_pooldensity_hole_table against the CPU statement's hole tables: same hole
+    strings (increasing), same created-string indices and signs, -1 where a created
+    orbital is occupied."""
+    import itertools
+    strs = np.array(sorted(sum(1 << o for o in c) for c in itertools.combinations(range(norb), ne)), np.uint64)
+    nh, tab = cuotf.hole_table(strs, norb, holes)
+    if norb > 12:   # the itertools tables of the CPU statement are too large here: spot checks
+        where = {int(s): i for i, s in enumerate(strs)}
+        rng = np.random.default_rng(0)
+        for h in rng.choice(nh, 20, replace=False):
+            for j in rng.choice(tab.shape[1], 30, replace=False):
+                e = int(tab[h, j])
+                x = int((np.sqrt(8 * j + 1) + 1) // 2)
+                while x * (x - 1) // 2 > j:
+                    x -= 1
+                y = j - x * (x - 1) // 2
+                s = int(strs[e >> 1]) if e >= 0 else None
+                if e >= 0:
+                    hs = s ^ (1 << x) ^ (1 << y)
+                    sg, s2 = tdm._create(hs, [x, y])
+                    assert s2 == s and (sg < 0) == bool(e & 1) and where[s] == e >> 1
+        return
+    idx, sgn = tdm.hole_table(strs, holes, norb)
+    assert nh == idx.shape[0]
+    if holes == 1:
+        want = np.where(sgn != 0, (idx << 1) | (sgn < 0), -1)
+    else:
+        pairs = [(x, y) for x in range(norb) for y in range(x)]
+        cols = [x * norb + y for x, y in pairs]
+        want = np.where(sgn[:, cols] != 0, (idx[:, cols] << 1) | (sgn[:, cols] < 0), -1)
+        order = np.argsort([x * (x - 1) // 2 + y for x, y in pairs])
+        want = want[:, order]
+    assert np.array_equal(tab, want)
+
+
+@pytest.mark.parametrize("norb,na,nb", [(5, 2, 3), (6, 3, 3), (6, 1, 2)])
+def test_device_density_arithmetic_matches_oracle(oracle, norb, na, nb):
+    """The density kernels' arithmetic (tables, C2 sign convention, D1 from Tab's traces,
+    assembly), restated in numpy on the library's hole tables, gives the oracle's pool
+    gradient at theta = 0."""
+    pool = nw.ucc_pool(norb)
+    kind, idx, coef = cuotf.pool_plan(pool.network)
+    B = oracle.basis(norb, na, nb)
+    rng = np.random.default_rng(norb * 10 + na)
+    l, r = rng.normal(size=B.dim), rng.normal(size=B.dim)
+    ref = oracle.batchgrad(B, oracle.network(pool.network), np.zeros(pool.network.ngs), l, r)
+    got = tdm.emulate_device(B.strings(0, 0), B.strings(0, 1), l, r, norb, kind, idx, coef, cuotf.hole_table)
+    assert np.abs(got - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max())

@@ -399,6 +399,19 @@ int density_create(DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t 
         return BSIM_ERR_UNSUPPORTED;
     }
     if ((i64)nA >= (1 << 30) || (i64)nB >= (1 << 30) || (nB + 255) / 256 > 65535) return BSIM_ERR_TOO_LARGE;
+    for (i64 g = 0; g < ngs; ++g) {   // the assembly reads tables at these orbitals
+        if (kind[g] < BSIM_POOL_GENERAL || kind[g] > BSIM_POOL_GBB) {
+            set_error("pool density gradient: group %lld has kind %d", (long long)g, (int)kind[g]);
+            return BSIM_ERR_ARG;
+        }
+        if (kind[g] > 0)
+            for (int j = 0; j < 4; ++j)
+                if (idx[4 * g + j] < 0 || idx[4 * g + j] >= n) {
+                    set_error("pool density gradient: group %lld names orbital %d of a %d-orbital basis",
+                              (long long)g, (int)idx[4 * g + j], n);
+                    return BSIM_ERR_ARG;
+                }
+    }
     std::vector<Ti> as(B->astrs.begin() + B->astart[0], B->astrs.begin() + B->astart[0] + nA);
     std::vector<Ti> bs(B->bstrs.begin() + B->bstart[0], B->bstrs.begin() + B->bstart[0] + nB);
     std::vector<u64> hA, hB, h2A, h2B;
@@ -455,7 +468,8 @@ int density_grad(PoolDensity *P, const double *l, const double *r, double *grads
     const i64 M = (i64)n * n, np2 = (i64)P->npair * P->npair;
     {
         dim3 g(nA, (nB + 255) / 256);
-        frame_pair_kernel<Ti><<<g, 256, 0, s>>>(nB, B->view.astrs, B->view.bstrs, l, r, P->lt, P->rt);
+        frame_pair_kernel<Ti><<<g, 256, 0, s>>>(nB, B->view.astrs + B->astart[0], B->view.bstrs + B->bstart[0], l, r,
+                                                P->lt, P->rt);
     }
     BSIM_CUDA(cudaMemsetAsync(P->C, 0, sizeof(double) * M * M, s));
     BSIM_CUDA(cudaMemsetAsync(P->C2a, 0, sizeof(double) * np2, s));

@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 SIGMA_CFGS = {
-    "16o": dict(norb=16, na=8, nb=8, seed=0),   # the sigma microbenchmark
+    "16o": dict(norb=16, na=8, nb=8, seed=0),   # the sigma microbenchmark, 16 orbitals 8a+8b (the headline line)
     "15o": dict(norb=15, na=7, nb=8, seed=0),   # a smaller case of the same kernels, for ncu captures
 }
 SIGMA_CFG = SIGMA_CFGS["16o"]
@@ -498,7 +498,7 @@ def timed_events(fn, k, w):
 # ---------------------------------------------------------------------------
 
 DAV_CFGS = {
-    # plain FP64 FCI Davidson, 12 orbitals 6a+6b, subspace 8
+    # the plain FP64 FCI Davidson workload, 12 orbitals 6a+6b, subspace 8
     "12o": dict(norb=12, na=6, nb=6, seed=0, maxspace=8, ncv=3),
     # the sigma microbenchmark's space, where sigma dominates the step
     "16o": dict(norb=16, na=8, nb=8, seed=0, maxspace=8, ncv=3),

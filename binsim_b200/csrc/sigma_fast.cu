@@ -727,7 +727,7 @@ __global__ void final_kernel(int nA, int nB, int ldB, int col_begin, int col_end
 // ---- host ------------------------------------------------------------------------------------
 // in: c~ (alpha side), then c~^T (beta side); tT: the alpha side's Z, then the
 // beta-side result t; Z: the beta side's Z, and the alpha side's when the
-// scratch budget allows a wider chunk than tT holds.
+// scratch limit allows a wider chunk than tT holds.
 template <typename Ti>
 struct FastScratch {
     void *in = nullptr, *tT = nullptr, *Z = nullptr;
@@ -762,7 +762,7 @@ static int get_fast(const DevBasis<Ti> *B, const DevNet<Ti> *N, FastState<Ti> **
     return BSIM_OK;
 }
 
-static size_t scratch_budget()
+static size_t scratch_limit()
 {
     const char *e = getenv("BSIM_SIGMA_SCRATCH_GB");
     double gb = e ? atof(e) : 24.0;
@@ -801,8 +801,8 @@ static size_t mixed_row_limit()
 
 // Intermediate Z of one stage: chunk width (columns, a multiple of kMixCols) and
 // buffer.  A buffer that is free during the stage (spare) is used when it holds
-// at least the width the scratch budget would give; otherwise the Z scratch
-// grows to the budget.
+// at least the width the scratch limit would give; otherwise the Z scratch
+// grows to the limit.
 struct ZSlot {
     void *p;
     size_t w;
@@ -810,7 +810,7 @@ struct ZSlot {
 static int z_slot(void **zbuf, size_t *zhave, void *spare, size_t spare_n, size_t per_col, int ncols, ZSlot *out)
 {
     const size_t need = ((size_t)ncols + kMixCols - 1) / kMixCols * kMixCols;
-    const size_t wb = std::min(need, std::max<size_t>(kMixCols, (scratch_budget() / per_col) / kMixCols * kMixCols));
+    const size_t wb = std::min(need, std::max<size_t>(kMixCols, (scratch_limit() / per_col) / kMixCols * kMixCols));
     const size_t ws = spare ? std::min(need, (spare_n / per_col) / kMixCols * kMixCols) : 0;
     if (ws >= wb) { *out = ZSlot{spare, ws}; return BSIM_OK; }
     const int rc = ensure(zbuf, zhave, per_col * wb);

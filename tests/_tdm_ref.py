@@ -118,12 +118,13 @@ def grads_from_plan(tab, kind, idx, coef):
     return g
 
 
-def emulate_device(astr, bstr, l, r, norb, kind, idx, coef, hole_table):
+def emulate_device(astr, bstr, l, r, norb, kind, idx, coef, hole_table, tables_out=None):
     """The arithmetic of the library's density kernels (pooldensity.cu), restated in numpy
     on the library's own hole tables (hole_table(strs, norb, holes) -> (nh, table) with
     entries (index << 1) | sign or -1): Tab as C[p n + r][q n + s], the same-spin tables
     as C2[pq][rs] = <a+_p a+_q a_s a_r> (p > q, r > s), D1 from Tab's traces, then
-    grads = coef (X[dagger] - X[idx]) with 0 for kind 0 and NaN for kind -1."""
+    grads = coef (X[dagger] - X[idx]) with 0 for kind 0 and NaN for kind -1.  tables_out
+    (a dict), when given, receives lt, rt, C, C2a, C2b."""
     n = norb
     nA, nB = len(astr), len(bstr)
     E = eps_frame(astr, bstr)
@@ -153,6 +154,8 @@ def emulate_device(astr, bstr, l, r, norb, kind, idx, coef, hole_table):
         A = (s2[:, :, None] * Ml[i2]).transpose(0, 2, 1).reshape(-1, npair)
         B = (s2[:, :, None] * Mr[i2]).transpose(0, 2, 1).reshape(-1, npair)
         C2[spin] = A.T @ B
+    if tables_out is not None:
+        tables_out.update(lt=lt, rt=rt, C=C, C2a=C2[0], C2b=C2[1])
     na_el, nb_el = bin(int(astr[0])).count("1"), bin(int(bstr[0])).count("1")
     D1a = np.array([[sum(C[x * n + k, y * n + k] for k in range(n)) / nb_el for y in range(n)] for x in range(n)])
     D1b = np.array([[sum(C[k * n + x, k * n + y] for k in range(n)) / na_el for y in range(n)] for x in range(n)])

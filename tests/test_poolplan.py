@@ -188,3 +188,30 @@ def test_device_density_arithmetic_matches_oracle(oracle, norb, na, nb):
     ref = oracle.batchgrad(B, oracle.network(pool.network), np.zeros(pool.network.ngs), l, r)
     got = tdm.emulate_device(B.strings(0, 0), B.strings(0, 1), l, r, norb, kind, idx, coef, cuotf.hole_table)
     assert np.abs(got - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("norb,na,nb,sms", [(9, 3, 3, 148), (12, 3, 2, 148), (9, 3, 3, 2)])
+def test_density_kernel_indexing_emulated(oracle, norb, na, nb, sms):
+    """tab_kernel and pair2_kernel emulated thread by thread (launch grid and K splits of
+    the host code, shared-memory fill items, mma.sync m8n8k4 lane fragments, atomic flush
+    addresses; every index bounds-checked) give the density tables.  The cases cover
+    several output tiles, a zero-padded last K slice, K splits of several hole strings per
+    CTA (a GPU of 2 multiprocessors) and split beta ranges."""
+    import _kernel_emu as emu
+    pool = nw.ucc_pool(norb)
+    kind, idx, coef = cuotf.pool_plan(pool.network)
+    B = oracle.basis(norb, na, nb)
+    A, Bs = B.strings(0, 0), B.strings(0, 1)
+    rng = np.random.default_rng(norb + sms)
+    l, r = rng.normal(size=B.dim), rng.normal(size=B.dim)
+    tb = {}
+    tdm.emulate_device(A, Bs, l, r, norb, kind, idx, coef, cuotf.hole_table, tables_out=tb)
+    _, tA = cuotf.hole_table(A, norb, 1)
+    _, tB = cuotf.hole_table(Bs, norb, 1)
+    C = emu.tab(norb, len(Bs), tA, tB, tb["lt"], tb["rt"], sms=sms)
+    assert np.abs(C - tb["C"]).max() <= 1e-13 * np.abs(tb["C"]).max()
+    for spin, strs in ((0, A), (1, Bs)):
+        _, t2 = cuotf.hole_table(strs, norb, 2)
+        C2 = emu.pair2(norb, len(A), len(Bs), t2, tb["lt"], tb["rt"], spin, sms=sms)
+        ref = tb["C2a" if spin == 0 else "C2b"]
+        assert np.abs(C2 - ref).max() <= 1e-13 * np.abs(ref).max()

@@ -880,6 +880,21 @@ def gpu_adapt(args):
         out["a"] = f.energy_grad(op_idx, param_idx, th, ref_idx, ref_val, lv, rv, ckpt_every=cfg["ckpt"])
     ms_adj = timed_events(adjoint, steps, 1)
     E, ga, _ = out["a"]
+    density = None
+    if args.pool_density:   # the transition-density pool gradient beside the pair-list one
+        t0 = time.time()
+        pd = cuotf.PoolDensity(B, pool.network)
+        plan_s = time.time() - t0
+        grads_d = torch.empty_like(grads)
+        ms_pd = timed_events(lambda: pd.grad(psi, hpsi, grads_d), steps, 1)
+        f.batchgrad(psi, hpsi, grads, zeros)
+        torch.cuda.synchronize()
+        a_, b_ = grads_d.cpu().numpy(), grads.cpu().numpy()
+        density = {"ms": ms_pd, "pair_list_ms": ms_bg, "plan_s": plan_s,
+                   "general_groups": int((pd.kind < 0).sum()),
+                   "max_abs_diff_vs_pair_list": float(np.nanmax(np.abs(a_ - b_))),
+                   "max_abs_grad": float(np.abs(b_).max())}
+        del pd
     res = {
         "metric": ADAPT_METRIC, "value": len(pool.components) / (ms * 1e-3), "unit": "generators/s", "n_gpus": 1,
         "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "replicas",
@@ -900,6 +915,8 @@ def gpu_adapt(args):
         "gpu_launches": launches * steps if launches is not None else None,
         "clocks": clk.summary(),
     }
+    if density is not None:
+        res["pool_density"] = density
     if not args.no_cpu_baseline:
         cpu = run_cpu_adapt(args, ham, pool, psi.cpu().numpy(), hpsi.cpu().numpy(), grads.cpu().numpy())
         if cpu and "seconds" in cpu:
@@ -1081,6 +1098,8 @@ def main():
     ap.add_argument("--adapt-state", default="")
     ap.add_argument("--adapt-sample", type=int, default=400)
     ap.add_argument("--adapt-norb", type=int, default=ADAPT_CFG["norb"])
+    ap.add_argument("--pool-density", action="store_true",
+                    help="adapt: also time the transition-density pool gradient and compare it with the pair lists")
     ap.add_argument("--dav-size", default="12o", choices=sorted(DAV_CFGS))
     ap.add_argument("--sigma-size", default="16o", choices=sorted(SIGMA_CFGS))
     ap.add_argument("--dav-oracle", action="store_true")

@@ -283,7 +283,7 @@ int bsim_poolplan_classify(int64_t norb, int64_t ngs, const uint64_t *axs, const
  * least one electron of each spin).  bsim_pooldensity_create takes a basis handle
  * and the host arrays of bsim_poolplan_classify (idx as 4 int32 per group) and
  * allocates the hole tables and the table scratch (2 dim + (norb^2)^2 doubles and
- * more); bsim_pooldensity_grad writes grads[g] = coef[g] (X[dagger(i)] - X[i]) for
+ * more); the basis handle must outlive the plan.  bsim_pooldensity_grad writes grads[g] = coef[g] (X[dagger(i)] - X[i]) for
  * every group on device vectors l, r (0 for BSIM_POOL_ZERO, NaN for
  * BSIM_POOL_GENERAL groups, whose gradient the pair-list call gives).
  * bsim_pooldensity_hole_table (host) lists the hole strings of a string list in

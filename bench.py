@@ -890,7 +890,18 @@ def gpu_adapt(args):
         f.batchgrad(psi, hpsi, grads, zeros)
         torch.cuda.synchronize()
         a_, b_ = grads_d.cpu().numpy(), grads.cpu().numpy()
-        density = {"ms": ms_pd, "pair_list_ms": ms_bg, "plan_s": plan_s,
+        # GEMM flops as launched: Tab (n^2 x n^2 over one-hole alpha x beta strings) and the
+        # two same-spin tables (pairs x pairs over two-hole strings x the other spin's strings)
+        from math import comb
+        n_, na_, nb_ = cfg["norb"], cfg["na"], cfg["nb"]
+        npair = n_ * (n_ - 1) // 2
+        flops = 2.0 * (n_ * n_) ** 2 * comb(n_, na_ - 1) * comb(n_, nb_ - 1)
+        flops += 2.0 * npair ** 2 * (comb(n_, na_ - 2) * comb(n_, nb_) if na_ >= 2 else 0)
+        flops += 2.0 * npair ** 2 * (comb(n_, nb_ - 2) * comb(n_, na_) if nb_ >= 2 else 0)
+        dmma = cuotf.fma_peak(dmma=True)
+        density = {"ms": ms_pd, "pair_list_ms": ms_bg, "plan_s": plan_s, "gemm_flops": flops,
+                   "tflops": flops / (ms_pd * 1e-3) / 1e12, "fp64_dmma_peak_tflops": dmma,
+                   "frac_of_measured_dmma_peak": flops / (ms_pd * 1e-3) / 1e12 / dmma,
                    "general_groups": int((pd.kind < 0).sum()),
                    "max_abs_diff_vs_pair_list": float(np.nanmax(np.abs(a_ - b_))),
                    "max_abs_grad": float(np.abs(b_).max())}

@@ -337,9 +337,14 @@ def ref_available() -> bool:
                ("libotf_native.so", "libbasis.so", "libdiag.so", "libham_real.so"))
 
 
+def ref_u64_available() -> bool:
+    """The reference's uint64 basis interface (ref_basis_ui64.cpp) next to its libraries."""
+    return ref_available() and os.path.exists(os.path.join(REF_DIR, "libbasis_ui64.so"))
+
+
 def build_ref() -> bool:
     """Compile oracle/_ref from the reference sources when they are present."""
-    if ref_available():
+    if ref_u64_available():
         return True
     if not os.path.isdir("/root/reference/src/include"):
         return False
@@ -643,3 +648,95 @@ class RefLibs:
         xt = np.empty(N)
         d.build_ritz_vector_f64(N, dim, P(coeffs), Vp, P(xt))
         return e_best, xt, maxiter, nsig
+
+
+class RefLibsU64:
+    """The reference's uint64 operators (the _ui64_f64 exports of libotf_native,
+    src/extern/otf_native.cpp:5) over a BasisManager<uint64> from the reference's own
+    basis interface instantiated for uint64 (ref_basis_ui64.cpp).  The reference's
+    dense string map (basis.hpp:271) limits this to small norb."""
+
+    def __init__(self, ref: "RefLibs"):
+        if not ref_u64_available():
+            raise RuntimeError("oracle/_ref/libbasis_ui64.so is not built")
+        self.otf = ref.otf
+        self.bas = C.CDLL(os.path.join(REF_DIR, "libbasis_ui64.so"))
+        self.bas.create_basis_manager_ui64.restype = vp
+        self.bas.create_basis_manager_ui64.argtypes = [i64, i64, i64, i64, vp, i64]
+        self.bas.get_subspace_dim_ui64.restype = i64
+        self.bas.get_subspace_dim_ui64.argtypes = [vp]
+        self.bas.destroy_basis_manager_ui64.argtypes = [vp]
+        o = self.otf
+        o.build_network_otf_ui64_f64.restype = vp
+        o.build_network_otf_ui64_f64.argtypes = [vp, i64, i64] + [vp] * 9
+        o.destroy_network_otf_ui64_f64.argtypes = [vp]
+        o.hvec_gather_contract_otf_ui64_f64.argtypes = [vp, vp, vp, vp]
+        o.get_diags_elements_ui64_f64.argtypes = [vp, vp, vp]
+        o.expm_contract_otf_ui64_f64.argtypes = [vp, vp, i64, dbl, vp]
+        o.grad_contract_otf_ui64_f64.restype = dbl
+        o.grad_contract_otf_ui64_f64.argtypes = [vp, vp, i64, dbl, vp, vp]
+        o.backgrad_contract_otf_ui64_f64.restype = dbl
+        o.backgrad_contract_otf_ui64_f64.argtypes = [vp, vp, i64, dbl, vp, vp]
+        o.batch_grad_contract_otf_ui64_f64.argtypes = [vp, vp, vp, vp, vp, vp]
+        o.tvec_contract_otf_ui64_f64.argtypes = [vp, vp, i64, vp, vp]
+        o.batch_tran_contract_otf_ui64_f64.argtypes = [vp, vp, vp, vp, vp]
+        self._keep = []
+
+    def basis(self, norb, na, nb, orbsym=None, total_sym=0, num_irreps=16):
+        orbsym = np.zeros(norb, np.int64) if orbsym is None else np.ascontiguousarray(orbsym, np.int64)
+        h = self.bas.create_basis_manager_ui64(norb, na, nb, total_sym, P(orbsym), num_irreps)
+        self._keep.append(orbsym)
+        return h, self.bas.get_subspace_dim_ui64(h)
+
+    def network(self, net):
+        a = [np.ascontiguousarray(net.orbsym, np.int64)]
+        arrs = [np.ascontiguousarray(net.axs, np.uint64), np.ascontiguousarray(net.bxs, np.uint64),
+                np.ascontiguousarray(net.ranks, np.int64), np.ascontiguousarray(net.num_zas, np.int64),
+                np.ascontiguousarray(net.num_zbs, np.int64), np.ascontiguousarray(net.flat_zas, np.uint64),
+                np.ascontiguousarray(net.flat_zbs, np.uint64), np.ascontiguousarray(net.flat_wa, np.float64),
+                np.ascontiguousarray(net.flat_wb, np.float64)]
+        h = self.otf.build_network_otf_ui64_f64(P(a[0]), net.norb, net.ngs, *[P(x) for x in arrs])
+        self._keep.append((a, arrs))
+        return h
+
+    def hvec(self, b, n, x, dim):
+        y = np.zeros(dim)
+        self.otf.hvec_gather_contract_otf_ui64_f64(b, n, P(np.ascontiguousarray(x, np.float64)), P(y))
+        return y
+
+    def diag_elems(self, b, n, dim):
+        d = np.zeros(dim)
+        self.otf.get_diags_elements_ui64_f64(b, n, P(d))
+        return d
+
+    def expm(self, b, n, idx, theta, v):
+        v = np.array(v, np.float64, copy=True)
+        self.otf.expm_contract_otf_ui64_f64(b, n, idx, theta, P(v))
+        return v
+
+    def grad(self, b, n, idx, theta, l, r):
+        return self.otf.grad_contract_otf_ui64_f64(b, n, idx, theta, P(np.ascontiguousarray(l, np.float64)),
+                                                   P(np.ascontiguousarray(r, np.float64)))
+
+    def backgrad(self, b, n, idx, theta, l, r):
+        l = np.array(l, np.float64, copy=True); r = np.array(r, np.float64, copy=True)
+        g = self.otf.backgrad_contract_otf_ui64_f64(b, n, idx, theta, P(l), P(r))
+        return g, l, r
+
+    def batchgrad(self, b, n, thetas, l, r, ngs):
+        g = np.zeros(ngs)
+        self.otf.batch_grad_contract_otf_ui64_f64(b, n, P(np.ascontiguousarray(thetas, np.float64)),
+                                                  P(np.ascontiguousarray(l, np.float64)),
+                                                  P(np.ascontiguousarray(r, np.float64)), P(g))
+        return g
+
+    def tvec(self, b, n, idx, src, dim):
+        dst = np.zeros(dim)
+        self.otf.tvec_contract_otf_ui64_f64(b, n, idx, P(np.ascontiguousarray(src, np.float64)), P(dst))
+        return dst
+
+    def batchtran(self, b, n, l, r, ngs):
+        t = np.zeros(ngs)
+        self.otf.batch_tran_contract_otf_ui64_f64(b, n, P(np.ascontiguousarray(l, np.float64)),
+                                                  P(np.ascontiguousarray(r, np.float64)), P(t))
+        return t

@@ -207,3 +207,50 @@ def test_oracle_c64_ops_match_reference_libs(oracle, reflibs, norb, na, nb, orbs
         np.testing.assert_allclose(oracle.batchgrad_c64(B, N, th, x, y), gr, atol=1e-10 * max(1.0, np.abs(gr).max()))
         tr = reflibs.batchtran_c64(rb, rn, x, y, net.ngs)
         np.testing.assert_allclose(oracle.batchtran_c64(B, N, x, y), tr, atol=1e-10 * max(1.0, np.abs(tr).max()))
+
+
+@pytest.mark.parametrize("norb,na,nb,orbsym,tsym", [
+    (8, 4, 3, None, 0),
+    (7, 3, 3, [0, 1, 2, 3, 0, 1, 2], 2),
+])
+def test_oracle_matches_reference_ui64_operators(oracle, reflibs, norb, na, nb, orbsym, tsym):
+    """The reference's uint64 operators (_ui64_f64, over its basis interface instantiated
+    for uint64) against the oracle, which keeps every string as a 64-bit word: sigma,
+    diagonal, expm, grad, backgrad, batch grad, tvec and batch tran."""
+    from oracle.oracle import RefLibsU64, ref_u64_available
+    from binsim_b200 import network as nw
+    if not ref_u64_available():
+        pytest.skip("oracle/_ref/libbasis_ui64.so not built")
+    ref = RefLibsU64(reflibs)
+    osym = np.zeros(norb, np.int64) if orbsym is None else np.asarray(orbsym, np.int64)
+    ham = nw.hamiltonian_network(norb, seed=norb * 5 + 2)
+    pool = nw.ucc_pool(norb).network
+    ham.orbsym = osym; pool.orbsym = osym
+    rb, dim = ref.basis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
+    B = oracle.basis(norb, na, nb, orbsym=osym, total_sym=tsym, num_irreps=4)
+    assert B.dim == dim
+    rh, rp = ref.network(ham), ref.network(pool)
+    H, Pn = oracle.network(ham), oracle.network(pool)
+    rng = np.random.default_rng(norb + 100)
+    x, y = rng.normal(size=dim), rng.normal(size=dim)
+    s = ref.hvec(rb, rh, x, dim)
+    np.testing.assert_allclose(oracle.hvec(B, H, x), s, rtol=0, atol=TOL * np.abs(s).max())
+    d = ref.diag_elems(rb, rh, dim)
+    np.testing.assert_allclose(oracle.diag(B, H), d, rtol=0, atol=TOL * np.abs(d).max())
+    for i in rng.choice(pool.ngs, 8, replace=False):
+        t = rng.normal(0, 0.7)
+        np.testing.assert_allclose(oracle.expm(B, Pn, int(i), t, x), ref.expm(rb, rp, int(i), t, x), rtol=0,
+                                   atol=1e-13)
+        assert abs(oracle.grad(B, Pn, int(i), t, x, y) - ref.grad(rb, rp, int(i), t, x, y)) < 1e-12
+        g1, l1, r1 = oracle.backgrad(B, Pn, int(i), t, x, y)
+        g2, l2, r2 = ref.backgrad(rb, rp, int(i), t, x, y)
+        assert abs(g1 - g2) < 1e-12
+        np.testing.assert_allclose(l1, l2, rtol=0, atol=1e-13)
+        np.testing.assert_allclose(r1, r2, rtol=0, atol=1e-13)
+        np.testing.assert_allclose(oracle.tvec(B, Pn, int(i), x), ref.tvec(rb, rp, int(i), x, dim), rtol=0,
+                                   atol=1e-13)
+    th = rng.normal(0, 0.3, size=pool.ngs)
+    bg = ref.batchgrad(rb, rp, th, x, y, pool.ngs)
+    np.testing.assert_allclose(oracle.batchgrad(B, Pn, th, x, y), bg, rtol=0, atol=TOL * np.abs(bg).max())
+    bt = ref.batchtran(rb, rp, x, y, pool.ngs)
+    np.testing.assert_allclose(oracle.batchtran(B, Pn, x, y), bt, rtol=0, atol=TOL * np.abs(bt).max())

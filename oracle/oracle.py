@@ -740,3 +740,37 @@ class RefLibsU64:
         self.otf.batch_tran_contract_otf_ui64_f64(b, n, P(np.ascontiguousarray(l, np.float64)),
                                                   P(np.ascontiguousarray(r, np.float64)), P(t))
         return t
+
+    def complex_view(self, ref: "RefLibs"):
+        """A RefLibs whose basis is the uint64 one and whose _c64 operators call the
+        reference's _ui64_c64 exports (otf_native.cpp:6), masks passed as uint64."""
+        import copy
+        o = self.otf
+        for name in ("build_network_otf", "destroy_network_otf", "hvec_gather_contract_otf", "get_diags_elements",
+                     "expm_contract_otf", "grad_contract_otf", "backgrad_contract_otf", "tvec_contract_otf",
+                     "backtran_contract_otf", "batch_expm_contract_otf", "batch_grad_contract_otf",
+                     "batch_tran_contract_otf"):
+            src, dst = getattr(o, name + "_c64"), getattr(o, name + "_ui64_c64")
+            dst.argtypes, dst.restype = src.argtypes, src.restype
+
+        class _Suffix:
+            def __getattr__(_, name):
+                return getattr(o, name[:-4] + "_ui64_c64") if name.endswith("_c64") else getattr(o, name)
+
+        view = copy.copy(ref)
+        view.otf = _Suffix()
+        view.basis = self.basis
+        keep = self._keep
+
+        def network_c64(net, wa, wb):
+            a = [np.ascontiguousarray(net.orbsym, np.int64)]
+            arrs = [np.ascontiguousarray(net.axs, np.uint64), np.ascontiguousarray(net.bxs, np.uint64),
+                    np.ascontiguousarray(net.ranks, np.int64), np.ascontiguousarray(net.num_zas, np.int64),
+                    np.ascontiguousarray(net.num_zbs, np.int64), np.ascontiguousarray(net.flat_zas, np.uint64),
+                    np.ascontiguousarray(net.flat_zbs, np.uint64), np.ascontiguousarray(wa, np.complex128),
+                    np.ascontiguousarray(wb, np.complex128)]
+            h = o.build_network_otf_ui64_c64(P(a[0]), net.norb, net.ngs, *[P(x) for x in arrs])
+            keep.append((a, arrs))
+            return h
+        view.network_c64 = network_c64
+        return view

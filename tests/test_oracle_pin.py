@@ -254,3 +254,17 @@ def test_oracle_matches_reference_ui64_operators(oracle, reflibs, norb, na, nb, 
     np.testing.assert_allclose(oracle.batchgrad(B, Pn, th, x, y), bg, rtol=0, atol=TOL * np.abs(bg).max())
     bt = ref.batchtran(rb, rp, x, y, pool.ngs)
     np.testing.assert_allclose(oracle.batchtran(B, Pn, x, y), bt, rtol=0, atol=TOL * np.abs(bt).max())
+
+
+@pytest.mark.parametrize("norb,na,nb,orbsym,tsym", [
+    (6, 3, 2, None, 0),
+    (7, 3, 3, [0, 1, 2, 3, 0, 1, 2], 2),
+])
+def test_oracle_c64_matches_reference_ui64_c64_operators(oracle, reflibs, norb, na, nb, orbsym, tsym):
+    """The complex restatement against the reference's uint64 complex operators
+    (_ui64_c64): the checks of the uint32 complex pin, on the uint64 basis."""
+    from oracle.oracle import RefLibsU64, ref_u64_available
+    if not ref_u64_available():
+        pytest.skip("oracle/_ref/libbasis_ui64.so not built")
+    view = RefLibsU64(reflibs).complex_view(reflibs)
+    test_oracle_c64_ops_match_reference_libs(oracle, view, norb, na, nb, orbsym, tsym)

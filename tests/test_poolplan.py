@@ -128,14 +128,12 @@ def test_plan_beyond_32_orbitals():
 
 
 def test_plan_argument_checks():
-    import ctypes as C
     L = cuotf.lib()
     z = np.zeros(4, np.int64)
     assert L.bsim_poolplan_classify(4, 0, *([None] * 12)) == 0
     assert L.bsim_poolplan_classify(4, 1, *([None] * 12)) == -1
     assert L.bsim_poolplan_classify(65, 1, *([z.ctypes.data] * 12)) == -2
     assert L.bsim_poolplan_classify(4, -1, *([z.ctypes.data] * 12)) == -2
-    del C
 
 
 @pytest.mark.parametrize("norb,ne,holes", [(6, 3, 1), (6, 3, 2), (7, 2, 2), (9, 4, 1), (40, 3, 2)])

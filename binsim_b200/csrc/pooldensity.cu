@@ -1,4 +1,6 @@
-// Pool gradient at theta = 0 through transition densities (single-block bases).
+// Pool gradient at theta = 0 through transition densities.  A symmetry-blocked
+// basis is embedded in the dense [all alpha strings x all beta strings] arrays
+// (zeros outside the basis), on which the single-block computation below is exact.
 //
 // For the groups that bsim_poolplan_classify recognises as coef * (t - t^dagger),
 // t one excitation with at most two creators and two annihilators, the gradient
@@ -72,6 +74,26 @@ __global__ void frame_pair_kernel(int nB, const Ti *__restrict__ astr, const Ti 
     const bool neg = __popcll((u64)bstr[b] & k) & 1;
     lt[i] = neg ? -l[i] : l[i];
     rt[i] = neg ? -r[i] : r[i];
+}
+
+// Blocked bases: block k's part of l and r (its alpha and beta string lists, at
+// offset off) scattered with the frame sign into the dense [all alpha strings x
+// all beta strings] arrays lt, rt (zeroed before; determinants outside the basis
+// stay zero).  gA, gB: each block-list string's index in the union lists.
+// grid (nAk, ceil(nBk / 256))
+template <typename Ti>
+__global__ void embed_frame_kernel(int nBk, int nBall, const Ti *__restrict__ astr, const Ti *__restrict__ bstr,
+                                   const int *__restrict__ gA, const int *__restrict__ gB,
+                                   const double *__restrict__ l, const double *__restrict__ r, double *__restrict__ lt,
+                                   double *__restrict__ rt)
+{
+    const int a = blockIdx.x, b = blockIdx.y * blockDim.x + threadIdx.x;
+    if (b >= nBk) return;
+    const u64 k = kmask(astr[a]);
+    const i64 i = (i64)a * nBk + b, o = (i64)gA[a] * nBall + gB[b];
+    const bool neg = __popcll((u64)bstr[b] & k) & 1;
+    lt[o] = neg ? -l[i] : l[i];
+    rt[o] = neg ? -r[i] : r[i];
 }
 
 // Accumulator of one 64 x 128 tile of C = A^T B: each step multiplies a 32-row K
@@ -327,6 +349,10 @@ struct PoolDensity {
     int n = 0, nA = 0, nB = 0, nel_a = 0, nel_b = 0;
     int nHa = 0, nHb = 0, nH2a = 0, nH2b = 0, npair = 0;
     i64 ngs = 0;
+    bool embed = false;                  // blocked basis: scatter into the union-string arrays
+    std::vector<int> blk_na, blk_nb, blk_as, blk_bs;
+    std::vector<i64> blk_off;
+    int *gA = nullptr, *gB = nullptr;    // [astrs.size()], [bstrs.size()]: union index of each block-list string
     Arena arena;
     int *idxA = nullptr, *idxB = nullptr, *idx2A = nullptr, *idx2B = nullptr, *kind = nullptr;
     int4 *idx = nullptr;
@@ -389,16 +415,25 @@ template <typename Ti>
 int density_create(DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t *idx, const double *coef,
                    PoolDensity **out)
 {
-    if (B->num_blocks != 1) {
-        set_error("pool density gradient: the basis has %d symmetry blocks (one is supported)", B->num_blocks);
-        return BSIM_ERR_UNSUPPORTED;
-    }
-    const int n = B->norb, nA = B->na[0], nB = B->nb[0];
     if (B->nel_a < 1 || B->nel_b < 1) {
         set_error("pool density gradient: needs at least one electron of each spin");
         return BSIM_ERR_UNSUPPORTED;
     }
-    if ((i64)nA >= (1 << 30) || (i64)nB >= (1 << 30) || (nB + 255) / 256 > 65535) return BSIM_ERR_TOO_LARGE;
+    const int n = B->norb, nbk = B->num_blocks;
+    // union string lists (increasing); for one block they are the block's lists
+    std::vector<Ti> as, bs;
+    for (int k = 0; k < nbk; ++k) {
+        as.insert(as.end(), B->astrs.begin() + B->astart[k], B->astrs.begin() + B->astart[k] + B->na[k]);
+        bs.insert(bs.end(), B->bstrs.begin() + B->bstart[k], B->bstrs.begin() + B->bstart[k] + B->nb[k]);
+    }
+    std::sort(as.begin(), as.end());
+    as.erase(std::unique(as.begin(), as.end()), as.end());
+    std::sort(bs.begin(), bs.end());
+    bs.erase(std::unique(bs.begin(), bs.end()), bs.end());
+    const int nA = (int)as.size(), nB = (int)bs.size();
+    if (as.size() >= (1u << 30) || bs.size() >= (1u << 30) || (nB + 255) / 256 > 65535) return BSIM_ERR_TOO_LARGE;
+    for (int k = 0; k < nbk; ++k)
+        if ((B->nb[k] + 255) / 256 > 65535) return BSIM_ERR_TOO_LARGE;
     for (i64 g = 0; g < ngs; ++g) {   // the assembly reads tables at these orbitals
         if (kind[g] < BSIM_POOL_GENERAL || kind[g] > BSIM_POOL_GBB) {
             set_error("pool density gradient: group %lld has kind %d", (long long)g, (int)kind[g]);
@@ -412,8 +447,15 @@ int density_create(DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t 
                     return BSIM_ERR_ARG;
                 }
     }
-    std::vector<Ti> as(B->astrs.begin() + B->astart[0], B->astrs.begin() + B->astart[0] + nA);
-    std::vector<Ti> bs(B->bstrs.begin() + B->bstart[0], B->bstrs.begin() + B->bstart[0] + nB);
+    std::vector<int> gA(B->astrs.size(), 0), gB(B->bstrs.size(), 0);
+    for (int k = 0; k < nbk; ++k) {
+        for (int i = 0; i < B->na[k]; ++i)
+            gA[B->astart[k] + i] =
+                (int)(std::lower_bound(as.begin(), as.end(), B->astrs[B->astart[k] + i]) - as.begin());
+        for (int i = 0; i < B->nb[k]; ++i)
+            gB[B->bstart[k] + i] =
+                (int)(std::lower_bound(bs.begin(), bs.end(), B->bstrs[B->bstart[k] + i]) - bs.begin());
+    }
     std::vector<u64> hA, hB, h2A, h2B;
     std::vector<int> tA, tB, t2A, t2B;
     int st;
@@ -428,8 +470,15 @@ int density_create(DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t 
     P->nHa = (int)hA.size(); P->nHb = (int)hB.size(); P->nH2a = (int)h2A.size(); P->nH2b = (int)h2B.size();
     P->npair = n * (n - 1) / 2;
     P->ngs = ngs;
+    P->embed = nbk > 1;
+    for (int k = 0; k < nbk; ++k) {
+        P->blk_na.push_back(B->na[k]); P->blk_nb.push_back(B->nb[k]);
+        P->blk_as.push_back(B->astart[k]); P->blk_bs.push_back(B->bstart[k]);
+        P->blk_off.push_back(B->off[k]);
+    }
     const i64 dim = (i64)nA * nB, M = (i64)n * n, np2 = (i64)P->npair * P->npair;
-    const size_t bytes = 256 * 16 + sizeof(int) * (tA.size() + tB.size() + t2A.size() + t2B.size() + ngs) +
+    const size_t bytes = 256 * 18 + sizeof(int) * (tA.size() + tB.size() + t2A.size() + t2B.size() + ngs) +
+                         sizeof(int) * (gA.size() + gB.size()) +
                          sizeof(int4) * ngs + sizeof(double) * (ngs + 2 * dim + M * M + 2 * np2 + 2 * M);
     if ((st = P->arena.reserve(bytes)) != BSIM_OK) { delete P; return st; }
     P->idxA = P->arena.take<int>(tA.size());
@@ -446,6 +495,8 @@ int density_create(DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t 
     P->C2b = P->arena.take<double>(np2);
     P->D1a = P->arena.take<double>(M);
     P->D1b = P->arena.take<double>(M);
+    P->gA = P->arena.take<int>(gA.size());
+    P->gB = P->arena.take<int>(gB.size());
     auto up = [&](void *d, const void *h, size_t nb) { return nb ? cudaMemcpy(d, h, nb, cudaMemcpyHostToDevice) : cudaSuccess; };
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = up(P->idxA, tA.data(), sizeof(int) * tA.size());
@@ -455,6 +506,8 @@ int density_create(DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t 
     if (e == cudaSuccess) e = up(P->kind, kind, sizeof(int) * ngs);
     if (e == cudaSuccess) e = up(P->idx, idx, sizeof(int4) * ngs);
     if (e == cudaSuccess) e = up(P->coef, coef, sizeof(double) * ngs);
+    if (e == cudaSuccess) e = up(P->gA, gA.data(), sizeof(int) * gA.size());
+    if (e == cudaSuccess) e = up(P->gB, gB.data(), sizeof(int) * gB.size());
     if (e != cudaSuccess) { delete P; return cuda_status(e, "pool density upload"); }
     *out = P;
     return BSIM_OK;
@@ -466,10 +519,21 @@ int density_grad(PoolDensity *P, const double *l, const double *r, double *grads
     const auto *B = static_cast<const DevBasis<Ti> *>(P->basis);
     const int n = P->n, nA = P->nA, nB = P->nB;
     const i64 M = (i64)n * n, np2 = (i64)P->npair * P->npair;
-    {
+    if (!P->embed) {
         dim3 g(nA, (nB + 255) / 256);
         frame_pair_kernel<Ti><<<g, 256, 0, s>>>(nB, B->view.astrs + B->astart[0], B->view.bstrs + B->bstart[0], l, r,
                                                 P->lt, P->rt);
+    } else {
+        BSIM_CUDA(cudaMemsetAsync(P->lt, 0, sizeof(double) * (i64)nA * nB, s));
+        BSIM_CUDA(cudaMemsetAsync(P->rt, 0, sizeof(double) * (i64)nA * nB, s));
+        for (size_t k = 0; k < P->blk_na.size(); ++k) {
+            const int nak = P->blk_na[k], nbk = P->blk_nb[k];
+            if (nak == 0 || nbk == 0) continue;
+            dim3 g(nak, (nbk + 255) / 256);
+            embed_frame_kernel<Ti><<<g, 256, 0, s>>>(nbk, nB, B->view.astrs + P->blk_as[k], B->view.bstrs + P->blk_bs[k],
+                                                     P->gA + P->blk_as[k], P->gB + P->blk_bs[k], l + P->blk_off[k],
+                                                     r + P->blk_off[k], P->lt, P->rt);
+        }
     }
     BSIM_CUDA(cudaMemsetAsync(P->C, 0, sizeof(double) * M * M, s));
     BSIM_CUDA(cudaMemsetAsync(P->C2a, 0, sizeof(double) * np2, s));

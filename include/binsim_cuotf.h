@@ -279,18 +279,20 @@ int bsim_poolplan_classify(int64_t norb, int64_t ngs, const uint64_t *axs, const
                            const int64_t *ranks, const int64_t *num_zas, const int64_t *num_zbs,
                            const uint64_t *flat_zas, const uint64_t *flat_zbs, const double *flat_wa,
                            const double *flat_wb, int32_t *kind, int32_t *idx, double *coef);
-/* The transition densities of the pool plan on the GPU (single-block bases with at
- * least one electron of each spin).  bsim_pooldensity_create takes a basis handle
- * and the host arrays of bsim_poolplan_classify (idx as 4 int32 per group) and
- * allocates the hole tables and the table scratch (2 dim + (norb^2)^2 doubles and
- * more); the basis handle must outlive the plan.  bsim_pooldensity_grad writes grads[g] = coef[g] (X[dagger(i)] - X[i]) for
- * every group on device vectors l, r (0 for BSIM_POOL_ZERO, NaN for
- * BSIM_POOL_GENERAL groups, whose gradient the pair-list call gives).
- * bsim_pooldensity_hole_table (host) lists the hole strings of a string list in
- * increasing order and, per hole string h and created orbital (holes = 1: p;
- * holes = 2: the pair x > y at x (x - 1) / 2 + y, created as a+_x a+_y |h>), the
- * entry (index of the created string << 1) | creation sign, or -1; table may be
- * NULL to get *nh only. */
+/* The transition densities of the pool plan on the GPU (bases with at least one
+ * electron of each spin; a symmetry-blocked basis is computed in the dense array
+ * over all alpha and beta strings, without a saving from its symmetry).
+ * bsim_pooldensity_create takes a basis handle and the host arrays of
+ * bsim_poolplan_classify (idx as 4 int32 per group) and allocates the hole tables
+ * and the table scratch (2 x alpha strings x beta strings + (norb^2)^2 doubles and
+ * more); the basis handle must outlive the plan.  bsim_pooldensity_grad writes
+ * grads[g] = coef[g] (X[dagger(i)] - X[i]) for every group on device vectors l, r
+ * (0 for BSIM_POOL_ZERO, NaN for BSIM_POOL_GENERAL groups, whose gradient the
+ * pair-list call gives).  bsim_pooldensity_hole_table (host) lists the hole
+ * strings of a string list in increasing order and, per hole string h and created
+ * orbital (holes = 1: p; holes = 2: the pair x > y at x (x - 1) / 2 + y, created as
+ * a+_x a+_y |h>), the entry (index of the created string << 1) | creation sign,
+ * or -1; table may be NULL to get *nh only. */
 int bsim_pooldensity_hole_table(int64_t norb, int64_t holes, int64_t nstr, const uint64_t *strs, int64_t *nh,
                                 int32_t *table);
 int bsim_pooldensity_create(void *basis, int64_t ngs, const int32_t *kind, const int32_t *idx, const double *coef,

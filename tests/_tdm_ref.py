@@ -189,3 +189,21 @@ def emulate_device(astr, bstr, l, r, norb, kind, idx, coef, hole_table, tables_o
         dag = at(k, i1, i0, 0, 0) if k in (1, 2) else (at(k, i1, i0, i3, i2) if k == 3 else at(k, i3, i2, i1, i0))
         out[g] = c * (dag - fwd)
     return out
+
+
+def embed_blocks(B, v):
+    """A vector of a symmetry-blocked oracle basis as a dense [all alpha strings x all beta
+    strings] array (zeros where the determinant is not in the basis), with the union string
+    lists in increasing order: the layout the density kernels use for blocked bases."""
+    A = np.unique(np.concatenate([B.strings(k, 0) for k in range(B.num_blocks)]))
+    Bs = np.unique(np.concatenate([B.strings(k, 1) for k in range(B.num_blocks)]))
+    ia = {int(s): i for i, s in enumerate(A)}
+    ib = {int(s): i for i, s in enumerate(Bs)}
+    M = np.zeros((len(A), len(Bs)))
+    v = np.asarray(v, float)
+    for k in range(B.num_blocks):
+        na, nb, off = int(B.blocks[k, 2]), int(B.blocks[k, 3]), int(B.blocks[k, 4])
+        ra = [ia[int(s)] for s in B.strings(k, 0)]
+        rb = [ib[int(s)] for s in B.strings(k, 1)]
+        M[np.ix_(ra, rb)] = v[off:off + na * nb].reshape(na, nb)
+    return A, Bs, M

@@ -48,8 +48,21 @@ def test_pooldensity_matches_batchgrad(cuda, norb, na, nb, bits):
     assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
 
 
-def test_pooldensity_rejects_symmetry_blocks(cuda):
-    pool = nw.ucc_pool(6)
-    B = cuotf.CuBasis(6, 3, 3, orbsym=[0, 1, 0, 1, 0, 1], num_irreps=2)
-    with pytest.raises(cuotf.CuOTFError):
-        cuotf.PoolDensity(B, pool.network)
+def test_pooldensity_on_symmetry_blocks(cuda):
+    """A blocked basis runs in the dense array over all alpha and beta strings."""
+    norb, orbsym = 8, [0, 1, 2, 3, 0, 1, 2, 3]
+    pool = nw.ucc_pool(norb)
+    pool.network.orbsym = np.asarray(orbsym, np.int64)
+    B = cuotf.CuBasis(norb, 4, 3, orbsym=orbsym, total_sym=1, num_irreps=4)
+    net = cuotf.CuNetwork(pool.network)
+    f = cuotf.CuOTFFunctions(B, net, net)
+    rng = np.random.default_rng(5)
+    l, r = dev(cuda, rng.normal(size=B.dim)), dev(cuda, rng.normal(size=B.dim))
+    ref = cuda.empty(pool.network.ngs, dtype=cuda.float64, device="cuda")
+    f.batchgrad(l, r, ref, cuda.zeros_like(ref))
+    g = cuda.empty_like(ref)
+    pd = cuotf.PoolDensity(B, pool.network)   # held until the kernels have finished
+    pd.grad(l, r, g)
+    cuda.cuda.synchronize()
+    a, b = g.cpu().numpy(), ref.cpu().numpy()
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()

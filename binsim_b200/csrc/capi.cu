@@ -210,6 +210,7 @@ double backgrad_cuda_2d(void *basis, void *net, int64_t idx, double theta, doubl
 // ============================== Part 2 ======================================
 const char *bsim_last_error(void) { return bsim::last_error(); }
 const char *bsim_version(void) { return "libcuotf sm_100a 0.1"; }
+int64_t bsim_device_alloc_count(void) { return (int64_t)bsim::device_alloc_count(); }
 
 int bsim_basis_create_u32(int64_t norb, int64_t na, int64_t nb, int64_t total_sym, const int64_t *orbsym,
                           int64_t num_irreps, void **out)
@@ -363,8 +364,8 @@ struct HostPipe {
     int init(int64_t dim)
     {
         for (int i = 0; i < 2; ++i) {
-            BSIM_CUDA(cudaMalloc(&in[i], sizeof(double) * std::max<int64_t>(dim, 1)));
-            BSIM_CUDA(cudaMalloc(&out[i], sizeof(double) * std::max<int64_t>(dim, 1)));
+            BSIM_CUDA(bsim::dmalloc(&in[i], sizeof(double) * std::max<int64_t>(dim, 1)));
+            BSIM_CUDA(bsim::dmalloc(&out[i], sizeof(double) * std::max<int64_t>(dim, 1)));
             BSIM_CUDA(cudaEventCreateWithFlags(&in_ready[i], cudaEventDisableTiming));
             BSIM_CUDA(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming));
             BSIM_CUDA(cudaEventCreateWithFlags(&out_read[i], cudaEventDisableTiming));

@@ -35,6 +35,24 @@ void set_error(const char *fmt, ...);
 const char *last_error();
 int cuda_status(cudaError_t e, const char *what);
 
+// Every device allocation of the library goes through dmalloc / dmalloc_async,
+// which count the calls; bsim_device_alloc_count() returns the count, so a
+// caller can check that a stretch of calls allocated nothing.
+void note_device_alloc();
+long long device_alloc_count();
+template <typename T>
+inline cudaError_t dmalloc(T **p, size_t bytes)
+{
+    note_device_alloc();
+    return cudaMalloc(reinterpret_cast<void **>(p), bytes);
+}
+template <typename T>
+inline cudaError_t dmalloc_async(T **p, size_t bytes, cudaStream_t s)
+{
+    note_device_alloc();
+    return cudaMallocAsync(reinterpret_cast<void **>(p), bytes, s);
+}
+
 #define BSIM_CUDA(call)                                              \
     do {                                                             \
         cudaError_t e__ = (call);                                    \

@@ -45,7 +45,7 @@ struct Vec {
     int alloc(size_t bytes)
     {
         reset();
-        cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 1));
+        cudaError_t e = dmalloc(&p, std::max<size_t>(bytes, 1));
         if (e != cudaSuccess) { p = nullptr; return cuda_status(e, "block davidson vector"); }
         return BSIM_OK;
     }
@@ -194,7 +194,7 @@ struct Ctx {
         double y[kMaxSub * kRotMax];
         for (int c = 0; c < ncv; ++c)
             for (int j = 0; j < dim; ++j) y[j + c * dim] = Y[j + (size_t)c * ldy];
-        if (!dY) BSIM_CUDA(cudaMalloc(&dY, sizeof(double) * kMaxSub * kRotMax));
+        if (!dY) BSIM_CUDA(dmalloc(&dY, sizeof(double) * kMaxSub * kRotMax));
         BSIM_CUDA(cudaMemcpyAsync(dY, y, sizeof(double) * dim * ncv, cudaMemcpyHostToDevice, s));
         BSIM_CUDA(cudaStreamSynchronize(s));   // y is a host local
         VP<TV> p{};

@@ -32,7 +32,7 @@ template <typename T>
 int alloc(DevBuf &b, size_t n, cudaStream_t s)
 {
     b.s = s;
-    cudaError_t e = cudaMallocAsync(&b.p, std::max<size_t>(1, n) * sizeof(T), s);
+    cudaError_t e = dmalloc_async(&b.p, std::max<size_t>(1, n) * sizeof(T), s);
     if (e != cudaSuccess) { b.p = nullptr; return cuda_status(e, "davidson buffer"); }
     return BSIM_OK;
 }

@@ -166,9 +166,9 @@ DavScratch::~DavScratch()
 int DavScratch::ensure()
 {
     if (part) return BSIM_OK;
-    cudaError_t e = cudaMalloc(&part, sizeof(double) * kRedCtas * kMaxSub);
+    cudaError_t e = dmalloc(&part, sizeof(double) * kRedCtas * kMaxSub);
     if (e != cudaSuccess) { part = nullptr; return cuda_status(e, "davidson scratch"); }
-    e = cudaMalloc(&res, sizeof(double) * (kMaxSub + 8));
+    e = dmalloc(&res, sizeof(double) * (kMaxSub + 8));
     if (e != cudaSuccess) { res = nullptr; return cuda_status(e, "davidson scratch"); }
     return BSIM_OK;
 }

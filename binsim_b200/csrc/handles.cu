@@ -3,6 +3,7 @@
 #include "refmirror.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstring>
 #include <mutex>
@@ -29,11 +30,15 @@ int cuda_status(cudaError_t e, const char *what)
     return BSIM_ERR_CUDA;
 }
 
+static std::atomic<long long> g_device_allocs{0};
+void note_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
+long long device_alloc_count() { return g_device_allocs.load(std::memory_order_relaxed); }
+
 // ---- arena --------------------------------------------------------------------
 int Arena::reserve(size_t bytes)
 {
     size = bytes + 4096;
-    cudaError_t e = cudaMalloc(&base, size);
+    cudaError_t e = dmalloc(&base, size);
     if (e != cudaSuccess) {
         base = nullptr;
         set_error("device allocation of %zu bytes failed: %s", size, cudaGetErrorString(e));
@@ -58,7 +63,7 @@ int Workspace::tile_table(const std::vector<i64> &pref, const i64 **out)
     if (tiles && pref == tiles_host) { *out = tiles; return BSIM_OK; }
     if (tiles) cudaFree(tiles);
     tiles = nullptr;
-    cudaError_t e = cudaMalloc(&tiles, pref.size() * sizeof(i64));
+    cudaError_t e = dmalloc(&tiles, pref.size() * sizeof(i64));
     if (e != cudaSuccess) { tiles = nullptr; return cuda_status(e, "workspace tile table"); }
     e = cudaMemcpy(tiles, pref.data(), pref.size() * sizeof(i64), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_status(e, "workspace tile table copy");
@@ -74,7 +79,7 @@ int Workspace::f32_buffer(size_t n, float **out)
         if (f32) cudaFree(f32);
         f32 = nullptr;
         f32_n = 0;
-        cudaError_t e = cudaMalloc(&f32, n * sizeof(float));
+        cudaError_t e = dmalloc(&f32, n * sizeof(float));
         if (e != cudaSuccess) { f32 = nullptr; return cuda_status(e, "workspace fp32 buffer"); }
         f32_n = n;
     }
@@ -88,7 +93,7 @@ int Workspace::partials(size_t n, double **out)
         if (part) cudaFree(part);
         part = nullptr;
         part_n = 0;
-        cudaError_t e = cudaMalloc(&part, n * sizeof(double));
+        cudaError_t e = dmalloc(&part, n * sizeof(double));
         if (e != cudaSuccess) { part = nullptr; return cuda_status(e, "workspace partials"); }
         // zeroed once: the tail holds the ticket counter of the last-CTA reductions
         e = cudaMemset(part, 0, n * sizeof(double));

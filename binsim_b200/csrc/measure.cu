@@ -55,7 +55,7 @@ int fma_peak(int mode, double *tflops, cudaStream_t s)
     BSIM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int blocks = sms * 8, threads = 256, iters = 8192;
     void *out = nullptr;
-    BSIM_CUDA(cudaMallocAsync(&out, sizeof(double) * blocks, s));
+    BSIM_CUDA(dmalloc_async(&out, sizeof(double) * blocks, s));
     cudaEvent_t e0, e1;
     BSIM_CUDA(cudaEventCreate(&e0));
     BSIM_CUDA(cudaEventCreate(&e1));

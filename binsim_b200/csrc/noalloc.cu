@@ -84,6 +84,7 @@ extern "C" int bsim_grad_noalloc(void *basis, void *net, int64_t idx, double the
     if (bsim::is_u64_basis(basis)) {   // UInt64 strings
         auto *b = static_cast<bsim::DevBasis<unsigned long long> *>(basis);
         auto *n = static_cast<bsim::DevNet<unsigned long long> *>(net);
+        if (!bsim::valid(b)) { bsim::set_error("invalid basis handle"); return bsim::BSIM_ERR_ARG; }
         if (!bsim::valid(n)) { bsim::set_error("invalid network handle"); return bsim::BSIM_ERR_ARG; }
         return bsim::grad_noalloc(b, n, idx, theta, l, r, out_dev, stream);
     }

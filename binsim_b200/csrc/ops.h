@@ -110,9 +110,11 @@ int pair_list_batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double
 // Pair operator over the precomputed pair lists (single-block bases, rank <= 4).
 // Sets *used = false (and launches nothing) when the row kernel must serve the
 // call.  grad/backgrad write at most max_slots partials before the ticket.
+// may_build = false: use the lists only if they exist already (building them
+// allocates device memory); otherwise leave the call to the row kernel.
 template <typename Ti, int OP>
 int pair_list_launch(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, PairAngles ang, double *l, double *r,
                      double *part, unsigned long long *ticket, i64 max_slots, double *out, bool accumulate,
-                     cudaStream_t s, bool *used);
+                     cudaStream_t s, bool *used, bool may_build = true);
 
 }  // namespace bsim

@@ -152,6 +152,15 @@ int get_pair_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N, PairPlan<Ti> **out
     return BSIM_OK;
 }
 
+// The cached plan of (B, N) if one exists; never builds one (no allocation).
+template <typename Ti>
+PairPlan<Ti> *find_pair_plan(const DevBasis<Ti> *B, const DevNet<Ti> *N)
+{
+    std::lock_guard<std::mutex> lk(g_pair_mu);
+    auto *p = static_cast<PairPlan<Ti> *>(N->pair_state);
+    return (p && p->basis == B && p->basis_dim == B->dim) ? p : nullptr;
+}
+
 struct ListArgs {
     int nB, acnt, bcnt, R, nza, nzb;
     const int2 *alist, *blist;   // nullptr: identity
@@ -452,12 +461,16 @@ pair_list_batchgrad_kernel(const Ti *__restrict__ astrs, const Ti *__restrict__ 
 template <typename Ti, int OP>
 int pair_list_launch(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, PairAngles ang, double *l, double *r,
                      double *part, unsigned long long *ticket, i64 max_slots, double *out, bool accumulate,
-                     cudaStream_t s, bool *used)
+                     cudaStream_t s, bool *used, bool may_build)
 {
     *used = false;
     PairPlan<Ti> *P = nullptr;
-    int st = get_pair_plan(B, N, &P);
-    if (st != BSIM_OK) return st;
+    if (may_build) {
+        int st = get_pair_plan(B, N, &P);
+        if (st != BSIM_OK) return st;
+    } else if (!(P = find_pair_plan(B, N))) {
+        return BSIM_OK;   // no plan yet: the row kernel serves the call
+    }
     const GroupDev &G = N->groups[gidx];
     if (!P->ok || G.rank > kListMaxRank || G.nza > kListMaxZ || G.nzb > kListMaxZ) return BSIM_OK;
     const int4 d = P->desc[gidx];
@@ -507,8 +520,8 @@ int pair_list_batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double
         }
         if (P->bg_state == 1 && !bg.empty()) {
             ts.push_back(ts.back());   // sentinel: tstart[n + 1] for the last group's boundary test
-            BSIM_CUDA(cudaMalloc(&P->d_bg, bg.size() * sizeof(BGroup)));
-            BSIM_CUDA(cudaMalloc(&P->d_tstart, ts.size() * sizeof(i64)));
+            BSIM_CUDA(dmalloc(&P->d_bg, bg.size() * sizeof(BGroup)));
+            BSIM_CUDA(dmalloc(&P->d_tstart, ts.size() * sizeof(i64)));
             BSIM_CUDA(cudaMemcpy(P->d_bg, bg.data(), bg.size() * sizeof(BGroup), cudaMemcpyHostToDevice));
             BSIM_CUDA(cudaMemcpy(P->d_tstart, ts.data(), ts.size() * sizeof(i64), cudaMemcpyHostToDevice));
             P->bg_n = (int)bg.size();
@@ -536,12 +549,12 @@ template int pair_list_batchgrad<unsigned long long>(const DevBasis<unsigned lon
 #define PAIR_LIST_INST(OP)                                                                                   \
     template int pair_list_launch<unsigned, OP>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64,     \
                                                 PairAngles, double *, double *, double *, unsigned long long *, \
-                                                i64, double *, bool, cudaStream_t, bool *);
+                                                i64, double *, bool, cudaStream_t, bool *, bool);
 #define PAIR_LIST_INST64(OP)                                                                                 \
     template int pair_list_launch<unsigned long long, OP>(const DevBasis<unsigned long long> *,                 \
                                                           const DevNet<unsigned long long> *, i64, PairAngles,  \
                                                           double *, double *, double *, unsigned long long *,   \
-                                                          i64, double *, bool, cudaStream_t, bool *);
+                                                          i64, double *, bool, cudaStream_t, bool *, bool);
 PAIR_LIST_INST(kPairExpm)
 PAIR_LIST_INST(kPairGrad)
 PAIR_LIST_INST(kPairBackgrad)

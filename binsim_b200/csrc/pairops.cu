@@ -235,7 +235,10 @@ static int launch_pair(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, Pai
     }
     if constexpr (OP <= kPairBackgrad) {   // the pair-list kernels serve expm, grad, backgrad
         bool used = false;
-        st = pair_list_launch<Ti, OP>(B, N, gidx, ang, l, r, part, ticket, pair_grid(B), out, accumulate, s, &used);
+        // with caller-provided scratch (the no-allocation entry point) the
+        // lists are used only if an earlier call built them
+        st = pair_list_launch<Ti, OP>(B, N, gidx, ang, l, r, part, ticket, pair_grid(B), out, accumulate, s, &used,
+                                      ext_part == nullptr);
         if (st != BSIM_OK || used) return st;
     }
     dim3 grid(B->max_na, B->num_blocks);
@@ -309,7 +312,7 @@ int batchtran(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *l, const
 {
     if (N->ngs == 0) return BSIM_OK;
     double *zeros = nullptr;
-    BSIM_CUDA(cudaMallocAsync(&zeros, sizeof(double) * N->ngs, s));
+    BSIM_CUDA(dmalloc_async(&zeros, sizeof(double) * N->ngs, s));
     cudaError_t e = cudaMemsetAsync(zeros, 0, sizeof(double) * N->ngs, s);
     int st = e == cudaSuccess ? BSIM_OK : cuda_status(e, "batchtran");
     if (st == BSIM_OK) e = cudaMemsetAsync(trans, 0, sizeof(double) * N->ngs, s);

@@ -776,7 +776,7 @@ static int ensure(void **p, size_t *have, size_t bytes)
     if (*p) cudaFree(*p);
     *p = nullptr;
     *have = 0;
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = dmalloc(p, bytes);
     if (e != cudaSuccess) { *p = nullptr; return cuda_status(e, "sigma scratch"); }
     *have = bytes;
     return BSIM_OK;

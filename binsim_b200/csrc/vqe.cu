@@ -30,7 +30,7 @@ struct Buf {
     ~Buf() { if (p) cudaFreeAsync(p, s); }
     int get(size_t bytes, cudaStream_t st) {
         s = st;
-        cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 8), st);
+        cudaError_t e = dmalloc_async(&p, std::max<size_t>(bytes, 8), st);
         if (e != cudaSuccess) { p = nullptr; return cuda_status(e, "vqe buffer"); }
         return BSIM_OK;
     }

@@ -63,6 +63,7 @@ def lib() -> C.CDLL:
         "backgrad_cuda_2d": (dbl, [vp, vp, i64, dbl, vp, vp]),
         # part 2
         "bsim_last_error": (C.c_char_p, []), "bsim_version": (C.c_char_p, []),
+        "bsim_device_alloc_count": (i64, []),
         "bsim_basis_create_u32": (ci, [i64, i64, i64, i64, vp, i64, vp]),
         "bsim_basis_create_u64": (ci, [i64, i64, i64, i64, vp, i64, vp]),
         "bsim_network_create_u64": (ci, [vp, i64, i64] + [vp] * 9 + [vp]),

@@ -99,6 +99,11 @@ enum {
 
 const char *bsim_last_error(void);
 const char *bsim_version(void);
+/* No counterpart in the reference.  Number of device allocations (cudaMalloc /
+ * cudaMallocAsync) the library has made in this process, on any device: a
+ * caller compares two readings to check that the calls between them allocated
+ * nothing. */
+int64_t bsim_device_alloc_count(void);
 
 /* Basis: create_basis_manager's arguments (basis/declare.hpp:24-33). */
 int bsim_basis_create_u32(int64_t norb, int64_t na, int64_t nb, int64_t total_sym, const int64_t *orbsym,

@@ -21,6 +21,21 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
+# Where the reference's sources lie (read-only; only oracle/Makefile compiles
+# them).  The one place this location is read: environment variable
+# BINSIM_REF_SRC, default /root/reference.  oracle/Makefile takes the same
+# variable with the same default.
+REF_SRC = os.environ.get("BINSIM_REF_SRC", "/root/reference")
+
+
+def ref_sources_present() -> bool:
+    """The reference's C++ headers are present (its CPU libraries can be built)."""
+    return os.path.isdir(os.path.join(REF_SRC, "src", "include"))
+
+
+def make_ref(target: str = "ref") -> None:
+    """Run oracle/Makefile's target with this module's reference location."""
+    subprocess.run(["make", "-s", "-C", HERE, target, f"BINSIM_REF_SRC={REF_SRC}"], check=True)
 _lock = threading.Lock()
 
 P = lambda a: a.ctypes.data_as(C.c_void_p)
@@ -346,9 +361,9 @@ def build_ref() -> bool:
     """Compile oracle/_ref from the reference sources when they are present."""
     if ref_u64_available():
         return True
-    if not os.path.isdir("/root/reference/src/include"):
+    if not ref_sources_present():
         return False
-    subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    make_ref("ref")
     return ref_available()
 
 

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 from binsim_b200 import cuotf
+from oracle import oracle as orc
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -55,7 +56,7 @@ def test_legacy_entry_points_do_not_exit_on_bad_handles(capfd):
     assert "hvec_cuda" in err and "grad_cuda" in err
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/src/include"), reason="reference headers absent")
+@pytest.mark.skipif(not orc.ref_sources_present(), reason="reference headers absent")
 def test_host_handle_layout_mirror_matches_reference(tmp_path):
     """refmirror.h reproduces the field offsets of the reference's host objects."""
     prog = r'''
@@ -84,7 +85,7 @@ int main(){
     src = tmp_path / "layout.cpp"
     src.write_text(prog)
     exe = tmp_path / "layout"
-    subprocess.run(["g++", "-std=c++20", "-fopenmp", "-Wno-invalid-offsetof", "-I/root/reference/src/include",
+    subprocess.run(["g++", "-std=c++20", "-fopenmp", "-Wno-invalid-offsetof", "-I" + os.path.join(orc.REF_SRC, "src", "include"),
                     "-I" + os.path.join(ROOT, "binsim_b200", "csrc"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
     for line in filter(None, out):

@@ -51,9 +51,12 @@ struct Workspace {
     size_t f32_n = 0;
     double *part = nullptr;
     size_t part_n = 0;
+    void *gen = nullptr;     // general scratch (the VQE sweep's checkpoints and terms)
+    size_t gen_n = 0;
     int tile_table(const std::vector<i64> &pref, const i64 **out);
     int f32_buffer(size_t n, float **out);
     int partials(size_t n, double **out);
+    int general(size_t bytes, void **out);
     void release();
 };
 
@@ -111,11 +114,16 @@ struct DevNet {
     // cached pair lists of the pair operators for the last basis they were used with
     void *pair_state = nullptr;
     void (*pair_free)(void *) = nullptr;
+    // cached theta = 0 route of the pool gradient (transition densities) for the
+    // last basis it was used with
+    void *density_state = nullptr;
+    void (*density_free)(void *) = nullptr;
 
     int finalize();   // derived tables + upload
     ~DevNet() {
         if (fast_state && fast_free) fast_free(fast_state);
         if (pair_state && pair_free) pair_free(pair_state);
+        if (density_state && density_free) density_free(density_state);
         arena.release();
         magic = 0;
     }

@@ -103,9 +103,28 @@ enum PairOpKind { kPairExpm = 0, kPairGrad = 1, kPairBackgrad = 2, kPairTvec = 3
 
 // Gradients of every group of a pool network in one launch over the pair lists
 // (single-block bases, ranks <= 4); *used = false when the tile kernel must run.
+// skip / flag (device, may be null): when *flag is nonzero the groups with
+// skip[orig] set are left out (the theta = 0 density route computes them).
 template <typename Ti>
 int pair_list_batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *thetas, const double *l,
-                        const double *r, double *grads, cudaStream_t s, bool *used);
+                        const double *r, double *grads, cudaStream_t s, bool *used,
+                        const unsigned char *skip = nullptr, const int *flag = nullptr);
+
+// Theta = 0 route of the pool gradient through transition densities
+// (pooldensity.cu), built on first use for (basis, network) and cached on the
+// network; *out = nullptr when it does not apply (complex weights, no groups
+// of the planned forms, tables too large).  begin: device flag = every theta
+// is zero; the flag and the per-group skip mask are then handed to the
+// pair-list / tile kernels; finish: the density kernels, which run only when
+// the flag is set, overwrite grads of the planned groups.
+struct DensityRoute;
+template <typename Ti>
+int density_route(const DevBasis<Ti> *B, const DevNet<Ti> *N, DensityRoute **out);
+int density_route_begin(DensityRoute *D, const double *thetas, cudaStream_t s);
+template <typename Ti>
+int density_route_finish(DensityRoute *D, const double *l, const double *r, double *grads, cudaStream_t s);
+const unsigned char *density_route_skip(const DensityRoute *D);
+const int *density_route_flag(const DensityRoute *D);
 
 // Pair operator over the precomputed pair lists (single-block bases, rank <= 4).
 // Sets *used = false (and launches nothing) when the row kernel must serve the

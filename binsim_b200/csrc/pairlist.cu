@@ -328,7 +328,8 @@ pair_list_batchgrad_kernel(const Ti *__restrict__ astrs, const Ti *__restrict__ 
                            const int2 *__restrict__ alist_all, const int2 *__restrict__ blist_all,
                            const BGroup *__restrict__ groups, const i64 *__restrict__ tstart, int ngroups, i64 T,
                            const double *__restrict__ thetas, const double *__restrict__ l,
-                           const double *__restrict__ r, double *__restrict__ grads)
+                           const double *__restrict__ r, double *__restrict__ grads,
+                           const unsigned char *__restrict__ skip, const int *__restrict__ flag)
 {
     __shared__ double spa[kBatchRows][kListMaxRank];
     __shared__ long long arow[kBatchRows], asrc[kBatchRows];
@@ -338,9 +339,11 @@ pair_list_batchgrad_kernel(const Ti *__restrict__ astrs, const Ti *__restrict__ 
     __shared__ BGroup G;
     __shared__ double ang0, ang1;
     __shared__ int gcur;
+    __shared__ bool skipG;   // the current group is left to the theta = 0 density route
     const int t = threadIdx.x;
     const i64 t0 = (i64)blockIdx.x * T / gridDim.x, t1 = (i64)(blockIdx.x + 1) * T / gridDim.x;
     if (t0 >= t1) return;
+    const bool route = skip && flag && *flag != 0;
     if (t == 0) {   // group of the first tile: last g with tstart[g] <= t0
         int lo = 0, hi = ngroups - 1;
         while (lo < hi) {
@@ -358,7 +361,7 @@ pair_list_batchgrad_kernel(const Ti *__restrict__ astrs, const Ti *__restrict__ 
         __syncthreads();
         if ((t & 31) == 0) red[t >> 5] = v;
         __syncthreads();
-        if (t == 0) {
+        if (t == 0 && !skipG) {
             double sum = 0.0;
             for (int i = 0; i < kListCols / 32; ++i) sum += red[i];
             atomicAdd(grads + G.orig, sum);
@@ -376,9 +379,14 @@ pair_list_batchgrad_kernel(const Ti *__restrict__ astrs, const Ti *__restrict__ 
                 const double th = thetas[G.orig];
                 ang0 = -sin(th);   // grad_update, core/math.hpp:148-162
                 ang1 = cos(th);
+                skipG = route && skip[G.orig];
             }
             __syncthreads();
             g = gcur;
+            if (skipG) {   // uniform: jump to the group's last tile in this CTA's range
+                tile = min(t1, tstart[g + 1]) - 1;
+                continue;
+            }
             for (int i = t; i < G.nza; i += kListCols) zsa[i] = (unsigned long long)zall[G.za_off + i];
             for (int i = t; i < G.nzb; i += kListCols) zsb[i] = (unsigned long long)zall[G.zb_off + i];
             for (int i = t; i < G.R * G.nza; i += kListCols) wsa[i] = wall[G.wa_off + i];
@@ -496,7 +504,8 @@ int pair_list_launch(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, PairA
 
 template <typename Ti>
 int pair_list_batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double *thetas, const double *l,
-                        const double *r, double *grads, cudaStream_t s, bool *used)
+                        const double *r, double *grads, cudaStream_t s, bool *used, const unsigned char *skip,
+                        const int *flag)
 {
     *used = false;
     PairPlan<Ti> *P = nullptr;
@@ -535,16 +544,18 @@ int pair_list_batchgrad(const DevBasis<Ti> *B, const DevNet<Ti> *N, const double
     const i64 grid = std::min<i64>(P->bg_tiles, (i64)148 * 32);
     pair_list_batchgrad_kernel<Ti><<<(unsigned)grid, kListCols, 0, s>>>(
         B->view.astrs, B->view.bstrs, B->nb[0], N->view.z, N->view.w, P->d_alist, P->d_blist, P->d_bg, P->d_tstart,
-        P->bg_n, P->bg_tiles, thetas, l, r, grads);
+        P->bg_n, P->bg_tiles, thetas, l, r, grads, skip, flag);
     BSIM_CUDA(cudaGetLastError());
     return BSIM_OK;
 }
 
 template int pair_list_batchgrad<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, const double *,
-                                           const double *, const double *, double *, cudaStream_t, bool *);
+                                           const double *, const double *, double *, cudaStream_t, bool *,
+                                           const unsigned char *, const int *);
 template int pair_list_batchgrad<unsigned long long>(const DevBasis<unsigned long long> *,
                                                      const DevNet<unsigned long long> *, const double *,
-                                                     const double *, const double *, double *, cudaStream_t, bool *);
+                                                     const double *, const double *, double *, cudaStream_t, bool *,
+                                                     const unsigned char *, const int *);
 
 #define PAIR_LIST_INST(OP)                                                                                   \
     template int pair_list_launch<unsigned, OP>(const DevBasis<unsigned> *, const DevNet<unsigned> *, i64,     \

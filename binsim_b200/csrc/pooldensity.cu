@@ -24,11 +24,12 @@
 // 32-row K slices in shared memory), split over K with FP64 atomics into the
 // tables.  At 36 orbitals and 3 + 3 electrons Tab is 1296 x 396,900 x 1296.
 #include "../../include/binsim_cuotf.h"
-#include "common.cuh"
-#include "handles.h"
+#include "ops.h"
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <mutex>
 #include <unordered_map>
 #include <vector>
 
@@ -40,6 +41,7 @@ constexpr unsigned kPoolDensityMagic = 0xB5B1D7A1u;
 constexpr int kTK = 32, kTM = 64, kTN = 128;     // K slice, output tile
 constexpr int kLS = kTM + 4, kXS = kTN + 4;      // shared strides (4 mod 16 doubles: no bank conflicts)
 constexpr int kNT = 512;
+constexpr i64 kMaxGridZ = 65535;
 constexpr size_t kSmem = sizeof(double) * kTK * (kLS + kXS);   // 51,200 bytes: dynamic shared memory
 
 __device__ __forceinline__ void dmma884(double &c0, double &c1, double a, double b)
@@ -65,10 +67,10 @@ __device__ __forceinline__ u64 kmask(Ti a)
 template <typename Ti>
 __global__ void frame_pair_kernel(int nB, const Ti *__restrict__ astr, const Ti *__restrict__ bstr,
                                   const double *__restrict__ l, const double *__restrict__ r, double *__restrict__ lt,
-                                  double *__restrict__ rt)
+                                  double *__restrict__ rt, const int *__restrict__ flag)
 {
     const int a = blockIdx.x, b = blockIdx.y * blockDim.x + threadIdx.x;
-    if (b >= nB) return;
+    if (b >= nB || (flag && *flag == 0)) return;
     const u64 k = kmask(astr[a]);
     const i64 i = (i64)a * nB + b;
     const bool neg = __popcll((u64)bstr[b] & k) & 1;
@@ -85,10 +87,10 @@ template <typename Ti>
 __global__ void embed_frame_kernel(int nBk, int nBall, const Ti *__restrict__ astr, const Ti *__restrict__ bstr,
                                    const int *__restrict__ gA, const int *__restrict__ gB,
                                    const double *__restrict__ l, const double *__restrict__ r, double *__restrict__ lt,
-                                   double *__restrict__ rt)
+                                   double *__restrict__ rt, const int *__restrict__ flag)
 {
     const int a = blockIdx.x, b = blockIdx.y * blockDim.x + threadIdx.x;
-    if (b >= nBk) return;
+    if (b >= nBk || (flag && *flag == 0)) return;
     const u64 k = kmask(astr[a]);
     const i64 i = (i64)a * nBk + b, o = (i64)gA[a] * nBall + gB[b];
     const bool neg = __popcll((u64)bstr[b] & k) & 1;
@@ -150,12 +152,14 @@ struct TabArgs {
     const int *idxB;   // [nHb][n]
     const double *lt, *rt;
     double *C;         // [M][M]
+    const int *flag;   // the launch does nothing when *flag == 0 (null: always runs)
 };
 
 // grid (ceil(M / 64), ceil(M / 128), ceil(nHa / hsplit)); K = (hA, hB), hA in the
 // CTA's split, hB in 32-row slices (the last one zero-padded).
 __global__ void __launch_bounds__(kNT, 1) tab_kernel(const TabArgs P)
 {
+    if (P.flag && *P.flag == 0) return;
     extern __shared__ __align__(16) double smem_tab[];
     double(*As)[kLS] = reinterpret_cast<double(*)[kLS]>(smem_tab);
     double(*Bs)[kXS] = reinterpret_cast<double(*)[kXS]>(smem_tab + kTK * kLS);
@@ -221,68 +225,80 @@ struct PairArgs {
     const int *idx2;     // [nH2][npair]
     const double *lt, *rt;
     double *C;           // [npair][npair]
+    const int *flag;     // as TabArgs::flag
 };
 
-// grid (ceil(npair / 64), ceil(npair / 128), nH2 * ceil(nO / osplit)); K = (h2, o),
-// o the other spin's string, in 32-row slices of o.
+// grid (ceil(npair / 64), ceil(npair / 128), min(nH2 * nos, 65535)), nos = ceil(nO / osplit).
+// K = (h2, o), o the other spin's string: item z = h2 * nos + (range of osplit
+// strings o); CTA z takes items z, z + gridDim.z, ... and each item in 32-row
+// slices of o.  All items of a CTA add into the same output tile, flushed once.
 __global__ void __launch_bounds__(kNT, 1) pair2_kernel(const PairArgs P)
 {
+    if (P.flag && *P.flag == 0) return;
     extern __shared__ __align__(16) double smem_pair[];
     double(*As)[kLS] = reinterpret_cast<double(*)[kLS]>(smem_pair);
     double(*Bs)[kXS] = reinterpret_cast<double(*)[kXS]>(smem_pair + kTK * kLS);
     const int m0 = blockIdx.x * kTM, c0 = blockIdx.y * kTN;
     const int nos = (P.nO + P.osplit - 1) / P.osplit;
-    const int h2 = blockIdx.z / nos, o0 = (blockIdx.z % nos) * P.osplit, o1 = min(P.nO, o0 + P.osplit);
+    const i64 nitems = (i64)P.nH2 * nos;
     constexpr int IA = kTK * kTM / kNT, IB = kTK * kTN / kNT;
-    int ak[IA], ia[IA], bk[IB], ib[IB];
+    int ak[IA], ja[IA], bk[IB], jb[IB];   // per fill item: slice row and pair column (or -1)
 #pragma unroll
     for (int it = 0; it < IA; ++it) {
         const int i = threadIdx.x + it * kNT, j = m0 + i % kTM;
         ak[it] = i / kTM;
-        ia[it] = j < P.npair ? __ldg(P.idx2 + (i64)h2 * P.npair + j) : -1;
+        ja[it] = j < P.npair ? j : -1;
     }
 #pragma unroll
     for (int it = 0; it < IB; ++it) {
         const int i = threadIdx.x + it * kNT, j = c0 + i % kTN;
         bk[it] = i / kTN;
-        ib[it] = j < P.npair ? __ldg(P.idx2 + (i64)h2 * P.npair + j) : -1;
+        jb[it] = j < P.npair ? j : -1;
     }
     Acc acc;
     acc.zero();
-    for (int s0 = o0; s0 < o1; s0 += kTK) {
+    for (i64 item = blockIdx.z; item < nitems; item += gridDim.z) {
+        const int h2 = (int)(item / nos), o0 = (int)(item % nos) * P.osplit, o1 = min(P.nO, o0 + P.osplit);
+        int ia[IA], ib[IB];
 #pragma unroll
-        for (int it = 0; it < IA; ++it) {
-            const int o = s0 + ak[it];
-            double v = 0.0;
-            if (ia[it] >= 0 && o < o1) {
-                const i64 e = P.spin == 0 ? (i64)(ia[it] >> 1) * P.nB + o : (i64)o * P.nB + (ia[it] >> 1);
-                v = signed_at(P.lt, e, ia[it] & 1);
-            }
-            As[ak[it]][(threadIdx.x + it * kNT) % kTM] = v;
-        }
+        for (int it = 0; it < IA; ++it) ia[it] = ja[it] >= 0 ? __ldg(P.idx2 + (i64)h2 * P.npair + ja[it]) : -1;
 #pragma unroll
-        for (int it = 0; it < IB; ++it) {
-            const int o = s0 + bk[it];
-            double v = 0.0;
-            if (ib[it] >= 0 && o < o1) {
-                const i64 e = P.spin == 0 ? (i64)(ib[it] >> 1) * P.nB + o : (i64)o * P.nB + (ib[it] >> 1);
-                v = signed_at(P.rt, e, ib[it] & 1);
+        for (int it = 0; it < IB; ++it) ib[it] = jb[it] >= 0 ? __ldg(P.idx2 + (i64)h2 * P.npair + jb[it]) : -1;
+        for (int s0 = o0; s0 < o1; s0 += kTK) {
+#pragma unroll
+            for (int it = 0; it < IA; ++it) {
+                const int o = s0 + ak[it];
+                double v = 0.0;
+                if (ia[it] >= 0 && o < o1) {
+                    const i64 e = P.spin == 0 ? (i64)(ia[it] >> 1) * P.nB + o : (i64)o * P.nB + (ia[it] >> 1);
+                    v = signed_at(P.lt, e, ia[it] & 1);
+                }
+                As[ak[it]][(threadIdx.x + it * kNT) % kTM] = v;
             }
-            Bs[bk[it]][(threadIdx.x + it * kNT) % kTN] = v;
+#pragma unroll
+            for (int it = 0; it < IB; ++it) {
+                const int o = s0 + bk[it];
+                double v = 0.0;
+                if (ib[it] >= 0 && o < o1) {
+                    const i64 e = P.spin == 0 ? (i64)(ib[it] >> 1) * P.nB + o : (i64)o * P.nB + (ib[it] >> 1);
+                    v = signed_at(P.rt, e, ib[it] & 1);
+                }
+                Bs[bk[it]][(threadIdx.x + it * kNT) % kTN] = v;
+            }
+            __syncthreads();
+            acc.step(As, Bs);
+            __syncthreads();
         }
-        __syncthreads();
-        acc.step(As, Bs);
-        __syncthreads();
     }
     acc.flush(P.C, P.npair, m0, c0, P.npair, P.npair);
 }
 
 // D1a[p][q] = sum_r C[p n + r][q n + r] / nel_b, D1b[r][s] = sum_p C[p n + r][p n + s] / nel_a
 __global__ void d1_kernel(int n, int nel_a, int nel_b, const double *__restrict__ C, double *__restrict__ D1a,
-                          double *__restrict__ D1b)
+                          double *__restrict__ D1b, const int *__restrict__ flag)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n * n) return;
+    if (i >= n * n || (flag && *flag == 0)) return;
     const int x = i / n, y = i % n;
     const i64 M = (i64)n * n;
     double sa = 0.0, sb = 0.0;
@@ -322,15 +338,18 @@ __device__ __forceinline__ double table_at(const Tables &T, int kind, int i0, in
     }
 }
 
-// grads[g] = coef (X[dagger(i)] - X[i]); 0 for zero groups, NaN for general ones
+// grads[g] = coef (X[dagger(i)] - X[i]); 0 for zero groups; general groups get
+// NaN, or keep their value when keep_general is set (the pair-list kernels wrote it)
 __global__ void assemble_kernel(i64 ngs, const int *__restrict__ kind, const int4 *__restrict__ idx,
-                                const double *__restrict__ coef, Tables T, double *__restrict__ grads)
+                                const double *__restrict__ coef, Tables T, double *__restrict__ grads,
+                                const int *__restrict__ flag, int keep_general)
 {
     const i64 g = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ngs) return;
+    if (g >= ngs || (flag && *flag == 0)) return;
     const int k = kind[g];
     if (k <= 0) {
-        grads[g] = k == 0 ? 0.0 : __longlong_as_double(0x7ff8000000000000ll);
+        if (k == 0) grads[g] = 0.0;
+        else if (!keep_general) grads[g] = __longlong_as_double(0x7ff8000000000000ll);
         return;
     }
     const int4 i = idx[g];
@@ -412,8 +431,8 @@ int hole_table(int norb, int holes, const std::vector<S> &strs, std::vector<u64>
 }
 
 template <typename Ti>
-int density_create(DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t *idx, const double *coef,
-                   PoolDensity **out)
+int density_create(const DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t *idx, const double *coef,
+                   PoolDensity **out, size_t max_bytes = ~size_t(0))
 {
     if (B->nel_a < 1 || B->nel_b < 1) {
         set_error("pool density gradient: needs at least one electron of each spin");
@@ -431,9 +450,17 @@ int density_create(DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t 
     std::sort(bs.begin(), bs.end());
     bs.erase(std::unique(bs.begin(), bs.end()), bs.end());
     const int nA = (int)as.size(), nB = (int)bs.size();
-    if (as.size() >= (1u << 30) || bs.size() >= (1u << 30) || (nB + 255) / 256 > 65535) return BSIM_ERR_TOO_LARGE;
-    for (int k = 0; k < nbk; ++k)
-        if ((B->nb[k] + 255) / 256 > 65535) return BSIM_ERR_TOO_LARGE;
+    // every launch size of density_grad is checked here, so a call never fails
+    // after part of its work is queued: table entries are (index << 1) | sign in
+    // an int, and the frame kernels put 256 beta strings per CTA on grid y
+    if (as.size() >= (1u << 30) || bs.size() >= (1u << 30)) {
+        set_error("pool density gradient: %zu alpha / %zu beta strings, above the 2^30 limit", as.size(), bs.size());
+        return BSIM_ERR_TOO_LARGE;
+    }
+    if ((nB + 255) / 256 > 65535) {
+        set_error("pool density gradient: %d beta strings, above the frame kernel's 65535 * 256", nB);
+        return BSIM_ERR_TOO_LARGE;
+    }
     for (i64 g = 0; g < ngs; ++g) {   // the assembly reads tables at these orbitals
         if (kind[g] < BSIM_POOL_GENERAL || kind[g] > BSIM_POOL_GBB) {
             set_error("pool density gradient: group %lld has kind %d", (long long)g, (int)kind[g]);
@@ -480,6 +507,11 @@ int density_create(DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t 
     const size_t bytes = 256 * 18 + sizeof(int) * (tA.size() + tB.size() + t2A.size() + t2B.size() + ngs) +
                          sizeof(int) * (gA.size() + gB.size()) +
                          sizeof(int4) * ngs + sizeof(double) * (ngs + 2 * dim + M * M + 2 * np2 + 2 * M);
+    if (bytes > max_bytes) {
+        delete P;
+        set_error("pool density gradient: %zu bytes of tables above the limit of %zu", bytes, max_bytes);
+        return BSIM_ERR_TOO_LARGE;
+    }
     if ((st = P->arena.reserve(bytes)) != BSIM_OK) { delete P; return st; }
     P->idxA = P->arena.take<int>(tA.size());
     P->idxB = P->arena.take<int>(tB.size());
@@ -514,7 +546,8 @@ int density_create(DevBasis<Ti> *B, i64 ngs, const int32_t *kind, const int32_t 
 }
 
 template <typename Ti>
-int density_grad(PoolDensity *P, const double *l, const double *r, double *grads, cudaStream_t s)
+int density_grad(PoolDensity *P, const double *l, const double *r, double *grads, cudaStream_t s,
+                 const int *flag = nullptr, bool keep_general = false)
 {
     const auto *B = static_cast<const DevBasis<Ti> *>(P->basis);
     const int n = P->n, nA = P->nA, nB = P->nB;
@@ -522,7 +555,7 @@ int density_grad(PoolDensity *P, const double *l, const double *r, double *grads
     if (!P->embed) {
         dim3 g(nA, (nB + 255) / 256);
         frame_pair_kernel<Ti><<<g, 256, 0, s>>>(nB, B->view.astrs + B->astart[0], B->view.bstrs + B->bstart[0], l, r,
-                                                P->lt, P->rt);
+                                                P->lt, P->rt, flag);
     } else {
         BSIM_CUDA(cudaMemsetAsync(P->lt, 0, sizeof(double) * (i64)nA * nB, s));
         BSIM_CUDA(cudaMemsetAsync(P->rt, 0, sizeof(double) * (i64)nA * nB, s));
@@ -532,20 +565,19 @@ int density_grad(PoolDensity *P, const double *l, const double *r, double *grads
             dim3 g(nak, (nbk + 255) / 256);
             embed_frame_kernel<Ti><<<g, 256, 0, s>>>(nbk, nB, B->view.astrs + P->blk_as[k], B->view.bstrs + P->blk_bs[k],
                                                      P->gA + P->blk_as[k], P->gB + P->blk_bs[k], l + P->blk_off[k],
-                                                     r + P->blk_off[k], P->lt, P->rt);
+                                                     r + P->blk_off[k], P->lt, P->rt, flag);
         }
     }
     BSIM_CUDA(cudaMemsetAsync(P->C, 0, sizeof(double) * M * M, s));
     BSIM_CUDA(cudaMemsetAsync(P->C2a, 0, sizeof(double) * np2, s));
     BSIM_CUDA(cudaMemsetAsync(P->C2b, 0, sizeof(double) * np2, s));
     if (P->nHa > 0 && P->nHb > 0) {
-        TabArgs A{n, nB, P->nHa, P->nHb, (int)M, 0, P->idxA, P->idxB, P->lt, P->rt, P->C};
+        TabArgs A{n, nB, P->nHa, P->nHb, (int)M, 0, P->idxA, P->idxB, P->lt, P->rt, P->C, flag};
         const int tiles = (int)(((M + kTM - 1) / kTM) * ((M + kTN - 1) / kTN));
         const int splits = std::max(1, std::min(P->nHa, (148 * 8 + tiles - 1) / tiles));
         A.hsplit = (P->nHa + splits - 1) / splits;
         dim3 g((unsigned)((M + kTM - 1) / kTM), (unsigned)((M + kTN - 1) / kTN),
-               (unsigned)((P->nHa + A.hsplit - 1) / A.hsplit));
-        if (g.z > 65535) return BSIM_ERR_TOO_LARGE;
+               (unsigned)((P->nHa + A.hsplit - 1) / A.hsplit));   // at most 148 * 8 K splits
         BSIM_CUDA(cudaFuncSetAttribute(tab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
         tab_kernel<<<g, kNT, kSmem, s>>>(A);
     }
@@ -553,25 +585,151 @@ int density_grad(PoolDensity *P, const double *l, const double *r, double *grads
         const int nH2 = spin == 0 ? P->nH2a : P->nH2b, nO = spin == 0 ? nB : nA;
         if (nH2 == 0 || P->npair == 0) continue;
         PairArgs A{P->npair, nB, nH2, nO, 0, spin, spin == 0 ? P->idx2A : P->idx2B, P->lt, P->rt,
-                   spin == 0 ? P->C2a : P->C2b};
+                   spin == 0 ? P->C2a : P->C2b, flag};
         const int tiles = ((P->npair + kTM - 1) / kTM) * ((P->npair + kTN - 1) / kTN);
         const int want = std::max(1, (148 * 8 + tiles * nH2 - 1) / (tiles * nH2));   // o-splits per hole string
         A.osplit = std::max(kTK, ((nO + want - 1) / want + kTK - 1) / kTK * kTK);
         const int nos = (nO + A.osplit - 1) / A.osplit;
-        dim3 g((unsigned)((P->npair + kTM - 1) / kTM), (unsigned)((P->npair + kTN - 1) / kTN), (unsigned)(nH2 * nos));
-        if ((i64)nH2 * nos > 65535) return BSIM_ERR_TOO_LARGE;
+        dim3 g((unsigned)((P->npair + kTM - 1) / kTM), (unsigned)((P->npair + kTN - 1) / kTN),
+               (unsigned)std::min<i64>((i64)nH2 * nos, kMaxGridZ));
         BSIM_CUDA(cudaFuncSetAttribute(pair2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
         pair2_kernel<<<g, kNT, kSmem, s>>>(A);
     }
-    d1_kernel<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(n, P->nel_a, P->nel_b, P->C, P->D1a, P->D1b);
+    d1_kernel<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(n, P->nel_a, P->nel_b, P->C, P->D1a, P->D1b, flag);
     Tables T{n, P->npair, P->D1a, P->D1b, P->C, P->nH2a ? P->C2a : nullptr, P->nH2b ? P->C2b : nullptr};
     if (P->ngs > 0)
-        assemble_kernel<<<(unsigned)((P->ngs + 255) / 256), 256, 0, s>>>(P->ngs, P->kind, P->idx, P->coef, T, grads);
+        assemble_kernel<<<(unsigned)((P->ngs + 255) / 256), 256, 0, s>>>(P->ngs, P->kind, P->idx, P->coef, T, grads,
+                                                                          flag, keep_general ? 1 : 0);
     BSIM_CUDA(cudaGetLastError());
     return BSIM_OK;
 }
 
+// ---- theta = 0 route of batchgrad --------------------------------------------------
+__global__ void theta_zero_kernel(const double *__restrict__ thetas, i64 n, int *__restrict__ flag)
+{
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+        if (thetas[i] != 0.0) *flag = 0;   // every writer writes 0
+}
+
 }  // namespace
+
+struct DensityRoute {
+    const void *basis = nullptr;
+    i64 basis_dim = 0;
+    bool ok = false;                 // false: the route does not apply to this (basis, network)
+    i64 ngs = 0;
+    PoolDensity *P = nullptr;
+    Arena arena;                     // skip mask and flag
+    unsigned char *skip = nullptr;   // [ngs]: 1 for groups of a planned form (kind >= 0)
+    int *flag = nullptr;             // nonzero: every theta of the current call is zero
+    ~DensityRoute() { delete P; arena.release(); }
+};
+
+static std::mutex g_route_mu;
+
+// Route for (B, N): groups classified by bsim_poolplan_classify from the
+// network's host copy; applies when some group has a planned form and the
+// dense tables take at most half of the free device memory (a blocked basis
+// only when its union string arrays hold at most 4x its determinants).
+// BSIM_POOL_DENSITY=0 turns the route off.
+template <typename Ti>
+int density_route(const DevBasis<Ti> *B, const DevNet<Ti> *N, DensityRoute **out)
+{
+    *out = nullptr;
+    static const bool off = [] {
+        const char *e = getenv("BSIM_POOL_DENSITY");
+        return e && e[0] == '0';
+    }();
+    if (off || N->cplx || B->nel_a < 1 || B->nel_b < 1 || B->dim == 0 || N->ngs == 0 || B->norb > 64) return BSIM_OK;
+    std::lock_guard<std::mutex> lk(g_route_mu);
+    auto *R = static_cast<DensityRoute *>(N->density_state);
+    if (R && R->basis == B && R->basis_dim == B->dim) {
+        *out = R->ok ? R : nullptr;
+        return BSIM_OK;
+    }
+    if (R) { delete R; const_cast<DevNet<Ti> *>(N)->density_state = nullptr; }
+    R = new DensityRoute;
+    R->basis = B;
+    R->basis_dim = B->dim;
+    R->ngs = N->ngs;
+    auto &net = const_cast<DevNet<Ti> &>(*N);
+    net.density_state = R;
+    net.density_free = [](void *q) { delete static_cast<DensityRoute *>(q); };
+    // the network in the flat form of bsim_poolplan_classify
+    const i64 ngs = N->ngs;
+    std::vector<uint64_t> axs(ngs), bxs(ngs), za, zb;
+    std::vector<int64_t> ranks(ngs), nza(ngs), nzb(ngs);
+    std::vector<double> wa, wb;
+    for (i64 g = 0; g < ngs; ++g) {
+        const GroupDev &G = N->groups[g];
+        axs[g] = G.ax; bxs[g] = G.bx; ranks[g] = G.rank; nza[g] = G.nza; nzb[g] = G.nzb;
+        for (int i = 0; i < G.nza; ++i) za.push_back((uint64_t)N->z[G.za_off + i]);
+        for (int i = 0; i < G.nzb; ++i) zb.push_back((uint64_t)N->z[G.zb_off + i]);
+        wa.insert(wa.end(), N->w.begin() + G.wa_off, N->w.begin() + G.wa_off + (i64)G.nza * G.rank);
+        wb.insert(wb.end(), N->w.begin() + G.wb_off, N->w.begin() + G.wb_off + (i64)G.nzb * G.rank);
+    }
+    za.push_back(0); zb.push_back(0); wa.push_back(0.0); wb.push_back(0.0);   // never empty arrays
+    std::vector<int32_t> kind(ngs), idx(4 * ngs);
+    std::vector<double> coef(ngs);
+    int st = bsim_poolplan_classify(B->norb, ngs, axs.data(), bxs.data(), ranks.data(), nza.data(), nzb.data(),
+                                    za.data(), zb.data(), wa.data(), wb.data(), kind.data(), idx.data(), coef.data());
+    if (st != BSIM_OK) return BSIM_OK;   // not applicable
+    std::vector<unsigned char> skip(ngs);
+    i64 planned = 0;
+    for (i64 g = 0; g < ngs; ++g) planned += (skip[g] = kind[g] >= 0 ? 1 : 0);
+    if (planned == 0) return BSIM_OK;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return cuda_status(cudaGetLastError(), "cudaMemGetInfo");
+    if (B->num_blocks > 1) {   // union string arrays of a blocked basis
+        std::vector<u64> as, bs;
+        for (int k = 0; k < B->num_blocks; ++k) {
+            for (int i = 0; i < B->na[k]; ++i) as.push_back((u64)B->astrs[B->astart[k] + i]);
+            for (int i = 0; i < B->nb[k]; ++i) bs.push_back((u64)B->bstrs[B->bstart[k] + i]);
+        }
+        std::sort(as.begin(), as.end());
+        std::sort(bs.begin(), bs.end());
+        const double u = (double)(std::unique(as.begin(), as.end()) - as.begin()) *
+                         (double)(std::unique(bs.begin(), bs.end()) - bs.begin());
+        if (u > 4.0 * (double)B->dim) return BSIM_OK;
+    }
+    PoolDensity *P = nullptr;
+    st = density_create(B, ngs, kind.data(), idx.data(), coef.data(), &P, free_b / 2);
+    if (st == BSIM_ERR_TOO_LARGE || st == BSIM_ERR_UNSUPPORTED) { set_error(""); return BSIM_OK; }
+    if (st != BSIM_OK) return st;
+    R->P = P;
+    if ((st = R->arena.reserve((size_t)ngs + 512)) != BSIM_OK) return st;
+    R->flag = R->arena.take<int>(1);
+    R->skip = R->arena.take<unsigned char>(ngs);
+    BSIM_CUDA(cudaMemcpy(R->skip, skip.data(), (size_t)ngs, cudaMemcpyHostToDevice));
+    R->ok = true;
+    *out = R;
+    return BSIM_OK;
+}
+
+int density_route_begin(DensityRoute *D, const double *thetas, cudaStream_t s)
+{
+    BSIM_CUDA(cudaMemsetAsync(D->flag, 0xff, sizeof(int), s));
+    const unsigned grid = (unsigned)std::min<i64>(148 * 4, (D->ngs + 255) / 256);
+    theta_zero_kernel<<<std::max(grid, 1u), 256, 0, s>>>(thetas, D->ngs, D->flag);
+    BSIM_CUDA(cudaGetLastError());
+    return BSIM_OK;
+}
+
+template <typename Ti>
+int density_route_finish(DensityRoute *D, const double *l, const double *r, double *grads, cudaStream_t s)
+{
+    return density_grad<Ti>(D->P, l, r, grads, s, D->flag, true);
+}
+
+const unsigned char *density_route_skip(const DensityRoute *D) { return D->skip; }
+const int *density_route_flag(const DensityRoute *D) { return D->flag; }
+
+template int density_route<unsigned>(const DevBasis<unsigned> *, const DevNet<unsigned> *, DensityRoute **);
+template int density_route<unsigned long long>(const DevBasis<unsigned long long> *,
+                                               const DevNet<unsigned long long> *, DensityRoute **);
+template int density_route_finish<unsigned>(DensityRoute *, const double *, const double *, double *, cudaStream_t);
+template int density_route_finish<unsigned long long>(DensityRoute *, const double *, const double *, double *,
+                                                      cudaStream_t);
 
 }  // namespace bsim
 

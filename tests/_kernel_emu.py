@@ -101,8 +101,9 @@ def tab(n, nB, tA, tB, lt, rt, sms=SMS):
     return C
 
 
-def pair2(n, nA, nB, t2, lt, rt, spin, sms=SMS):
-    """C2 [npair x npair] of one spin as pair2_kernel computes it."""
+def pair2(n, nA, nB, t2, lt, rt, spin, sms=SMS, zcap=65535):
+    """C2 [npair x npair] of one spin as pair2_kernel computes it: grid z capped at
+    zcap, CTA z taking items z, z + zcap, ... (item = h2 * nos + o range)."""
     npair = n * (n - 1) // 2
     nH2 = t2.shape[0]
     nO = nB if spin == 0 else nA
@@ -111,31 +112,34 @@ def pair2(n, nA, nB, t2, lt, rt, spin, sms=SMS):
     want = max(1, -(-sms * 8 // (tiles * nH2)))
     osplit = max(TK, -(-(-(-nO // want)) // TK) * TK)
     nos = -(-nO // osplit)
-    grid = (-(-npair // TM), -(-npair // TN), nH2 * nos)
+    nitems = nH2 * nos
+    grid = (-(-npair // TM), -(-npair // TN), min(nitems, zcap))
     tid = np.arange(NT)
     iA = tid[None, :] + np.arange(TK * TM // NT)[:, None] * NT
     iB = tid[None, :] + np.arange(TK * TN // NT)[:, None] * NT
     for bx in range(grid[0]):
         for by in range(grid[1]):
             m0, c0 = bx * TM, by * TN
+            jA, jB = m0 + iA % TM, c0 + iB % TN
             for bz in range(grid[2]):
-                h2, o0 = bz // nos, (bz % nos) * osplit
-                o1 = min(nO, o0 + osplit)
-                jA, jB = m0 + iA % TM, c0 + iB % TN
-                _check(h2 * npair + jA[jA < npair], t2.size, "idx2")
-                ia = np.where(jA < npair, t2[h2, np.minimum(jA, npair - 1)], -1)
-                ib = np.where(jB < npair, t2[h2, np.minimum(jB, npair - 1)], -1)
                 D = np.zeros((16, 8, 8, 8))
-                for s0 in range(o0, o1, TK):
-                    As, Bs = np.zeros((TK, LS)), np.zeros((TK, XS))
-                    for (ii, ii_flat, src, sm, width, step) in ((ia, iA, lt, As, TM, TM), (ib, iB, rt, Bs, TN, TN)):
-                        kk = ii_flat // step
-                        o = s0 + kk
-                        ok = (ii >= 0) & (o < o1)
-                        row = ii >> 1
-                        e = np.where(ok, row * nB + o if spin == 0 else o * nB + row, 0)
-                        v = np.where(ok, _signed(src, e, (ii & 1) == 1), 0.0)
-                        sm[kk, ii_flat % width] = v
-                    _step(As, Bs, D)
+                for item in range(bz, nitems, grid[2]):
+                    h2, o0 = item // nos, (item % nos) * osplit
+                    o1 = min(nO, o0 + osplit)
+                    _check(h2 * npair + jA[jA < npair], t2.size, "idx2")
+                    ia = np.where(jA < npair, t2[h2, np.minimum(jA, npair - 1)], -1)
+                    ib = np.where(jB < npair, t2[h2, np.minimum(jB, npair - 1)], -1)
+                    for s0 in range(o0, o1, TK):
+                        As, Bs = np.zeros((TK, LS)), np.zeros((TK, XS))
+                        for (ii, ii_flat, src, sm, width, step) in ((ia, iA, lt, As, TM, TM),
+                                                                     (ib, iB, rt, Bs, TN, TN)):
+                            kk = ii_flat // step
+                            o = s0 + kk
+                            ok = (ii >= 0) & (o < o1)
+                            row = ii >> 1
+                            e = np.where(ok, row * nB + o if spin == 0 else o * nB + row, 0)
+                            v = np.where(ok, _signed(src, e, (ii & 1) == 1), 0.0)
+                            sm[kk, ii_flat % width] = v
+                        _step(As, Bs, D)
                 _flush(D, C2, m0, c0, npair, npair)
     return C2

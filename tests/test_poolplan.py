@@ -188,13 +188,15 @@ def test_device_density_arithmetic_matches_oracle(oracle, norb, na, nb):
     assert np.abs(got - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max())
 
 
-@pytest.mark.parametrize("norb,na,nb,sms", [(9, 3, 3, 148), (12, 3, 2, 148), (9, 3, 3, 2)])
-def test_density_kernel_indexing_emulated(oracle, norb, na, nb, sms):
+@pytest.mark.parametrize("norb,na,nb,sms,zcap", [(9, 3, 3, 148, 65535), (12, 3, 2, 148, 65535), (9, 3, 3, 2, 65535),
+                                                   (9, 3, 3, 148, 5)])
+def test_density_kernel_indexing_emulated(oracle, norb, na, nb, sms, zcap):
     """tab_kernel and pair2_kernel emulated thread by thread (launch grid and K splits of
     the host code, shared-memory fill items, mma.sync m8n8k4 lane fragments, atomic flush
     addresses; every index bounds-checked) give the density tables.  The cases cover
     several output tiles, a zero-padded last K slice, K splits of several hole strings per
-    CTA (a GPU of 2 multiprocessors) and split beta ranges."""
+    CTA (a GPU of 2 multiprocessors), split beta ranges, and a pair2 grid capped below
+    its item count (CTAs looping over several hole strings, as for large nH2)."""
     import _kernel_emu as emu
     pool = nw.ucc_pool(norb)
     kind, idx, coef = cuotf.pool_plan(pool.network)
@@ -210,7 +212,7 @@ def test_density_kernel_indexing_emulated(oracle, norb, na, nb, sms):
     assert np.abs(C - tb["C"]).max() <= 1e-13 * np.abs(tb["C"]).max()
     for spin, strs in ((0, A), (1, Bs)):
         _, t2 = cuotf.hole_table(strs, norb, 2)
-        C2 = emu.pair2(norb, len(A), len(Bs), t2, tb["lt"], tb["rt"], spin, sms=sms)
+        C2 = emu.pair2(norb, len(A), len(Bs), t2, tb["lt"], tb["rt"], spin, sms=sms, zcap=zcap)
         ref = tb["C2a" if spin == 0 else "C2b"]
         assert np.abs(C2 - ref).max() <= 1e-13 * np.abs(ref).max()
 

@@ -118,6 +118,30 @@ def cpu_worker(args):
         ref.otf.destroy_network_otf_f64(rn)
         return dt, float(pairs[keep].sum())
 
+    full = float(pairs.sum())
+    threads = int(os.environ.get("OMP_NUM_THREADS", "0"))
+    if args.cpu_full:
+        # warm-up (OpenMP threads, first touch of the output): a sigma of every
+        # 200th group, untimed
+        run(np.arange(0, net.ngs, 200))
+        # whole sigma, every group: the reference's contract_network_otf as the
+        # Julia host calls it (one network, one hvec_gather_contract_otf_f64)
+        rn = ref.network(net)
+        times = []
+        t_start = time.perf_counter()
+        while True:
+            t0 = time.perf_counter()
+            ref.otf.hvec_gather_contract_otf_f64(rb, rn, P(x), P(y))
+            times.append(time.perf_counter() - t0)
+            spent = time.perf_counter() - t_start
+            if len(times) >= max(1, args.cpu_reps) or spent + times[-1] > args.cpu_seconds:
+                break
+        ref.otf.destroy_network_otf_f64(rn)
+        dt = float(np.median(times))
+        print(json.dumps({"value": 1.0 / dt, "sec_per_sigma": dt, "sample_pairs": full, "full_pairs": full,
+                          "sample_groups": int(net.ngs), "stride": 1, "sample_seconds": dt, "reps": len(times),
+                          "times": times, "threads": threads, "full": True}))
+        return
     off = np.flatnonzero(net.type_codes() != 0)
     # probe with a small stride, then size the sample to ~args.cpu_seconds
     stride = max(1, len(off) // 40)
@@ -129,19 +153,27 @@ def cpu_worker(args):
     keep = off[::stride]
     times = []
     for _ in range(max(1, args.cpu_reps)):
+        y[:] = 0.0
         dt, pr = run(keep)
         times.append(dt)
     dt = float(np.median(times))
-    full = float(pairs.sum())
     sec_per_sigma = dt * full / pr
+    if args.cpu_out:
+        # the sampled sub-network's reference sigma, for the GPU parity check
+        np.save(os.path.join(args.cpu_out, "keep.npy"), keep)
+        np.save(os.path.join(args.cpu_out, "sigma_ref.npy"), y)
     print(json.dumps({
         "value": 1.0 / sec_per_sigma, "sec_per_sigma": sec_per_sigma, "sample_pairs": pr, "full_pairs": full,
         "sample_groups": int(len(keep)), "stride": int(stride), "sample_seconds": dt, "reps": len(times),
-        "threads": int(os.environ.get("OMP_NUM_THREADS", "0")),
+        "threads": threads,
     }))
 
 
-def run_cpu_baseline(args):
+def run_cpu_baseline(args, full=False, out_dir=None, seconds=None, reps=None):
+    """The reference's sigma on the host cores in a worker process (no torch):
+    a sample of the groups scaled by pair counts, or with full=True whole sigmas
+    (reps of them, as many as fit in `seconds`, at least one).  out_dir: the
+    sampled run saves its groups and its sigma there."""
     try:
         import psutil
         cores = psutil.cpu_count(logical=False) or os.cpu_count()
@@ -149,8 +181,13 @@ def run_cpu_baseline(args):
         cores = os.cpu_count()
     env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close", OMP_PLACES="cores")
     env.pop("CUDA_VISIBLE_DEVICES", None)
-    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--cpu-seconds", str(args.cpu_seconds),
-           "--cpu-reps", str(args.cpu_reps), "--sigma-size", args.sigma_size]
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker",
+           "--cpu-seconds", str(args.cpu_seconds if seconds is None else seconds),
+           "--cpu-reps", str(args.cpu_reps if reps is None else reps), "--sigma-size", args.sigma_size]
+    if full:
+        cmd.append("--cpu-full")
+    if out_dir:
+        cmd += ["--cpu-out", out_dir]
     r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
     if r.returncode != 0:
         log(r.stderr[-2000:])
@@ -453,7 +490,79 @@ def gpu_sigma(args, rank, world, local_rank):
             "gpu_launches": launches * args.steps if launches else None,
             "clocks": clk.summary(),
         }
-    return result
+    return result, net
+
+
+def sampled_parity(args, net, sample_dir):
+    """The GPU sigma (FP64 and FP32 bulk) of the sub-network the CPU leg ran
+    through the reference's hvec_gather_contract_otf_f64 (op/hvec.hpp:481-496),
+    on the same input, against the reference's result."""
+    import torch
+    from binsim_b200 import cuotf
+    cfg = SIGMA_CFGS[args.sigma_size]
+    keep = np.load(os.path.join(sample_dir, "keep.npy"))
+    yref = np.load(os.path.join(sample_dir, "sigma_ref.npy"))
+    sub = subnetwork(net, keep)
+    B = cuotf.CuBasis(cfg["norb"], cfg["na"], cfg["nb"])
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(sub))
+    rng = np.random.default_rng(1)   # the CPU leg's input
+    xh = rng.normal(size=B.dim)
+    xh /= np.linalg.norm(xh)
+    x = torch.from_numpy(xh).cuda()
+    y = torch.empty_like(x)
+    scale = float(np.abs(yref).max())
+    out = {"groups": int(len(keep)), "of_groups": int(net.ngs), "sigma_path": f.sigma_path()[0],
+           "max_abs_ref": scale,
+           "note": "the CPU leg's sampled sub-network (every k-th off-diagonal group), same input c: GPU sigma "
+                   "vs the reference's hvec_gather_contract_otf_f64 on the host; rel = abs / max|sigma_ref|"}
+    for name, fn in (("fp64", f.hvec), ("fp32_bulk", f.hvec_mixed)):
+        fn(x, y)
+        d = float(np.abs(y.cpu().numpy() - yref).max())
+        out[name] = {"max_abs_err_vs_reference": d, "max_rel_err_vs_reference": d / scale}
+    del f, B, x, y
+    torch.cuda.empty_cache()
+    return out
+
+
+def north_star(args):
+    """The task's two targets at their named sizes, for the default line: FCI
+    Davidson at 12 orbitals 6a+6b (FP64 and mixed, time to the root, energy error
+    against the reference's CPU Davidson) and VQE energy + adjoint gradient at 14
+    orbitals 7a+7b with 2000 generators (against the reference-style backgrad
+    sweep and the per-parameter gradient by central differences)."""
+    import copy
+    import torch
+    a = copy.copy(args)
+    a.steps, a.warmup, a.dav_size = 3, 3, "12o"
+    t0 = time.time()
+    dav = gpu_davidson(a)
+    torch.cuda.empty_cache()
+    t1 = time.time()
+    vqe = gpu_vqe(a)
+    torch.cuda.empty_cache()
+    t2 = time.time()
+    pp = vqe["adjoint_vs_per_parameter"]
+    return {
+        "fci_davidson_12o": {
+            "workload": dav["config"]["workload"], "fp64_s": dav["fp64"]["seconds"],
+            "mixed_s": dav["mixed"]["seconds"], "mixed_speedup_vs_fp64": dav["mixed"]["speedup_vs_fp64"],
+            "fp64_abs_err_vs_oracle_eh": dav["fp64"]["abs_err_vs_oracle"],
+            "mixed_abs_err_vs_oracle_eh": dav["mixed"]["abs_err_vs_oracle"],
+            "fp64_iterations": dav["fp64"]["iterations"], "mixed_iterations": dav["mixed"]["iterations"],
+            "mixed_sigma_fp32": dav["mixed"]["sigma_fp32"], "mixed_sigma_fp64": dav["mixed"]["sigma_fp64"],
+            "oracle_energy": dav["oracle_energy"], "reference_cpu_s": (dav.get("cpu_baseline") or {}).get("value"),
+            "solves_timed": dav["steps"], "target": "mixed >= 1.5x faster than FP64 within 1e-8 Eh"},
+        "vqe_14o": {
+            "workload": vqe["config"]["workload"], "evals_per_s": vqe["value"], "ms_per_eval": vqe["ms_per_step"],
+            "energy": vqe["energy"],
+            "reference_sweep_ms": vqe["adjoint_vs_reference_sweep"]["sweep_ms"],
+            "adjoint_vs_reference_sweep": vqe["adjoint_vs_reference_sweep"]["speedup"],
+            "max_abs_grad_diff_vs_sweep": vqe["adjoint_vs_reference_sweep"]["max_abs_grad_diff"],
+            "per_parameter_gradient_ms": pp["fd_ms"], "adjoint_vs_per_parameter": pp["speedup"],
+            "per_parameter_sample": pp["sample"], "max_abs_fd_err": pp["max_abs_fd_err"],
+            "target": "adjoint >= 10x faster than the per-parameter gradient at 1e-7 agreement"},
+        "seconds": {"davidson": round(t1 - t0, 1), "vqe": round(t2 - t1, 1)},
+    }
 
 
 def count_launches(fn, prefix="bsim::"):
@@ -491,6 +600,49 @@ def timed_events(fn, k, w):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / k
+
+
+# ---------------------------------------------------------------------------
+# Band overhead of the sharded sigma, measured on one GPU
+# ---------------------------------------------------------------------------
+
+def gpu_bands(args):
+    """The per-rank unit of the N-GPU sigma (bsim_hvec_cols, one beta-column
+    band) timed band by band on one GPU for N = 2, 4, 8: the sum over the N bands
+    against one whole sigma is the work the split adds (with a band, the beta
+    same-spin doubles go through the row lists instead of the intermediate-string
+    GEMM), and the largest band bounds the N-GPU step before its all-gather."""
+    import torch
+    from binsim_b200 import cuotf, network as nw
+    from binsim_b200.shard import column_bands
+    cfg = SIGMA_CFGS[args.sigma_size]
+    torch.cuda.set_device(0)
+    net = nw.hamiltonian_network(cfg["norb"], seed=cfg["seed"])
+    B = cuotf.CuBasis(cfg["norb"], cfg["na"], cfg["nb"])
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    nA, nB = math.comb(cfg["norb"], cfg["na"]), math.comb(cfg["norb"], cfg["nb"])
+    rng = np.random.default_rng(1)
+    xh = rng.normal(size=B.dim)
+    xh /= np.linalg.norm(xh)
+    x = torch.from_numpy(xh).cuda()
+    y = torch.empty_like(x)
+    steps, warm = max(1, args.steps), max(3, args.warmup)
+    out = {}
+    for mixed in (False, True):
+        key = "fp32_bulk" if mixed else "fp64"
+        whole = timed_events(lambda: (f.hvec_mixed if mixed else f.hvec)(x, y), steps, warm)
+        per_n = {}
+        for n in (2, 4, 8):
+            bands = column_bands(nB, n)
+            ms = [timed_events(lambda lo=lo, hi=hi: f.hvec_cols(x, y, lo, hi, mixed=mixed), steps, 1)
+                  for lo, hi in bands if hi > lo]
+            per_n[str(n)] = {"bands_ms": [round(v, 3) for v in ms], "sum_ms": sum(ms), "max_ms": max(ms),
+                             "overhead_vs_whole": sum(ms) / whole - 1.0, "ideal_speedup": whole / max(ms)}
+        out[key] = {"whole_ms": whole, "splits": per_n}
+    return {"metric": "sigma band overhead on one GPU", "unit": "ms", "n_gpus": 1, "steps": steps, "warmup": warm,
+            "config": {"workload": f"sigma, {cfg['norb']} orbitals {cfg['na']}a+{cfg['nb']}b, beta-column bands of "
+                                   f"{nB} columns (starts on multiples of 128), {nA} alpha rows"},
+            "bands": out}
 
 
 # ---------------------------------------------------------------------------
@@ -766,15 +918,21 @@ def gpu_vqe(args):
         f.hvec(lv, rv)
         return float(lv @ rv) / float(lv @ lv)
     ms_energy = timed_events(lambda: energy(th), steps, 1)
+    # measured on a sample: the central-difference gradient of the 8 steepest
+    # parameters (16 energies), timed with CUDA events, scaled to every parameter
     h = 1e-5
-    fd_err = 0.0
-    fd_params = [int(p) for p in np.argsort(-np.abs(g))[:4]]   # the steepest parameters
-    for p in fd_params:
-        tp, tm = th.copy(), th.copy()
-        tp[p] += h
-        tm[p] -= h
-        fd_err = max(fd_err, abs((energy(tp) - energy(tm)) / (2 * h) - g[p]))
-    ms_fd = 2 * len(th) * ms_energy
+    fd_params = [int(p) for p in np.argsort(-np.abs(g))[:8]]
+    fd = {}
+
+    def fd_sample():
+        for p in fd_params:
+            tp, tm = th.copy(), th.copy()
+            tp[p] += h
+            tm[p] -= h
+            fd[p] = (energy(tp) - energy(tm)) / (2 * h)
+    ms_fd_sample = timed_events(fd_sample, 1, 0)
+    fd_err = max(abs(fd[p] - g[p]) for p in fd_params)
+    ms_fd = ms_fd_sample * len(th) / len(fd_params)
     # e2e: parameters from the host, energy and gradient back to the host (the call does both)
     res = {
         "metric": VQE_METRIC, "value": 1000.0 / ms_adj, "unit": "evals/s", "n_gpus": 1, "steps": steps,
@@ -793,8 +951,11 @@ def gpu_vqe(args):
         "adjoint_vs_per_parameter": {"fd_ms": ms_fd, "energy_ms": ms_energy, "speedup": ms_fd / ms_adj,
                                      "max_abs_fd_err": fd_err, "fd_params": fd_params,
                                      "fd_grads": [float(g[p]) for p in fd_params],
-                                     "note": "central differences h=1e-5: 2 energies per parameter, "
-                                             "time = 2 * params * one energy evaluation"},
+                                     "sample": f"central differences (h = 1e-5) of the {len(fd_params)} steepest "
+                                               f"parameters measured ({ms_fd_sample:.1f} ms for "
+                                               f"{2 * len(fd_params)} energies), scaled by {len(th)} / "
+                                               f"{len(fd_params)} parameters",
+                                     "note": "the plain per-parameter gradient: 2 energies per parameter"},
         "e2e": {"value": 1000.0 / ms_adj, "unit": "evals/s", "h2d_bytes_per_step": int(8 * (len(th) + 2 * len(op_idx))),
                 "d2h_bytes_per_step": int(8 * (len(th) + 2)), "ms_per_step": ms_adj,
                 "note": "the public call takes host parameters and returns host energy and gradient"},
@@ -864,6 +1025,13 @@ def gpu_adapt(args):
         f.hvec(psi, hpsi)
         f.batchgrad(psi, hpsi, grads, zeros)
         gen_grads.zero_().index_add_(0, comp_gen_t, grads)
+    # first call: builds the sigma plan and the theta = 0 route (pool classification,
+    # hole tables, density scratch) outside the timed region
+    t0 = time.time()
+    f.hvec(psi, hpsi)
+    f.batchgrad(psi, hpsi, grads, zeros)
+    torch.cuda.synchronize()
+    first_call_s = time.time() - t0
     steps, warm = max(1, args.steps), max(3, args.warmup)
     with Clocks(0) as clk:
         ms = timed_events(screen, steps, warm)
@@ -881,15 +1049,16 @@ def gpu_adapt(args):
     ms_adj = timed_events(adjoint, steps, 1)
     E, ga, _ = out["a"]
     density = None
-    if args.pool_density:   # the transition-density pool gradient beside the pair-list one
-        t0 = time.time()
-        pd = cuotf.PoolDensity(B, pool.network)
-        plan_s = time.time() - t0
-        grads_d = torch.empty_like(grads)
-        ms_pd = timed_events(lambda: pd.grad(psi, hpsi, grads_d), steps, 1)
+    if args.pool_density:
+        # the pair-list gradient beside the theta = 0 route: every theta 1e-300 sends
+        # every group to the pair lists (the same work as at theta = 0, gradients equal
+        # to rounding)
+        tiny = torch.full_like(zeros, 1e-300)
+        grads_p = torch.empty_like(grads)
+        ms_pl = timed_events(lambda: f.batchgrad(psi, hpsi, grads_p, tiny), max(1, min(steps, 2)), 1)
         f.batchgrad(psi, hpsi, grads, zeros)
         torch.cuda.synchronize()
-        a_, b_ = grads_d.cpu().numpy(), grads.cpu().numpy()
+        a_, b_ = grads.cpu().numpy(), grads_p.cpu().numpy()
         # GEMM flops as launched: Tab (n^2 x n^2 over one-hole alpha x beta strings) and the
         # two same-spin tables (pairs x pairs over two-hole strings x the other spin's strings)
         from math import comb
@@ -899,13 +1068,16 @@ def gpu_adapt(args):
         flops += 2.0 * npair ** 2 * (comb(n_, na_ - 2) * comb(n_, nb_) if na_ >= 2 else 0)
         flops += 2.0 * npair ** 2 * (comb(n_, nb_ - 2) * comb(n_, na_) if nb_ >= 2 else 0)
         dmma = cuotf.fma_peak(dmma=True)
-        density = {"ms": ms_pd, "pair_list_ms": ms_bg, "plan_s": plan_s, "gemm_flops": flops,
-                   "tflops": flops / (ms_pd * 1e-3) / 1e12, "fp64_dmma_peak_tflops": dmma,
-                   "frac_of_measured_dmma_peak": flops / (ms_pd * 1e-3) / 1e12 / dmma,
-                   "general_groups": int((pd.kind < 0).sum()),
-                   "max_abs_diff_vs_pair_list": float(np.nanmax(np.abs(a_ - b_))),
-                   "max_abs_grad": float(np.abs(b_).max())}
-        del pd
+        kind, _, _ = cuotf.pool_plan(pool.network)
+        density = {"ms": ms_bg, "pair_list_ms": ms_pl, "speedup_vs_pair_list": ms_pl / ms_bg,
+                   "first_call_s": first_call_s, "gemm_flops": flops,
+                   "tflops": flops / (ms_bg * 1e-3) / 1e12, "fp64_dmma_peak_tflops": dmma,
+                   "frac_of_measured_dmma_peak": flops / (ms_bg * 1e-3) / 1e12 / dmma,
+                   "general_groups": int((kind < 0).sum()),
+                   "max_abs_diff_vs_pair_list": float(np.abs(a_ - b_).max()),
+                   "max_abs_grad": float(np.abs(b_).max()),
+                   "note": "batchgrad at theta = 0 takes the transition-density route; the pair lists are timed "
+                           "with every theta = 1e-300"}
     res = {
         "metric": ADAPT_METRIC, "value": len(pool.components) / (ms * 1e-3), "unit": "generators/s", "n_gpus": 1,
         "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "replicas",
@@ -1103,14 +1275,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="sigma", choices=["sigma", "davidson", "vqe", "adapt", "block"])
+    ap.add_argument("--workload", default="sigma", choices=["sigma", "davidson", "vqe", "adapt", "block", "bands"])
     ap.add_argument("--block-size", default="16o", choices=sorted(BLOCK_CFGS))
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--adapt-state", default="")
     ap.add_argument("--adapt-sample", type=int, default=400)
     ap.add_argument("--adapt-norb", type=int, default=ADAPT_CFG["norb"])
     ap.add_argument("--pool-density", action="store_true",
-                    help="adapt: also time the transition-density pool gradient and compare it with the pair lists")
+                    help="adapt: also time the pair-list pool gradient and compare it with the theta = 0 "
+                         "density route batchgrad takes")
     ap.add_argument("--dav-size", default="12o", choices=sorted(DAV_CFGS))
     ap.add_argument("--sigma-size", default="16o", choices=sorted(SIGMA_CFGS))
     ap.add_argument("--dav-oracle", action="store_true")
@@ -1119,6 +1292,10 @@ def main():
     ap.add_argument("--cpu-reps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-worker", action="store_true")
+    ap.add_argument("--cpu-full", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-out", default="", help=argparse.SUPPRESS)
+    ap.add_argument("--no-north-star", action="store_true",
+                    help="default line: skip the Davidson (12 orbitals) and VQE (14 orbitals) figures")
     args = ap.parse_args()
 
     if args.cpu_worker:
@@ -1141,7 +1318,7 @@ def main():
         if rank != 0:
             return
         result = {"davidson": gpu_davidson, "vqe": gpu_vqe, "adapt": gpu_adapt,
-                  "block": gpu_block_davidson}[args.workload](args)
+                  "block": gpu_block_davidson, "bands": gpu_bands}[args.workload](args)
         if args.workload == "vqe" and not args.no_cpu_baseline:
             cpu = run_cpu_vqe(args)
             if cpu and "seconds" in cpu:
@@ -1155,43 +1332,80 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     try:
-        result = gpu_sigma(args, rank, world, local_rank)
+        result, net = gpu_sigma(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
     if rank == 0:
         if not args.no_cpu_baseline:
-            res, cores = run_cpu_baseline(args)
-            if res and "value" in res:
-                result["cpu_baseline"] = {
-                    "value": res["value"], "unit": UNIT, "cores": cores, "kind": "reference",
-                    "sample": f"reference libotf_native sigma on every {res['stride']}-th off-diagonal group "
-                              f"({res['sample_pairs']:.3e} of {res['full_pairs']:.3e} pair updates, "
-                              f"{res['sample_seconds']:.1f} s), scaled by exact pair counts; {cpu_model()}"}
-            else:
-                result["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
-                                          "sample": "unavailable: oracle/_ref not built"}
+            import shutil
+            import tempfile
+            tmp = tempfile.mkdtemp(prefix="bsim_ref_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+            try:
+                res, cores = run_cpu_baseline(args, out_dir=tmp if world == 1 else None)
+                if res and "value" in res:
+                    result["cpu_baseline"] = {
+                        "value": res["value"], "unit": UNIT, "cores": cores, "kind": "reference",
+                        "sample": f"reference libotf_native sigma on every {res['stride']}-th off-diagonal group "
+                                  f"({res['sample_pairs']:.3e} of {res['full_pairs']:.3e} pair updates, "
+                                  f"{res['sample_seconds']:.1f} s), scaled by exact pair counts; {cpu_model()}"}
+                    if world == 1:
+                        result["parity_vs_reference"] = sampled_parity(args, net, tmp)
+                else:
+                    result["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
+                                              "sample": "unavailable: oracle/_ref not built"}
+            finally:
+                shutil.rmtree(tmp, ignore_errors=True)
+        if world == 1 and not args.no_north_star and args.sigma_size == "16o":
+            result["north_star"] = north_star(args)
         print(json.dumps(result))
+
+
+REF_SIGMA_SECONDS = 150.0
+
+
+def reference_gpu_sigma(cfg):
+    """The reference's own GPU library (src/extern/cuotf.cu built unchanged for
+    sm_100a into oracle/_ref/libcuotf_ref.so) on the same sigma, driven through
+    its C-ABI with the reference's host handles, as jl/cuda/cunetwork.jl does."""
+    try:
+        from oracle import time_ref_gpu
+        r = time_ref_gpu.time_sigma(cfg["norb"], compare=False)
+        return {"seconds_per_sigma": r["reference_gpu_s"], "value": 1.0 / r["reference_gpu_s"], "unit": UNIT,
+                "reps": r["reps"], "what": r["what"],
+                "note": "reference libcuotf hvec_cuda, legacy default stream, wall time around reps with "
+                        "sync_device_cuda"}
+    except Exception as e:   # library not built, or no GPU
+        return {"unavailable": f"{type(e).__name__}: {str(e)[:200]}"}
 
 
 def reference_arm(args):
     """The reference's own CPU implementation of the workload, on the host cores."""
     base = {"impl": "reference", "n_gpus": args.gpus, "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
     if args.workload == "sigma":
-        res, cores = run_cpu_baseline(args)
+        # whole sigmas of the full network, as many as fit in REF_SIGMA_SECONDS
+        # (at least one; ~70 s each at 16 orbitals on 16 cores)
+        res, cores = run_cpu_baseline(args, full=True, seconds=REF_SIGMA_SECONDS, reps=max(1, args.steps))
         if res is None or "unavailable" in res:
             print(json.dumps({"impl": "reference", "unavailable": (res or {}).get("unavailable", "worker failed")}))
             return
-        sample = (f"reference libotf_native hvec_gather_contract_otf_f64 on every {res['stride']}-th off-diagonal "
-                  f"group ({res['sample_groups']} groups, {res['sample_pairs']:.3e} of {res['full_pairs']:.3e} pair "
-                  f"updates), scaled by exact pair counts; {cpu_model()}")
-        line = dict(base, metric=METRIC, value=res["value"], unit=UNIT, steps=res["reps"], warmup=1,
+        cfg = SIGMA_CFGS[args.sigma_size]
+        sample = (f"reference libotf_native hvec_gather_contract_otf_f64 over the whole network ({res['sample_groups']} "
+                  f"groups, {res['full_pairs']:.3e} pair updates per sigma), {res['reps']} sigma(s) measured "
+                  f"(median), {res['threads']} OpenMP threads; {cpu_model()}")
+        line = dict(base, metric=METRIC, value=res["value"], unit=UNIT, steps=res["reps"],
+                    requested_steps=args.steps,
+                    warmup="1 untimed sigma of every 200th group (threads, first touch)",
                     ms_per_step=res["sec_per_sigma"] * 1e3, higher_is_better=True, scaling="strong",
-                    config={"workload": "sigma microbenchmark (config 1): H*c, 16 orbitals 8a+8b"},
+                    config={"workload": f"sigma microbenchmark: H*c, {cfg['norb']} orbitals {cfg['na']}a+{cfg['nb']}b, "
+                                        "seeded synthetic integrals (seed 0), c ~ N(0,1) normalised"},
+                    seconds_per_sigma=res["times"],
                     cpu_baseline={"value": res["value"], "unit": UNIT, "cores": cores, "kind": "reference",
                                   "sample": sample},
                     e2e={"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        if args.gpus == 1:
+            line["reference_gpu"] = reference_gpu_sigma(cfg)
     elif args.workload == "davidson":
         if args.dav_size != "12o":
             print(json.dumps({"impl": "reference", "unavailable": "the CPU reference solve of the 16-orbital space "
@@ -1213,6 +1427,10 @@ def reference_arm(args):
                                                               "one root; it has no block solver for the lowest 2 roots, "
                                                               "and one reference sigma at 18 orbitals takes ~2,900 s on "
                                                               "the host cores"}))
+        return
+    elif args.workload == "bands":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no sharded sigma (single process, "
+                                                              "one device)"}))
         return
     elif args.workload == "adapt":
         print(json.dumps({"impl": "reference", "unavailable": "the reference's basis library is UInt32-only and its "

@@ -49,9 +49,11 @@ def ref_gpu_lib():
     return L
 
 
-def time_sigma(norb):
+def time_sigma(norb, compare=True):
+    """hvec_cuda of the reference GPU library at norb orbitals (norb/2 + norb/2
+    electrons); with compare, also this library's sigma on the same input."""
     import torch
-    from binsim_b200 import cuotf, network as nw
+    from binsim_b200 import network as nw
     from oracle.oracle import RefLibs
     ne = norb // 2
     R, L = RefLibs(), ref_gpu_lib()
@@ -70,6 +72,10 @@ def time_sigma(norb):
         L.hvec_cuda(db, dn, x.data_ptr(), y.data_ptr())
     L.sync_device_cuda()
     ref_s = (time.perf_counter() - t0) / reps
+    if not compare:
+        return {"what": f"hvec_cuda, {norb} orbitals {ne}a+{ne}b, dim {dim}", "reference_gpu_s": ref_s,
+                "reps": reps}
+    from binsim_b200 import cuotf
     B = cuotf.CuBasis(norb, ne, ne)
     f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
     y2 = torch.empty_like(x)

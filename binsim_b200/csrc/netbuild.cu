@@ -8,8 +8,9 @@
 // tol are kept (rank), wa = U sqrt(S), wb = V sqrt(S), entries below 1e-12 are
 // zeroed, and the weights are stored column-major [num_z x rank] as the
 // reference's build_network_otf expects (otf.hpp:84-85).  Groups are
-// independent and compressed on all host threads.  No device code: the result
-// feeds bsim_network_create_u32 / _u64.
+// independent and compressed on all host threads, or (bsim_netbuild_compress_device)
+// with the Jacobi sweeps of every group on the GPU, one CTA per group.  The
+// result feeds bsim_network_create_u32 / _u64.
 #include "../../include/binsim_cuotf.h"
 #include "common.cuh"
 
@@ -77,19 +78,36 @@ void jacobi_svd(int m, int n, std::vector<double> &A, std::vector<double> &V)
     }
 }
 
-// M (m x n, column-major) -> rank, wa (m x rank), wb (n x rank), column-major
-void compress(int m, int n, const std::vector<double> &M, double tol, BuiltGroup &G)
+// The factored matrix: A = M (m x n, column-major) when m >= n, else A = M^T, so
+// that A is at least as tall as it is wide (one-sided Jacobi rotates columns).
+void factored(int m, int n, const std::vector<double> &M, bool tr, double *A)
 {
-    const bool tr = m < n;   // factor the transpose when it is the taller one
-    const int mm = tr ? n : m, nn = tr ? m : n;
-    std::vector<double> A((size_t)mm * nn), V;
+    const int mm = tr ? n : m;
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < m; ++i) {
             const double v = M[(size_t)j * m + i];
             if (tr) A[(size_t)i * mm + j] = v;   // A = M^T
             else A[(size_t)j * mm + i] = v;
         }
+}
+
+// After the Jacobi sweeps (A's columns = U S, V the right vectors): the rank
+// above tol and the weights wa, wb of the original orientation.
+void finish_factors(int mm, int nn, bool tr, const double *A, const double *V, double tol, BuiltGroup &G);
+
+// M (m x n, column-major) -> rank, wa (m x rank), wb (n x rank), column-major
+void compress(int m, int n, const std::vector<double> &M, double tol, BuiltGroup &G)
+{
+    const bool tr = m < n;   // factor the transpose when it is the taller one
+    const int mm = tr ? n : m, nn = tr ? m : n;
+    std::vector<double> A((size_t)mm * nn), V;
+    factored(m, n, M, tr, A.data());
     jacobi_svd(mm, nn, A, V);
+    finish_factors(mm, nn, tr, A.data(), V.data(), tol, G);
+}
+
+void finish_factors(int mm, int nn, bool tr, const double *A, const double *V, double tol, BuiltGroup &G)
+{
     std::vector<double> sv(nn);
     for (int k = 0; k < nn; ++k) {
         double s = 0.0;
@@ -121,6 +139,120 @@ void compress(int m, int n, const std::vector<double> &M, double tol, BuiltGroup
         if (std::fabs(x) < 1e-12) x = 0.0;
 }
 
+// ---- device SVD: one CTA per group -----------------------------------------------
+struct SvdJob {
+    i64 a_off, v_off;   // A (m x n, column-major, m >= n) and V (n x n) in the packed buffers
+    int m, n;
+};
+
+// The one-sided Jacobi SVD of jacobi_svd on the device: each sweep visits every
+// column pair once in n' - 1 rounds of the round-robin (circle) schedule, n' = n
+// rounded up to even; the pairs of a round are disjoint and go to the warps of
+// the CTA, each warp reducing the pair's dot products over the rows with its
+// lanes.  Same rotation, skip and convergence rules as the host code.
+__global__ void __launch_bounds__(512) jacobi_svd_kernel(const SvdJob *__restrict__ jobs, double *__restrict__ A,
+                                                         double *__restrict__ V, int max_sweeps)
+{
+    const SvdJob J = jobs[blockIdx.x];
+    const int m = J.m, n = J.n;
+    double *a = A + J.a_off, *v = V + J.v_off;
+    for (i64 i = threadIdx.x; i < (i64)n * n; i += blockDim.x) v[i] = (i % (n + 1) == 0) ? 1.0 : 0.0;
+    if (n < 2) return;
+    __syncthreads();
+    const int np = n + (n & 1);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __shared__ unsigned long long offbits;   // max |gamma| / scale of the sweep (non-negative: bits order like values)
+    for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+        if (threadIdx.x == 0) offbits = 0ull;
+        __syncthreads();
+        double off = 0.0;
+        for (int r = 0; r < np - 1; ++r) {
+            for (int k = w; k < np / 2; k += nw) {
+                int p = k == 0 ? np - 1 : (r + k) % (np - 1);
+                int q = k == 0 ? r : (r - k + np - 1) % (np - 1);
+                if (p > q) { const int t = p; p = q; q = t; }
+                if (q >= n) continue;   // paired with the bye
+                double *ap = a + (i64)p * m, *aq = a + (i64)q * m;
+                double al = 0.0, be = 0.0, ga = 0.0;
+                for (int i = lane; i < m; i += 32) {
+                    const double x = ap[i], y = aq[i];
+                    al += x * x;
+                    be += y * y;
+                    ga += x * y;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    al += __shfl_xor_sync(0xffffffffu, al, o);
+                    be += __shfl_xor_sync(0xffffffffu, be, o);
+                    ga += __shfl_xor_sync(0xffffffffu, ga, o);
+                }
+                if (fabs(ga) <= 1e-300) continue;
+                const double scale = sqrt(al * be);
+                if (scale <= 0.0) continue;
+                off = fmax(off, fabs(ga) / scale);
+                if (fabs(ga) <= 1e-15 * scale) continue;
+                const double zeta = (be - al) / (2.0 * ga);
+                const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+                for (int i = lane; i < m; i += 32) {
+                    const double x = ap[i], y = aq[i];
+                    ap[i] = c * x - s * y;
+                    aq[i] = s * x + c * y;
+                }
+                double *vp = v + (i64)p * n, *vq = v + (i64)q * n;
+                for (int i = lane; i < n; i += 32) {
+                    const double x = vp[i], y = vq[i];
+                    vp[i] = c * x - s * y;
+                    vq[i] = s * x + c * y;
+                }
+            }
+            __syncthreads();   // the next round's pairs reuse these columns
+        }
+        if (lane == 0) atomicMax(&offbits, (unsigned long long)__double_as_longlong(off));
+        __syncthreads();
+        const double o = __longlong_as_double((long long)offbits);
+        __syncthreads();   // every thread has read offbits before it is reset
+        if (o <= 1e-15) break;
+    }
+}
+
+// Jacobi SVDs of the packed factored matrices on the current device, small
+// jobs (n <= 8) with 64 threads per CTA and the rest with 512.
+int device_svds(const std::vector<SvdJob> &jobs, std::vector<double> &A, std::vector<double> &V, cudaStream_t s)
+{
+    if (jobs.empty()) return BSIM_OK;
+    std::vector<SvdJob> small, large;
+    for (const SvdJob &j : jobs) (j.n <= 8 ? small : large).push_back(j);
+    SvdJob *dj = nullptr;
+    double *dA = nullptr, *dV = nullptr;
+    int st = BSIM_OK;
+    cudaError_t e = dmalloc(&dj, sizeof(SvdJob) * jobs.size());
+    if (e == cudaSuccess) e = dmalloc(&dA, sizeof(double) * std::max<size_t>(A.size(), 1));
+    if (e == cudaSuccess) e = dmalloc(&dV, sizeof(double) * std::max<size_t>(V.size(), 1));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dA, A.data(), sizeof(double) * A.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && !small.empty())
+        e = cudaMemcpyAsync(dj, small.data(), sizeof(SvdJob) * small.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && !large.empty())
+        e = cudaMemcpyAsync(dj + small.size(), large.data(), sizeof(SvdJob) * large.size(), cudaMemcpyHostToDevice, s);
+    // grid x is limited to 2^31 - 1 CTAs; one launch per kind of job
+    if (e == cudaSuccess && !small.empty()) {
+        jacobi_svd_kernel<<<(unsigned)small.size(), 64, 0, s>>>(dj, dA, dV, 60);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && !large.empty()) {
+        jacobi_svd_kernel<<<(unsigned)large.size(), 512, 0, s>>>(dj + small.size(), dA, dV, 60);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(A.data(), dA, sizeof(double) * A.size(), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(V.data(), dV, sizeof(double) * V.size(), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_status(e, "device network SVD");
+    cudaFree(dj);
+    cudaFree(dA);
+    cudaFree(dV);
+    return st;
+}
+
 NetBuild *nb_of(void *h)
 {
     auto *p = static_cast<NetBuild *>(h);
@@ -131,7 +263,8 @@ NetBuild *nb_of(void *h)
 }  // namespace bsim
 
 static int netbuild(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx, const uint64_t *bz,
-                    const double *coef, double tol, int64_t nruns, const int64_t *run_sizes, void **out)
+                    const double *coef, double tol, int64_t nruns, const int64_t *run_sizes, void **out,
+                    bool device = false, cudaStream_t stream = nullptr)
 {
     using bsim::u64;
     if (!out) { bsim::set_error("null out"); return BSIM_ERR_NULL; }
@@ -182,28 +315,72 @@ static int netbuild(int64_t nterms, const uint64_t *ax, const uint64_t *az, cons
     for (size_t g = 0; g < members.size(); ++g) { B->g[g].ax = keys[g].first; B->g[g].bx = keys[g].second; }
     const int ng = (int)members.size();
     const int nth = std::max(1, std::min(32, (int)std::thread::hardware_concurrency()));
-    auto work = [&](int w) {
-        for (int g = w; g < ng; g += nth) {
-            bsim::BuiltGroup &G = B->g[g];
-            for (int64_t t : members[g]) { G.za.push_back((u64)az[t]); G.zb.push_back((u64)bz[t]); }
-            std::sort(G.za.begin(), G.za.end());
-            G.za.erase(std::unique(G.za.begin(), G.za.end()), G.za.end());
-            std::sort(G.zb.begin(), G.zb.end());
-            G.zb.erase(std::unique(G.zb.begin(), G.zb.end()), G.zb.end());
-            const int m = (int)G.za.size(), n = (int)G.zb.size();
-            std::vector<double> M((size_t)m * n, 0.0);
-            for (int64_t t : members[g]) {
-                const int i = (int)(std::lower_bound(G.za.begin(), G.za.end(), (u64)az[t]) - G.za.begin());
-                const int j = (int)(std::lower_bound(G.zb.begin(), G.zb.end(), (u64)bz[t]) - G.zb.begin());
-                M[(size_t)j * m + i] += coef[t];
-            }
-            bsim::compress(m, n, M, tol, G);
+    auto run = [&](auto &&fn) {
+        std::vector<std::thread> th;
+        for (int w = 1; w < nth; ++w) th.emplace_back(fn, w);
+        fn(0);
+        for (auto &x : th) x.join();
+    };
+    // the group's Z lists and coefficient matrix M[za, zb] (column-major)
+    auto matrix = [&](int g, std::vector<double> &M) {
+        bsim::BuiltGroup &G = B->g[g];
+        for (int64_t t : members[g]) { G.za.push_back((u64)az[t]); G.zb.push_back((u64)bz[t]); }
+        std::sort(G.za.begin(), G.za.end());
+        G.za.erase(std::unique(G.za.begin(), G.za.end()), G.za.end());
+        std::sort(G.zb.begin(), G.zb.end());
+        G.zb.erase(std::unique(G.zb.begin(), G.zb.end()), G.zb.end());
+        const int m = (int)G.za.size(), n = (int)G.zb.size();
+        M.assign((size_t)m * n, 0.0);
+        for (int64_t t : members[g]) {
+            const int i = (int)(std::lower_bound(G.za.begin(), G.za.end(), (u64)az[t]) - G.za.begin());
+            const int j = (int)(std::lower_bound(G.zb.begin(), G.zb.end(), (u64)bz[t]) - G.zb.begin());
+            M[(size_t)j * m + i] += coef[t];
         }
     };
-    std::vector<std::thread> th;
-    for (int w = 1; w < nth; ++w) th.emplace_back(work, w);
-    work(0);
-    for (auto &x : th) x.join();
+    if (!device) {
+        run([&](int w) {
+            std::vector<double> M;
+            for (int g = w; g < ng; g += nth) {
+                matrix(g, M);
+                bsim::compress((int)B->g[g].za.size(), (int)B->g[g].zb.size(), M, tol, B->g[g]);
+            }
+        });
+        *out = B;
+        return BSIM_OK;
+    }
+    // device SVDs: the host groups the terms and packs every group's factored
+    // matrix; the Jacobi sweeps run on the GPU, one CTA per group; the host then
+    // keeps the singular values above tol and scales the factors
+    std::vector<bsim::SvdJob> jobs(ng);
+    std::vector<std::vector<double>> Ms(ng);
+    run([&](int w) {
+        for (int g = w; g < ng; g += nth) matrix(g, Ms[g]);
+    });
+    int64_t na_tot = 0, nv_tot = 0;
+    for (int g = 0; g < ng; ++g) {
+        const int m = (int)B->g[g].za.size(), n = (int)B->g[g].zb.size();
+        const int mm = std::max(m, n), nn = std::min(m, n);
+        jobs[g] = bsim::SvdJob{na_tot, nv_tot, mm, nn};
+        na_tot += (int64_t)mm * nn;
+        nv_tot += (int64_t)nn * nn;
+    }
+    std::vector<double> A((size_t)na_tot), V((size_t)nv_tot);
+    run([&](int w) {
+        for (int g = w; g < ng; g += nth) {
+            const int m = (int)B->g[g].za.size(), n = (int)B->g[g].zb.size();
+            bsim::factored(m, n, Ms[g], m < n, A.data() + jobs[g].a_off);
+            std::vector<double>().swap(Ms[g]);
+        }
+    });
+    int st = bsim::device_svds(jobs, A, V, stream);
+    if (st != BSIM_OK) { delete B; return st; }
+    run([&](int w) {
+        for (int g = w; g < ng; g += nth) {
+            const int m = (int)B->g[g].za.size(), n = (int)B->g[g].zb.size();
+            bsim::finish_factors(jobs[g].m, jobs[g].n, m < n, A.data() + jobs[g].a_off, V.data() + jobs[g].v_off,
+                                 tol, B->g[g]);
+        }
+    });
     *out = B;
     return BSIM_OK;
 }
@@ -224,6 +401,16 @@ int bsim_netbuild_compress_runs(int64_t nterms, const uint64_t *ax, const uint64
     if (nruns < 0) { bsim::set_error("nruns = %lld", (long long)nruns); return BSIM_ERR_ARG; }
     static const int64_t none = 0;
     return netbuild(nterms, ax, az, bx, bz, coef, tol, nruns, nruns > 0 ? run_sizes : &none, out);
+}
+
+int bsim_netbuild_compress_device(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx,
+                                  const uint64_t *bz, const double *coef, double tol, int64_t nruns,
+                                  const int64_t *run_sizes, bsim_stream_t stream, void **out)
+{
+    if (nruns > 0 && !run_sizes) { bsim::set_error("null run_sizes"); return BSIM_ERR_NULL; }
+    if (nruns < 0) { bsim::set_error("nruns = %lld", (long long)nruns); return BSIM_ERR_ARG; }
+    return netbuild(nterms, ax, az, bx, bz, coef, tol, nruns, nruns > 0 ? run_sizes : nullptr, out, true,
+                    static_cast<cudaStream_t>(stream));
 }
 
 int bsim_netbuild_sizes(void *h, int64_t *ngs, int64_t *nza_total, int64_t *nzb_total, int64_t *nwa_total,

@@ -367,15 +367,17 @@ def group_range(net: OTFNetwork, lo: int, hi: int) -> OTFNetwork:
                       flat_wa=c(net.flat_wa[wa0:wa1]), flat_wb=c(net.flat_wb[wb0:wb1]))
 
 
-def hamiltonian_network(norb: int, seed: int = 0, tol: float = 1e-12, e_nuc=None, native: bool = False) -> OTFNetwork:
+def hamiltonian_network(norb: int, seed: int = 0, tol: float = 1e-12, e_nuc=None, native: bool = False,
+                        device: bool = False) -> OTFNetwork:
     """OTF network of the seeded synthetic Hamiltonian on ``norb`` orbitals.  native:
-    group and compress with the library's builder (bsim_netbuild_*, host threads)."""
+    group and compress with the library's builder (bsim_netbuild_*, host threads);
+    device: the same with every group's SVD on the current GPU."""
     h, g, e0 = synthetic_integrals(norb, seed)
     x, z, c = jw_hamiltonian_terms(h, g, e0 if e_nuc is None else e_nuc, tol)
     ax, az, bx, bz = split_aabb(x, z, norb)
-    if native:
+    if native or device:
         from binsim_b200 import cuotf
-        return cuotf.compress_groups_native(ax, az, bx, bz, c, norb, tol)
+        return cuotf.compress_groups_native(ax, az, bx, bz, c, norb, tol, device=device)
     return compress_groups(ax, az, bx, bz, c, norb, tol)
 
 
@@ -429,7 +431,8 @@ def _component(cre, ann, norb):
     return ax, az, bx, bz, C
 
 
-def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None, native: bool = False) -> Pool:
+def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None, native: bool = False,
+             device: bool = False) -> Pool:
     """Spin-adapted generalised singles and doubles as ordered products of
     spin-orbital generators (alpha = 2p, beta = 2p+1).
 
@@ -502,9 +505,9 @@ def ucc_pool(norb: int, singles=True, doubles=True, generalized=True, nelec=None
     BX = np.concatenate([g[2] for g in groups]); BZ = np.concatenate([g[3] for g in groups])
     CC = np.concatenate([g[4] for g in groups])
     sizes = [len(g[4]) for g in groups]
-    if native:   # the library's builder, one group per component run (bsim_netbuild_compress_runs)
+    if native or device:   # the library's builder, one group per component run (device: SVDs on the GPU)
         from binsim_b200 import cuotf
-        net = cuotf.compress_groups_native(AX, AZ, BX, BZ, CC, norb, run_sizes=sizes)
+        net = cuotf.compress_groups_native(AX, AZ, BX, BZ, CC, norb, run_sizes=sizes, device=device)
     else:
         net = _compress_each(AX, AZ, BX, BZ, CC, sizes, norb)
     return Pool(network=net, components=gens2, labels=labels2, excitations=excitations)

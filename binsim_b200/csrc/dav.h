@@ -9,10 +9,17 @@ constexpr int kMaxSub = 64;   // subspace limit, as the reference's 64-entry loc
 struct Coeffs { double v[kMaxSub]; };
 
 // Per-driver scratch for reductions: partials and small device result slots.
+// Device scratch of the reductions: part [kDavPartDoubles] (per-CTA partial
+// sums) and res [kDavResDoubles].  ensure() allocates it; attach() points it at
+// memory the caller owns (then nothing is freed here).
+constexpr int kDavPartDoubles = 148 * 8 * kMaxSub;
+constexpr int kDavResDoubles = kMaxSub + 8;
 struct DavScratch {
     double *part = nullptr;
-    double *res = nullptr;   // kMaxSub + 8 device doubles
+    double *res = nullptr;
+    bool owned = true;
     int ensure();
+    void attach(double *part_mem, double *res_mem) { part = part_mem; res = res_mem; owned = false; }
     ~DavScratch();
 };
 

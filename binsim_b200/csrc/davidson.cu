@@ -157,8 +157,11 @@ __global__ void dot_kernel(i64 n, const double *__restrict__ a, const double *__
 }
 
 // ---- host wrappers -----------------------------------------------------------------
+static_assert(kDavPartDoubles == kRedCtas * kMaxSub, "partial-sum scratch of the reductions");
+
 DavScratch::~DavScratch()
 {
+    if (!owned) return;
     if (part) cudaFree(part);
     if (res) cudaFree(res);
 }
@@ -166,9 +169,10 @@ DavScratch::~DavScratch()
 int DavScratch::ensure()
 {
     if (part) return BSIM_OK;
-    cudaError_t e = dmalloc(&part, sizeof(double) * kRedCtas * kMaxSub);
+    owned = true;
+    cudaError_t e = dmalloc(&part, sizeof(double) * kDavPartDoubles);
     if (e != cudaSuccess) { part = nullptr; return cuda_status(e, "davidson scratch"); }
-    e = dmalloc(&res, sizeof(double) * (kMaxSub + 8));
+    e = dmalloc(&res, sizeof(double) * kDavResDoubles);
     if (e != cudaSuccess) { res = nullptr; return cuda_status(e, "davidson scratch"); }
     return BSIM_OK;
 }

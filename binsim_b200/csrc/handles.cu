@@ -104,13 +104,28 @@ int Workspace::partials(size_t n, double **out)
     return BSIM_OK;
 }
 
+int Workspace::general(size_t bytes, void **out)
+{
+    if (gen_n < bytes) {
+        if (gen) cudaFree(gen);
+        gen = nullptr;
+        gen_n = 0;
+        cudaError_t e = dmalloc(&gen, bytes);
+        if (e != cudaSuccess) { gen = nullptr; return cuda_status(e, "workspace general buffer"); }
+        gen_n = bytes;
+    }
+    *out = gen;
+    return BSIM_OK;
+}
+
 void Workspace::release()
 {
     if (tiles) cudaFree(tiles);
     if (f32) cudaFree(f32);
     if (part) cudaFree(part);
-    tiles = nullptr; f32 = nullptr; part = nullptr;
-    tiles_n = f32_n = part_n = 0;
+    if (gen) cudaFree(gen);
+    tiles = nullptr; f32 = nullptr; part = nullptr; gen = nullptr;
+    tiles_n = f32_n = part_n = gen_n = 0;
     tiles_host.clear();
 }
 

@@ -16,6 +16,7 @@
 //     parameter and the gradient sums the component terms.
 #include "vqe.h"
 #include "dav.h"
+#include "ops.h"
 
 #include <algorithm>
 #include <cmath>
@@ -86,11 +87,14 @@ int vqe_energy_grad(const DevBasis<Ti> *B, const DevNet<Ti> *H, const DevNet<Ti>
         for (i64 i = 0; i < n_ops; ++i)
             if ((i == 0 || param_idx[i] != param_idx[i - 1]) && param_idx[i] % ckpt_every == 0 && i > 0)
                 ck_pos.push_back(i);
-    Buf ck, terms, scal;
-    if (!ck_pos.empty()) TRY(ck.get(sizeof(double) * n * ck_pos.size(), s));
-    TRY(terms.get(sizeof(double) * std::max<i64>(1, n_ops), s));
-    TRY(scal.get(sizeof(double) * 4, s));
-    double *ckp = (double *)ck.p, *tp = (double *)terms.p, *sc = (double *)scal.p;
+    // checkpoints, gradient terms, scalars and the reduction scratch live in the
+    // basis workspace (grown on demand, kept between calls): no allocation per call
+    const size_t n_ck = (size_t)n * ck_pos.size(), n_terms = (size_t)std::max<i64>(1, n_ops);
+    void *wsp = nullptr;
+    TRY(workspace_for(B).general(sizeof(double) * (n_ck + n_terms + 8 + kDavPartDoubles + kDavResDoubles), &wsp));
+    double *ckp = static_cast<double *>(wsp), *tp = ckp + n_ck, *sc = tp + n_terms;
+    DavScratch S;
+    S.attach(sc + 8, sc + 8 + kDavPartDoubles);
 
     // forward: psi_0 = reference, psi_{i+1} = exp(theta G_i) psi_i
     TRY(prepare_state(B, P, 0, op_idx, param_idx, thetas, ref_idx, ref_val, n_ref, lv, s));
@@ -104,8 +108,6 @@ int vqe_energy_grad(const DevBasis<Ti> *B, const DevNet<Ti> *H, const DevNet<Ti>
     }
     // energy: r = H l, E = <l|r>/<l|l>
     TRY(sigma(B, H, lv, nullptr, rv, false, s));
-    DavScratch S;
-    TRY(S.ensure());
     TRY(dav_dot(S, n, lv, lv, sc + 0, s));
     TRY(dav_dot(S, n, lv, rv, sc + 1, s));
     TRY(dav_dot(S, n, rv, rv, sc + 2, s));

@@ -1,6 +1,7 @@
 // extern "C" entry points of libcuotf (declared in include/binsim_cuotf.h).
 #include "../../include/binsim_cuotf.h"
 #include "dav.h"
+#include "mixed.cuh"
 #include "vqe.h"
 
 #include <cstdio>
@@ -211,6 +212,20 @@ double backgrad_cuda_2d(void *basis, void *net, int64_t idx, double theta, doubl
 const char *bsim_last_error(void) { return bsim::last_error(); }
 const char *bsim_version(void) { return "libcuotf sm_100a 0.1"; }
 int64_t bsim_device_alloc_count(void) { return (int64_t)bsim::device_alloc_count(); }
+int bsim_release_cached_memory(void)
+{
+    const cudaError_t e = bsim::trim_library_pool();
+    return e == cudaSuccess ? bsim::BSIM_OK : bsim::cuda_status(e, "release cached memory");
+}
+
+int bsim_tensor_core_timeouts(int32_t *count, int32_t reset)
+{
+    if (!count) { bsim::set_error("null count"); return bsim::BSIM_ERR_NULL; }
+    int c = 0;
+    const int st = bsim::mixed_tc_timeouts(&c, reset != 0);
+    *count = c;
+    return st;
+}
 
 int bsim_basis_create_u32(int64_t norb, int64_t na, int64_t nb, int64_t total_sym, const int64_t *orbsym,
                           int64_t num_irreps, void **out)

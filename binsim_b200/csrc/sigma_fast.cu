@@ -19,10 +19,12 @@
 // column-chunk-major so the chunk of every source row stays in L2 while all
 // destination rows use it.
 #include "fastplan.h"
+#include "mixed.cuh"
 #include "ops.h"
 #include "tiles.cuh"
 
 #include <cstdlib>
+#include <cstring>
 #include <mutex>
 #include <type_traits>
 
@@ -160,41 +162,7 @@ pure_rows_kernel(int row_begin, int col_begin, int ncols, int ld_in, const SideC
 }
 
 // ---- 4a. mixed GEMM -----------------------------------------------------------------
-struct MixedArgs {
-    int nA, nB, nE, nF, M, ldA, ldG;
-    int cend;               // end of the column range being computed (nB for a whole sigma)
-    const u64 *Emask, *mA;
-    const void *Lam;        // T [nE x nF]
-    const int *gidx;        // [nF x ldG]: (rank(b^F) << 1 | sign) or -1
-};
-
-// Builds this row's connected alpha excitations (E order) into conn/sgn; returns the count.
-template <int NT>
-__device__ __forceinline__ int connected_excitations(const MixedArgs &P, u64 sa, int *conn, int *sgn, int *wcnt,
-                                                     int *cnt)
-{
-    constexpr int NW = NT / 32;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (threadIdx.x == 0) *cnt = 0;
-    __syncthreads();
-    for (int base = 0; base < P.nE; base += NT) {
-        const int e = base + threadIdx.x;
-        const bool ok = e < P.nE && __popcll(sa & P.Emask[e]) == 1;
-        const unsigned m = __ballot_sync(0xffffffffu, ok);
-        if (lane == 0) wcnt[wid] = __popc(m);
-        __syncthreads();
-        int off = *cnt;
-        for (int w2 = 0; w2 < wid; ++w2) off += wcnt[w2];
-        if (ok) {
-            const int j = off + __popc(m & ((1u << lane) - 1u));
-            if (j < kMaxConn) { conn[j] = e; sgn[j] = (__popcll(sa & P.mA[e]) & 1) ? -1 : 1; }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) for (int w2 = 0; w2 < NW; ++w2) *cnt += wcnt[w2];
-        __syncthreads();
-    }
-    return min(*cnt, kMaxConn);
-}
+// (MixedArgs and connected_excitations: mixed.cuh)
 
 // EPT consecutive Lam_conn values (32 bytes) from shared memory
 template <int EPT>
@@ -890,6 +858,21 @@ static int launch_mixed_shape(const DevBasis<Ti> *B, FastPlan<Ti> &P, const Mixe
     return BSIM_OK;
 }
 
+// BSIM_MIXED_TC selects the FP32-bulk mixed GEMM kernel (read on every call:
+// tests compare the paths): "0" the CUDA-core kernel, "global64" / "global80"
+// the tensor-core kernel with the source row read from global memory and 64 /
+// 80 excitations per pass wherever it applies, unset the automatic choice.
+enum class MixedTc { off, automatic, global64, global80 };
+static MixedTc mixed_tc_mode()
+{
+    const char *e = getenv("BSIM_MIXED_TC");
+    if (!e || !e[0]) return MixedTc::automatic;
+    if (e[0] == '0') return MixedTc::off;
+    if (!strcmp(e, "global64")) return MixedTc::global64;
+    if (!strcmp(e, "global80")) return MixedTc::global80;
+    return MixedTc::automatic;
+}
+
 template <typename Ti, typename T, int EPT>
 static int launch_mixed(const DevBasis<Ti> *B, FastPlan<Ti> &P, FastScratch<Ti> &S, const T *ct, double *dst,
                         int c0, int c1, cudaStream_t s, StageTimer *tm)
@@ -900,6 +883,37 @@ static int launch_mixed(const DevBasis<Ti> *B, FastPlan<Ti> &P, FastScratch<Ti> 
     if (rc != BSIM_OK) return rc;
     MixedArgs ma{P.nA, P.nB, P.nE, P.nF, P.M, P.ldA, P.ldG, c1, P.d_Emask, P.d_mA,
                  sizeof(T) == 8 ? (const void *)P.d_Lam : (const void *)P.d_Lam32, P.d_gidx};
+    if constexpr (sizeof(T) == 4) {
+        // FP32 bulk: the tensor-core (TF32 x 3) kernel, with the source row on chip
+        // where it fits, else gathered from global memory (80 excitations per pass
+        // when 65..80 are connected, as at 18 orbitals with 8 electrons)
+        int tcN = 0;
+        bool tcGrow = false;
+        const MixedTc mode = mixed_tc_mode();
+        const bool fit80 = P.M <= 80 && mixed_tc_smem(P.ldA, P.nF, 80, true) <= kSmemMax;
+        const bool fit64g = mixed_tc_smem(P.ldA, P.nF, 64, true) <= kSmemMax;
+        if (mode == MixedTc::global80 && fit80) tcN = 80, tcGrow = true;
+        else if (mode == MixedTc::global64 && fit64g) tcN = 64, tcGrow = true;
+        else if (mode != MixedTc::off) {
+            if (mixed_tc_smem(P.ldA, P.nF, 64, false) <= std::min(kSmemMax, mixed_row_limit())) tcN = 64;
+            else if (P.M > 64 && fit80) tcN = 80, tcGrow = true;
+            else if (fit64g) tcN = 64, tcGrow = true;
+        }
+        if (tcN > 0) {
+            const int passes = (P.M + tcN - 1) / tcN;
+            T *Z = static_cast<T *>(z.p);
+            const size_t Wz = z.w;
+            for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
+                for (int pass = 0; pass < passes; ++pass)
+                    STAGE(tm, 3, s, rc = mixed_gemm_tc<Ti>(ma, P.d_astr, ct, Z, z0, (int)Wz, tcN * pass, tcN,
+                                                           tcGrow, s));
+                if (rc != BSIM_OK) return rc;
+                dim3 g(P.nA, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
+                STAGE(tm, 4, s, (mixed_gather_kernel<Ti, T><<<g, 256, 0, s>>>(ma, B->view, Z, dst, z0, (int)Wz)));
+            }
+            return BSIM_OK;
+        }
+    }
     const int rows = (sizeof(T) == 4 && EPT == 10) ? 80 : 64;
     const MixedShape sh = mixed_shape(P.nB, P.nF, sizeof(T), mixed_row_limit(), rows);
     if (sh.smem > kSmemMax) { set_error("mixed kernel needs %zu bytes of shared memory", sh.smem); return BSIM_ERR_UNSUPPORTED; }

@@ -64,6 +64,8 @@ def lib() -> C.CDLL:
         # part 2
         "bsim_last_error": (C.c_char_p, []), "bsim_version": (C.c_char_p, []),
         "bsim_device_alloc_count": (i64, []),
+        "bsim_release_cached_memory": (ci, []),
+        "bsim_tensor_core_timeouts": (ci, [vp, ci]),
         "bsim_basis_create_u32": (ci, [i64, i64, i64, i64, vp, i64, vp]),
         "bsim_basis_create_u64": (ci, [i64, i64, i64, i64, vp, i64, vp]),
         "bsim_network_create_u64": (ci, [vp, i64, i64] + [vp] * 9 + [vp]),
@@ -87,6 +89,7 @@ def lib() -> C.CDLL:
         "bsim_hvec_host": (ci, [vp, vp, i64, vp, vp, ci, vp]),
         "bsim_netbuild_compress": (ci, [i64, vp, vp, vp, vp, vp, dbl, vp]),
         "bsim_netbuild_compress_runs": (ci, [i64, vp, vp, vp, vp, vp, dbl, i64, vp, vp]),
+        "bsim_netbuild_compress_device": (ci, [i64, vp, vp, vp, vp, vp, dbl, i64, vp, vp, vp]),
         "bsim_netbuild_sizes": (ci, [vp, vp, vp, vp, vp, vp]),
         "bsim_netbuild_export": (ci, [vp] * 10),
         "bsim_netbuild_destroy": (ci, [vp]),
@@ -163,15 +166,21 @@ def _host(a, dtype):
 
 
 def compress_groups_native(ax, az, bx, bz, c, norb: int, tol: float = 1e-12, orbsym=None,
-                           run_sizes=None) -> nw.OTFNetwork:
+                           run_sizes=None, device: bool = False, stream=None) -> nw.OTFNetwork:
     """The grouping and SVD compression of network.compress_groups (jl/network.jl:158-246)
     in the library's native builder (host threads); groups in order of first appearance,
-    or with run_sizes one group per run of consecutive terms (the pool form)."""
+    or with run_sizes one group per run of consecutive terms (the pool form).  device:
+    every group's SVD in one batched launch on the current GPU (or the given stream)."""
     L = lib()
     arrs = [_host(ax, np.uint64), _host(az, np.uint64), _host(bx, np.uint64), _host(bz, np.uint64),
             _host(c, np.float64)]
     h = vp()
-    if run_sizes is None:
+    if device:
+        rs = _host(run_sizes if run_sizes is not None else [], np.int64)
+        _check(L.bsim_netbuild_compress_device(len(arrs[4]), *[a.ctypes.data for a in arrs], tol, len(rs),
+                                               rs.ctypes.data if len(rs) else None, _stream(stream),
+                                               C.byref(h)), "bsim_netbuild_compress_device")
+    elif run_sizes is None:
         _check(L.bsim_netbuild_compress(len(arrs[4]), *[a.ctypes.data for a in arrs], tol, C.byref(h)),
                "bsim_netbuild_compress")
     else:

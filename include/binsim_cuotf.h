@@ -104,6 +104,19 @@ const char *bsim_version(void);
  * caller compares two readings to check that the calls between them allocated
  * nothing. */
 int64_t bsim_device_alloc_count(void);
+/* No counterpart in the reference.  The solvers' stream-ordered buffers come from
+ * a memory pool of the library that keeps freed memory for the next call (a
+ * Davidson or VQE call then does not map its vectors anew each time).  This call
+ * hands the current device's unused pool memory back (it synchronises the
+ * device); the library also does so by itself when a cudaMalloc of its own runs
+ * out of memory. */
+int bsim_release_cached_memory(void);
+/* No counterpart in the reference.  Waits inside the library's tensor-core
+ * (tcgen05) kernels are bounded; a wait that gives up makes its CTA skip the
+ * rest of its work (the result is then wrong) and is counted.  *count = the
+ * count on the current device since the last reset (0 in normal operation);
+ * reset != 0 clears it.  Synchronous (reads device memory). */
+int bsim_tensor_core_timeouts(int32_t *count, int32_t reset);
 
 /* Basis: create_basis_manager's arguments (basis/declare.hpp:24-33). */
 int bsim_basis_create_u32(int64_t norb, int64_t na, int64_t nb, int64_t total_sym, const int64_t *orbsym,
@@ -243,6 +256,16 @@ int bsim_netbuild_compress(int64_t nterms, const uint64_t *ax, const uint64_t *a
 int bsim_netbuild_compress_runs(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx,
                                 const uint64_t *bz, const double *coef, double tol, int64_t nruns,
                                 const int64_t *run_sizes, void **out);
+/* The same compression with every group's SVD on the GPU: groups (by key, or
+ * one per run when nruns > 0) formed on the host, then all groups' one-sided
+ * Jacobi SVDs in one batched launch on the stream (one CTA per group, the
+ * disjoint column pairs of each round-robin round rotated in parallel, the host
+ * builder's rotation, skip and convergence rules); the result handle is read
+ * with bsim_netbuild_sizes / bsim_netbuild_export.  No reference counterpart
+ * (the reference compresses on the host: jl/network.jl:158-301). */
+int bsim_netbuild_compress_device(int64_t nterms, const uint64_t *ax, const uint64_t *az, const uint64_t *bx,
+                                  const uint64_t *bz, const double *coef, double tol, int64_t nruns,
+                                  const int64_t *run_sizes, bsim_stream_t stream, void **out);
 int bsim_netbuild_sizes(void *h, int64_t *ngs, int64_t *nza_total, int64_t *nzb_total, int64_t *nwa_total,
                         int64_t *nwb_total);
 int bsim_netbuild_export(void *h, uint64_t *axs, uint64_t *bxs, int64_t *ranks, int64_t *num_zas, int64_t *num_zbs,

@@ -191,8 +191,11 @@ def test_structured_sigma_two_passes_and_streamed_lam(cuda, norb, na, nb, bits):
 @pytest.mark.parametrize("mixed", [False, True])
 def test_mixed_gemm_source_row_in_global_memory(cuda, oracle, monkeypatch, mixed):
     """The mixed GEMM reading its source row from global memory (the kernel shape used
-    when a beta row exceeds shared memory: FP64 at 18 orbitals, 8 electrons) gives the
-    same bits as the row staged on chip, and the oracle's sigma."""
+    when a beta row exceeds shared memory: FP64 at 18 orbitals, 8 electrons) against
+    the row staged on chip and the oracle's sigma.  FP64: the same bits (both run the
+    same DMMA sums in the same order).  FP32 bulk: the on-chip shape runs on the
+    tcgen05 tensor cores (TF32 hi/lo products) and the global-row shape on the CUDA
+    cores, so they agree to the FP32-bulk tolerance, 2e-6 x max|sigma|."""
     from binsim_b200 import cuotf, network as nw
     norb, na, nb = 11, 5, 5
     net = nw.hamiltonian_network(norb, seed=5)
@@ -207,9 +210,12 @@ def test_mixed_gemm_source_row_in_global_memory(cuda, oracle, monkeypatch, mixed
     monkeypatch.setenv("BSIM_MIXED_ROW_SMEM", "1")
     run(x, y_glob)
     monkeypatch.delenv("BSIM_MIXED_ROW_SMEM")
-    assert cuda.equal(y_chip, y_glob)
     ref = oracle.hvec(oracle.basis(norb, na, nb), oracle.network(net), xh)
     tol = 2e-6 if mixed else 1e-12
+    if mixed:
+        assert float((y_chip - y_glob).abs().max()) <= tol * np.abs(ref).max()
+    else:
+        assert cuda.equal(y_chip, y_glob)
     assert np.abs(y_glob.cpu().numpy() - ref).max() <= tol * np.abs(ref).max()
 
 
@@ -262,8 +268,10 @@ def test_hvec_host_pipeline(cuda):
 def test_fp32_mixed_gemm_80_row_tile_matches_64_row_passes(cuda, monkeypatch):
     """65..80 connected alpha singles (18 orbitals, 5 alpha electrons: 65): the FP32 80-row
     tile gives the same bits as a 64-row and a 16-row pass (each output accumulates the
-    same FMAs in the same order)."""
+    same FMAs in the same order).  CUDA-core kernels (BSIM_MIXED_TC=0): the tensor-core
+    kernel takes this size otherwise."""
     from binsim_b200 import cuotf
+    monkeypatch.setenv("BSIM_MIXED_TC", "0")
     net = sparse_hamiltonian_network(18, seed=23)
     B = cuotf.CuBasis(18, 5, 2)
     f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))

@@ -40,17 +40,31 @@ int cuda_status(cudaError_t e, const char *what);
 // caller can check that a stretch of calls allocated nothing.
 void note_device_alloc();
 long long device_alloc_count();
+cudaError_t trim_library_pool();   // hand the pool's unused memory back to the device
 template <typename T>
 inline cudaError_t dmalloc(T **p, size_t bytes)
 {
     note_device_alloc();
-    return cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    if (e == cudaErrorMemoryAllocation) {   // memory the library's pool keeps may be what is missing
+        (void)cudaGetLastError();
+        if (trim_library_pool() == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    }
+    return e;
 }
+// Stream-ordered allocations come from the library's own pool on the current
+// device, whose release threshold keeps freed memory for the next allocation:
+// a solver that allocates its vectors on every call then pays the mapping of
+// that memory once per process, not once per call.
+cudaError_t library_pool(cudaMemPool_t *pool);
 template <typename T>
 inline cudaError_t dmalloc_async(T **p, size_t bytes, cudaStream_t s)
 {
     note_device_alloc();
-    return cudaMallocAsync(reinterpret_cast<void **>(p), bytes, s);
+    cudaMemPool_t pool;
+    const cudaError_t e = library_pool(&pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(reinterpret_cast<void **>(p), bytes, pool, s);
 }
 
 #define BSIM_CUDA(call)                                              \

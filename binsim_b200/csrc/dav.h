@@ -18,7 +18,8 @@ struct DavScratch {
     double *part = nullptr;
     double *res = nullptr;
     bool owned = true;
-    int ensure();
+    cudaStream_t stream = nullptr;   // stream of the allocation and of its release
+    int ensure(cudaStream_t s = nullptr);
     void attach(double *part_mem, double *res_mem) { part = part_mem; res = res_mem; owned = false; }
     ~DavScratch();
 };
@@ -40,6 +41,28 @@ template <typename TV, typename TW>
 int dav_multidot(DavScratch &S, i64 n, int k, const TV *const *V, const TW *w, double *out_dev, cudaStream_t s);
 
 void jacobi_eigh(int k, const double *A, int lda, double *evals, double *evecs);
+
+// Device-scalar helpers of the device-resident drivers (davidson.cu): the
+// Ritz coefficients, energy and norms stay on the device.
+int dav_eigh_dev(int k, const double *h, int ldh, double *evals, double *evecs, double *work, cudaStream_t s);
+template <typename TV>
+int dav_ritz_residual_dev(DavScratch &S, i64 n, int k, const double *coeffs_dev, const double *e_dev,
+                          const TV *const *V, const TV *const *AV, double *r, double *x, double *norm_dev,
+                          cudaStream_t s);
+template <typename TV, typename TX>
+int dav_combine_dev(i64 n, int k, const double *coeffs_dev, const TV *const *V, TX *x, cudaStream_t s);
+template <typename TD>
+int dav_precondition_dev(DavScratch &S, i64 n, double *r, const TD *d, const double *e_dev,
+                         const double *rnorm_dev, double *norm_dev, cudaStream_t s);
+template <typename TV>
+int dav_cgs2_dev(DavScratch &S, i64 n, int k, const TV *const *V, double *v, double *nrm, double *proj,
+                 cudaStream_t s);
+template <typename TO>
+int dav_normalize_into(i64 n, const double *v, const double *nrm_dev, TO *out, double *breakdown_dev,
+                       cudaStream_t s);
+int dav_mirror_col(int dim, double *h, int ld, cudaStream_t s);
+int dav_sym_avg(int dim, double *h, int ld, cudaStream_t s);
+int dav_axpby_dev(i64 n, const double *a_dev, double *x, const double *t, cudaStream_t s);
 
 // Result/statistics of a Davidson run.
 struct DavStats {

@@ -594,7 +594,7 @@ int davidson_block(const DevBasis<Ti> *B, const DevNet<Ti> *N, int nroots, doubl
     }
     if (n < maxspace) { set_error("subspace of %d vectors in a %lld-dimensional space", maxspace, (long long)n); return BSIM_ERR_ARG; }
     Ctx<Ti> C{B, N, n, k, diag, diag32, tol, verbose, s};
-    TRY(C.S.ensure());
+    TRY(C.S.ensure(s));
     std::vector<double *> Xp(k);
     for (int j = 0; j < k; ++j) Xp[j] = X + (i64)j * n;
     double *sc = C.S.res + kMaxSub;

@@ -1,11 +1,18 @@
 // Device-resident Davidson drivers.
 //
-// davidson_fp64 restates jl/davidson.jl:1-185 step for step: Rayleigh-Ritz on
-// the host (FP64 Jacobi on <= 64 x 64), Ritz vector and residual, restart to
-// ncv vectors when the subspace is full, preconditioner r/(d - e) clamped at
-// max(1e-2 |r|, 1e-4), modified Gram-Schmidt repeated when the norm drops
-// below 0.717 of its value, normalisation, one sigma per expansion.
-// Vectors never leave the device; each iteration reads back a few scalars.
+// davidson_fp64 restates jl/davidson.jl:1-185 step for step: Rayleigh-Ritz
+// (Jacobi on the <= 64 x 64 projected matrix), Ritz vector and residual,
+// restart to ncv vectors when the subspace is full, preconditioner r/(d - e)
+// clamped at max(1e-2 |r|, 1e-4), Gram-Schmidt repeated when the norm drops
+// below 0.717 of its value, normalisation, one sigma per expansion.  Every
+// step runs on the device, the Jacobi eigensolve included (one warp), and the
+// decisions that depend on scalars (the preconditioner's shift, the second
+// Gram-Schmidt pass, breakdown) are taken there too: the host reads one
+// residual norm per iteration for the convergence test, instead of a handful of
+// scalars each followed by a synchronisation.  The orthogonalisation is
+// classical Gram-Schmidt against the whole subspace at once (a few launches)
+// where the reference uses modified Gram-Schmidt (one reduction per vector);
+// with the 0.717 repetition both give an orthogonal direction to rounding.
 //
 // davidson_mixed keeps the subspace V, AV in FP32 and expands it with the
 // FP32-bulk sigma (FP64 accumulation inside), while every outer iteration
@@ -37,13 +44,6 @@ int alloc(DevBuf &b, size_t n, cudaStream_t s)
     return BSIM_OK;
 }
 
-int fetch(double *host, const double *dev, int n, cudaStream_t s)
-{
-    BSIM_CUDA(cudaMemcpyAsync(host, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-    BSIM_CUDA(cudaStreamSynchronize(s));
-    return BSIM_OK;
-}
-
 __global__ void cvt_kernel_d2f(const double *__restrict__ x, float *__restrict__ y, i64 n)
 {
     for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) y[i] = (float)x[i];
@@ -57,16 +57,50 @@ __global__ void resid_kernel(i64 n, const double *__restrict__ x, const double *
         r[i] = ax[i] - e * x[i];
 }
 
-// x = a * x + t
-__global__ void axpby_kernel(i64 n, double a, double *__restrict__ x, const double *__restrict__ t)
-{
-    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
-        x[i] = a * x[i] + t[i];
-}
-
 }  // namespace
 
 #define TRY(...) do { int st__ = (__VA_ARGS__); if (st__ != BSIM_OK) return st__; } while (0)
+
+namespace {
+// Device state of a driver: the projected matrix, its eigenpairs and the scalars
+// the iteration reads on the device.  sc[0] residual norm, sc[1] breakdown flag
+// of the last expansion, sc[2] / sc[3] norm before / after Gram-Schmidt.
+struct DavState {
+    DevBuf buf;
+    double *h = nullptr, *evals = nullptr, *evecs = nullptr, *work = nullptr, *proj = nullptr, *sc = nullptr;
+    int init(cudaStream_t s)
+    {
+        constexpr size_t kSq = (size_t)kMaxSub * kMaxSub;
+        TRY(alloc<double>(buf, 3 * kSq + 2 * kMaxSub + 8, s));
+        h = (double *)buf.p;
+        evecs = h + kSq;
+        work = evecs + kSq;
+        evals = work + kSq;
+        proj = evals + kMaxSub;
+        sc = proj + kMaxSub;
+        BSIM_CUDA(cudaMemsetAsync(buf.p, 0, sizeof(double) * (3 * kSq + 2 * kMaxSub + 8), s));
+        return BSIM_OK;
+    }
+    // the one read of an iteration: residual norm, breakdown flag, lowest Ritz value
+    int read(double *rnorm, bool *breakdown, double *e0, cudaStream_t s) const
+    {
+        double v[2], e;
+        BSIM_CUDA(cudaMemcpyAsync(v, sc, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+        BSIM_CUDA(cudaMemcpyAsync(&e, evals, sizeof(double), cudaMemcpyDeviceToHost, s));
+        BSIM_CUDA(cudaStreamSynchronize(s));
+        *rnorm = v[0];
+        *breakdown = v[1] != 0.0;
+        *e0 = e;
+        return BSIM_OK;
+    }
+    int set_scalar(int i, double v, cudaStream_t s)
+    {
+        BSIM_CUDA(cudaMemcpyAsync(sc + i, &v, sizeof(double), cudaMemcpyHostToDevice, s));
+        BSIM_CUDA(cudaStreamSynchronize(s));   // v lives on the host stack
+        return BSIM_OK;
+    }
+};
+}  // namespace
 
 template <typename Ti>
 int davidson_fp64(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const double *diags, double tol,
@@ -78,10 +112,12 @@ int davidson_fp64(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const 
         return BSIM_ERR_ARG;
     }
     DavScratch S;
-    TRY(S.ensure());
-    std::vector<DevBuf> vb(maxspace), avb(maxspace), tb(ncv), tab(ncv);
+    TRY(S.ensure(s));
+    DavState D;
+    TRY(D.init(s));
+    std::vector<DevBuf> vb(maxspace), avb(maxspace), tb(ncv), tab(ncv), xb(2);
     DevBuf axb;
-    std::vector<double *> V(maxspace), AV(maxspace), Vt(ncv), AVt(ncv);
+    std::vector<double *> V(maxspace), AV(maxspace), Vt(ncv), AVt(ncv), xk(2);
     for (int j = 0; j < maxspace; ++j) {
         TRY(alloc<double>(vb[j], n, s)); TRY(alloc<double>(avb[j], n, s));
         V[j] = (double *)vb[j].p; AV[j] = (double *)avb[j].p;
@@ -90,82 +126,71 @@ int davidson_fp64(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const 
         TRY(alloc<double>(tb[j], n, s)); TRY(alloc<double>(tab[j], n, s));
         Vt[j] = (double *)tb[j].p; AVt[j] = (double *)tab[j].p;
     }
+    for (int j = 0; j < 2; ++j) { TRY(alloc<double>(xb[j], n, s)); xk[j] = (double *)xb[j].p; }
     TRY(alloc<double>(axb, n, s));
     double *axt = (double *)axb.p;
-    double *sc = S.res + kMaxSub;   // scalar slots
     DavStats st{};
 
     BSIM_CUDA(cudaMemcpyAsync(V[0], v0, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-    TRY(dav_normalize(S, n, V[0], sc, s));
+    TRY(dav_normalize(S, n, V[0], D.sc + 4, s));
     TRY(sigma(B, N, V[0], nullptr, AV[0], false, s));
     st.sigma_fp64++;
-    TRY(dav_dot(S, n, V[0], AV[0], sc, s));
-    double h[kMaxSub * kMaxSub] = {0};
-    TRY(fetch(&h[0], sc, 1, s));
+    TRY(dav_multidot<double, double>(S, n, 1, V.data(), AV[0], D.h, s));
     int dim = 1;
-    double es[kMaxSub], vs[kMaxSub * kMaxSub], col[kMaxSub];
-    double e_best = h[0];
+    double e_prev = 0.0;
     for (int iter = 1; iter <= maxiter; ++iter) {
-        jacobi_eigh(dim, h, kMaxSub, es, vs);
-        const double min_e = es[0];
-        TRY(dav_ritz_residual<double>(S, n, dim, vs, min_e, V.data(), AV.data(), axt, sc, s));
-        double norm_r;
-        TRY(fetch(&norm_r, sc, 1, s));
-        if (verbose) printf("  Step %03d:  residual: %.4e,  e: %.14f\n", iter, norm_r, min_e);
-        e_best = min_e;
-        st.iterations = iter;
-        st.residual = norm_r;
-        if (norm_r < tol) {
-            TRY(dav_combine<double, double>(n, dim, vs, V.data(), x_out, s));
-            st.energy = e_best;
-            st.converged = 1;
+        TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, D.work, s));
+        TRY(dav_ritz_residual_dev<double>(S, n, dim, D.evecs, D.evals, V.data(), AV.data(), axt, xk[iter & 1],
+                                          D.sc, s));
+        double norm_r, e;
+        bool breakdown;
+        TRY(D.read(&norm_r, &breakdown, &e, s));
+        if (breakdown) {   // the last expansion lay in the subspace: the previous Ritz vector is the answer
+            BSIM_CUDA(cudaMemcpyAsync(x_out, xk[(iter - 1) & 1], sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+            st.energy = e_prev;
             if (stats) *stats = st;
+            BSIM_CUDA(cudaStreamSynchronize(s));
             return BSIM_OK;
         }
-        if (dim >= maxspace) {
+        if (verbose) printf("  Step %03d:  residual: %.4e,  e: %.14f\n", iter, norm_r, e);
+        e_prev = e;
+        st.iterations = iter;
+        st.residual = norm_r;
+        st.energy = e;
+        if (norm_r < tol) {
+            BSIM_CUDA(cudaMemcpyAsync(x_out, xk[iter & 1], sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+            st.converged = 1;
+            if (stats) *stats = st;
+            BSIM_CUDA(cudaStreamSynchronize(s));
+            return BSIM_OK;
+        }
+        if (dim >= maxspace) {   // restart to the ncv lowest Ritz vectors, rebuild_heff (davidson.hpp:221-272)
             const int nsave = std::min(ncv, dim);
             for (int i = 0; i < nsave; ++i) {
-                TRY(dav_combine<double, double>(n, dim, vs + (size_t)i * dim, V.data(), Vt[i], s));
-                TRY(dav_combine<double, double>(n, dim, vs + (size_t)i * dim, AV.data(), AVt[i], s));
+                TRY(dav_combine_dev<double, double>(n, dim, D.evecs + (size_t)i * dim, V.data(), Vt[i], s));
+                TRY(dav_combine_dev<double, double>(n, dim, D.evecs + (size_t)i * dim, AV.data(), AVt[i], s));
             }
             for (int i = 0; i < nsave; ++i) { std::swap(V[i], Vt[i]); std::swap(AV[i], AVt[i]); }
             dim = nsave;
-            for (int j = 0; j < dim; ++j) {   // rebuild_heff, davidson.hpp:221-272
-                TRY(dav_multidot<double, double>(S, n, dim, V.data(), AV[j], S.res, s));
-                TRY(fetch(col, S.res, dim, s));
-                for (int i = 0; i < dim; ++i) h[i + j * kMaxSub] = col[i];
-            }
             for (int j = 0; j < dim; ++j)
-                for (int i = 0; i < j; ++i) h[i + j * kMaxSub] = h[j + i * kMaxSub] = 0.5 * (h[i + j * kMaxSub] + h[j + i * kMaxSub]);
+                TRY(dav_multidot<double, double>(S, n, dim, V.data(), AV[j], D.h + (size_t)j * kMaxSub, s));
+            TRY(dav_sym_avg(dim, D.h, kMaxSub, s));
         }
-        const double shift = std::max(norm_r * 1e-2, 1e-4);
-        TRY(dav_precondition(S, n, axt, diags, min_e, shift, sc, s));
-        double nrm[2];
-        TRY(fetch(&nrm[0], sc, 1, s));
-        TRY(dav_mgs<double>(S, n, dim, V.data(), axt, sc + 1, s));
-        TRY(fetch(&nrm[1], sc + 1, 1, s));
-        if (nrm[1] < 0.717 * nrm[0]) {
-            TRY(dav_mgs<double>(S, n, dim, V.data(), axt, sc + 1, s));
-            TRY(fetch(&nrm[1], sc + 1, 1, s));
-        }
-        if (nrm[1] < 1e-12) {   // breakdown: the new direction lies in the subspace
-            TRY(dav_combine<double, double>(n, dim, vs, V.data(), x_out, s));
-            st.energy = e_best;
-            if (stats) *stats = st;
-            return BSIM_OK;
-        }
-        TRY(dav_normalize(S, n, axt, sc, s));
-        BSIM_CUDA(cudaMemcpyAsync(V[dim], axt, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        TRY(dav_precondition_dev<double>(S, n, axt, diags, D.evals, D.sc, D.sc + 2, s));
+        TRY(dav_cgs2_dev<double>(S, n, dim, V.data(), axt, D.sc + 2, D.proj, s));
+        TRY(dav_normalize_into<double>(n, axt, D.sc + 3, V[dim], D.sc + 1, s));
         TRY(sigma(B, N, V[dim], nullptr, AV[dim], false, s));
         st.sigma_fp64++;
         ++dim;
-        TRY(dav_multidot<double, double>(S, n, dim, V.data(), AV[dim - 1], S.res, s));
-        TRY(fetch(col, S.res, dim, s));
-        for (int i = 0; i < dim; ++i) h[i + (dim - 1) * kMaxSub] = h[(dim - 1) + i * kMaxSub] = col[i];
+        TRY(dav_multidot<double, double>(S, n, dim, V.data(), AV[dim - 1], D.h + (size_t)(dim - 1) * kMaxSub, s));
+        TRY(dav_mirror_col(dim, D.h, kMaxSub, s));
     }
-    jacobi_eigh(dim, h, kMaxSub, es, vs);
-    TRY(dav_combine<double, double>(n, dim, vs, V.data(), x_out, s));
-    st.energy = e_best;
+    TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, D.work, s));
+    TRY(dav_combine_dev<double, double>(n, dim, D.evecs, V.data(), x_out, s));
+    double e;
+    BSIM_CUDA(cudaMemcpyAsync(&e, D.evals, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BSIM_CUDA(cudaStreamSynchronize(s));
+    st.energy = e;
     if (stats) *stats = st;
     return BSIM_OK;
 }
@@ -177,26 +202,29 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
     const i64 n = B->dim;
     if (maxspace > kMaxSub || maxspace < 3) { set_error("need 3 <= maxspace <= %d", kMaxSub); return BSIM_ERR_ARG; }
     DavScratch S;
-    TRY(S.ensure());
+    TRY(S.ensure(s));
+    DavState D;
+    TRY(D.init(s));
     std::vector<DevBuf> vb(maxspace), avb(maxspace);
     std::vector<float *> V(maxspace), AV(maxspace);
     for (int j = 0; j < maxspace; ++j) {
         TRY(alloc<float>(vb[j], n, s)); TRY(alloc<float>(avb[j], n, s));
         V[j] = (float *)vb[j].p; AV[j] = (float *)avb[j].p;
     }
-    DevBuf xb, axb, rb, tb, ayb;
+    DevBuf xb, axb, rb, tb, ayb, xkb[2];
     TRY(alloc<double>(xb, n, s)); TRY(alloc<double>(axb, n, s)); TRY(alloc<double>(rb, n, s));
     TRY(alloc<double>(tb, n, s)); TRY(alloc<double>(ayb, n, s));
+    TRY(alloc<double>(xkb[0], n, s)); TRY(alloc<double>(xkb[1], n, s));
     // x: current FP64 vector, ax = H x (FP64), r = ax - E x, t: expansion vector,
-    // ay: FP32-bulk sigma of the newest subspace vector
+    // ay: FP32-bulk sigma of the newest subspace vector, xk: Ritz vectors of the
+    // last two phase-A iterations
     double *x = (double *)xb.p, *ax = (double *)axb.p, *r = (double *)rb.p, *t = (double *)tb.p;
-    double *ay = (double *)ayb.p;
+    double *ay = (double *)ayb.p, *xk[2] = {(double *)xkb[0].p, (double *)xkb[1].p};
     double *sc = S.res + kMaxSub;
     DavStats st{};
     const int grid = 1184;
     BSIM_CUDA(cudaMemcpyAsync(x, v0, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     TRY(dav_normalize(S, n, x, sc, s));
-    double h[kMaxSub * kMaxSub], es[kMaxSub], vs[kMaxSub * kMaxSub], col[kMaxSub];
     int total_inner = 0;
 
     // ---- phase A: the reference driver's Davidson (restart to ncv Ritz vectors)
@@ -215,17 +243,19 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
         TRY(sigma(B, N, nullptr, V[0], ay, true, s));
         st.sigma_fp32++;
         cvt_kernel_d2f<<<grid, 256, 0, s>>>(ay, AV[0], n);
-        TRY(dav_multidot<float, float>(S, n, 1, V.data(), AV[0], S.res, s));
-        TRY(fetch(&h[0], S.res, 1, s));
-        int dim = 1;
+        TRY(dav_multidot<float, float>(S, n, 1, V.data(), AV[0], D.h, s));
+        int dim = 1, last = 0;
         double best = 1e300;   // smallest residual so far and the iterations since it
         int since_best = 0;
         for (int iter = 1; iter <= maxiter; ++iter) {
-            jacobi_eigh(dim, h, kMaxSub, es, vs);
-            const double e = es[0];
-            double norm_r;
-            TRY(dav_ritz_residual<float>(S, n, dim, vs, e, V.data(), AV.data(), t, sc, s));
-            TRY(fetch(&norm_r, sc, 1, s));
+            TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, D.work, s));
+            TRY(dav_ritz_residual_dev<float>(S, n, dim, D.evecs, D.evals, V.data(), AV.data(), t, xk[iter & 1],
+                                             D.sc, s));
+            double norm_r, e;
+            bool breakdown;
+            TRY(D.read(&norm_r, &breakdown, &e, s));
+            if (breakdown) { last = (iter - 1) & 1; break; }   // the previous Ritz vector
+            last = iter & 1;
             if (verbose) printf("  fp32 step %03d: residual %.4e e %.14f\n", iter, norm_r, e);
             // leave at the tolerance, or when the FP32 residual has stopped improving
             // (its noise floor) for a whole subspace cycle
@@ -235,49 +265,33 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
             if (dim >= maxspace) {
                 const int nsave = std::min(ncv, dim);
                 for (int i = 0; i < nsave; ++i) {
-                    TRY(dav_combine<float, float>(n, dim, vs + (size_t)i * dim, V.data(), Vt[i], s));
-                    TRY(dav_combine<float, float>(n, dim, vs + (size_t)i * dim, AV.data(), AVt[i], s));
+                    TRY(dav_combine_dev<float, float>(n, dim, D.evecs + (size_t)i * dim, V.data(), Vt[i], s));
+                    TRY(dav_combine_dev<float, float>(n, dim, D.evecs + (size_t)i * dim, AV.data(), AVt[i], s));
                 }
                 for (int i = 0; i < nsave; ++i) { std::swap(V[i], Vt[i]); std::swap(AV[i], AVt[i]); }
                 dim = nsave;
-                for (int j = 0; j < dim; ++j) {
-                    TRY(dav_multidot<float, float>(S, n, dim, V.data(), AV[j], S.res, s));
-                    TRY(fetch(col, S.res, dim, s));
-                    for (int i = 0; i < dim; ++i) h[i + j * kMaxSub] = col[i];
-                }
                 for (int j = 0; j < dim; ++j)
-                    for (int i = 0; i < j; ++i)
-                        h[i + j * kMaxSub] = h[j + i * kMaxSub] = 0.5 * (h[i + j * kMaxSub] + h[j + i * kMaxSub]);
+                    TRY(dav_multidot<float, float>(S, n, dim, V.data(), AV[j], D.h + (size_t)j * kMaxSub, s));
+                TRY(dav_sym_avg(dim, D.h, kMaxSub, s));
             }
-            const double shift = std::max(norm_r * 1e-2, 1e-4);
-            double nrm[2];
-            TRY(dav_precondition(S, n, t, diags, e, shift, sc, s));
-            TRY(fetch(&nrm[0], sc, 1, s));
-            TRY(dav_mgs<float>(S, n, dim, V.data(), t, sc + 1, s));
-            TRY(fetch(&nrm[1], sc + 1, 1, s));
-            if (nrm[1] < 0.717 * nrm[0]) {
-                TRY(dav_mgs<float>(S, n, dim, V.data(), t, sc + 1, s));
-                TRY(fetch(&nrm[1], sc + 1, 1, s));
-            }
-            if (nrm[1] < 1e-12) break;
-            TRY(dav_normalize(S, n, t, sc, s));
-            cvt_kernel_d2f<<<grid, 256, 0, s>>>(t, V[dim], n);
+            TRY(dav_precondition_dev<double>(S, n, t, diags, D.evals, D.sc, D.sc + 2, s));
+            TRY(dav_cgs2_dev<float>(S, n, dim, V.data(), t, D.sc + 2, D.proj, s));
+            TRY(dav_normalize_into<float>(n, t, D.sc + 3, V[dim], D.sc + 1, s));
             TRY(sigma(B, N, nullptr, V[dim], ay, true, s));
             st.sigma_fp32++;
             ++total_inner;
             cvt_kernel_d2f<<<grid, 256, 0, s>>>(ay, AV[dim], n);
             ++dim;
-            TRY(dav_multidot<float, float>(S, n, dim, V.data(), AV[dim - 1], S.res, s));
-            TRY(fetch(col, S.res, dim, s));
-            for (int i = 0; i < dim; ++i) h[i + (dim - 1) * kMaxSub] = h[(dim - 1) + i * kMaxSub] = col[i];
+            TRY(dav_multidot<float, float>(S, n, dim, V.data(), AV[dim - 1], D.h + (size_t)(dim - 1) * kMaxSub, s));
+            TRY(dav_mirror_col(dim, D.h, kMaxSub, s));
         }
-        jacobi_eigh(dim, h, kMaxSub, es, vs);
-        TRY(dav_combine<float, double>(n, dim, vs, V.data(), x, s));
+        BSIM_CUDA(cudaMemcpyAsync(x, xk[last], sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
         TRY(dav_normalize(S, n, x, sc, s));
         // restarts swapped subspace slots with the temporaries freed at the end of
-        // this scope (stream-ordered, after the combine): point V/AV back at the
+        // this scope (stream-ordered, after the copy above): point V/AV back at the
         // buffers that live through phase B
         for (int j = 0; j < maxspace; ++j) { V[j] = (float *)vb[j].p; AV[j] = (float *)avb[j].p; }
+        TRY(D.set_scalar(1, 0.0, s));   // a phase-A breakdown flag does not carry into phase B
     }
 
     // ---- phase B: FP64 residual refinement ----
@@ -287,11 +301,13 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
         st.sigma_fp64++;
         TRY(dav_dot(S, n, x, ax, sc, s));
         double E;
-        TRY(fetch(&E, sc, 1, s));
+        BSIM_CUDA(cudaMemcpyAsync(&E, sc, sizeof(double), cudaMemcpyDeviceToHost, s));
+        BSIM_CUDA(cudaStreamSynchronize(s));
         resid_kernel<<<grid, 256, 0, s>>>(n, x, ax, E, r);
         TRY(dav_dot(S, n, r, r, sc, s));
         double rr;
-        TRY(fetch(&rr, sc, 1, s));
+        BSIM_CUDA(cudaMemcpyAsync(&rr, sc, sizeof(double), cudaMemcpyDeviceToHost, s));
+        BSIM_CUDA(cudaStreamSynchronize(s));
         const double rnorm = sqrt(std::max(rr, 0.0));
         st.energy = E;
         st.residual = rnorm;
@@ -302,54 +318,58 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
         cvt_kernel_d2f<<<grid, 256, 0, s>>>(x, V[0], n);
         cvt_kernel_d2f<<<grid, 256, 0, s>>>(ax, AV[0], n);
         int dim = 1;
-        h[0] = E;
+        {   // h[0][0] = E, the first Ritz value E and the residual norm on the device
+            const double init[2] = {E, rnorm};
+            BSIM_CUDA(cudaMemcpyAsync(D.h, &init[0], sizeof(double), cudaMemcpyHostToDevice, s));
+            BSIM_CUDA(cudaMemcpyAsync(D.evals, &init[0], sizeof(double), cudaMemcpyHostToDevice, s));
+            BSIM_CUDA(cudaMemcpyAsync(D.sc, &init[1], sizeof(double), cudaMemcpyHostToDevice, s));
+            BSIM_CUDA(cudaStreamSynchronize(s));
+        }
         BSIM_CUDA(cudaMemcpyAsync(t, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-        double rin = rnorm, e_in = E;
+        double rin = rnorm;
+        bool have_eigh = false;   // evecs hold the eigenpairs of the current dim
         for (int it = 0; it < maxspace - 1; ++it) {
-            const double shift = std::max(rin * 1e-2, 1e-4);
-            double nrm[2];
-            TRY(dav_precondition(S, n, t, diags, e_in, shift, sc, s));
-            TRY(fetch(&nrm[0], sc, 1, s));
-            TRY(dav_mgs<float>(S, n, dim, V.data(), t, sc + 1, s));
-            TRY(fetch(&nrm[1], sc + 1, 1, s));
-            if (nrm[1] < 0.717 * nrm[0]) {
-                TRY(dav_mgs<float>(S, n, dim, V.data(), t, sc + 1, s));
-                TRY(fetch(&nrm[1], sc + 1, 1, s));
-            }
-            if (nrm[1] < 1e-12) break;
-            TRY(dav_normalize(S, n, t, sc, s));
-            cvt_kernel_d2f<<<grid, 256, 0, s>>>(t, V[dim], n);
+            TRY(dav_precondition_dev<double>(S, n, t, diags, D.evals, D.sc, D.sc + 2, s));
+            TRY(dav_cgs2_dev<float>(S, n, dim, V.data(), t, D.sc + 2, D.proj, s));
+            TRY(dav_normalize_into<float>(n, t, D.sc + 3, V[dim], D.sc + 1, s));
             // FP32-bulk sigma straight from the FP32 basis vector
             TRY(sigma(B, N, nullptr, V[dim], ay, true, s));
             st.sigma_fp32++;
             ++total_inner;
             cvt_kernel_d2f<<<grid, 256, 0, s>>>(ay, AV[dim], n);
             ++dim;
-            TRY(dav_multidot<float, float>(S, n, dim, V.data(), AV[dim - 1], S.res, s));
+            double *hc = D.h + (size_t)(dim - 1) * kMaxSub;
+            TRY(dav_multidot<float, float>(S, n, dim, V.data(), AV[dim - 1], hc, s));
             // the coupling to the current vector, <x|H|V_j> = <H x|V_j>, from the
             // FP64 sigma of x: near convergence it drives the correction, so it
             // must not carry the FP32-bulk sigma's rounding
-            TRY(dav_multidot<float, double>(S, n, 1, V.data() + (dim - 1), ax, S.res + dim, s));
-            TRY(fetch(col, S.res, dim + 1, s));
-            col[0] = col[dim];
-            for (int i = 0; i < dim; ++i) h[i + (dim - 1) * kMaxSub] = h[(dim - 1) + i * kMaxSub] = col[i];
-            jacobi_eigh(dim, h, kMaxSub, es, vs);
-            e_in = es[0];
+            TRY(dav_multidot<float, double>(S, n, 1, V.data() + (dim - 1), ax, hc, s));
+            TRY(dav_mirror_col(dim, D.h, kMaxSub, s));
+            TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, D.work, s));
             const double rprev = rin;
-            TRY(dav_ritz_residual<float>(S, n, dim, vs, e_in, V.data(), AV.data(), t, sc, s));
-            TRY(fetch(&rin, sc, 1, s));
+            TRY(dav_ritz_residual_dev<float>(S, n, dim, D.evecs, D.evals, V.data(), AV.data(), t, nullptr, D.sc,
+                                             s));
+            double e_in;
+            bool breakdown;
+            TRY(D.read(&rin, &breakdown, &e_in, s));
+            have_eigh = true;
+            if (breakdown) {   // the last direction lay in the space: drop it
+                --dim;
+                TRY(D.set_scalar(1, 0.0, s));
+                TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, D.work, s));
+                break;
+            }
             if (verbose) printf("    inner %02d: residual %.4e e %.14f\n", it, rin, e_in);
             // leave for an FP64 refinement once the inner residual dropped enough or
             // stalls at the FP32 noise floor
             if (rin < 0.05 * rnorm || rin < 0.5 * tol || (it >= 2 && rin > rprev) || total_inner >= maxiter)
                 break;
         }
-        jacobi_eigh(dim, h, kMaxSub, es, vs);
         // x <- y0 * x + sum_{j>=1} y_j V_j: the FP64 vector keeps its precision and
         // only the correction, small near convergence, carries FP32 rounding.
-        if (dim > 1) {
-            TRY(dav_combine<float, double>(n, dim - 1, vs + 1, V.data() + 1, t, s));
-            axpby_kernel<<<grid, 256, 0, s>>>(n, vs[0], x, t);
+        if (have_eigh && dim > 1) {
+            TRY(dav_combine_dev<float, double>(n, dim - 1, D.evecs + 1, V.data() + 1, t, s));
+            TRY(dav_axpby_dev(n, D.evecs, x, t, s));
         }
         TRY(dav_normalize(S, n, x, sc, s));
     }

@@ -30,6 +30,41 @@ int cuda_status(cudaError_t e, const char *what)
     return BSIM_ERR_CUDA;
 }
 
+cudaError_t library_pool(cudaMemPool_t *pool)
+{
+    constexpr int kMaxDev = 64;
+    static std::mutex mu;
+    static cudaMemPool_t pools[kMaxDev] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p;
+        if ((e = cudaMemPoolCreate(&p, &props)) != cudaSuccess) return e;
+        unsigned long long keep = ~0ull;   // never hand freed memory back on synchronisation
+        if ((e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+        pools[dev] = p;
+    }
+    *pool = pools[dev];
+    return cudaSuccess;
+}
+
+cudaError_t trim_library_pool()
+{
+    cudaMemPool_t pool;
+    cudaError_t e = library_pool(&pool);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return e;   // frees still queued on streams land first
+    return cudaMemPoolTrimTo(pool, 0);
+}
+
 static std::atomic<long long> g_device_allocs{0};
 void note_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
 long long device_alloc_count() { return g_device_allocs.load(std::memory_order_relaxed); }

@@ -59,7 +59,9 @@ def _lowest(oracle, Bo, No, k=1):
     return np.sort(eigsh(op, k=k, which="SA", tol=1e-13)[0])
 
 
-def test_davidson_fp64_and_mixed(cuda, oracle):
+@pytest.mark.parametrize("maxspace", [12, 5])
+def test_davidson_fp64_and_mixed(cuda, oracle, maxspace):
+    """The device-resident drivers against eigsh; maxspace 5 restarts every few steps."""
     from binsim_b200 import cuotf, network as nw
     norb, na, nb = 9, 4, 4
     net = nw.hamiltonian_network(norb, seed=21)
@@ -72,7 +74,7 @@ def test_davidson_fp64_and_mixed(cuda, oracle):
     v0 = cuda.zeros_like(diags)
     v0[B.hf_index()] = 1.0
     x = cuda.empty_like(diags)
-    st = f.davidson(v0.clone(), diags, x, tol=1e-6, maxiter=300, ncv=3, maxspace=12)
+    st = f.davidson(v0.clone(), diags, x, tol=1e-6, maxiter=300, ncv=3, maxspace=maxspace)
     assert abs(st["energy"] - e_ref) < 1e-9, (st, e_ref)
     assert st["residual"] < 1e-6
     # the eigenvector: H x = E x
@@ -80,7 +82,7 @@ def test_davidson_fp64_and_mixed(cuda, oracle):
     f.hvec(x, hx)
     assert float((hx - st["energy"] * x).norm()) < 1e-5
     xm = cuda.empty_like(diags)
-    sm = f.davidson(v0.clone(), diags, xm, tol=1e-6, maxiter=300, maxspace=12, mixed=True)
+    sm = f.davidson(v0.clone(), diags, xm, tol=1e-6, maxiter=300, maxspace=maxspace, mixed=True)
     assert abs(sm["energy"] - e_ref) < 1e-8, (sm, e_ref)
     assert sm["sigma_fp32"] > 0 and sm["residual"] < 1e-6
 

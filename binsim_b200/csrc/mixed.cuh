@@ -1,5 +1,6 @@
-// Shared pieces of the mixed-excitation GEMM kernels (sigma_fast.cu: CUDA-core
-// and DMMA paths; sigma_tc.cu: the tcgen05 path).
+// Shared pieces of the structured sigma's GEMM kernels, the mixed-excitation and
+// the intermediate-string products (sigma_fast.cu: CUDA-core and DMMA paths;
+// sigma_tc.cu: the tcgen05 paths).
 #pragma once
 #include "fastplan.h"
 
@@ -11,6 +12,12 @@ struct MixedArgs {
     const u64 *Emask, *mA;
     const void *Lam;        // T [nE x nF]
     const int *gidx;        // [nF x ldG]: (rank(b^F) << 1 | sign) or -1
+};
+
+struct RIArgs {
+    int nM, nU, npr, nP, ld_in, cend;
+    const int *src, *pid;
+    const void *W;          // T [nP x nP]
 };
 
 // Builds this row's connected alpha excitations (E order) into conn/sgn; returns the count.
@@ -50,6 +57,12 @@ size_t mixed_tc_smem(int ldA, int nF, int N, bool grow);
 template <typename Ti>
 int mixed_gemm_tc(const MixedArgs &ma, const Ti *astr, const float *ct, float *Z, int z0, int W, int jbase, int N,
                   bool grow, cudaStream_t s);
+// FP32-bulk intermediate-string GEMM on the tensor cores: whether a side with
+// nU pairs outside an intermediate has a kernel, the shared memory it needs, one
+// launch over the Z window [z0, z0 + W).
+bool ri_tc_supported(int nU);
+size_t ri_tc_smem(int nU);
+int ri_gemm_tc(const RIArgs &ra, const float *in, float *Z, int z0, int W, cudaStream_t s);
 int mixed_tc_timeouts(int *count, bool reset);
 
 }  // namespace bsim

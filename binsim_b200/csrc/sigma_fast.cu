@@ -469,6 +469,106 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
     }
 }
 
+// FP64 mixed GEMM with per-warp B fragments.  Warp w owns columns 8w..8w+7 of
+// each 128-column chunk and all 64 output rows (eight 8x8 DMMA tiles, those
+// past the pass's connected rows skipped); lane (g, t) gathers its own B
+// fragment elements X[f0 + 4i + t][8w + g] from the source row (shared memory,
+// or L2 with GROW), a 32-row F slice ahead.  No X slice is shared, so the warps
+// never synchronise inside the loop; Lam_conn (the A fragments, read by every
+// warp) is staged once per CTA, zero-padded to whole 32-row slices.
+inline size_t mixed_dmma_smem(int ldA, int nF, bool grow)
+{
+    return (grow ? 0 : (size_t)ldA * 8) + (size_t)((nF + 31) & ~31) * GemmLayout<double>::LS * 8 + 2 * kMaxConn * 4;
+}
+
+template <typename Ti, bool GROW>
+__global__ void __launch_bounds__(512, 1)
+mixed_dmma_kernel(const MixedArgs P, const Ti *__restrict__ astr, const double *__restrict__ ct,
+                  double *__restrict__ Z, int z0, int W, int jbase)
+{
+    constexpr int NT = 512, LS = GemmLayout<double>::LS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int K = P.nF, M = P.M;
+    const int Kp = (K + 31) & ~31;
+    double *srow = reinterpret_cast<double *>(smem_raw);          // [ldA] unless GROW
+    double *lam = srow + (GROW ? 0 : P.ldA);                       // [Kp][LS], rows past K zero
+    int *conn = reinterpret_cast<int *>(lam + (size_t)Kp * LS);   // [kMaxConn]
+    int *sgn = conn + kMaxConn;                                    // [kMaxConn]
+    __shared__ int wcnt[NT / 32], cnt;
+    const int a = blockIdx.x;
+    const int m = connected_excitations<NT>(P, (u64)astr[a], conn, sgn, wcnt, &cnt);
+    const int jm = min(64, m - jbase);   // output rows of this pass
+    if (jm <= 0) return;                 // uniform across the CTA
+    const double *grow = ct + (i64)a * P.ldA;
+    if (!GROW) {
+        const int4 *src = reinterpret_cast<const int4 *>(grow);
+        int4 *dst = reinterpret_cast<int4 *>(srow);
+        const int n16 = P.ldA / 2;
+        for (int i = threadIdx.x; i < n16; i += NT) dst[i] = __ldg(src + i);
+    }
+    const double *Lam = static_cast<const double *>(P.Lam);
+    for (int i = threadIdx.x; i < Kp * LS; i += NT) {
+        const int f = i / LS, j = i % LS;
+        lam[i] = (j < jm && f < K) ? (double)sgn[jbase + j] * Lam[(i64)conn[jbase + j] * K + f] : 0.0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const int nrb = (jm + 7) >> 3;   // 8-row blocks holding connected rows
+    const int zend = min(P.cend, z0 + W);
+    const int ncb = (zend - z0 + kMixCols - 1) / kMixCols;
+    const int nfc = (K + 31) / 32;
+    const int nsteps = ncb * nfc;
+    const int col = 8 * wid + g;     // this lane's B column within a chunk
+    int gp[8];
+    double gv[GROW ? 8 : 1];
+    auto load = [&](int step) {
+        const int cb = z0 + (step / nfc) * kMixCols, f0 = (step % nfc) * 32;
+        const int *gb = P.gidx + (i64)(f0 + t) * P.ldG + cb + col;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) gp[i] = f0 + 4 * i + t < K ? __ldg(gb + (i64)(4 * i) * P.ldG) : -1;
+        if constexpr (GROW) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) gv[i] = gp[i] >= 0 ? __ldg(grow + (gp[i] >> 1)) : 0.0;
+        }
+    };
+    double c[8][2];
+#pragma unroll
+    for (int rb = 0; rb < 8; ++rb) c[rb][0] = c[rb][1] = 0.0;
+    if (nsteps > 0) load(0);
+    for (int step = 0; step < nsteps; ++step) {
+        const int cbi = step / nfc, fci = step % nfc;
+        const int f0 = fci * 32, nk = (min(32, K - f0) + 3) >> 2;
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int gg = gp[i];
+            double v;
+            if constexpr (GROW) v = gv[i];
+            else v = gg >= 0 ? srow[gg >> 1] : 0.0;
+            x[i] = (gg >= 0 && (gg & 1)) ? -v : v;
+        }
+        if (step + 1 < nsteps) load(step + 1);
+        const double *la = lam + (size_t)(f0 + t) * LS + g;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (i < nk) {
+#pragma unroll
+                for (int rb = 0; rb < 8; ++rb)
+                    if (rb < nrb) dmma_8x8x4(c[rb][0], c[rb][1], la[(size_t)(4 * i) * LS + rb * 8], x[i]);
+            }
+        }
+        if (fci == nfc - 1) {
+            double *zr = Z + ((i64)a * M + jbase + g) * W + cbi * kMixCols + 8 * wid + 2 * t;
+#pragma unroll
+            for (int rb = 0; rb < 8; ++rb) {
+                if (rb < nrb && rb * 8 + g < jm)
+                    *reinterpret_cast<double2 *>(zr + (i64)(rb * 8) * W) = make_double2(c[rb][0], c[rb][1]);
+                c[rb][0] = c[rb][1] = 0.0;
+            }
+        }
+    }
+}
+
 // ---- 4b. gather of the mixed contributions ------------------------------------------------
 template <typename Ti, typename T>
 __global__ void __launch_bounds__(256)
@@ -516,11 +616,6 @@ mixed_gather_kernel(const MixedArgs P, const BasisView<Ti> BV, const T *__restri
 }
 
 // ---- 2b/3b. same-spin doubles through intermediate strings ----------------------------
-struct RIArgs {
-    int nM, nU, npr, nP, ld_in, cend;
-    const int *src, *pid;
-    const void *W;          // T [nP x nP]
-};
 
 // 16-byte asynchronous copy global -> shared (cp.async, L2 only); src_bytes 0
 // writes zeros without reading.
@@ -858,6 +953,14 @@ static int launch_mixed_shape(const DevBasis<Ti> *B, FastPlan<Ti> &P, const Mixe
     return BSIM_OK;
 }
 
+// BSIM_MIXED_DMMA=0 sends the FP64 mixed GEMM to the shared-X-slice kernel
+// (read on every call: tests compare the two)
+static bool mixed_dmma_on()
+{
+    const char *e = getenv("BSIM_MIXED_DMMA");
+    return !(e && e[0] == '0');
+}
+
 // BSIM_MIXED_TC selects the FP32-bulk mixed GEMM kernel (read on every call:
 // tests compare the paths): "0" the CUDA-core kernel, "global64" / "global80"
 // the tensor-core kernel with the source row read from global memory and 64 /
@@ -914,6 +1017,27 @@ static int launch_mixed(const DevBasis<Ti> *B, FastPlan<Ti> &P, FastScratch<Ti> 
             return BSIM_OK;
         }
     }
+    if constexpr (sizeof(T) == 8) {
+        // FP64: per-warp B fragments, the source row on chip where it fits
+        if (mixed_dmma_on()) {
+            const bool on_chip = mixed_dmma_smem(P.ldA, P.nF, false) <= std::min(kSmemMax, mixed_row_limit());
+            const size_t smem = mixed_dmma_smem(P.ldA, P.nF, !on_chip);
+            if (smem <= kSmemMax) {
+                auto kern = on_chip ? mixed_dmma_kernel<Ti, false> : mixed_dmma_kernel<Ti, true>;
+                BSIM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                const int passes = (P.M + 63) / 64;
+                T *Z = static_cast<T *>(z.p);
+                const size_t Wz = z.w;
+                for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
+                    for (int pass = 0; pass < passes; ++pass)
+                        STAGE(tm, 3, s, (kern<<<P.nA, 512, smem, s>>>(ma, P.d_astr, ct, Z, z0, (int)Wz, 64 * pass)));
+                    dim3 g(P.nA, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
+                    STAGE(tm, 4, s, (mixed_gather_kernel<Ti, T><<<g, 256, 0, s>>>(ma, B->view, Z, dst, z0, (int)Wz)));
+                }
+                return BSIM_OK;
+            }
+        }
+    }
     const int rows = (sizeof(T) == 4 && EPT == 10) ? 80 : 64;
     const MixedShape sh = mixed_shape(P.nB, P.nF, sizeof(T), mixed_row_limit(), rows);
     if (sh.smem > kSmemMax) { set_error("mixed kernel needs %zu bytes of shared memory", sh.smem); return BSIM_ERR_UNSUPPORTED; }
@@ -923,6 +1047,14 @@ static int launch_mixed(const DevBasis<Ti> *B, FastPlan<Ti> &P, FastScratch<Ti> 
                          : launch_mixed_shape<Ti, T, EPT, false, true>(B, P, ma, ct, Z, dst, c0, c1, z.w, sh.smem, s, tm);
     return sh.stream ? launch_mixed_shape<Ti, T, EPT, true, false>(B, P, ma, ct, Z, dst, c0, c1, z.w, sh.smem, s, tm)
                      : launch_mixed_shape<Ti, T, EPT, false, false>(B, P, ma, ct, Z, dst, c0, c1, z.w, sh.smem, s, tm);
+}
+
+// BSIM_RI_TC=0 sends the FP32-bulk intermediate-string GEMM to the CUDA-core
+// kernel (read on every call: tests compare the two paths)
+static bool ri_tc_on()
+{
+    const char *e = getenv("BSIM_RI_TC");
+    return !(e && e[0] == '0');
 }
 
 // Same-spin doubles of one side through the intermediate strings, columns [c0, c1)
@@ -943,8 +1075,17 @@ static int launch_ri(const RISide &R, const T *in, int ld_in, double *out, int l
     const size_t smem = ri_smem_bytes(R.nU, sizeof(T));
     BSIM_CUDA(cudaFuncSetAttribute(ri_gemm_kernel<T, EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     T *Z = static_cast<T *>(z.p);
+    // FP32 bulk: the tensor-core (TF32 x 3) kernel
+    bool tc = false;
+    if constexpr (sizeof(T) == 4) tc = ri_tc_on() && ri_tc_supported(R.nU) && ri_tc_smem(R.nU) <= kSmemMax;
     for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
-        STAGE(tm, 7, s, (ri_gemm_kernel<T, EPT><<<R.nM, NT, smem, s>>>(ra, in, Z, z0, (int)Wz)));
+        if constexpr (sizeof(T) == 4) {
+            if (tc) {
+                STAGE(tm, 7, s, rc = ri_gemm_tc(ra, in, Z, z0, (int)Wz, s));
+                if (rc != BSIM_OK) return rc;
+            }
+        }
+        if (!tc) STAGE(tm, 7, s, (ri_gemm_kernel<T, EPT><<<R.nM, NT, smem, s>>>(ra, in, Z, z0, (int)Wz)));
         dim3 g(nrows, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
         STAGE(tm, 8, s, (ri_gather_kernel<T><<<g, 256, 0, s>>>(ra, R.gath, Z, out, ld_out, z0, (int)Wz)));
     }

@@ -1,31 +1,39 @@
-// FP32-bulk mixed GEMM of the structured sigma on the 5th-generation tensor
-// cores (tcgen05.mma kind::tf32, accumulators in tensor memory).
+// FP32-bulk GEMMs of the structured sigma on the 5th-generation tensor cores
+// (tcgen05.mma kind::tf32, accumulators in tensor memory): the mixed-excitation
+// product and the same-spin doubles through intermediate strings.
 //
-// Per source row a' the mixed part of sigma needs Y[j][b] = sum_F Lam_conn[j][F]
-// X[F][b], X[F][b] = sB_F c~[a'][b ^ F] gathered from the row (see
-// mixed_gemm_kernel in sigma_fast.cu).  Here the product is computed transposed,
-// D[b][j] = sum_F X^T[b][F] Lam_conn^T[F][j], so that 128 columns b of a chunk are
-// the MMA's M = 128 rows (one TMEM lane each) and the <= 64 connected excitations
-// j are its N = 64 columns.  FP32 accuracy from TF32 inputs: every operand is
+// Both are, per CTA, Y[j][b] = sum_k B[j][k] X[k][b] over the columns b of a Z
+// window, with a CTA-specific B and X rows taken from c~:
+//   mixed (one CTA per source row a'): B = Lam_conn (the row's connected alpha
+//     excitations j), X[F][b] = sB_F c~[a'][b ^ F] gathered from the row (see
+//     mixed_gemm_kernel in sigma_fast.cu);
+//   intermediate (one CTA per intermediate string m): B = W_m (pair-pair
+//     integrals of the pairs outside m, the sign of each source row folded in),
+//     X[k][b] = c~[m + pair_k][b], whole rows of c~ (ri_gemm_kernel).
+// The product is computed transposed, D[b][j] = sum_k X^T[b][k] B^T[k][j], so that
+// 128 columns b of a chunk are the MMA's M = 128 rows (one TMEM lane each) and
+// the j are its N columns.  FP32 accuracy from TF32 inputs: every operand is
 // split into x = hi + lo, hi = x with its 13 low mantissa bits cleared (exact in
 // TF32) and lo = x - hi (exact in FP32), and D accumulates hi*hi + hi*lo + lo*hi
 // in FP32 (Ootomo & Yokota 2022, "Recovering single precision accuracy from
 // Tensor Cores while surpassing the FP32 theoretical peak"; the lo*lo term,
 // ~2^-22 relative, is dropped).
 //
-// Shapes: N = 64 connected excitations per pass with the source row staged in
-// shared memory (up to 16 orbitals with 8 electrons), or, when the row does not
-// fit (18 orbitals: a 175 KB FP32 row), the row gathered from global memory (L2)
-// with N = 64 or 80 (the 80 connected singles of 8 electrons in 18 orbitals in
-// one pass).
+// Mixed shapes: N = 64 connected excitations per pass with the source row staged
+// in shared memory (up to 16 orbitals with 8 electrons), or, when the row does
+// not fit (18 orbitals: a 175 KB FP32 row), the row gathered from global memory
+// (L2) with N = 64 or 80 (the 80 connected singles of 8 electrons in 18 orbitals
+// in one pass).  Intermediate shapes: N = the pairs outside an intermediate
+// rounded up to 16 (45 -> 48 at 16 orbitals, 66 -> 80 at 18).
 //
-// Warp roles (672 threads, one CTA per source row, one pass of N excitations):
+// Warp roles (672 threads, one CTA per row or intermediate):
 //   warps 0-3   epilogue: tcgen05.ld of D (warp w reads TMEM lanes 32w..32w+31)
-//               and the store of Z[a'][j][b];
-//   warps 4-19  producers: the X^T slice of 40 F rows, gathered from the source
-//               row in shared memory, split, written in the canonical K-major
-//               layout (8-row x 16-byte core matrices) into a double buffer (the
-//               gathers bound the kernel: 16 warps keep the tensor pipe fed);
+//               and the store of Z[row][j][b];
+//   warps 4-19  producers: the X^T slice of KS k rows (gathered from the source
+//               row, or read from the c~ rows), split, written in the canonical
+//               K-major layout (8-row x 16-byte core matrices) into a double
+//               buffer (the loads bound the kernel: 16 warps keep the tensor pipe
+//               fed);
 //   warp 20     TMEM allocation (two N-column accumulators) and, lane 0, the
 //               MMA issue: 3 MMAs of 128 x N x 8 per K step.
 // Handoffs are mbarriers: afull/aempty per A buffer (producers -> MMA; the MMA
@@ -47,14 +55,15 @@ namespace {
 constexpr int kTcThreads = 672;
 constexpr int kTcProdWarps = 16;          // warps 4..19
 constexpr int kTcMmaWarp = 20;
-constexpr int kTcKS = 40;                 // F rows per A slice (a multiple of 8)
 constexpr int kTcM = 128;                 // columns b per chunk: MMA M
-template <int N> struct TcShape {
-    static constexpr uint32_t tmem_cols = N <= 64 ? 128u : 256u;   // two N-column accumulators, a power of 2
-};
+constexpr int kMixKS = 40;                // F rows per A slice of the mixed product (a multiple of 8)
 constexpr unsigned long long kTcWaitNs = 20000000ull;   // a wait gives up after 20 ms
 constexpr long kTcSpinCap = 1L << 26;                   // and after this many rounds in any case
 constexpr uint32_t kCoreBytes = 128;      // one core matrix: 8 rows x 16 bytes (4 TF32)
+
+// two N-column accumulators, allocated as a power of 2 of at least 32 columns
+template <int N>
+constexpr uint32_t tmem_cols() { return N <= 16 ? 32u : N <= 32 ? 64u : N <= 64 ? 128u : 256u; }
 // instruction descriptor of kind::tf32: D FP32 (bits 4-5 = 1), A and B TF32
 // (bits 7-9, 10-12 = 2), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
 template <int N>
@@ -66,32 +75,51 @@ __device__ int g_tc_abort;      // set with the first of them: later CTAs return
 
 // Shared-memory layout (bytes from the dynamic base, 128-byte aligned pieces).
 struct TcLayout {
-    uint32_t srow, bh, bl, ah0, ah1, al0, al1, conn, sgn, bars, tmem, total;
+    uint32_t srow, bh, bl, ah0, ah1, al0, al1, raw, tab, bars, tmem, total;
     int kp8;        // K rounded up to the MMA's K step (8)
     uint32_t sbo_b; // byte stride between 8-row groups of B (all K chunks of a group)
 };
 __host__ __device__ inline uint32_t align128(uint32_t x) { return (x + 127u) & ~127u; }
-__host__ __device__ inline TcLayout tc_layout(int ldA, int nF, int N, bool grow)
+// srow_bytes: the source row staged on chip (0 when it is not); raw_bytes: the
+// producers' copy ring (0 when they load into registers); tab_bytes: the CTA's
+// index tables
+__host__ __device__ inline TcLayout tc_layout(uint32_t srow_bytes, int K, int N, int KS, uint32_t raw_bytes,
+                                              uint32_t tab_bytes)
 {
     TcLayout L{};
-    L.kp8 = (nF + 7) & ~7;
+    L.kp8 = (K + 7) & ~7;
     L.sbo_b = (uint32_t)(L.kp8 / 4) * kCoreBytes;
     const uint32_t bbytes = (uint32_t)(N / 8) * L.sbo_b;
-    const uint32_t abytes = (uint32_t)(kTcM / 8) * (kTcKS / 4) * kCoreBytes;
+    const uint32_t abytes = (uint32_t)(kTcM / 8) * (uint32_t)(KS / 4) * kCoreBytes;
     uint32_t o = 0;
-    L.srow = o; o = align128(o + (grow ? 0u : (uint32_t)ldA * 4));
+    L.srow = o; o = align128(o + srow_bytes);
     L.bh = o; o = align128(o + bbytes);
     L.bl = o; o = align128(o + bbytes);
     L.ah0 = o; o = align128(o + abytes);
     L.ah1 = o; o = align128(o + abytes);
     L.al0 = o; o = align128(o + abytes);
     L.al1 = o; o = align128(o + abytes);
-    L.conn = o; o = align128(o + kMaxConn * 4);
-    L.sgn = o; o = align128(o + kMaxConn * 4);
+    L.raw = o; o = align128(o + raw_bytes);
+    L.tab = o; o = align128(o + tab_bytes);
     L.bars = o; o = align128(o + 9 * 8);
     L.tmem = o; o = align128(o + 4);
     L.total = o;
     return L;
+}
+__host__ __device__ inline TcLayout mixed_layout(int ldA, int nF, int N, bool grow)
+{
+    return tc_layout(grow ? 0u : (uint32_t)ldA * 4u, nF, N, kMixKS, 0u, 2u * kMaxConn * 4u);
+}
+// intermediate product: K = pairs outside the intermediate, KS rows per slice
+// (a multiple of 16: each producer copies KS / 16 quads of a slice), kRiRing
+// slices in the copy ring
+constexpr int kRiRing = 4;
+__host__ __device__ inline int ri_ks(int K) { return K > 32 && K <= 48 ? 48 : 32; }
+__host__ __device__ inline int ri_n(int K) { return (K + 15) & ~15; }
+__host__ __device__ inline TcLayout ri_layout(int K)
+{
+    const int KS = ri_ks(K);
+    return tc_layout(0u, K, ri_n(K), KS, (uint32_t)(kRiRing * KS * kTcM * 4), (uint32_t)kRiMaxU * 8u);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count)
@@ -205,75 +233,46 @@ __device__ __forceinline__ uint32_t kmajor_off(int r, int k, uint32_t sbo)
     return (uint32_t)(r >> 3) * sbo + (uint32_t)(k >> 2) * kCoreBytes + (uint32_t)(r & 7) * 16u + (uint32_t)(k & 3) * 4u;
 }
 
-template <typename Ti, int N, bool GROW>
-__global__ void __launch_bounds__(kTcThreads, 1)
-mixed_gemm_tc_kernel(const MixedArgs P, const Ti *__restrict__ astr, const float *__restrict__ ct,
-                     float *__restrict__ Z, int z0, int W, int jbase)
+// B = [N x kp8] K-major, hi and lo parts: bval(j, k) for j < jm and k < K, zero
+// elsewhere.
+template <int N, typename BVal>
+__device__ __forceinline__ void stage_b(const TcLayout &L, unsigned char *smem, int jm, int K, BVal bval)
 {
-    static_assert(N % 16 == 0 && N >= 16 && N <= 128, "MMA N for M = 128: a multiple of 16");
-    constexpr uint32_t kTmemCols = TcShape<N>::tmem_cols;
-    constexpr uint32_t kIdesc = idesc_tf32<N>();
-    extern __shared__ __align__(1024) unsigned char smem[];
-    const TcLayout L = tc_layout(P.ldA, P.nF, N, GROW);
-    const int K = P.nF;
-    float *srow = reinterpret_cast<float *>(smem + L.srow);
-    int *conn = reinterpret_cast<int *>(smem + L.conn);
-    int *sgn = reinterpret_cast<int *>(smem + L.sgn);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L.tmem);
-    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
-    const uint32_t bar0 = sbase + L.bars;   // afull[2], aempty[2], dfull[2], dempty[2], done
-    auto afull = [&](int i) { return bar0 + 8u * (uint32_t)i; };
-    auto aempty = [&](int i) { return bar0 + 8u * (uint32_t)(2 + i); };
-    auto dfull = [&](int i) { return bar0 + 8u * (uint32_t)(4 + i); };
-    auto dempty = [&](int i) { return bar0 + 8u * (uint32_t)(6 + i); };
-    const uint32_t done = bar0 + 64u;
-    __shared__ int wcnt[kTcThreads / 32], cnt;
-    __shared__ volatile int abort_flag;
-    __shared__ int skip_all;
-    const int a = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) skip_all = *(volatile int *)&g_tc_abort;
-    __syncthreads();
-    if (skip_all) return;   // an earlier CTA gave up a wait: the result is void (counted)
-    const int m = connected_excitations<kTcThreads>(P, (u64)astr[a], conn, sgn, wcnt, &cnt);
-    const int jm = min(N, m - jbase);
-    if (jm <= 0) return;   // uniform across the CTA
-
-    // ---- stage the source row and B = Lam_conn^T (hi and lo) ----
-    {
-        if (!GROW) {
-            const int4 *src = reinterpret_cast<const int4 *>(ct + (i64)a * P.ldA);
-            int4 *dst = reinterpret_cast<int4 *>(srow);
-            const int n16 = P.ldA / 4;
-            for (int i = threadIdx.x; i < n16; i += kTcThreads) dst[i] = __ldg(src + i);
-        }
-        const float *Lam = static_cast<const float *>(P.Lam);
-        const int nk4 = L.kp8 / 4;
-        // core matrix cm = (row group rg, K chunk kc); element e = (row r, k within chunk)
-        for (int i = threadIdx.x; i < N * L.kp8; i += kTcThreads) {
-            const int cm = i >> 5, e = i & 31;
-            const int j = (cm / nk4) * 8 + (e & 7), f = (cm % nk4) * 4 + (e >> 3);
-            const float x = (j < jm && f < K) ? (float)sgn[jbase + j] * Lam[(i64)conn[jbase + j] * K + f] : 0.f;
-            float hi, lo;
-            tf32_split(x, hi, lo);
-            const uint32_t off = kmajor_off(j, f, L.sbo_b);
-            *reinterpret_cast<float *>(smem + L.bh + off) = hi;
-            *reinterpret_cast<float *>(smem + L.bl + off) = lo;
-        }
+    const int nk4 = L.kp8 / 4;
+    // core matrix cm = (row group, K chunk); element e = (row r, k within chunk)
+    for (int i = threadIdx.x; i < N * L.kp8; i += kTcThreads) {
+        const int cm = i >> 5, e = i & 31;
+        const int j = (cm / nk4) * 8 + (e & 7), k = (cm % nk4) * 4 + (e >> 3);
+        const float x = (j < jm && k < K) ? bval(j, k) : 0.f;
+        float hi, lo;
+        tf32_split(x, hi, lo);
+        const uint32_t off = kmajor_off(j, k, L.sbo_b);
+        *reinterpret_cast<float *>(smem + L.bh + off) = hi;
+        *reinterpret_cast<float *>(smem + L.bl + off) = lo;
     }
+}
+
+// Barrier initialisation and TMEM allocation; every thread leaves with the
+// accumulators' TMEM address (B and any staged row are visible to the MMAs).
+template <int N>
+__device__ __forceinline__ uint32_t tc_begin(const TcLayout &L, uint32_t sbase, unsigned char *smem,
+                                             volatile int *abort_flag)
+{
+    const uint32_t bar0 = sbase + L.bars;   // afull[2], aempty[2], dfull[2], dempty[2], done
     if (threadIdx.x == 0) {
         for (int i = 0; i < 2; ++i) {
-            mbar_init(afull(i), 32 * kTcProdWarps);
-            mbar_init(aempty(i), 1);
-            mbar_init(dfull(i), 1);
-            mbar_init(dempty(i), 128);
+            mbar_init(bar0 + 8u * (uint32_t)i, 32 * kTcProdWarps);
+            mbar_init(bar0 + 8u * (uint32_t)(2 + i), 1);
+            mbar_init(bar0 + 8u * (uint32_t)(4 + i), 1);
+            mbar_init(bar0 + 8u * (uint32_t)(6 + i), 128);
         }
-        mbar_init(done, 1);
-        abort_flag = 0;
+        mbar_init(bar0 + 64u, 1);
+        *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == kTcMmaWarp) {
+    if ((threadIdx.x >> 5) == kTcMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + L.tmem),
-                     "r"(kTmemCols)
+                     "r"(tmem_cols<N>())
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -281,83 +280,78 @@ mixed_gemm_tc_kernel(const MixedArgs P, const Ti *__restrict__ astr, const float
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
+    return *reinterpret_cast<volatile uint32_t *>(smem + L.tmem);
+}
 
-    const int zend = min(P.cend, z0 + W);
-    const int ncb = (zend - z0 + kTcM - 1) / kTcM;
-    const int nsl = (L.kp8 + kTcKS - 1) / kTcKS;
+template <int N>
+__device__ __forceinline__ void tc_end(uint32_t tmem)
+{
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if ((threadIdx.x >> 5) == kTcMmaWarp)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols<N>())
+                     : "memory");
+}
+
+// The pipelined product over ncb column chunks of 128 (from z0) and the KS-row
+// slices of each: producers fill A slices through src, lane 0 of the MMA warp
+// issues the MMAs into the two accumulators, the epilogue warps store D's first
+// jm columns to zrow[j * W + c * 128 + b].
+//
+// Src (one per producer thread) fills the A slices; each producer calls
+// setup(pw, lane) once, begin(nq) once, then per slice q: wait(q) (its data of
+// slice q has arrived), write(q, hi, lo) (split its elements of slice q, rows
+// past K zero, into the canonical buffers), next(q) (start loading a later
+// slice), and finish() before it leaves.  Slice q covers rows (q % nsl) * KS..
+// and chunk columns (q / nsl) * 128.. from z0.
+template <int N, int KS, typename Src>
+__device__ __forceinline__ void tc_pipeline(const TcLayout &L, unsigned char *smem, uint32_t sbase, uint32_t tmem,
+                                            int ncb, int jm, float *zrow, int W, Src &src, volatile int *abort_flag)
+{
+    static_assert(N % 16 == 0 && N >= 16 && N <= 128, "MMA N for M = 128: a multiple of 16");
+    static_assert(KS % 8 == 0, "slices of whole MMA K steps");
+    constexpr uint32_t kIdesc = idesc_tf32<N>();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t bar0 = sbase + L.bars;
+    auto afull = [&](int i) { return bar0 + 8u * (uint32_t)i; };
+    auto aempty = [&](int i) { return bar0 + 8u * (uint32_t)(2 + i); };
+    auto dfull = [&](int i) { return bar0 + 8u * (uint32_t)(4 + i); };
+    auto dempty = [&](int i) { return bar0 + 8u * (uint32_t)(6 + i); };
+    const uint32_t done = bar0 + 64u;
+    const int nsl = (L.kp8 + KS - 1) / KS;
     const int nq = ncb * nsl;
     const uint32_t ah[2] = {sbase + L.ah0, sbase + L.ah1}, al[2] = {sbase + L.al0, sbase + L.al1};
-    constexpr uint32_t kSboA = (kTcKS / 4) * kCoreBytes;   // 8-row groups of an A slice
+    constexpr uint32_t kSboA = (KS / 4) * kCoreBytes;   // 8-row groups of an A slice
 
     if (warp >= 4 && warp < 4 + kTcProdWarps) {
         // ---- producers ----
-        // Producer warp pw owns core matrices cm = pw + 16 it (it < 10) of every
-        // slice: 8 rows b (lanes & 7) x 4 slice rows f (lanes >> 3).  Their offsets
-        // into the gather table (without the slice's f0 * ldG + cb), their slice
-        // rows and their shared-memory offsets do not change between slices.
-        const int pw = warp - 4;
-        constexpr int nkc = kTcKS / 4, ncm = (kTcM / 8) * nkc;   // 160 core matrices per slice
-        constexpr int PI = ncm / kTcProdWarps;
-        static_assert(PI * kTcProdWarps == ncm, "every producer warp owns the same number of core matrices");
-        int goff[PI], foff[PI], gp[PI];
-        float gv[GROW ? PI : 1];   // GROW: the next slice's values, gathered from the row in L2
-        const float *grow = ct + (i64)a * P.ldA;
-        uint32_t soff[PI];
-#pragma unroll
-        for (int it = 0; it < PI; ++it) {
-            const int cm = pw + it * kTcProdWarps;
-            const int rg = cm / nkc, kc = cm % nkc;
-            foff[it] = kc * 4 + (lane >> 3);
-            goff[it] = foff[it] * P.ldG + rg * 8 + (lane & 7);
-            soff[it] = (uint32_t)rg * kSboA + (uint32_t)kc * kCoreBytes + (uint32_t)(lane & 7) * 16u +
-                       (uint32_t)(lane >> 3) * 4u;
-        }
-        auto prefetch = [&](int q) {
-            const int f0 = (q % nsl) * kTcKS;
-            const int *gbase = P.gidx + (i64)f0 * P.ldG + z0 + (q / nsl) * kTcM;
-#pragma unroll
-            for (int it = 0; it < PI; ++it) gp[it] = f0 + foff[it] < K ? __ldg(gbase + goff[it]) : -1;
-            if constexpr (GROW) {
-#pragma unroll
-                for (int it = 0; it < PI; ++it) gv[it] = gp[it] >= 0 ? __ldg(grow + (gp[it] >> 1)) : 0.f;
-            }
-        };
-        if (nq > 0) prefetch(0);
+        src.setup(warp - 4, lane);
+        src.begin(nq);
         for (int q = 0; q < nq; ++q) {
             const int buf = q & 1;
-            if (q >= 2 && !mbar_wait(aempty(buf), (uint32_t)(((q >> 1) - 1) & 1), &abort_flag)) break;
-            unsigned char *ahp = smem + (buf ? L.ah1 : L.ah0), *alp = smem + (buf ? L.al1 : L.al0);
-#pragma unroll
-            for (int it = 0; it < PI; ++it) {
-                const int g = gp[it];
-                float x;
-                if constexpr (GROW) x = gv[it];
-                else x = g >= 0 ? srow[g >> 1] : 0.f;
-                if (g & 1) x = -x;
-                float hi, lo;
-                tf32_split(x, hi, lo);
-                *reinterpret_cast<float *>(ahp + soff[it]) = hi;
-                *reinterpret_cast<float *>(alp + soff[it]) = lo;
-            }
+            if (q >= 2 && !mbar_wait(aempty(buf), (uint32_t)(((q >> 1) - 1) & 1), abort_flag)) break;
+            src.wait(q);
+            src.write(q, smem + (buf ? L.ah1 : L.ah0), smem + (buf ? L.al1 : L.al0));
             fence_async_smem();
             mbar_arrive(afull(buf));
-            if (q + 1 < nq) prefetch(q + 1);
+            src.next(q);
         }
+        src.finish();
     } else if (warp == kTcMmaWarp) {
         // ---- MMA issue ----
         if (lane == 0) {
             bool ok = true;
             for (int c = 0; c < ncb && ok; ++c) {
                 const int dbuf = c & 1;
-                if (c >= 2 && !mbar_wait(dempty(dbuf), (uint32_t)(((c >> 1) - 1) & 1), &abort_flag)) break;
+                if (c >= 2 && !mbar_wait(dempty(dbuf), (uint32_t)(((c >> 1) - 1) & 1), abort_flag)) break;
                 tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)dbuf * N;
                 for (int s = 0; s < nsl; ++s) {
                     const int q = c * nsl + s, buf = q & 1;
-                    if (!mbar_wait(afull(buf), (uint32_t)((q >> 1) & 1), &abort_flag)) { ok = false; break; }
+                    if (!mbar_wait(afull(buf), (uint32_t)((q >> 1) & 1), abort_flag)) { ok = false; break; }
                     tc_fence_after();
-                    const int f0 = s * kTcKS, nks = (min(kTcKS, L.kp8 - f0) + 7) / 8;
+                    const int f0 = s * KS, nks = (min(KS, L.kp8 - f0) + 7) / 8;
                     for (int ks = 0; ks < nks; ++ks) {
                         const uint32_t aoff = (uint32_t)ks * 2u * kCoreBytes;
                         const uint32_t boff = (uint32_t)(f0 / 4 + 2 * ks) * kCoreBytes;
@@ -378,13 +372,13 @@ mixed_gemm_tc_kernel(const MixedArgs P, const Ti *__restrict__ astr, const float
         }
         __syncwarp();
     } else if (warp < 4) {
-        // ---- epilogue: D (TMEM lanes 32 warp .. +31 = columns b) -> Z[a'][j][b] ----
+        // ---- epilogue: D (TMEM lanes 32 warp .. +31 = columns b) -> Z[row][j][b] ----
         for (int c = 0; c < ncb; ++c) {
             const int dbuf = c & 1;
-            if (!mbar_wait(dfull(dbuf), (uint32_t)((c >> 1) & 1), &abort_flag)) break;
+            if (!mbar_wait(dfull(dbuf), (uint32_t)((c >> 1) & 1), abort_flag)) break;
             tc_fence_after();
             const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)dbuf * N;
-            float *zb = Z + ((i64)a * P.M + jbase) * W + c * kTcM + warp * 32 + lane;
+            float *zb = zrow + c * kTcM + warp * 32 + lane;
             // 16 columns (excitations j) at a time: TMEM -> registers -> Z
             for (int i = 0; i < N / 16 && 16 * i < jm; ++i) {
                 float v[16];
@@ -397,17 +391,243 @@ mixed_gemm_tc_kernel(const MixedArgs P, const Ti *__restrict__ astr, const float
             if (c + 2 < ncb) mbar_arrive(dempty(dbuf));
         }
     }
-    tc_fence_before();
+}
+
+// byte offset of element (column b, slice row k) in an A slice of KS rows
+template <int KS>
+__device__ __forceinline__ uint32_t a_off(int b, int k)
+{
+    return (uint32_t)(b >> 3) * (uint32_t)((KS / 4) * kCoreBytes) + (uint32_t)(k >> 2) * kCoreBytes +
+           (uint32_t)(b & 7) * 16u + (uint32_t)(k & 3) * 4u;
+}
+__device__ __forceinline__ void put_split(unsigned char *hi, unsigned char *lo, uint32_t off, float x)
+{
+    float h, l;
+    tf32_split(x, h, l);
+    *reinterpret_cast<float *>(hi + off) = h;
+    *reinterpret_cast<float *>(lo + off) = l;
+}
+
+// X^T[b][F] = sB_F c~[a'][b ^ F] through the gather table (rank(b ^ F) << 1 |
+// sign, or -1), from the row staged in shared memory or (GROW) read from
+// global memory a slice ahead into registers.  Producer warp pw owns core
+// matrices cm = pw + 16 it of every slice: 8 columns b (lanes & 7) x 4 slice
+// rows (lanes >> 3), conflict-free stores.
+template <int KS, bool GROW>
+struct GatherSrc {
+    static constexpr int nkc = KS / 4, PI = (kTcM / 8) * nkc / kTcProdWarps;
+    static_assert(PI * kTcProdWarps == (kTcM / 8) * nkc, "every producer warp owns the same number of core matrices");
+    const int *gidx;
+    const float *row;
+    int ldG, K, z0, nsl, nq;
+    int goff[PI], foff[PI], gp[PI];
+    uint32_t soff[PI];
+    float gv[GROW ? PI : 1];
+    __device__ __forceinline__ void setup(int pw, int lane)
+    {
+#pragma unroll
+        for (int it = 0; it < PI; ++it) {
+            const int cm = pw + it * kTcProdWarps;
+            const int b = (cm / nkc) * 8 + (lane & 7), k = (cm % nkc) * 4 + (lane >> 3);
+            foff[it] = k;
+            goff[it] = k * ldG + b;
+            soff[it] = a_off<KS>(b, k);
+        }
+    }
+    __device__ __forceinline__ void prefetch(int q)
+    {
+        const int f0 = (q % nsl) * KS;
+        const int *gbase = gidx + (i64)f0 * ldG + z0 + (q / nsl) * kTcM;
+#pragma unroll
+        for (int it = 0; it < PI; ++it) gp[it] = f0 + foff[it] < K ? __ldg(gbase + goff[it]) : -1;
+        if constexpr (GROW) {
+#pragma unroll
+            for (int it = 0; it < PI; ++it) gv[it] = gp[it] >= 0 ? __ldg(row + (gp[it] >> 1)) : 0.f;
+        }
+    }
+    __device__ __forceinline__ void begin(int n) { nq = n; if (nq > 0) prefetch(0); }
+    __device__ __forceinline__ void wait(int) {}
+    __device__ __forceinline__ void write(int, unsigned char *hi, unsigned char *lo)
+    {
+#pragma unroll
+        for (int it = 0; it < PI; ++it) {
+            const int g = gp[it];
+            float x;
+            if constexpr (GROW) x = gv[it];
+            else x = g >= 0 ? row[g >> 1] : 0.f;
+            put_split(hi, lo, soff[it], (g & 1) ? -x : x);
+        }
+    }
+    __device__ __forceinline__ void next(int q) { if (q + 1 < nq) prefetch(q + 1); }
+    __device__ __forceinline__ void finish() {}
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+
+// X^T[b][k] = c~[row_k][b]: whole rows of c~ at the element offsets roff[k]
+// (shared memory), columns past ld and rows past K read as zero.  Each producer
+// thread copies 16-byte quads (4 columns of one row) of every slice with
+// cp.async into its own part of an RS-slice ring and later splits exactly those
+// quads, so the ring needs no barrier among the producers; RS - 1 slices are in
+// flight.  Warp pw's quad i covers rows 4 (id / 4) + (lane & 3) and columns
+// 32 (id % 4) + 4 (lane / 4) .. + 3, id = pw + 16 i (four 128-byte row segments
+// per warp load); the 4 columns of a quad are stored in an order rotated by
+// lane / 8 so that a warp's stores hit 32 distinct banks.
+template <int KS, int RS>
+struct RowRingSrc {
+    static constexpr int QI = KS / 16;
+    static_assert(QI * 16 == KS, "KS / 16 quads per producer and slice");
+    const float *in;
+    const long long *roff;
+    float4 *raw;   // [RS][QI][512]
+    int K, ld, z0, nsl, nq;
+    int p, pw, rot, kq, bq;
+    __device__ __forceinline__ int krow(int i) const { return ((pw + kTcProdWarps * i) >> 2) * 4 + kq; }
+    __device__ __forceinline__ int bcol(int i) const { return ((pw + kTcProdWarps * i) & 3) * 32 + bq; }
+    __device__ __forceinline__ void setup(int w, int lane)
+    {
+        pw = w;
+        p = w * 32 + lane;
+        rot = lane >> 3;
+        kq = lane & 3;
+        bq = (lane >> 2) * 4;
+    }
+    __device__ __forceinline__ void issue(int q)
+    {
+        if (q < nq) {
+            const int f0 = (q % nsl) * KS, cb = z0 + (q / nsl) * kTcM;
+            float4 *dst = raw + (size_t)(q % RS) * QI * 512 + p;
+#pragma unroll
+            for (int i = 0; i < QI; ++i) {
+                const int r = f0 + krow(i), col = cb + bcol(i);
+                const bool ok = r < K && col < ld;
+                cp_async16(dst + i * 512, ok ? (const void *)(in + roff[r] + col) : (const void *)in, ok ? 16 : 0);
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");   // one group per slice, empty past the last
+    }
+    __device__ __forceinline__ void begin(int n)
+    {
+        nq = n;
+#pragma unroll
+        for (int q = 0; q < RS - 1; ++q) issue(q);
+    }
+    __device__ __forceinline__ void wait(int) { asm volatile("cp.async.wait_group %0;\n" ::"n"(RS - 2) : "memory"); }
+    __device__ __forceinline__ void write(int q, unsigned char *hi, unsigned char *lo)
+    {
+        const float4 *src = raw + (size_t)(q % RS) * QI * 512 + p;
+#pragma unroll
+        for (int i = 0; i < QI; ++i) {
+            const float4 v = src[i * 512];
+#pragma unroll
+            for (int e2 = 0; e2 < 4; ++e2) {
+                const int e = (e2 + rot) & 3;
+                const float x01 = (e & 1) ? v.y : v.x, x23 = (e & 1) ? v.w : v.z;
+                const float x = (e & 2) ? x23 : x01;
+                put_split(hi, lo, a_off<KS>(bcol(i) + e, krow(i)), x);
+            }
+        }
+    }
+    __device__ __forceinline__ void next(int q) { issue(q + RS - 1); }
+    __device__ __forceinline__ void finish() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+};
+
+template <typename Ti, int N, bool GROW>
+__global__ void __launch_bounds__(kTcThreads, 1)
+mixed_gemm_tc_kernel(const MixedArgs P, const Ti *__restrict__ astr, const float *__restrict__ ct,
+                     float *__restrict__ Z, int z0, int W, int jbase)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const TcLayout L = mixed_layout(P.ldA, P.nF, N, GROW);
+    const int K = P.nF;
+    float *srow = reinterpret_cast<float *>(smem + L.srow);
+    int *conn = reinterpret_cast<int *>(smem + L.tab);
+    int *sgn = conn + kMaxConn;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
+    __shared__ int wcnt[kTcThreads / 32], cnt;
+    __shared__ volatile int abort_flag;
+    __shared__ int skip_all;
+    const int a = blockIdx.x;
+    if (threadIdx.x == 0) skip_all = *(volatile int *)&g_tc_abort;
     __syncthreads();
-    tc_fence_after();
-    if (warp == kTcMmaWarp)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
-                     : "memory");
+    if (skip_all) return;   // an earlier CTA gave up a wait: the result is void (counted)
+    const int m = connected_excitations<kTcThreads>(P, (u64)astr[a], conn, sgn, wcnt, &cnt);
+    const int jm = min(N, m - jbase);
+    if (jm <= 0) return;   // uniform across the CTA
+
+    // ---- stage the source row and B = Lam_conn^T (hi and lo) ----
+    if (!GROW) {
+        const int4 *src = reinterpret_cast<const int4 *>(ct + (i64)a * P.ldA);
+        int4 *dst = reinterpret_cast<int4 *>(srow);
+        const int n16 = P.ldA / 4;
+        for (int i = threadIdx.x; i < n16; i += kTcThreads) dst[i] = __ldg(src + i);
+    }
+    const float *Lam = static_cast<const float *>(P.Lam);
+    stage_b<N>(L, smem, jm, K, [&](int j, int f) {
+        return (float)sgn[jbase + j] * Lam[(i64)conn[jbase + j] * K + f];
+    });
+    const uint32_t tmem = tc_begin<N>(L, sbase, smem, &abort_flag);
+
+    const int zend = min(P.cend, z0 + W);
+    const int ncb = (zend - z0 + kTcM - 1) / kTcM;
+    GatherSrc<kMixKS, GROW> src;
+    src.gidx = P.gidx;
+    src.row = GROW ? ct + (i64)a * P.ldA : srow;
+    src.ldG = P.ldG;
+    src.K = K;
+    src.z0 = z0;
+    src.nsl = (L.kp8 + kMixKS - 1) / kMixKS;
+    tc_pipeline<N, kMixKS>(L, smem, sbase, tmem, ncb, jm, Z + ((i64)a * P.M + jbase) * W, W, src, &abort_flag);
+    tc_end<N>(tmem);
+}
+
+// One CTA per intermediate m: Z[m][j][b] = sum_k W[pair_j][pair_k] s(m, pair_k)
+// c~[m + pair_k][b] for the K pairs outside m.
+template <int N, int KS>
+__global__ void __launch_bounds__(kTcThreads, 1)
+ri_gemm_tc_kernel(const RIArgs P, const float *__restrict__ in, float *__restrict__ Z, int z0, int W)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int K = P.nU;
+    const TcLayout L = ri_layout(K);
+    long long *roff = reinterpret_cast<long long *>(smem + L.tab);
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
+    __shared__ volatile int abort_flag;
+    __shared__ int skip_all;
+    const int m = blockIdx.x;
+    if (threadIdx.x == 0) skip_all = *(volatile int *)&g_tc_abort;
+    __syncthreads();
+    if (skip_all) return;   // an earlier CTA gave up a wait: the result is void (counted)
+    const int *srcm = P.src + (i64)m * K, *pidm = P.pid + (i64)m * K;
+    for (int i = threadIdx.x; i < K; i += kTcThreads) roff[i] = (long long)(__ldg(srcm + i) >> 1) * P.ld_in;
+    const float *Wt = static_cast<const float *>(P.W);
+    stage_b<N>(L, smem, K, K, [&](int j, int k) {
+        const float w = Wt[(i64)__ldg(pidm + j) * P.nP + __ldg(pidm + k)];
+        return (__ldg(srcm + k) & 1) ? -w : w;
+    });
+    const uint32_t tmem = tc_begin<N>(L, sbase, smem, &abort_flag);   // its barrier also publishes roff
+
+    const int zend = min(P.cend, z0 + W);
+    const int ncb = (zend - z0 + kTcM - 1) / kTcM;
+    RowRingSrc<KS, kRiRing> src;
+    src.in = in;
+    src.roff = roff;
+    src.raw = reinterpret_cast<float4 *>(smem + L.raw);
+    src.K = K;
+    src.ld = P.ld_in;
+    src.z0 = z0;
+    src.nsl = (L.kp8 + KS - 1) / KS;
+    tc_pipeline<N, KS>(L, smem, sbase, tmem, ncb, K, Z + (i64)m * K * W, W, src, &abort_flag);
+    tc_end<N>(tmem);
 }
 
 }  // namespace
 
-size_t mixed_tc_smem(int ldA, int nF, int N, bool grow) { return tc_layout(ldA, nF, N, grow).total; }
+size_t mixed_tc_smem(int ldA, int nF, int N, bool grow) { return mixed_layout(ldA, nF, N, grow).total; }
 
 template <typename Ti>
 int mixed_gemm_tc(const MixedArgs &ma, const Ti *astr, const float *ct, float *Z, int z0, int W, int jbase, int N,
@@ -424,6 +644,31 @@ int mixed_gemm_tc(const MixedArgs &ma, const Ti *astr, const float *ct, float *Z
     if (N == 80 && grow) return launch(mixed_gemm_tc_kernel<Ti, 80, true>);
     set_error("tensor-core mixed GEMM: no kernel for %d excitations per pass", N);
     return BSIM_ERR_UNSUPPORTED;
+}
+
+bool ri_tc_supported(int nU) { return nU >= 1 && nU <= kRiMaxU && ri_n(nU) <= 80; }
+size_t ri_tc_smem(int nU) { return ri_layout(nU).total; }
+
+int ri_gemm_tc(const RIArgs &ra, const float *in, float *Z, int z0, int W, cudaStream_t s)
+{
+    if (!ri_tc_supported(ra.nU)) {
+        set_error("tensor-core intermediate GEMM: %d pairs outside an intermediate", ra.nU);
+        return BSIM_ERR_UNSUPPORTED;
+    }
+    const size_t smem = ri_tc_smem(ra.nU);
+    auto launch = [&](auto kern) -> int {
+        BSIM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<ra.nM, kTcThreads, smem, s>>>(ra, in, Z, z0, W);
+        BSIM_CUDA(cudaGetLastError());
+        return BSIM_OK;
+    };
+    switch (ri_n(ra.nU)) {
+    case 16: return launch(ri_gemm_tc_kernel<16, 32>);
+    case 32: return launch(ri_gemm_tc_kernel<32, 32>);
+    case 48: return launch(ri_gemm_tc_kernel<48, 48>);
+    case 64: return launch(ri_gemm_tc_kernel<64, 32>);
+    default: return launch(ri_gemm_tc_kernel<80, 32>);
+    }
 }
 
 int mixed_tc_timeouts(int *count, bool reset)

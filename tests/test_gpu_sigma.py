@@ -219,6 +219,33 @@ def test_mixed_gemm_source_row_in_global_memory(cuda, oracle, monkeypatch, mixed
     assert np.abs(y_glob.cpu().numpy() - ref).max() <= tol * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("norb,na,nb", [(11, 5, 5), (12, 6, 5), (13, 3, 4)])
+@pytest.mark.parametrize("row_on_chip", [True, False])
+def test_fp64_mixed_gemm_kernels_agree(cuda, oracle, monkeypatch, norb, na, nb, row_on_chip):
+    """The FP64 mixed GEMM with per-warp B fragments (default) against the kernel
+    with a shared X slice (BSIM_MIXED_DMMA=0): the same DMMA sums in the same
+    order per output tile, so the same bits; both against the oracle at
+    1e-12 x max|sigma|.  row_on_chip False reads the source row from global
+    memory (BSIM_MIXED_ROW_SMEM=1).  Connected rows per pass 30, 36 / 30 and 30:
+    partial 8-row blocks."""
+    from binsim_b200 import cuotf, network as nw
+    net = nw.hamiltonian_network(norb, seed=9)
+    B = cuotf.CuBasis(norb, na, nb)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    assert f.sigma_path()[0] == 1
+    xh = np.random.default_rng(norb).normal(size=B.dim)
+    x = dev(cuda, xh)
+    if not row_on_chip:
+        monkeypatch.setenv("BSIM_MIXED_ROW_SMEM", "1")
+    y_new, y_old = cuda.empty_like(x), cuda.empty_like(x)
+    f.hvec(x, y_new)
+    monkeypatch.setenv("BSIM_MIXED_DMMA", "0")
+    f.hvec(x, y_old)
+    assert cuda.equal(y_new, y_old)
+    ref = oracle.hvec(oracle.basis(norb, na, nb), oracle.network(net), xh)
+    assert np.abs(y_new.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
 @pytest.mark.parametrize("norb,na,nb", [(13, 3, 3), (13, 3, 4), (14, 4, 4)])
 def test_intermediate_string_gemm_beyond_64_pairs(cuda, oracle, norb, na, nb):
     """66 pairs outside each (n-2)-electron intermediate string (the count at 18 orbitals,

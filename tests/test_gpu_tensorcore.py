@@ -1,4 +1,5 @@
-"""FP32-bulk sigma whose mixed part runs on the tcgen05 tensor cores (kind::tf32
+"""FP32-bulk sigma whose mixed part and intermediate-string (same-spin doubles)
+product run on the tcgen05 tensor cores (kind::tf32
 with every operand split into TF32 hi + lo, FP32 accumulation in tensor memory),
 against the oracle's FP64 sigma.  The sizes cover ragged K slices (F excitations
 not a multiple of the 40-row slice or of the MMA's K step of 8), ragged column
@@ -70,3 +71,33 @@ def test_tensor_core_and_cuda_core_fp32_paths_agree(cuda, monkeypatch):
     assert float((y_tc - y_cc).abs().max()) <= 2e-6 * scale
     assert float((y_tc - y64).abs().max()) <= 2e-6 * scale
     assert float((y_cc - y64).abs().max()) <= 2e-6 * scale
+
+
+@pytest.mark.parametrize("norb,na,nb", [(8, 4, 4), (10, 5, 5), (11, 3, 3), (12, 3, 3), (13, 3, 3), (12, 2, 4)])
+def test_intermediate_string_gemm_on_tensor_cores(cuda, oracle, monkeypatch, norb, na, nb):
+    """The same-spin doubles through intermediate strings on the tensor cores, at
+    every accumulator width: pairs outside an intermediate 15 (N = 16), 21 (32),
+    45 (48), 55 (64), 66 (80; alpha of 12o 2a+4b, whose beta side has 45).  FP32
+    bulk against the oracle's FP64 sigma, and against the CUDA-core kernel
+    (BSIM_RI_TC=0)."""
+    from binsim_b200 import cuotf, network as nw
+    L = cuotf.lib()
+    _timeouts(L, reset=True)
+    net = nw.hamiltonian_network(norb, seed=5)
+    B = cuotf.CuBasis(norb, na, nb)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    path = f.sigma_path()
+    assert path[0] == 1 and "ri-alpha" in path[1] and "ri-beta" in path[1], path
+    x = np.random.default_rng(norb + na).normal(size=B.dim)
+    x /= np.linalg.norm(x)
+    ref = oracle.hvec(oracle.basis(norb, na, nb), oracle.network(net), x)
+    scale = np.abs(ref).max()
+    xd = dev(cuda, x)
+    y_tc, y_cc = cuda.empty_like(xd), cuda.empty_like(xd)
+    f.hvec_mixed(xd, y_tc)
+    cuda.cuda.synchronize()
+    assert np.abs(y_tc.cpu().numpy() - ref).max() <= 2e-6 * scale
+    monkeypatch.setenv("BSIM_RI_TC", "0")
+    f.hvec_mixed(xd, y_cc)
+    assert float((y_tc - y_cc).abs().max()) <= 2e-6 * scale
+    assert _timeouts(L) == 0

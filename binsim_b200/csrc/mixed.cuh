@@ -14,6 +14,16 @@ struct MixedArgs {
     const int *gidx;        // [nF x ldG]: (rank(b^F) << 1 | sign) or -1
 };
 
+// Layout of the GEMM outputs Z (a window of W columns, W a multiple of 128):
+// for output row group r (a source row, or an intermediate string) of R rows,
+// chunk c of 128 columns is one contiguous [R][128] block, so a chunk's output
+// is written as one piece.  zchunk gives the block of (r, c).
+template <typename T>
+__host__ __device__ __forceinline__ T *zchunk(T *Z, int r, int R, int W, int c)
+{
+    return Z + (i64)r * R * W + (i64)c * R * kMixCols;
+}
+
 struct RIArgs {
     int nM, nU, npr, nP, ld_in, cend;
     const int *src, *pid;

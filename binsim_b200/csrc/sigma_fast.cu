@@ -463,7 +463,7 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
         if (step + 1 < nsteps) load_g(step + 1);
         if (active) acc.template step<LS>(lam, xs, STREAM ? 0 : f0, nf);
         if (fci == nfc - 1) {
-            if (active) acc.store(Z + ((i64)a * M + jbase) * W + cbi * kMixCols, W, jm);
+            if (active) acc.store(zchunk(Z, a, M, W, cbi) + jbase * kMixCols, kMixCols, jm);
             acc.zero();
         }
     }
@@ -558,11 +558,11 @@ mixed_dmma_kernel(const MixedArgs P, const Ti *__restrict__ astr, const double *
             }
         }
         if (fci == nfc - 1) {
-            double *zr = Z + ((i64)a * M + jbase + g) * W + cbi * kMixCols + 8 * wid + 2 * t;
+            double *zr = zchunk(Z, a, M, W, cbi) + (jbase + g) * kMixCols + 8 * wid + 2 * t;
 #pragma unroll
             for (int rb = 0; rb < 8; ++rb) {
                 if (rb < nrb && rb * 8 + g < jm)
-                    *reinterpret_cast<double2 *>(zr + (i64)(rb * 8) * W) = make_double2(c[rb][0], c[rb][1]);
+                    *reinterpret_cast<double2 *>(zr + rb * 8 * kMixCols) = make_double2(c[rb][0], c[rb][1]);
                 c[rb][0] = c[rb][1] = 0.0;
             }
         }
@@ -610,7 +610,8 @@ mixed_gather_kernel(const MixedArgs P, const BasisView<Ti> BV, const T *__restri
     for (int b = z0 + blockIdx.y * kRowChunk + threadIdx.x; b < min(zend, z0 + (blockIdx.y + 1) * kRowChunk);
          b += blockDim.x) {
         T part = T(0);
-        for (int e = 0; e < n; ++e) part += __ldg(Z + ((i64)esrc[e] * P.M + ej[e]) * W + (b - z0));
+        const T *zc = Z + (i64)((b - z0) / kMixCols) * P.M * kMixCols + (b - z0) % kMixCols;
+        for (int e = 0; e < n; ++e) part += __ldg(zc + (i64)esrc[e] * P.M * W + ej[e] * kMixCols);
         sig[(i64)a * P.nB + b] += (double)part;
     }
 }
@@ -724,12 +725,12 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
             }
         }
         if (fci == nfc - 1) {
-            if (active) acc.store(Z + (i64)m * K * W + cbi * kMixCols, W, K);
+            if (active) acc.store(zchunk(Z, m, K, W, cbi), kMixCols, K);
             acc.zero();
 #pragma unroll
             for (int q = 0; q < TQ; ++q) {
                 const int o = threadIdx.x + q * NT;
-                if (o < ntail) Z[((i64)m * K + 64 + o / kMixCols) * W + cbi * kMixCols + o % kMixCols] = tacc[q];
+                if (o < ntail) zchunk(Z, m, K, W, cbi)[(64 + o / kMixCols) * kMixCols + o % kMixCols] = tacc[q];
                 tacc[q] = T(0);
             }
         }
@@ -747,16 +748,18 @@ ri_gather_kernel(const RIArgs P, const int2 *__restrict__ gath, const T *__restr
     const int row = blockIdx.x;
     for (int e = threadIdx.x; e < P.npr; e += blockDim.x) {
         const int2 g = gath[(i64)row * P.npr + e];
-        eoff[e] = (long long)g.x * W * 2 + (g.y & 1);
+        const int m = g.x / P.nU, slot = g.x % P.nU;
+        eoff[e] = ((long long)m * P.nU * W + slot * kMixCols) * 2 + (g.y & 1);
     }
     __syncthreads();
     const int zend = min(P.cend, z0 + W);
     for (int b = z0 + blockIdx.y * kRowChunk + threadIdx.x; b < min(zend, z0 + (blockIdx.y + 1) * kRowChunk);
          b += blockDim.x) {
         T part = T(0);
+        const T *zc = Z + (i64)((b - z0) / kMixCols) * P.nU * kMixCols + (b - z0) % kMixCols;
         for (int e = 0; e < P.npr; ++e) {
             const long long o = eoff[e];
-            const T v = __ldg(Z + (o >> 1) + (b - z0));
+            const T v = __ldg(zc + (o >> 1));
             part += (o & 1) ? -v : v;
         }
         out[(i64)row * ld_out + b] += (double)part;

@@ -28,12 +28,13 @@
 //
 // Warp roles (672 threads, one CTA per row or intermediate):
 //   warps 0-3   epilogue: tcgen05.ld of D (warp w reads TMEM lanes 32w..32w+31)
-//               and the store of Z[row][j][b];
+//               and the store of the chunk's contiguous [j][128] block of Z;
 //   warps 4-19  producers: the X^T slice of KS k rows (gathered from the source
-//               row, or read from the c~ rows), split, written in the canonical
-//               K-major layout (8-row x 16-byte core matrices) into a double
-//               buffer (the loads bound the kernel: 16 warps keep the tensor pipe
-//               fed);
+//               row; or copied from the c~ rows with cp.async into a ring of
+//               slices, RS - 1 ahead, then transposed), split, written in the
+//               canonical K-major layout (8-row x 16-byte core matrices) into a
+//               double buffer (the loads bound the kernel: 16 warps keep the
+//               tensor pipe fed);
 //   warp 20     TMEM allocation (two N-column accumulators) and, lane 0, the
 //               MMA issue: 3 MMAs of 128 x N x 8 per K step.
 // Handoffs are mbarriers: afull/aempty per A buffer (producers -> MMA; the MMA
@@ -57,6 +58,8 @@ constexpr int kTcProdWarps = 16;          // warps 4..19
 constexpr int kTcMmaWarp = 20;
 constexpr int kTcM = 128;                 // columns b per chunk: MMA M
 constexpr int kMixKS = 40;                // F rows per A slice of the mixed product (a multiple of 8)
+constexpr int kMixStages = 2;             // its A stages
+constexpr int kRiStages = 2, kRiRing = 4; // the intermediate product's A stages and copy-ring slots
 constexpr unsigned long long kTcWaitNs = 20000000ull;   // a wait gives up after 20 ms
 constexpr long kTcSpinCap = 1L << 26;                   // and after this many rounds in any case
 constexpr uint32_t kCoreBytes = 128;      // one core matrix: 8 rows x 16 bytes (4 TF32)
@@ -75,16 +78,14 @@ __device__ int g_tc_abort;      // set with the first of them: later CTAs return
 
 // Shared-memory layout (bytes from the dynamic base, 128-byte aligned pieces).
 struct TcLayout {
-    uint32_t srow, bh, bl, ah0, ah1, al0, al1, raw, tab, bars, tmem, total;
+    uint32_t srow, bh, bl, ah, al, abytes, tab, bars, tmem, total;
     int kp8;        // K rounded up to the MMA's K step (8)
     uint32_t sbo_b; // byte stride between 8-row groups of B (all K chunks of a group)
 };
 __host__ __device__ inline uint32_t align128(uint32_t x) { return (x + 127u) & ~127u; }
-// srow_bytes: the source row staged on chip (0 when it is not); raw_bytes: the
-// producers' copy ring (0 when they load into registers); tab_bytes: the CTA's
-// index tables
-__host__ __device__ inline TcLayout tc_layout(uint32_t srow_bytes, int K, int N, int KS, uint32_t raw_bytes,
-                                              uint32_t tab_bytes)
+// srow_bytes: the source row staged on chip (0 when it is not); S: A stages of
+// KS rows (hi and lo parts); tab_bytes: the CTA's index tables
+__host__ __device__ inline TcLayout tc_layout(uint32_t srow_bytes, int K, int N, int KS, int S, uint32_t tab_bytes)
 {
     TcLayout L{};
     L.kp8 = (K + 7) & ~7;
@@ -95,31 +96,30 @@ __host__ __device__ inline TcLayout tc_layout(uint32_t srow_bytes, int K, int N,
     L.srow = o; o = align128(o + srow_bytes);
     L.bh = o; o = align128(o + bbytes);
     L.bl = o; o = align128(o + bbytes);
-    L.ah0 = o; o = align128(o + abytes);
-    L.ah1 = o; o = align128(o + abytes);
-    L.al0 = o; o = align128(o + abytes);
-    L.al1 = o; o = align128(o + abytes);
-    L.raw = o; o = align128(o + raw_bytes);
+    L.abytes = abytes;
+    L.ah = o; o = align128(o + (uint32_t)S * abytes);
+    L.al = o; o = align128(o + (uint32_t)S * abytes);
     L.tab = o; o = align128(o + tab_bytes);
-    L.bars = o; o = align128(o + 9 * 8);
+    L.bars = o; o = align128(o + (uint32_t)(2 * S + 5) * 8);
     L.tmem = o; o = align128(o + 4);
     L.total = o;
     return L;
 }
 __host__ __device__ inline TcLayout mixed_layout(int ldA, int nF, int N, bool grow)
 {
-    return tc_layout(grow ? 0u : (uint32_t)ldA * 4u, nF, N, kMixKS, 0u, 2u * kMaxConn * 4u);
+    return tc_layout(grow ? 0u : (uint32_t)ldA * 4u, nF, N, kMixKS, kMixStages, 2u * kMaxConn * 4u);
 }
-// intermediate product: K = pairs outside the intermediate, KS rows per slice
-// (a multiple of 16: each producer copies KS / 16 quads of a slice), kRiRing
-// slices in the copy ring
-constexpr int kRiRing = 4;
-__host__ __device__ inline int ri_ks(int K) { return K > 32 && K <= 48 ? 48 : 32; }
+// intermediate product: K = pairs outside the intermediate, slices of KS rows
+// (a multiple of 16), kRiStages A stages and a copy ring of kRiRing slices
+// (kRiRing - 1 in flight), placed in the table area after the row offsets
 __host__ __device__ inline int ri_n(int K) { return (K + 15) & ~15; }
+__host__ __device__ inline int ri_ks(int K) { return K > 32 && K <= 48 ? 48 : 32; }
+__host__ __device__ inline uint32_t ri_raw_off() { return align128((uint32_t)kRiMaxU * 8u); }
 __host__ __device__ inline TcLayout ri_layout(int K)
 {
     const int KS = ri_ks(K);
-    return tc_layout(0u, K, ri_n(K), KS, (uint32_t)(kRiRing * KS * kTcM * 4), (uint32_t)kRiMaxU * 8u);
+    return tc_layout(0u, K, ri_n(K), KS, kRiStages,
+                     ri_raw_off() + (uint32_t)(kRiRing * KS * kTcM * 4));
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count)
@@ -150,13 +150,17 @@ __device__ __forceinline__ unsigned long long global_ns()
 
 // Bounded wait for the phase of the given parity; false when the CTA aborts
 // (its own wait gave up, another wait of the CTA did, or another CTA's did).
+// The device-wide flag (a global load) and the clock are read once every 1024
+// rounds, the CTA's flag every 16: a waiter is never parked on a slow load when
+// its phase completes.
 __device__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int *abort_flag)
 {
+    if (mbar_try(a, parity)) return true;
     const unsigned long long t0 = global_ns();
-    for (long i = 0; i < kTcSpinCap; ++i) {
+    for (long i = 1; i < kTcSpinCap; ++i) {
         if (mbar_try(a, parity)) return true;
-        if (*abort_flag) return false;
-        if ((i & 63) == 63) {
+        if ((i & 15) == 0 && *abort_flag) return false;
+        if ((i & 1023) == 0) {
             if (*(volatile int *)&g_tc_abort) { *abort_flag = 1; return false; }
             if (global_ns() - t0 > kTcWaitNs) break;
         }
@@ -174,7 +178,7 @@ __device__ void mbar_wait_drain(uint32_t a, uint32_t parity)
     const unsigned long long t0 = global_ns();
     for (long i = 0; i < kTcSpinCap; ++i) {
         if (mbar_try(a, parity)) return;
-        if ((i & 63) == 63 && global_ns() - t0 > kTcWaitNs) break;
+        if ((i & 1023) == 1023 && global_ns() - t0 > kTcWaitNs) break;
     }
     atomicExch(&g_tc_abort, 1);
     atomicAdd(&g_tc_timeouts, 1);
@@ -254,19 +258,21 @@ __device__ __forceinline__ void stage_b(const TcLayout &L, unsigned char *smem, 
 
 // Barrier initialisation and TMEM allocation; every thread leaves with the
 // accumulators' TMEM address (B and any staged row are visible to the MMAs).
-template <int N>
+template <int N, int S>
 __device__ __forceinline__ uint32_t tc_begin(const TcLayout &L, uint32_t sbase, unsigned char *smem,
                                              volatile int *abort_flag)
 {
-    const uint32_t bar0 = sbase + L.bars;   // afull[2], aempty[2], dfull[2], dempty[2], done
+    const uint32_t bar0 = sbase + L.bars;   // afull[S], aempty[S], dfull[2], dempty[2], done
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < S; ++i) {
             mbar_init(bar0 + 8u * (uint32_t)i, 32 * kTcProdWarps);
-            mbar_init(bar0 + 8u * (uint32_t)(2 + i), 1);
-            mbar_init(bar0 + 8u * (uint32_t)(4 + i), 1);
-            mbar_init(bar0 + 8u * (uint32_t)(6 + i), 128);
+            mbar_init(bar0 + 8u * (uint32_t)(S + i), 1);
         }
-        mbar_init(bar0 + 64u, 1);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(bar0 + 8u * (uint32_t)(2 * S + i), 1);
+            mbar_init(bar0 + 8u * (uint32_t)(2 * S + 2 + i), 128);
+        }
+        mbar_init(bar0 + 8u * (uint32_t)(2 * S + 4), 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -297,17 +303,19 @@ __device__ __forceinline__ void tc_end(uint32_t tmem)
 // The pipelined product over ncb column chunks of 128 (from z0) and the KS-row
 // slices of each: producers fill A slices through src, lane 0 of the MMA warp
 // issues the MMAs into the two accumulators, the epilogue warps store D's first
-// jm columns to zrow[j * W + c * 128 + b].
+// jm columns to zrow[(c * zrows + j) * 128 + b] (zrow: row j = 0 of chunk 0 of
+// this CTA's Z block, zrows: rows per chunk block).
 //
-// Src (one per producer thread) fills the A slices; each producer calls
-// setup(pw, lane) once, begin(nq) once, then per slice q: wait(q) (its data of
-// slice q has arrived), write(q, hi, lo) (split its elements of slice q, rows
-// past K zero, into the canonical buffers), next(q) (start loading a later
-// slice), and finish() before it leaves.  Slice q covers rows (q % nsl) * KS..
-// and chunk columns (q / nsl) * 128.. from z0.
-template <int N, int KS, typename Src>
+// Slice q covers rows (q % nsl) * KS.. and chunk columns (q / nsl) * 128.. from
+// z0 and lives in A stage q % S (hi and lo parts, K-major).  Src (one per producer thread) fills the slices: setup(pw, lane) once,
+// begin(nq) once, then per slice produce(q, free) (its elements of slice q, rows
+// past K zero, split into the stage; free(t) waits until stage t % S may be
+// overwritten for slice t and is false when the CTA aborts; produce is false
+// then too), and finish() before the producer leaves.
+template <int N, int KS, int S, typename Src>
 __device__ __forceinline__ void tc_pipeline(const TcLayout &L, unsigned char *smem, uint32_t sbase, uint32_t tmem,
-                                            int ncb, int jm, float *zrow, int W, Src &src, volatile int *abort_flag)
+                                            int ncb, int jm, float *zrow, int zrows, Src &src,
+                                            volatile int *abort_flag)
 {
     static_assert(N % 16 == 0 && N >= 16 && N <= 128, "MMA N for M = 128: a multiple of 16");
     static_assert(KS % 8 == 0, "slices of whole MMA K steps");
@@ -315,27 +323,27 @@ __device__ __forceinline__ void tc_pipeline(const TcLayout &L, unsigned char *sm
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t bar0 = sbase + L.bars;
     auto afull = [&](int i) { return bar0 + 8u * (uint32_t)i; };
-    auto aempty = [&](int i) { return bar0 + 8u * (uint32_t)(2 + i); };
-    auto dfull = [&](int i) { return bar0 + 8u * (uint32_t)(4 + i); };
-    auto dempty = [&](int i) { return bar0 + 8u * (uint32_t)(6 + i); };
-    const uint32_t done = bar0 + 64u;
+    auto aempty = [&](int i) { return bar0 + 8u * (uint32_t)(S + i); };
+    auto dfull = [&](int i) { return bar0 + 8u * (uint32_t)(2 * S + i); };
+    auto dempty = [&](int i) { return bar0 + 8u * (uint32_t)(2 * S + 2 + i); };
+    const uint32_t done = bar0 + 8u * (uint32_t)(2 * S + 4);
     const int nsl = (L.kp8 + KS - 1) / KS;
     const int nq = ncb * nsl;
-    const uint32_t ah[2] = {sbase + L.ah0, sbase + L.ah1}, al[2] = {sbase + L.al0, sbase + L.al1};
-    constexpr uint32_t kSboA = (KS / 4) * kCoreBytes;   // 8-row groups of an A slice
+    // A descriptors: core matrices 8 rows b x 4 k, K chunks 128 bytes apart,
+    // 8-row groups KS / 4 chunks apart; one K step of 8 is two chunks
+    constexpr uint32_t kLboA = kCoreBytes, kSboA = (KS / 4) * kCoreBytes, kStepA = 2u * kCoreBytes;
 
     if (warp >= 4 && warp < 4 + kTcProdWarps) {
         // ---- producers ----
+        auto free_stage = [&](int t) -> bool {
+            return t < S || mbar_wait(aempty(t % S), (uint32_t)(((t / S) - 1) & 1), abort_flag);
+        };
         src.setup(warp - 4, lane);
         src.begin(nq);
         for (int q = 0; q < nq; ++q) {
-            const int buf = q & 1;
-            if (q >= 2 && !mbar_wait(aempty(buf), (uint32_t)(((q >> 1) - 1) & 1), abort_flag)) break;
-            src.wait(q);
-            src.write(q, smem + (buf ? L.ah1 : L.ah0), smem + (buf ? L.al1 : L.al0));
+            if (!src.produce(q, free_stage)) break;
             fence_async_smem();
-            mbar_arrive(afull(buf));
-            src.next(q);
+            mbar_arrive(afull(q % S));
         }
         src.finish();
     } else if (warp == kTcMmaWarp) {
@@ -348,22 +356,23 @@ __device__ __forceinline__ void tc_pipeline(const TcLayout &L, unsigned char *sm
                 tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)dbuf * N;
                 for (int s = 0; s < nsl; ++s) {
-                    const int q = c * nsl + s, buf = q & 1;
-                    if (!mbar_wait(afull(buf), (uint32_t)((q >> 1) & 1), abort_flag)) { ok = false; break; }
+                    const int q = c * nsl + s, st = q % S;
+                    if (!mbar_wait(afull(st), (uint32_t)((q / S) & 1), abort_flag)) { ok = false; break; }
                     tc_fence_after();
                     const int f0 = s * KS, nks = (min(KS, L.kp8 - f0) + 7) / 8;
+                    const uint32_t ah = sbase + L.ah + (uint32_t)st * L.abytes, al = sbase + L.al + (uint32_t)st * L.abytes;
                     for (int ks = 0; ks < nks; ++ks) {
-                        const uint32_t aoff = (uint32_t)ks * 2u * kCoreBytes;
+                        const uint32_t aoff = (uint32_t)ks * kStepA;
                         const uint32_t boff = (uint32_t)(f0 / 4 + 2 * ks) * kCoreBytes;
-                        const uint64_t dah = umma_desc(ah[buf] + aoff, kCoreBytes, kSboA);
-                        const uint64_t dal = umma_desc(al[buf] + aoff, kCoreBytes, kSboA);
+                        const uint64_t dah = umma_desc(ah + aoff, kLboA, kSboA);
+                        const uint64_t dal = umma_desc(al + aoff, kLboA, kSboA);
                         const uint64_t dbh = umma_desc(sbase + L.bh + boff, kCoreBytes, L.sbo_b);
                         const uint64_t dbl = umma_desc(sbase + L.bl + boff, kCoreBytes, L.sbo_b);
                         umma_tf32(d, dah, dbh, kIdesc, (s | ks) != 0 ? 1u : 0u);
                         umma_tf32(d, dah, dbl, kIdesc, 1u);
                         umma_tf32(d, dal, dbh, kIdesc, 1u);
                     }
-                    umma_commit(aempty(buf));   // the slice buffer is free once these MMAs completed
+                    umma_commit(aempty(st));   // the stage is free once these MMAs completed
                 }
                 if (ok) umma_commit(dfull(dbuf));
             }
@@ -378,14 +387,14 @@ __device__ __forceinline__ void tc_pipeline(const TcLayout &L, unsigned char *sm
             if (!mbar_wait(dfull(dbuf), (uint32_t)((c >> 1) & 1), abort_flag)) break;
             tc_fence_after();
             const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)dbuf * N;
-            float *zb = zrow + c * kTcM + warp * 32 + lane;
+            float *zb = zrow + (i64)c * zrows * kTcM + warp * 32 + lane;
             // 16 columns (excitations j) at a time: TMEM -> registers -> Z
             for (int i = 0; i < N / 16 && 16 * i < jm; ++i) {
                 float v[16];
                 tmem_ld16(taddr + 16u * (uint32_t)i, v);
 #pragma unroll
                 for (int k = 0; k < 16; ++k)
-                    if (16 * i + k < jm) zb[(i64)(16 * i + k) * W] = v[k];
+                    if (16 * i + k < jm) zb[(16 * i + k) * kTcM] = v[k];
             }
             tc_fence_before();
             if (c + 2 < ncb) mbar_arrive(dempty(dbuf));
@@ -445,10 +454,14 @@ struct GatherSrc {
             for (int it = 0; it < PI; ++it) gv[it] = gp[it] >= 0 ? __ldg(row + (gp[it] >> 1)) : 0.f;
         }
     }
+    unsigned char *ah, *al;   // A stages (hi, lo)
+    uint32_t abytes;
     __device__ __forceinline__ void begin(int n) { nq = n; if (nq > 0) prefetch(0); }
-    __device__ __forceinline__ void wait(int) {}
-    __device__ __forceinline__ void write(int, unsigned char *hi, unsigned char *lo)
+    template <typename Free>
+    __device__ __forceinline__ bool produce(int q, Free &free)
     {
+        if (!free(q)) return false;
+        unsigned char *hi = ah + (size_t)(q % kMixStages) * abytes, *lo = al + (size_t)(q % kMixStages) * abytes;
 #pragma unroll
         for (int it = 0; it < PI; ++it) {
             const int g = gp[it];
@@ -457,55 +470,59 @@ struct GatherSrc {
             else x = g >= 0 ? row[g >> 1] : 0.f;
             put_split(hi, lo, soff[it], (g & 1) ? -x : x);
         }
+        if (q + 1 < nq) prefetch(q + 1);
+        return true;
     }
-    __device__ __forceinline__ void next(int q) { if (q + 1 < nq) prefetch(q + 1); }
     __device__ __forceinline__ void finish() {}
 };
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes)
+// AND of a predicate over the 512 producer threads (named barrier 1); also a
+// barrier among them.
+__device__ __forceinline__ bool producers_all(bool p)
 {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred pi, po;\n\tsetp.ne.u32 pi, %1, 0;\n\t"
+                 "bar.red.and.pred po, 1, %2, pi;\n\tselp.u32 %0, 1, 0, po;\n\t}"
+                 : "=r"(r)
+                 : "r"(p ? 1u : 0u), "n"(32 * kTcProdWarps)
+                 : "memory");
+    return r != 0;
 }
 
 // X^T[b][k] = c~[row_k][b]: whole rows of c~ at the element offsets roff[k]
-// (shared memory), columns past ld and rows past K read as zero.  Each producer
-// thread copies 16-byte quads (4 columns of one row) of every slice with
-// cp.async into its own part of an RS-slice ring and later splits exactly those
-// quads, so the ring needs no barrier among the producers; RS - 1 slices are in
-// flight.  Warp pw's quad i covers rows 4 (id / 4) + (lane & 3) and columns
-// 32 (id % 4) + 4 (lane / 4) .. + 3, id = pw + 16 i (four 128-byte row segments
-// per warp load); the 4 columns of a quad are stored in an order rotated by
-// lane / 8 so that a warp's stores hit 32 distinct banks.
+// (shared memory), columns past ld and rows past K read as zero.  The rows of a
+// slice are copied with cp.async as they lie (a warp copies one 512-byte row
+// segment) into a ring of RS slices, RS - 1 slices ahead; once a slice has
+// landed (every producer's copies: a named barrier, which also makes the
+// producers agree on going on), warp w reads columns 32 (w % 4) .. + 31 of four
+// consecutive rows 4 kc .. 4 kc + 3 (conflict-free 4-byte loads) and writes each
+// column's four values, split, as one 16-byte K-major core-matrix row of the hi
+// and of the lo stage.
 template <int KS, int RS>
 struct RowRingSrc {
-    static constexpr int QI = KS / 16;
-    static_assert(QI * 16 == KS, "KS / 16 quads per producer and slice");
+    static constexpr int QI = KS / 16;   // quads copied and core rows written per thread and slice
+    static_assert(QI * 16 == KS, "KS a multiple of 16");
     const float *in;
     const long long *roff;
-    float4 *raw;   // [RS][QI][512]
-    int K, ld, z0, nsl, nq;
-    int p, pw, rot, kq, bq;
-    __device__ __forceinline__ int krow(int i) const { return ((pw + kTcProdWarps * i) >> 2) * 4 + kq; }
-    __device__ __forceinline__ int bcol(int i) const { return ((pw + kTcProdWarps * i) & 3) * 32 + bq; }
-    __device__ __forceinline__ void setup(int w, int lane)
+    unsigned char *ah, *al;   // A stages (hi, lo)
+    uint32_t abytes;
+    float *raw;               // [RS][KS][128]
+    uint32_t raw_s;           // its shared address
+    int K, ld, z0, nsl, nq, p;
+    __device__ __forceinline__ void setup(int pw, int lane) { p = pw * 32 + lane; }
+    __device__ __forceinline__ void issue(int t)
     {
-        pw = w;
-        p = w * 32 + lane;
-        rot = lane >> 3;
-        kq = lane & 3;
-        bq = (lane >> 2) * 4;
-    }
-    __device__ __forceinline__ void issue(int q)
-    {
-        if (q < nq) {
-            const int f0 = (q % nsl) * KS, cb = z0 + (q / nsl) * kTcM;
-            float4 *dst = raw + (size_t)(q % RS) * QI * 512 + p;
+        if (t < nq) {
+            const int f0 = (t % nsl) * KS, cb = z0 + (t / nsl) * kTcM;
 #pragma unroll
             for (int i = 0; i < QI; ++i) {
-                const int r = f0 + krow(i), col = cb + bcol(i);
+                const int id = p + 32 * kTcProdWarps * i, k = id >> 5, c4 = (id & 31) * 4;
+                const int r = f0 + k, col = cb + c4;
                 const bool ok = r < K && col < ld;
-                cp_async16(dst + i * 512, ok ? (const void *)(in + roff[r] + col) : (const void *)in, ok ? 16 : 0);
+                const void *g = ok ? (const void *)(in + roff[r] + col) : (const void *)in;
+                const uint32_t d = raw_s + (uint32_t)(((t % RS) * KS + k) * kTcM + c4) * 4u;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(g), "r"(ok ? 16 : 0)
+                             : "memory");
             }
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");   // one group per slice, empty past the last
@@ -514,25 +531,32 @@ struct RowRingSrc {
     {
         nq = n;
 #pragma unroll
-        for (int q = 0; q < RS - 1; ++q) issue(q);
+        for (int t = 0; t < RS - 1; ++t) issue(t);
     }
-    __device__ __forceinline__ void wait(int) { asm volatile("cp.async.wait_group %0;\n" ::"n"(RS - 2) : "memory"); }
-    __device__ __forceinline__ void write(int q, unsigned char *hi, unsigned char *lo)
+    template <typename Free>
+    __device__ __forceinline__ bool produce(int q, Free &free)
     {
-        const float4 *src = raw + (size_t)(q % RS) * QI * 512 + p;
+        const bool mine = free(q);
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(RS - 2) : "memory");   // this thread's copies of slice q
+        if (!producers_all(mine)) return false;                                // everyone's, and all go on
+        const float *src = raw + (size_t)(q % RS) * KS * kTcM;
+        unsigned char *hi = ah + (size_t)(q % kRiStages) * abytes, *lo = al + (size_t)(q % kRiStages) * abytes;
 #pragma unroll
         for (int i = 0; i < QI; ++i) {
-            const float4 v = src[i * 512];
-#pragma unroll
-            for (int e2 = 0; e2 < 4; ++e2) {
-                const int e = (e2 + rot) & 3;
-                const float x01 = (e & 1) ? v.y : v.x, x23 = (e & 1) ? v.w : v.z;
-                const float x = (e & 2) ? x23 : x01;
-                put_split(hi, lo, a_off<KS>(bcol(i) + e, krow(i)), x);
-            }
+            const int id = p + 32 * kTcProdWarps * i, kc = id >> 7, b = id & 127;
+            const float *col = src + 4 * kc * kTcM + b;
+            float4 h, l;
+            tf32_split(col[0], h.x, l.x);
+            tf32_split(col[kTcM], h.y, l.y);
+            tf32_split(col[2 * kTcM], h.z, l.z);
+            tf32_split(col[3 * kTcM], h.w, l.w);
+            const uint32_t off = a_off<KS>(b, 4 * kc);
+            *reinterpret_cast<float4 *>(hi + off) = h;
+            *reinterpret_cast<float4 *>(lo + off) = l;
         }
+        issue(q + RS - 1);   // into the slot of slice q - 1, which every producer has read
+        return true;
     }
-    __device__ __forceinline__ void next(int q) { issue(q + RS - 1); }
     __device__ __forceinline__ void finish() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 };
 
@@ -570,7 +594,7 @@ mixed_gemm_tc_kernel(const MixedArgs P, const Ti *__restrict__ astr, const float
     stage_b<N>(L, smem, jm, K, [&](int j, int f) {
         return (float)sgn[jbase + j] * Lam[(i64)conn[jbase + j] * K + f];
     });
-    const uint32_t tmem = tc_begin<N>(L, sbase, smem, &abort_flag);
+    const uint32_t tmem = tc_begin<N, kMixStages>(L, sbase, smem, &abort_flag);
 
     const int zend = min(P.cend, z0 + W);
     const int ncb = (zend - z0 + kTcM - 1) / kTcM;
@@ -581,7 +605,11 @@ mixed_gemm_tc_kernel(const MixedArgs P, const Ti *__restrict__ astr, const float
     src.K = K;
     src.z0 = z0;
     src.nsl = (L.kp8 + kMixKS - 1) / kMixKS;
-    tc_pipeline<N, kMixKS>(L, smem, sbase, tmem, ncb, jm, Z + ((i64)a * P.M + jbase) * W, W, src, &abort_flag);
+    src.ah = smem + L.ah;
+    src.al = smem + L.al;
+    src.abytes = L.abytes;
+    tc_pipeline<N, kMixKS, kMixStages>(L, smem, sbase, tmem, ncb, jm, zchunk(Z, a, P.M, W, 0) + jbase * kTcM,
+                                              P.M, src, &abort_flag);
     tc_end<N>(tmem);
 }
 
@@ -609,19 +637,23 @@ ri_gemm_tc_kernel(const RIArgs P, const float *__restrict__ in, float *__restric
         const float w = Wt[(i64)__ldg(pidm + j) * P.nP + __ldg(pidm + k)];
         return (__ldg(srcm + k) & 1) ? -w : w;
     });
-    const uint32_t tmem = tc_begin<N>(L, sbase, smem, &abort_flag);   // its barrier also publishes roff
+    const uint32_t tmem = tc_begin<N, kRiStages>(L, sbase, smem, &abort_flag);   // its barrier also publishes roff
 
     const int zend = min(P.cend, z0 + W);
     const int ncb = (zend - z0 + kTcM - 1) / kTcM;
     RowRingSrc<KS, kRiRing> src;
     src.in = in;
     src.roff = roff;
-    src.raw = reinterpret_cast<float4 *>(smem + L.raw);
+    src.ah = smem + L.ah;
+    src.al = smem + L.al;
+    src.abytes = L.abytes;
+    src.raw = reinterpret_cast<float *>(smem + L.tab + ri_raw_off());
+    src.raw_s = sbase + L.tab + ri_raw_off();
     src.K = K;
     src.ld = P.ld_in;
     src.z0 = z0;
     src.nsl = (L.kp8 + KS - 1) / KS;
-    tc_pipeline<N, KS>(L, smem, sbase, tmem, ncb, K, Z + (i64)m * K * W, W, src, &abort_flag);
+    tc_pipeline<N, KS, kRiStages>(L, smem, sbase, tmem, ncb, K, zchunk(Z, m, K, W, 0), K, src, &abort_flag);
     tc_end<N>(tmem);
 }
 

@@ -738,6 +738,85 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
     cp_async_wait<0>();
 }
 
+// FP64 intermediate-string GEMM with per-warp B fragments (as mixed_dmma_kernel):
+// warp w owns columns 8w..8w+7 of each 128-column chunk and all K output rows
+// (ceil(K / 8) <= 9 DMMA tiles); lane (g, t) loads its B fragment elements
+// X[f0 + 4i + t][8w + g] = c~[row][col] straight from global memory (L2), a
+// 32-row K slice ahead, so the main loop has no block barrier; W_m (the A
+// fragments, k-major rows of kRiLS elements, zero past K) is staged once.
+constexpr int kRiLS = 84;   // 4 mod 16 doubles: conflict-free A fragment loads
+inline size_t ri_dmma_smem(int nU) { return (size_t)((nU + 31) & ~31) * kRiLS * 8 + kRiMaxU * 8; }
+
+__global__ void __launch_bounds__(512, 1)
+ri_dmma_kernel(const RIArgs P, const double *__restrict__ in, double *__restrict__ Z, int z0, int W)
+{
+    constexpr int NT = 512, MAXRB = (kRiMaxU + 7) / 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int K = P.nU, Kp = (K + 31) & ~31;
+    double *wm = reinterpret_cast<double *>(smem_raw);                       // [Kp][kRiLS]
+    long long *soff = reinterpret_cast<long long *>(wm + (size_t)Kp * kRiLS);  // [kRiMaxU]
+    const int m = blockIdx.x;
+    const int *srcm = P.src + (i64)m * K, *pidm = P.pid + (i64)m * K;
+    for (int i = threadIdx.x; i < K; i += NT) soff[i] = (long long)(__ldg(srcm + i) >> 1) * P.ld_in;
+    const double *Wt = static_cast<const double *>(P.W);
+    for (int i = threadIdx.x; i < Kp * kRiLS; i += NT) {
+        const int k = i / kRiLS, j = i % kRiLS;
+        double w = 0.0;
+        if (j < K && k < K) {
+            w = Wt[(i64)__ldg(pidm + j) * P.nP + __ldg(pidm + k)];
+            if (__ldg(srcm + k) & 1) w = -w;
+        }
+        wm[i] = w;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const int nrb = (K + 7) >> 3;
+    const int zend = min(P.cend, z0 + W);
+    const int ncb = (zend - z0 + kMixCols - 1) / kMixCols;
+    const int nfc = (K + 31) / 32;
+    const int nsteps = ncb * nfc;
+    const int col = 8 * wid + g;
+    double xp[8];
+    auto load = [&](int step) {
+        const int c = z0 + (step / nfc) * kMixCols + col, f0 = (step % nfc) * 32;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int r = f0 + 4 * i + t;
+            xp[i] = (r < K && c < P.ld_in) ? __ldg(in + soff[r] + c) : 0.0;
+        }
+    };
+    double c_[MAXRB][2];
+#pragma unroll
+    for (int rb = 0; rb < MAXRB; ++rb) c_[rb][0] = c_[rb][1] = 0.0;
+    if (nsteps > 0) load(0);
+    for (int step = 0; step < nsteps; ++step) {
+        const int cbi = step / nfc, fci = step % nfc;
+        const int f0 = fci * 32, nk = (min(32, K - f0) + 3) >> 2;
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = xp[i];
+        if (step + 1 < nsteps) load(step + 1);
+        const double *la = wm + (size_t)(f0 + t) * kRiLS + g;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (i < nk) {
+#pragma unroll
+                for (int rb = 0; rb < MAXRB; ++rb)
+                    if (rb < nrb) dmma_8x8x4(c_[rb][0], c_[rb][1], la[(size_t)(4 * i) * kRiLS + rb * 8], x[i]);
+            }
+        }
+        if (fci == nfc - 1) {
+            double *zr = zchunk(Z, m, K, W, cbi) + g * kMixCols + 8 * wid + 2 * t;
+#pragma unroll
+            for (int rb = 0; rb < MAXRB; ++rb) {
+                if (rb < nrb && rb * 8 + g < K)
+                    *reinterpret_cast<double2 *>(zr + rb * 8 * kMixCols) = make_double2(c_[rb][0], c_[rb][1]);
+                c_[rb][0] = c_[rb][1] = 0.0;
+            }
+        }
+    }
+}
+
 // out[row][b] += sum over the pairs pq in the row's string of s(m, pq) Z[m][slot(pq)][b]
 template <typename T>
 __global__ void __launch_bounds__(256)
@@ -1052,6 +1131,17 @@ static int launch_mixed(const DevBasis<Ti> *B, FastPlan<Ti> &P, FastScratch<Ti> 
                      : launch_mixed_shape<Ti, T, EPT, false, false>(B, P, ma, ct, Z, dst, c0, c1, z.w, sh.smem, s, tm);
 }
 
+// BSIM_RI_DMMA selects the FP64 intermediate-string GEMM (read on every call:
+// tests compare the two): "0" always the shared-slice kernel, "1" always the
+// per-warp-fragment kernel, unset the automatic choice (2 = forced, 0 = off,
+// 1 = automatic in the return value)
+static int ri_dmma_mode()
+{
+    const char *e = getenv("BSIM_RI_DMMA");
+    if (!e || !e[0]) return 1;
+    return e[0] == '0' ? 0 : 2;
+}
+
 // BSIM_RI_TC=0 sends the FP32-bulk intermediate-string GEMM to the CUDA-core
 // kernel (read on every call: tests compare the two paths)
 static bool ri_tc_on()
@@ -1078,6 +1168,23 @@ static int launch_ri(const RISide &R, const T *in, int ld_in, double *out, int l
     const size_t smem = ri_smem_bytes(R.nU, sizeof(T));
     BSIM_CUDA(cudaFuncSetAttribute(ri_gemm_kernel<T, EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     T *Z = static_cast<T *>(z.p);
+    if constexpr (sizeof(T) == 8) {
+        // FP64 with more than 64 pairs outside an intermediate (18 orbitals, 8
+        // electrons: 66): per-warp B fragments, all rows on the DMMA path
+        // (measured: 676 against 742 ms per sigma at 18o; with <= 64 pairs the
+        // shared-slice kernel is faster, 50 against 56 ms at 16o)
+        if (ri_dmma_mode() != 0 && (R.nU > 64 || ri_dmma_mode() == 2) && R.nU <= kRiMaxU &&
+            ri_dmma_smem(R.nU) <= kSmemMax) {
+            const size_t sm = ri_dmma_smem(R.nU);
+            BSIM_CUDA(cudaFuncSetAttribute(ri_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            for (int z0 = c0; z0 < c1; z0 += (int)Wz) {
+                STAGE(tm, 7, s, (ri_dmma_kernel<<<R.nM, 512, sm, s>>>(ra, in, Z, z0, (int)Wz)));
+                dim3 g(nrows, (unsigned)((std::min<size_t>(Wz, c1 - z0) + kRowChunk - 1) / kRowChunk));
+                STAGE(tm, 8, s, (ri_gather_kernel<T><<<g, 256, 0, s>>>(ra, R.gath, Z, out, ld_out, z0, (int)Wz)));
+            }
+            return BSIM_OK;
+        }
+    }
     // FP32 bulk: the tensor-core (TF32 x 3) kernel
     bool tc = false;
     if constexpr (sizeof(T) == 4) tc = ri_tc_on() && ri_tc_supported(R.nU) && ri_tc_smem(R.nU) <= kSmemMax;

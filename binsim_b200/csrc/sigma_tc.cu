@@ -62,6 +62,7 @@ constexpr int kMixStages = 2;             // its A stages
 constexpr int kRiStages = 2, kRiRing = 4; // the intermediate product's A stages and copy-ring slots
 constexpr unsigned long long kTcWaitNs = 20000000ull;   // a wait gives up after 20 ms
 constexpr long kTcSpinCap = 1L << 26;                   // and after this many rounds in any case
+constexpr unsigned kTcSuspendNs = 20000;                // longest sleep in one test of a phase
 constexpr uint32_t kCoreBytes = 128;      // one core matrix: 8 rows x 16 bytes (4 TF32)
 
 // two N-column accumulators, allocated as a power of 2 of at least 32 columns
@@ -105,6 +106,7 @@ __host__ __device__ inline TcLayout tc_layout(uint32_t srow_bytes, int K, int N,
     L.total = o;
     return L;
 }
+// mixed product: the connected lists (conn, sgn) in the table area
 __host__ __device__ inline TcLayout mixed_layout(int ldA, int nF, int N, bool grow)
 {
     return tc_layout(grow ? 0u : (uint32_t)ldA * 4u, nF, N, kMixKS, kMixStages, 2u * kMaxConn * 4u);
@@ -130,13 +132,15 @@ __device__ __forceinline__ void mbar_arrive(uint32_t a)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
 }
+// One test of the phase; the thread may sleep in it (up to kTcSuspendNs) until
+// the phase completes, so a waiting warp takes no issue slots from the others.
 __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity)
 {
     uint32_t ok;
-    asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+    asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
                  "selp.b32 %0, 1, 0, P1;\n\t}"
                  : "=r"(ok)
-                 : "r"(a), "r"(parity)
+                 : "r"(a), "r"(parity), "n"(kTcSuspendNs)
                  : "memory");
     return ok != 0;
 }
@@ -150,20 +154,17 @@ __device__ __forceinline__ unsigned long long global_ns()
 
 // Bounded wait for the phase of the given parity; false when the CTA aborts
 // (its own wait gave up, another wait of the CTA did, or another CTA's did).
-// The device-wide flag (a global load) and the clock are read once every 1024
-// rounds, the CTA's flag every 16: a waiter is never parked on a slow load when
-// its phase completes.
+// The flags and the clock are read after each test that came back without the
+// phase, i.e. at most once per suspend period.
 __device__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int *abort_flag)
 {
     if (mbar_try(a, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (long i = 1; i < kTcSpinCap; ++i) {
         if (mbar_try(a, parity)) return true;
-        if ((i & 15) == 0 && *abort_flag) return false;
-        if ((i & 1023) == 0) {
-            if (*(volatile int *)&g_tc_abort) { *abort_flag = 1; return false; }
-            if (global_ns() - t0 > kTcWaitNs) break;
-        }
+        if (*abort_flag) return false;
+        if (*(volatile int *)&g_tc_abort) { *abort_flag = 1; return false; }
+        if (global_ns() - t0 > kTcWaitNs) break;
     }
     *abort_flag = 1;
     atomicExch(&g_tc_abort, 1);
@@ -178,7 +179,7 @@ __device__ void mbar_wait_drain(uint32_t a, uint32_t parity)
     const unsigned long long t0 = global_ns();
     for (long i = 0; i < kTcSpinCap; ++i) {
         if (mbar_try(a, parity)) return;
-        if ((i & 1023) == 1023 && global_ns() - t0 > kTcWaitNs) break;
+        if (global_ns() - t0 > kTcWaitNs) break;
     }
     atomicExch(&g_tc_abort, 1);
     atomicAdd(&g_tc_timeouts, 1);
@@ -417,6 +418,19 @@ __device__ __forceinline__ void put_split(unsigned char *hi, unsigned char *lo, 
     *reinterpret_cast<float *>(lo + off) = l;
 }
 
+// AND of a predicate over the 512 producer threads (named barrier 1); also a
+// barrier among them.
+__device__ __forceinline__ bool producers_all(bool p)
+{
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred pi, po;\n\tsetp.ne.u32 pi, %1, 0;\n\t"
+                 "bar.red.and.pred po, 1, %2, pi;\n\tselp.u32 %0, 1, 0, po;\n\t}"
+                 : "=r"(r)
+                 : "r"(p ? 1u : 0u), "n"(32 * kTcProdWarps)
+                 : "memory");
+    return r != 0;
+}
+
 // X^T[b][F] = sB_F c~[a'][b ^ F] through the gather table (rank(b ^ F) << 1 |
 // sign, or -1), from the row staged in shared memory or (GROW) read from
 // global memory a slice ahead into registers.  Producer warp pw owns core
@@ -475,19 +489,6 @@ struct GatherSrc {
     }
     __device__ __forceinline__ void finish() {}
 };
-
-// AND of a predicate over the 512 producer threads (named barrier 1); also a
-// barrier among them.
-__device__ __forceinline__ bool producers_all(bool p)
-{
-    uint32_t r;
-    asm volatile("{\n\t.reg .pred pi, po;\n\tsetp.ne.u32 pi, %1, 0;\n\t"
-                 "bar.red.and.pred po, 1, %2, pi;\n\tselp.u32 %0, 1, 0, po;\n\t}"
-                 : "=r"(r)
-                 : "r"(p ? 1u : 0u), "n"(32 * kTcProdWarps)
-                 : "memory");
-    return r != 0;
-}
 
 // X^T[b][k] = c~[row_k][b]: whole rows of c~ at the element offsets roff[k]
 // (shared memory), columns past ld and rows past K read as zero.  The rows of a
@@ -608,8 +609,8 @@ mixed_gemm_tc_kernel(const MixedArgs P, const Ti *__restrict__ astr, const float
     src.ah = smem + L.ah;
     src.al = smem + L.al;
     src.abytes = L.abytes;
-    tc_pipeline<N, kMixKS, kMixStages>(L, smem, sbase, tmem, ncb, jm, zchunk(Z, a, P.M, W, 0) + jbase * kTcM,
-                                              P.M, src, &abort_flag);
+    tc_pipeline<N, kMixKS, kMixStages>(L, smem, sbase, tmem, ncb, jm, zchunk(Z, a, P.M, W, 0) + jbase * kTcM, P.M,
+                                       src, &abort_flag);
     tc_end<N>(tmem);
 }
 
@@ -659,13 +660,16 @@ ri_gemm_tc_kernel(const RIArgs P, const float *__restrict__ in, float *__restric
 
 }  // namespace
 
-size_t mixed_tc_smem(int ldA, int nF, int N, bool grow) { return mixed_layout(ldA, nF, N, grow).total; }
+// shared memory of a CTA: the dynamic layout plus the kernels' static part
+// (1 KB with the dynamic base aligned to 1 KB)
+constexpr size_t kTcStaticSmem = 1024;
+size_t mixed_tc_smem(int ldA, int nF, int N, bool grow) { return mixed_layout(ldA, nF, N, grow).total + kTcStaticSmem; }
 
 template <typename Ti>
 int mixed_gemm_tc(const MixedArgs &ma, const Ti *astr, const float *ct, float *Z, int z0, int W, int jbase, int N,
                   bool grow, cudaStream_t s)
 {
-    const size_t smem = mixed_tc_smem(ma.ldA, ma.nF, N, grow);
+    const size_t smem = mixed_layout(ma.ldA, ma.nF, N, grow).total;
     auto launch = [&](auto kern) -> int {
         BSIM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<ma.nA, kTcThreads, smem, s>>>(ma, astr, ct, Z, z0, W, jbase);
@@ -679,7 +683,7 @@ int mixed_gemm_tc(const MixedArgs &ma, const Ti *astr, const float *ct, float *Z
 }
 
 bool ri_tc_supported(int nU) { return nU >= 1 && nU <= kRiMaxU && ri_n(nU) <= 80; }
-size_t ri_tc_smem(int nU) { return ri_layout(nU).total; }
+size_t ri_tc_smem(int nU) { return ri_layout(nU).total + kTcStaticSmem; }
 
 int ri_gemm_tc(const RIArgs &ra, const float *in, float *Z, int z0, int W, cudaStream_t s)
 {
@@ -687,7 +691,7 @@ int ri_gemm_tc(const RIArgs &ra, const float *in, float *Z, int z0, int W, cudaS
         set_error("tensor-core intermediate GEMM: %d pairs outside an intermediate", ra.nU);
         return BSIM_ERR_UNSUPPORTED;
     }
-    const size_t smem = ri_tc_smem(ra.nU);
+    const size_t smem = ri_layout(ra.nU).total;
     auto launch = [&](auto kern) -> int {
         BSIM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<ra.nM, kTcThreads, smem, s>>>(ra, in, Z, z0, W);

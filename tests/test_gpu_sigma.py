@@ -246,6 +246,35 @@ def test_fp64_mixed_gemm_kernels_agree(cuda, oracle, monkeypatch, norb, na, nb, 
     assert np.abs(y_new.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("norb,na,nb", [(11, 5, 5), (12, 6, 5), (12, 2, 4)])
+def test_fp64_intermediate_gemm_kernels_agree(cuda, oracle, monkeypatch, norb, na, nb):
+    """The FP64 intermediate-string GEMM with per-warp B fragments (forced with
+    BSIM_RI_DMMA=1; by default it runs only above 64 pairs outside an intermediate)
+    against the shared-slice kernel (BSIM_RI_DMMA=0), both against the oracle at
+    1e-12 x max|sigma|.  Pairs outside an intermediate 28 / 28, 28 / 36 and 66 / 45;
+    up to 64 the two run the same DMMA sums per tile in the same order (same
+    bits); the shared-slice kernel computes rows 64.. with scalar FMAs."""
+    from binsim_b200 import cuotf, network as nw
+    net = nw.hamiltonian_network(norb, seed=11)
+    B = cuotf.CuBasis(norb, na, nb)
+    f = cuotf.CuOTFFunctions(B, cuotf.CuNetwork(net))
+    path = f.sigma_path()
+    assert path[0] == 1 and "ri-alpha" in path[1], path
+    xh = np.random.default_rng(norb + 1).normal(size=B.dim)
+    x = dev(cuda, xh)
+    y_new, y_old = cuda.empty_like(x), cuda.empty_like(x)
+    monkeypatch.setenv("BSIM_RI_DMMA", "1")
+    f.hvec(x, y_new)
+    monkeypatch.setenv("BSIM_RI_DMMA", "0")
+    f.hvec(x, y_old)
+    ref = oracle.hvec(oracle.basis(norb, na, nb), oracle.network(net), xh)
+    scale = np.abs(ref).max()
+    if na != 2:
+        assert cuda.equal(y_new, y_old)
+    assert float((y_new - y_old).abs().max()) <= 1e-12 * scale
+    assert np.abs(y_new.cpu().numpy() - ref).max() <= 1e-12 * scale
+
+
 @pytest.mark.parametrize("norb,na,nb", [(13, 3, 3), (13, 3, 4), (14, 4, 4)])
 def test_intermediate_string_gemm_beyond_64_pairs(cuda, oracle, norb, na, nb):
     """66 pairs outside each (n-2)-electron intermediate string (the count at 18 orbitals,

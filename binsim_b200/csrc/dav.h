@@ -44,7 +44,7 @@ void jacobi_eigh(int k, const double *A, int lda, double *evals, double *evecs);
 
 // Device-scalar helpers of the device-resident drivers (davidson.cu): the
 // Ritz coefficients, energy and norms stay on the device.
-int dav_eigh_dev(int k, const double *h, int ldh, double *evals, double *evecs, double *work, cudaStream_t s);
+int dav_eigh_dev(int k, const double *h, int ldh, double *evals, double *evecs, cudaStream_t s);
 template <typename TV>
 int dav_ritz_residual_dev(DavScratch &S, i64 n, int k, const double *coeffs_dev, const double *e_dev,
                           const TV *const *V, const TV *const *AV, double *r, double *x, double *norm_dev,

@@ -64,33 +64,34 @@ __global__ void resid_kernel(i64 n, const double *__restrict__ x, const double *
 namespace {
 // Device state of a driver: the projected matrix, its eigenpairs and the scalars
 // the iteration reads on the device.  sc[0] residual norm, sc[1] breakdown flag
-// of the last expansion, sc[2] / sc[3] norm before / after Gram-Schmidt.
+// of the last expansion, then the Ritz values (evals = sc + 2), so that the one
+// read of an iteration is one copy; aux[0] / aux[1] norm before / after
+// Gram-Schmidt, aux[2] the start vector's norm.
 struct DavState {
     DevBuf buf;
-    double *h = nullptr, *evals = nullptr, *evecs = nullptr, *work = nullptr, *proj = nullptr, *sc = nullptr;
+    double *h = nullptr, *evals = nullptr, *evecs = nullptr, *proj = nullptr, *sc = nullptr, *aux = nullptr;
     int init(cudaStream_t s)
     {
-        constexpr size_t kSq = (size_t)kMaxSub * kMaxSub;
-        TRY(alloc<double>(buf, 3 * kSq + 2 * kMaxSub + 8, s));
+        constexpr size_t kSq = (size_t)kMaxSub * kMaxSub, kAll = 2 * kSq + 2 * kMaxSub + 8;
+        TRY(alloc<double>(buf, kAll, s));
         h = (double *)buf.p;
         evecs = h + kSq;
-        work = evecs + kSq;
-        evals = work + kSq;
-        proj = evals + kMaxSub;
-        sc = proj + kMaxSub;
-        BSIM_CUDA(cudaMemsetAsync(buf.p, 0, sizeof(double) * (3 * kSq + 2 * kMaxSub + 8), s));
+        sc = evecs + kSq;
+        evals = sc + 2;
+        aux = evals + kMaxSub;
+        proj = aux + 4;
+        BSIM_CUDA(cudaMemsetAsync(buf.p, 0, sizeof(double) * kAll, s));
         return BSIM_OK;
     }
     // the one read of an iteration: residual norm, breakdown flag, lowest Ritz value
     int read(double *rnorm, bool *breakdown, double *e0, cudaStream_t s) const
     {
-        double v[2], e;
-        BSIM_CUDA(cudaMemcpyAsync(v, sc, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
-        BSIM_CUDA(cudaMemcpyAsync(&e, evals, sizeof(double), cudaMemcpyDeviceToHost, s));
+        double v[3];
+        BSIM_CUDA(cudaMemcpyAsync(v, sc, sizeof(double) * 3, cudaMemcpyDeviceToHost, s));
         BSIM_CUDA(cudaStreamSynchronize(s));
         *rnorm = v[0];
         *breakdown = v[1] != 0.0;
-        *e0 = e;
+        *e0 = v[2];
         return BSIM_OK;
     }
     int set_scalar(int i, double v, cudaStream_t s)
@@ -132,14 +133,14 @@ int davidson_fp64(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const 
     DavStats st{};
 
     BSIM_CUDA(cudaMemcpyAsync(V[0], v0, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-    TRY(dav_normalize(S, n, V[0], D.sc + 4, s));
+    TRY(dav_normalize(S, n, V[0], D.aux + 2, s));
     TRY(sigma(B, N, V[0], nullptr, AV[0], false, s));
     st.sigma_fp64++;
     TRY(dav_multidot<double, double>(S, n, 1, V.data(), AV[0], D.h, s));
     int dim = 1;
     double e_prev = 0.0;
     for (int iter = 1; iter <= maxiter; ++iter) {
-        TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, D.work, s));
+        TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, s));
         TRY(dav_ritz_residual_dev<double>(S, n, dim, D.evecs, D.evals, V.data(), AV.data(), axt, xk[iter & 1],
                                           D.sc, s));
         double norm_r, e;
@@ -176,16 +177,16 @@ int davidson_fp64(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const 
                 TRY(dav_multidot<double, double>(S, n, dim, V.data(), AV[j], D.h + (size_t)j * kMaxSub, s));
             TRY(dav_sym_avg(dim, D.h, kMaxSub, s));
         }
-        TRY(dav_precondition_dev<double>(S, n, axt, diags, D.evals, D.sc, D.sc + 2, s));
-        TRY(dav_cgs2_dev<double>(S, n, dim, V.data(), axt, D.sc + 2, D.proj, s));
-        TRY(dav_normalize_into<double>(n, axt, D.sc + 3, V[dim], D.sc + 1, s));
+        TRY(dav_precondition_dev<double>(S, n, axt, diags, D.evals, D.sc, D.aux, s));
+        TRY(dav_cgs2_dev<double>(S, n, dim, V.data(), axt, D.aux, D.proj, s));
+        TRY(dav_normalize_into<double>(n, axt, D.aux + 1, V[dim], D.sc + 1, s));
         TRY(sigma(B, N, V[dim], nullptr, AV[dim], false, s));
         st.sigma_fp64++;
         ++dim;
         TRY(dav_multidot<double, double>(S, n, dim, V.data(), AV[dim - 1], D.h + (size_t)(dim - 1) * kMaxSub, s));
         TRY(dav_mirror_col(dim, D.h, kMaxSub, s));
     }
-    TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, D.work, s));
+    TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, s));
     TRY(dav_combine_dev<double, double>(n, dim, D.evecs, V.data(), x_out, s));
     double e;
     BSIM_CUDA(cudaMemcpyAsync(&e, D.evals, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -248,7 +249,7 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
         double best = 1e300;   // smallest residual so far and the iterations since it
         int since_best = 0;
         for (int iter = 1; iter <= maxiter; ++iter) {
-            TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, D.work, s));
+            TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, s));
             TRY(dav_ritz_residual_dev<float>(S, n, dim, D.evecs, D.evals, V.data(), AV.data(), t, xk[iter & 1],
                                              D.sc, s));
             double norm_r, e;
@@ -274,9 +275,9 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
                     TRY(dav_multidot<float, float>(S, n, dim, V.data(), AV[j], D.h + (size_t)j * kMaxSub, s));
                 TRY(dav_sym_avg(dim, D.h, kMaxSub, s));
             }
-            TRY(dav_precondition_dev<double>(S, n, t, diags, D.evals, D.sc, D.sc + 2, s));
-            TRY(dav_cgs2_dev<float>(S, n, dim, V.data(), t, D.sc + 2, D.proj, s));
-            TRY(dav_normalize_into<float>(n, t, D.sc + 3, V[dim], D.sc + 1, s));
+            TRY(dav_precondition_dev<double>(S, n, t, diags, D.evals, D.sc, D.aux, s));
+            TRY(dav_cgs2_dev<float>(S, n, dim, V.data(), t, D.aux, D.proj, s));
+            TRY(dav_normalize_into<float>(n, t, D.aux + 1, V[dim], D.sc + 1, s));
             TRY(sigma(B, N, nullptr, V[dim], ay, true, s));
             st.sigma_fp32++;
             ++total_inner;
@@ -329,9 +330,9 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
         double rin = rnorm;
         bool have_eigh = false;   // evecs hold the eigenpairs of the current dim
         for (int it = 0; it < maxspace - 1; ++it) {
-            TRY(dav_precondition_dev<double>(S, n, t, diags, D.evals, D.sc, D.sc + 2, s));
-            TRY(dav_cgs2_dev<float>(S, n, dim, V.data(), t, D.sc + 2, D.proj, s));
-            TRY(dav_normalize_into<float>(n, t, D.sc + 3, V[dim], D.sc + 1, s));
+            TRY(dav_precondition_dev<double>(S, n, t, diags, D.evals, D.sc, D.aux, s));
+            TRY(dav_cgs2_dev<float>(S, n, dim, V.data(), t, D.aux, D.proj, s));
+            TRY(dav_normalize_into<float>(n, t, D.aux + 1, V[dim], D.sc + 1, s));
             // FP32-bulk sigma straight from the FP32 basis vector
             TRY(sigma(B, N, nullptr, V[dim], ay, true, s));
             st.sigma_fp32++;
@@ -345,7 +346,7 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
             // must not carry the FP32-bulk sigma's rounding
             TRY(dav_multidot<float, double>(S, n, 1, V.data() + (dim - 1), ax, hc, s));
             TRY(dav_mirror_col(dim, D.h, kMaxSub, s));
-            TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, D.work, s));
+            TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, s));
             const double rprev = rin;
             TRY(dav_ritz_residual_dev<float>(S, n, dim, D.evecs, D.evals, V.data(), AV.data(), t, nullptr, D.sc,
                                              s));
@@ -356,7 +357,7 @@ int davidson_mixed(const DevBasis<Ti> *B, const DevNet<Ti> *N, double *v0, const
             if (breakdown) {   // the last direction lay in the space: drop it
                 --dim;
                 TRY(D.set_scalar(1, 0.0, s));
-                TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, D.work, s));
+                TRY(dav_eigh_dev(dim, D.h, kMaxSub, D.evals, D.evecs, s));
                 break;
             }
             if (verbose) printf("    inner %02d: residual %.4e e %.14f\n", it, rin, e_in);

@@ -321,13 +321,20 @@ template int dav_multidot<float, double>(DavScratch &, i64, int, const float *co
 // norms, the re-orthogonalisation test) stays on the device; the drivers read
 // one residual norm per iteration.
 
-// The cyclic Jacobi of jacobi_eigh (same rotation order, formulas and stopping
-// rule) by one warp on the leading k x k block of h (column-major, ld ldh):
-// evals ascending, evecs[i + j k] = component i of eigenvector j; work: k * k doubles.
+// Jacobi eigensolver of the leading k x k block of the symmetric h (column-
+// major, ld ldh) by one warp, A and the eigenvectors V in shared memory: the
+// rotation formulas and stopping rule of jacobi_eigh, with the disjoint pairs of
+// a round-robin round (k / 2 of them, k rounded up to even) rotated together
+// (parallel ordering: each round's rotations are computed from the same A,
+// then applied to the columns, to the rows and to V).  evals ascending,
+// evecs[i + j k] = component i of eigenvector j.
 __global__ void eigh_kernel(int k, const double *__restrict__ h, int ldh, double *__restrict__ evals,
-                            double *__restrict__ evecs, double *__restrict__ work)
+                            double *__restrict__ evecs)
 {
-    extern __shared__ double A[];   // k * k
+    extern __shared__ double A[];   // A[k * k], then V[k * k]
+    __shared__ double rc[32], rs[32];
+    __shared__ int rp[32], rq[32];
+    double *work = A + k * k;
     const int lane = threadIdx.x;
     for (int i = lane; i < k * k; i += 32) {
         const int r = i % k, c = i / k;
@@ -335,6 +342,7 @@ __global__ void eigh_kernel(int k, const double *__restrict__ h, int ldh, double
         work[i] = r == c ? 1.0 : 0.0;
     }
     __syncwarp();
+    const int ke = (k + 1) & ~1, npair = ke / 2;
     for (int sweep = 0; sweep < 100; ++sweep) {
         double off = 0.0, tot = 0.0;
         for (int i = lane; i < k * k; i += 32) {
@@ -348,31 +356,47 @@ __global__ void eigh_kernel(int k, const double *__restrict__ h, int ldh, double
             tot += __shfl_xor_sync(0xffffffffu, tot, o);
         }
         if (off <= 1e-30 * fmax(tot, 1e-300)) break;
-        for (int p = 0; p < k - 1; ++p)
-            for (int q = p + 1; q < k; ++q) {
-                const double apq = A[p + q * k];
-                if (fabs(apq) < 1e-300) continue;   // the same shared value in every lane
-                const double app = A[p + p * k], aqq = A[q + q * k];
-                const double tau = (aqq - app) / (2.0 * apq);
-                const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                const double c = 1.0 / sqrt(1.0 + t * t), sn = t * c;
-                __syncwarp();
-                for (int r = lane; r < k; r += 32) {   // A = J^T A J: columns, then rows
-                    const double arp = A[r + p * k], arq = A[r + q * k];
-                    A[r + p * k] = c * arp - sn * arq;
-                    A[r + q * k] = sn * arp + c * arq;
+        for (int round = 0; round < ke - 1; ++round) {
+            // pair i of the round: positions i and ke - 1 - i of the sequence
+            // 0, 1 + (round + 0) % (ke - 1), 1 + (round + 1) % (ke - 1), ...
+            for (int pi = lane; pi < npair; pi += 32) {
+                auto pos = [&](int j) { return j == 0 ? 0 : 1 + (j - 1 + round) % (ke - 1); };
+                int p = pos(pi), q = pos(ke - 1 - pi);
+                if (p > q) { const int t = p; p = q; q = t; }
+                double c = 1.0, sn = 0.0;
+                if (q < k) {
+                    const double apq = A[p + q * k];
+                    if (fabs(apq) >= 1e-300) {
+                        const double app = A[p + p * k], aqq = A[q + q * k];
+                        const double tau = (aqq - app) / (2.0 * apq);
+                        const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        sn = t * c;
+                    }
                 }
-                __syncwarp();
-                for (int r = lane; r < k; r += 32) {
-                    const double apr = A[p + r * k], aqr = A[q + r * k];
-                    A[p + r * k] = c * apr - sn * aqr;
-                    A[q + r * k] = sn * apr + c * aqr;
-                    const double vrp = work[r + p * k], vrq = work[r + q * k];
-                    work[r + p * k] = c * vrp - sn * vrq;
-                    work[r + q * k] = sn * vrp + c * vrq;
-                }
-                __syncwarp();
+                rp[pi] = p; rq[pi] = q < k ? q : p; rc[pi] = c; rs[pi] = sn;
             }
+            __syncwarp();
+            for (int w = lane; w < npair * k; w += 32) {   // A = A J: columns p, q of every pair
+                const int pi = w / k, r = w % k, p = rp[pi], q = rq[pi];
+                if (p == q) continue;
+                const double c = rc[pi], sn = rs[pi], arp = A[r + p * k], arq = A[r + q * k];
+                A[r + p * k] = c * arp - sn * arq;
+                A[r + q * k] = sn * arp + c * arq;
+            }
+            __syncwarp();
+            for (int w = lane; w < npair * k; w += 32) {   // A = J^T A: rows p, q; V = V J
+                const int pi = w / k, r = w % k, p = rp[pi], q = rq[pi];
+                if (p == q) continue;
+                const double c = rc[pi], sn = rs[pi], apr = A[p + r * k], aqr = A[q + r * k];
+                A[p + r * k] = c * apr - sn * aqr;
+                A[q + r * k] = sn * apr + c * aqr;
+                const double vrp = work[r + p * k], vrq = work[r + q * k];
+                work[r + p * k] = c * vrp - sn * vrq;
+                work[r + q * k] = sn * vrp + c * vrq;
+            }
+            __syncwarp();
+        }
     }
     // ascending order (ties by index): each lane places its eigenpairs
     for (int j = lane; j < k; j += 32) {
@@ -554,11 +578,13 @@ __global__ void axpby_dev_kernel(i64 n, const double *__restrict__ a, double *__
         x[i] = s * x[i] + t[i];
 }
 
-int dav_eigh_dev(int k, const double *h, int ldh, double *evals, double *evecs, double *work, cudaStream_t s)
+int dav_eigh_dev(int k, const double *h, int ldh, double *evals, double *evecs, cudaStream_t s)
 {
     if (k < 1 || k > kMaxSub) { set_error("subspace size %d out of range", k); return BSIM_ERR_ARG; }
-    const int smem = (int)(sizeof(double) * k * k);   // <= 32 KB (k <= 64)
-    eigh_kernel<<<1, 32, smem, s>>>(k, h, ldh, evals, evecs, work);
+    const int smem = (int)(sizeof(double) * 2 * k * k);   // <= 64 KB (k <= 64)
+    if (smem > 48 * 1024)
+        BSIM_CUDA(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    eigh_kernel<<<1, 32, smem, s>>>(k, h, ldh, evals, evecs);
     BSIM_CUDA(cudaGetLastError());
     return BSIM_OK;
 }

@@ -255,20 +255,20 @@ struct GemmTile<float, EPT> {
 
 // Shared-memory strides of the GEMM operands: Lam/W_m rows of LS elements and
 // X-slice rows of XS elements.  The FP64 tiles are read as mma fragments (lane
-// (g, t) = (lane / 4, lane % 4) reads row t, column g of a 4 x 8 block); a row
-// stride of 4 mod 16 doubles puts the 16 lanes of each half-warp on distinct
-// banks.
+// (g, t) = (lane / 4, lane % 4) reads row t, column g (and g + 8) of a block); a
+// row stride of 4 mod 16 doubles puts the 16 lanes of each half-warp on
+// distinct banks.
 template <typename T> struct GemmLayout { static constexpr int LS = 64, XS = kMixCols; };
 template <> struct GemmLayout<double> { static constexpr int LS = 68, XS = kMixCols + 4; };
 
-// FP64 core: warp w computes rows 8*(w/2)..+7 and columns 64*(w%2)..+63 of the
-// 64 x kMixCols output chunk as eight 8x8 tiles with mma.sync m8n8k4 (FP64 on
-// the tensor cores' DMMA path), 4 slice rows per instruction.
-__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b)
+// FP64 on the tensor cores' DMMA path: 16x8 tile += 16x4 A (rows g, g + 8 of column t in lane (g, t)) x 4x8 B
+// (row t, column g); the accumulator holds rows g and g + 8, columns 2t, 2t + 1.
+__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double2 a, double b)
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(c0), "+d"(c1)
-                 : "d"(a), "d"(b));
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, "
+                 "{%0, %1, %2, %3};"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a.x), "d"(a.y), "d"(b));
 }
 
 template <typename T, int EPT>
@@ -308,40 +308,48 @@ struct GemmCore {
 
 template <int EPT>
 struct GemmCore<double, EPT> {
-    static_assert(EPT == 4, "16 warps: 8 row blocks x 2 column halves");
-    double c[8][2];
+    // warp w computes rows 16 (w / 4) .. + 15 and columns 32 (w % 4) .. + 31 of the
+    // 64 x kMixCols output chunk as four 16x8 tiles of mma.sync m16n8k4
+    static_assert(EPT == 4, "16 warps: 4 row groups x 4 column quarters");
+    double c[4][4];
     __device__ __forceinline__ void zero()
     {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) c[k][0] = c[k][1] = 0.0;
+        for (int k = 0; k < 4; ++k) c[k][0] = c[k][1] = c[k][2] = c[k][3] = 0.0;
     }
-    __device__ __forceinline__ static bool active(int rows) { return (int)(threadIdx.x >> 6) * 8 < rows; }
+    __device__ __forceinline__ static bool active(int rows) { return (int)(threadIdx.x >> 7) * 16 < rows; }
     template <int LS = GemmLayout<double>::LS>
     __device__ __forceinline__ void step(const double *lam, const double *xs, int f0, int nf)
     {
         constexpr int XS = GemmLayout<double>::XS;
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        const int g = lane >> 2, t = lane & 3, rb = wid >> 1, ch = wid & 1;
-        const double *la = lam + (size_t)(f0 + t) * LS + rb * 8 + g;
-        const double *xb = xs + t * XS + ch * 64 + g;
+        const int g = lane >> 2, t = lane & 3, rg = wid >> 2, cq = wid & 3;
+        const double *la = lam + (size_t)(f0 + t) * LS + rg * 16 + g;
+        const double *xb = xs + t * XS + cq * 32 + g;
         for (int kk = 0; kk < nf; kk += 4) {   // slice rows past nf are zero in X and in Lam
-            const double a = la[(size_t)kk * LS];
-            double b[8];
+            const double2 a = make_double2(la[(size_t)kk * LS], la[(size_t)kk * LS + 8]);
+            double b[4];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) b[k] = xb[kk * XS + 8 * k];
+            for (int k = 0; k < 4; ++k) b[k] = xb[kk * XS + 8 * k];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) dmma_8x8x4(c[k][0], c[k][1], a, b[k]);
+            for (int k = 0; k < 4; ++k) dmma_16x8x4(c[k], a, b[k]);
         }
     }
     __device__ __forceinline__ void store(double *zbase, int W, int rows) const
     {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        const int g = lane >> 2, t = lane & 3, rb = wid >> 1, ch = wid & 1;
-        const int j = rb * 8 + g;
-        if (j >= rows) return;
-        double *zr = zbase + (i64)j * W + ch * 64 + 2 * t;
+        const int g = lane >> 2, t = lane & 3, rg = wid >> 2, cq = wid & 3;
+        const int j = rg * 16 + g;
+        double *zr = zbase + (i64)j * W + cq * 32 + 2 * t;
+        if (j < rows) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) *reinterpret_cast<double2 *>(zr + 8 * k) = make_double2(c[k][0], c[k][1]);
+            for (int k = 0; k < 4; ++k) *reinterpret_cast<double2 *>(zr + 8 * k) = make_double2(c[k][0], c[k][1]);
+        }
+        if (j + 8 < rows) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                *reinterpret_cast<double2 *>(zr + (i64)8 * W + 8 * k) = make_double2(c[k][2], c[k][3]);
+        }
     }
 };
 
@@ -470,15 +478,18 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
 }
 
 // FP64 mixed GEMM with per-warp B fragments.  Warp w owns columns 8w..8w+7 of
-// each 128-column chunk and all 64 output rows (eight 8x8 DMMA tiles, those
-// past the pass's connected rows skipped); lane (g, t) gathers its own B
-// fragment elements X[f0 + 4i + t][8w + g] from the source row (shared memory,
-// or L2 with GROW), a 32-row F slice ahead.  No X slice is shared, so the warps
-// never synchronise inside the loop; Lam_conn (the A fragments, read by every
-// warp) is staged once per CTA, zero-padded to whole 32-row slices.
+// each 128-column chunk and all 64 output rows: four 16x8 tiles of
+// mma.sync m16n8k4 (FP64 on the tensor cores' DMMA path), those past the pass's
+// connected rows skipped; lane (g, t) gathers its own B fragment elements
+// X[f0 + 4i + t][8w + g] from the source row (shared memory, or L2 with GROW),
+// a 32-row F slice ahead.  No X slice is shared, so the warps never
+// synchronise inside the loop.  Lam_conn (the A fragments, read by every warp)
+// is staged once per CTA with rows g and g + 8 of each 16-row tile side by
+// side, so a lane's two A elements of a K step are one 16-byte load.
+constexpr int kDmmaLS = 34;   // double2 per F row: 32 + 2 (2 mod 8: conflict-free 16-byte fragment loads)
 inline size_t mixed_dmma_smem(int ldA, int nF, bool grow)
 {
-    return (grow ? 0 : (size_t)ldA * 8) + (size_t)((nF + 31) & ~31) * GemmLayout<double>::LS * 8 + 2 * kMaxConn * 4;
+    return (grow ? 0 : (size_t)ldA * 8) + (size_t)((nF + 31) & ~31) * kDmmaLS * 16 + 2 * kMaxConn * 4;
 }
 
 template <typename Ti, bool GROW>
@@ -486,14 +497,14 @@ __global__ void __launch_bounds__(512, 1)
 mixed_dmma_kernel(const MixedArgs P, const Ti *__restrict__ astr, const double *__restrict__ ct,
                   double *__restrict__ Z, int z0, int W, int jbase)
 {
-    constexpr int NT = 512, LS = GemmLayout<double>::LS;
+    constexpr int NT = 512;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.nF, M = P.M;
     const int Kp = (K + 31) & ~31;
-    double *srow = reinterpret_cast<double *>(smem_raw);          // [ldA] unless GROW
-    double *lam = srow + (GROW ? 0 : P.ldA);                       // [Kp][LS], rows past K zero
-    int *conn = reinterpret_cast<int *>(lam + (size_t)Kp * LS);   // [kMaxConn]
-    int *sgn = conn + kMaxConn;                                    // [kMaxConn]
+    double *srow = reinterpret_cast<double *>(smem_raw);            // [ldA] unless GROW
+    double2 *lam = reinterpret_cast<double2 *>(srow + (GROW ? 0 : P.ldA));   // [Kp][kDmmaLS], rows past K zero
+    int *conn = reinterpret_cast<int *>(lam + (size_t)Kp * kDmmaLS);        // [kMaxConn]
+    int *sgn = conn + kMaxConn;                                              // [kMaxConn]
     __shared__ int wcnt[NT / 32], cnt;
     const int a = blockIdx.x;
     const int m = connected_excitations<NT>(P, (u64)astr[a], conn, sgn, wcnt, &cnt);
@@ -506,14 +517,21 @@ mixed_dmma_kernel(const MixedArgs P, const Ti *__restrict__ astr, const double *
         const int n16 = P.ldA / 2;
         for (int i = threadIdx.x; i < n16; i += NT) dst[i] = __ldg(src + i);
     }
+    // lam[f][8 rb + g] = (Lam_conn[16 rb + g][f], Lam_conn[16 rb + g + 8][f])
     const double *Lam = static_cast<const double *>(P.Lam);
-    for (int i = threadIdx.x; i < Kp * LS; i += NT) {
-        const int f = i / LS, j = i % LS;
-        lam[i] = (j < jm && f < K) ? (double)sgn[jbase + j] * Lam[(i64)conn[jbase + j] * K + f] : 0.0;
+    for (int i = threadIdx.x; i < Kp * kDmmaLS; i += NT) {
+        const int f = i / kDmmaLS, q = i % kDmmaLS;
+        const int j0 = (q >> 3) * 16 + (q & 7), j1 = j0 + 8;
+        double2 v = make_double2(0.0, 0.0);
+        if (q < 32 && f < K) {
+            if (j0 < jm) v.x = (double)sgn[jbase + j0] * Lam[(i64)conn[jbase + j0] * K + f];
+            if (j1 < jm) v.y = (double)sgn[jbase + j1] * Lam[(i64)conn[jbase + j1] * K + f];
+        }
+        lam[i] = v;
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-    const int nrb = (jm + 7) >> 3;   // 8-row blocks holding connected rows
+    const int nrb = (jm + 15) >> 4;   // 16-row tiles holding connected rows
     const int zend = min(P.cend, z0 + W);
     const int ncb = (zend - z0 + kMixCols - 1) / kMixCols;
     const int nfc = (K + 31) / 32;
@@ -531,9 +549,9 @@ mixed_dmma_kernel(const MixedArgs P, const Ti *__restrict__ astr, const double *
             for (int i = 0; i < 8; ++i) gv[i] = gp[i] >= 0 ? __ldg(grow + (gp[i] >> 1)) : 0.0;
         }
     };
-    double c[8][2];
+    double c[4][4];
 #pragma unroll
-    for (int rb = 0; rb < 8; ++rb) c[rb][0] = c[rb][1] = 0.0;
+    for (int rb = 0; rb < 4; ++rb) c[rb][0] = c[rb][1] = c[rb][2] = c[rb][3] = 0.0;
     if (nsteps > 0) load(0);
     for (int step = 0; step < nsteps; ++step) {
         const int cbi = step / nfc, fci = step % nfc;
@@ -548,22 +566,24 @@ mixed_dmma_kernel(const MixedArgs P, const Ti *__restrict__ astr, const double *
             x[i] = (gg >= 0 && (gg & 1)) ? -v : v;
         }
         if (step + 1 < nsteps) load(step + 1);
-        const double *la = lam + (size_t)(f0 + t) * LS + g;
+        const double2 *la = lam + (size_t)(f0 + t) * kDmmaLS + g;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             if (i < nk) {
 #pragma unroll
-                for (int rb = 0; rb < 8; ++rb)
-                    if (rb < nrb) dmma_8x8x4(c[rb][0], c[rb][1], la[(size_t)(4 * i) * LS + rb * 8], x[i]);
+                for (int rb = 0; rb < 4; ++rb)
+                    if (rb < nrb) dmma_16x8x4(c[rb], la[(size_t)(4 * i) * kDmmaLS + rb * 8], x[i]);
             }
         }
         if (fci == nfc - 1) {
             double *zr = zchunk(Z, a, M, W, cbi) + (jbase + g) * kMixCols + 8 * wid + 2 * t;
 #pragma unroll
-            for (int rb = 0; rb < 8; ++rb) {
-                if (rb < nrb && rb * 8 + g < jm)
-                    *reinterpret_cast<double2 *>(zr + rb * 8 * kMixCols) = make_double2(c[rb][0], c[rb][1]);
-                c[rb][0] = c[rb][1] = 0.0;
+            for (int rb = 0; rb < 4; ++rb) {
+                if (rb < nrb && rb * 16 + g < jm)
+                    *reinterpret_cast<double2 *>(zr + rb * 16 * kMixCols) = make_double2(c[rb][0], c[rb][1]);
+                if (rb < nrb && rb * 16 + g + 8 < jm)
+                    *reinterpret_cast<double2 *>(zr + (rb * 16 + 8) * kMixCols) = make_double2(c[rb][2], c[rb][3]);
+                c[rb][0] = c[rb][1] = c[rb][2] = c[rb][3] = 0.0;
             }
         }
     }
@@ -740,7 +760,7 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
 
 // FP64 intermediate-string GEMM with per-warp B fragments (as mixed_dmma_kernel):
 // warp w owns columns 8w..8w+7 of each 128-column chunk and all K output rows
-// (ceil(K / 8) <= 9 DMMA tiles); lane (g, t) loads its B fragment elements
+// (ceil(K / 16) <= 5 m16n8k4 tiles); lane (g, t) loads its B fragment elements
 // X[f0 + 4i + t][8w + g] = c~[row][col] straight from global memory (L2), a
 // 32-row K slice ahead, so the main loop has no block barrier; W_m (the A
 // fragments, k-major rows of kRiLS elements, zero past K) is staged once.
@@ -750,7 +770,7 @@ inline size_t ri_dmma_smem(int nU) { return (size_t)((nU + 31) & ~31) * kRiLS * 
 __global__ void __launch_bounds__(512, 1)
 ri_dmma_kernel(const RIArgs P, const double *__restrict__ in, double *__restrict__ Z, int z0, int W)
 {
-    constexpr int NT = 512, MAXRB = (kRiMaxU + 7) / 8;
+    constexpr int NT = 512, MAXRB = (kRiMaxU + 15) / 16;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.nU, Kp = (K + 31) & ~31;
     double *wm = reinterpret_cast<double *>(smem_raw);                       // [Kp][kRiLS]
@@ -770,7 +790,7 @@ ri_dmma_kernel(const RIArgs P, const double *__restrict__ in, double *__restrict
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-    const int nrb = (K + 7) >> 3;
+    const int nrb = (K + 15) >> 4;
     const int zend = min(P.cend, z0 + W);
     const int ncb = (zend - z0 + kMixCols - 1) / kMixCols;
     const int nfc = (K + 31) / 32;
@@ -785,9 +805,9 @@ ri_dmma_kernel(const RIArgs P, const double *__restrict__ in, double *__restrict
             xp[i] = (r < K && c < P.ld_in) ? __ldg(in + soff[r] + c) : 0.0;
         }
     };
-    double c_[MAXRB][2];
+    double c_[MAXRB][4];
 #pragma unroll
-    for (int rb = 0; rb < MAXRB; ++rb) c_[rb][0] = c_[rb][1] = 0.0;
+    for (int rb = 0; rb < MAXRB; ++rb) c_[rb][0] = c_[rb][1] = c_[rb][2] = c_[rb][3] = 0.0;
     if (nsteps > 0) load(0);
     for (int step = 0; step < nsteps; ++step) {
         const int cbi = step / nfc, fci = step % nfc;
@@ -802,16 +822,20 @@ ri_dmma_kernel(const RIArgs P, const double *__restrict__ in, double *__restrict
             if (i < nk) {
 #pragma unroll
                 for (int rb = 0; rb < MAXRB; ++rb)
-                    if (rb < nrb) dmma_8x8x4(c_[rb][0], c_[rb][1], la[(size_t)(4 * i) * kRiLS + rb * 8], x[i]);
+                    if (rb < nrb)
+                        dmma_16x8x4(c_[rb], make_double2(la[(size_t)(4 * i) * kRiLS + rb * 16],
+                                                         la[(size_t)(4 * i) * kRiLS + rb * 16 + 8]), x[i]);
             }
         }
         if (fci == nfc - 1) {
             double *zr = zchunk(Z, m, K, W, cbi) + g * kMixCols + 8 * wid + 2 * t;
 #pragma unroll
             for (int rb = 0; rb < MAXRB; ++rb) {
-                if (rb < nrb && rb * 8 + g < K)
-                    *reinterpret_cast<double2 *>(zr + rb * 8 * kMixCols) = make_double2(c_[rb][0], c_[rb][1]);
-                c_[rb][0] = c_[rb][1] = 0.0;
+                if (rb < nrb && rb * 16 + g < K)
+                    *reinterpret_cast<double2 *>(zr + rb * 16 * kMixCols) = make_double2(c_[rb][0], c_[rb][1]);
+                if (rb < nrb && rb * 16 + g + 8 < K)
+                    *reinterpret_cast<double2 *>(zr + (rb * 16 + 8) * kMixCols) = make_double2(c_[rb][2], c_[rb][3]);
+                c_[rb][0] = c_[rb][1] = c_[rb][2] = c_[rb][3] = 0.0;
             }
         }
     }

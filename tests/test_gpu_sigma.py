@@ -222,12 +222,13 @@ def test_mixed_gemm_source_row_in_global_memory(cuda, oracle, monkeypatch, mixed
 @pytest.mark.parametrize("norb,na,nb", [(11, 5, 5), (12, 6, 5), (13, 3, 4)])
 @pytest.mark.parametrize("row_on_chip", [True, False])
 def test_fp64_mixed_gemm_kernels_agree(cuda, oracle, monkeypatch, norb, na, nb, row_on_chip):
-    """The FP64 mixed GEMM with per-warp B fragments (default) against the kernel
-    with a shared X slice (BSIM_MIXED_DMMA=0): the same DMMA sums in the same
-    order per output tile, so the same bits; both against the oracle at
+    """The FP64 mixed GEMM with per-warp B fragments (default; m16n8k4 DMMA tiles)
+    against the kernel with a shared X slice (BSIM_MIXED_DMMA=0; m8n8k4 tiles):
+    the same products in the same K order, to 1e-13 x max|sigma| (the two MMA
+    shapes may round their 4-term sums differently); both against the oracle at
     1e-12 x max|sigma|.  row_on_chip False reads the source row from global
     memory (BSIM_MIXED_ROW_SMEM=1).  Connected rows per pass 30, 36 / 30 and 30:
-    partial 8-row blocks."""
+    partial 16-row tiles."""
     from binsim_b200 import cuotf, network as nw
     net = nw.hamiltonian_network(norb, seed=9)
     B = cuotf.CuBasis(norb, na, nb)
@@ -241,8 +242,8 @@ def test_fp64_mixed_gemm_kernels_agree(cuda, oracle, monkeypatch, norb, na, nb, 
     f.hvec(x, y_new)
     monkeypatch.setenv("BSIM_MIXED_DMMA", "0")
     f.hvec(x, y_old)
-    assert cuda.equal(y_new, y_old)
     ref = oracle.hvec(oracle.basis(norb, na, nb), oracle.network(net), xh)
+    assert float((y_new - y_old).abs().max()) <= 1e-13 * np.abs(ref).max()
     assert np.abs(y_new.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
@@ -252,8 +253,8 @@ def test_fp64_intermediate_gemm_kernels_agree(cuda, oracle, monkeypatch, norb, n
     BSIM_RI_DMMA=1; by default it runs only above 64 pairs outside an intermediate)
     against the shared-slice kernel (BSIM_RI_DMMA=0), both against the oracle at
     1e-12 x max|sigma|.  Pairs outside an intermediate 28 / 28, 28 / 36 and 66 / 45;
-    up to 64 the two run the same DMMA sums per tile in the same order (same
-    bits); the shared-slice kernel computes rows 64.. with scalar FMAs."""
+    both run m16n8k4 DMMA tiles over the same K order (the shared-slice kernel
+    computes rows 64.. with scalar FMAs)."""
     from binsim_b200 import cuotf, network as nw
     net = nw.hamiltonian_network(norb, seed=11)
     B = cuotf.CuBasis(norb, na, nb)
@@ -269,8 +270,6 @@ def test_fp64_intermediate_gemm_kernels_agree(cuda, oracle, monkeypatch, norb, n
     f.hvec(x, y_old)
     ref = oracle.hvec(oracle.basis(norb, na, nb), oracle.network(net), xh)
     scale = np.abs(ref).max()
-    if na != 2:
-        assert cuda.equal(y_new, y_old)
     assert float((y_new - y_old).abs().max()) <= 1e-12 * scale
     assert np.abs(y_new.cpu().numpy() - ref).max() <= 1e-12 * scale
 

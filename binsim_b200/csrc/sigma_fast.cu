@@ -271,6 +271,16 @@ __device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double2 a, double b)
                  : "d"(a.x), "d"(a.y), "d"(b));
 }
 
+// The same with K = 8: A rows g, g + 8 of columns t (a01) and t + 4 (a23), B rows
+// t (b.x) and t + 4 (b.y) of column g.
+__device__ __forceinline__ void dmma_16x8x8(double (&c)[4], double2 a01, double2 a23, double2 b)
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+                 "{%0, %1, %2, %3};"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a01.x), "d"(a01.y), "d"(a23.x), "d"(a23.y), "d"(b.x), "d"(b.y));
+}
+
 template <typename T, int EPT>
 struct GemmCore {
     // FP32 bulk: EPT rows x 4 columns per thread with packed f32x2 FMAs
@@ -479,7 +489,7 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
 
 // FP64 mixed GEMM with per-warp B fragments.  Warp w owns columns 8w..8w+7 of
 // each 128-column chunk and all 64 output rows: four 16x8 tiles of
-// mma.sync m16n8k4 (FP64 on the tensor cores' DMMA path), those past the pass's
+// mma.sync m16n8k8 (FP64 on the tensor cores' DMMA path), those past the pass's
 // connected rows skipped; lane (g, t) gathers its own B fragment elements
 // X[f0 + 4i + t][8w + g] from the source row (shared memory, or L2 with GROW),
 // a 32-row F slice ahead.  No X slice is shared, so the warps never
@@ -568,11 +578,13 @@ mixed_dmma_kernel(const MixedArgs P, const Ti *__restrict__ astr, const double *
         if (step + 1 < nsteps) load(step + 1);
         const double2 *la = lam + (size_t)(f0 + t) * kDmmaLS + g;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            if (i < nk) {
+        for (int i = 0; i < 4; ++i) {   // K steps of 8: F rows f0 + 8i + t and f0 + 8i + 4 + t
+            if (2 * i < nk) {
 #pragma unroll
                 for (int rb = 0; rb < 4; ++rb)
-                    if (rb < nrb) dmma_16x8x4(c[rb], la[(size_t)(4 * i) * kDmmaLS + rb * 8], x[i]);
+                    if (rb < nrb)
+                        dmma_16x8x8(c[rb], la[(size_t)(8 * i) * kDmmaLS + rb * 8],
+                                    la[(size_t)(8 * i + 4) * kDmmaLS + rb * 8], make_double2(x[2 * i], x[2 * i + 1]));
             }
         }
         if (fci == nfc - 1) {

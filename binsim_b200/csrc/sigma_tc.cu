@@ -57,7 +57,8 @@ constexpr int kTcThreads = 672;
 constexpr int kTcProdWarps = 16;          // warps 4..19
 constexpr int kTcMmaWarp = 20;
 constexpr int kTcM = 128;                 // columns b per chunk: MMA M
-constexpr int kMixKS = 40;                // F rows per A slice of the mixed product (a multiple of 8)
+constexpr int kMixKS = 48;                // F rows per A slice of the mixed product, row on chip
+constexpr int kMixKSGrow = 40;            // the same, row read from global memory
 constexpr int kMixStages = 2;             // its A stages
 constexpr int kRiStages = 2, kRiRing = 4; // the intermediate product's A stages and copy-ring slots
 constexpr unsigned long long kTcWaitNs = 20000000ull;   // a wait gives up after 20 ms
@@ -109,7 +110,8 @@ __host__ __device__ inline TcLayout tc_layout(uint32_t srow_bytes, int K, int N,
 // mixed product: the connected lists (conn, sgn) in the table area
 __host__ __device__ inline TcLayout mixed_layout(int ldA, int nF, int N, bool grow)
 {
-    return tc_layout(grow ? 0u : (uint32_t)ldA * 4u, nF, N, kMixKS, kMixStages, 2u * kMaxConn * 4u);
+    return tc_layout(grow ? 0u : (uint32_t)ldA * 4u, nF, N, grow ? kMixKSGrow : kMixKS, kMixStages,
+                     2u * kMaxConn * 4u);
 }
 // intermediate product: K = pairs outside the intermediate, slices of KS rows
 // (a multiple of 16), kRiStages A stages and a copy ring of kRiRing slices
@@ -490,6 +492,67 @@ struct GatherSrc {
     __device__ __forceinline__ void finish() {}
 };
 
+// X^T[b][F] = sB_F c~[a'][b ^ F] from the row staged in shared memory, one
+// slice of gather indices prefetched into registers.  A thread's element
+// group is (column b, four F rows 4 kc .. 4 kc + 3): a warp reads the gather
+// indices of 32 consecutive columns of an F row (coalesced), gathers their
+// values from the row (consecutive columns of one F land on few banks), and
+// writes each column's four values, split, as one 16-byte K-major core row of
+// the hi and of the lo stage.
+template <int KS>
+struct GatherColSrc {
+    static constexpr int QI = KS / 16;   // (column, 4 rows) groups per thread and slice
+    static_assert(QI * 16 == KS, "KS a multiple of 16");
+    const int *gidx;
+    const float *row;         // the source row, shared memory
+    unsigned char *ah, *al;   // A stages (hi, lo)
+    uint32_t abytes;
+    int ldG, K, z0, nsl, nq, p;
+    int gp[QI][4];
+    __device__ __forceinline__ void setup(int pw, int lane) { p = pw * 32 + lane; }
+    __device__ __forceinline__ void prefetch(int q)
+    {
+        const int f0 = (q % nsl) * KS, cb = z0 + (q / nsl) * kTcM;
+#pragma unroll
+        for (int i = 0; i < QI; ++i) {
+            const int id = p + 32 * kTcProdWarps * i, kc = id >> 7, b = id & 127;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int f = f0 + 4 * kc + e;
+                gp[i][e] = f < K ? __ldg(gidx + (i64)f * ldG + cb + b) : -1;
+            }
+        }
+    }
+    __device__ __forceinline__ void begin(int n) { nq = n; if (nq > 0) prefetch(0); }
+    __device__ __forceinline__ float value(int g) const
+    {
+        if (g < 0) return 0.f;
+        const float x = row[g >> 1];
+        return (g & 1) ? -x : x;
+    }
+    template <typename Free>
+    __device__ __forceinline__ bool produce(int q, Free &free)
+    {
+        if (!free(q)) return false;
+        unsigned char *hi = ah + (size_t)(q % kMixStages) * abytes, *lo = al + (size_t)(q % kMixStages) * abytes;
+#pragma unroll
+        for (int i = 0; i < QI; ++i) {
+            const int id = p + 32 * kTcProdWarps * i, kc = id >> 7, b = id & 127;
+            float4 h, l;
+            tf32_split(value(gp[i][0]), h.x, l.x);
+            tf32_split(value(gp[i][1]), h.y, l.y);
+            tf32_split(value(gp[i][2]), h.z, l.z);
+            tf32_split(value(gp[i][3]), h.w, l.w);
+            const uint32_t off = a_off<KS>(b, 4 * kc);
+            *reinterpret_cast<float4 *>(hi + off) = h;
+            *reinterpret_cast<float4 *>(lo + off) = l;
+        }
+        if (q + 1 < nq) prefetch(q + 1);
+        return true;
+    }
+    __device__ __forceinline__ void finish() {}
+};
+
 // X^T[b][k] = c~[row_k][b]: whole rows of c~ at the element offsets roff[k]
 // (shared memory), columns past ld and rows past K read as zero.  The rows of a
 // slice are copied with cp.async as they lie (a warp copies one 512-byte row
@@ -599,18 +662,32 @@ mixed_gemm_tc_kernel(const MixedArgs P, const Ti *__restrict__ astr, const float
 
     const int zend = min(P.cend, z0 + W);
     const int ncb = (zend - z0 + kTcM - 1) / kTcM;
-    GatherSrc<kMixKS, GROW> src;
-    src.gidx = P.gidx;
-    src.row = GROW ? ct + (i64)a * P.ldA : srow;
-    src.ldG = P.ldG;
-    src.K = K;
-    src.z0 = z0;
-    src.nsl = (L.kp8 + kMixKS - 1) / kMixKS;
-    src.ah = smem + L.ah;
-    src.al = smem + L.al;
-    src.abytes = L.abytes;
-    tc_pipeline<N, kMixKS, kMixStages>(L, smem, sbase, tmem, ncb, jm, zchunk(Z, a, P.M, W, 0) + jbase * kTcM, P.M,
-                                       src, &abort_flag);
+    float *zrow = zchunk(Z, a, P.M, W, 0) + jbase * kTcM;
+    if constexpr (GROW) {
+        GatherSrc<kMixKSGrow, true> src;
+        src.gidx = P.gidx;
+        src.row = ct + (i64)a * P.ldA;
+        src.ldG = P.ldG;
+        src.K = K;
+        src.z0 = z0;
+        src.nsl = (L.kp8 + kMixKSGrow - 1) / kMixKSGrow;
+        src.ah = smem + L.ah;
+        src.al = smem + L.al;
+        src.abytes = L.abytes;
+        tc_pipeline<N, kMixKSGrow, kMixStages>(L, smem, sbase, tmem, ncb, jm, zrow, P.M, src, &abort_flag);
+    } else {
+        GatherColSrc<kMixKS> src;
+        src.gidx = P.gidx;
+        src.row = srow;
+        src.ldG = P.ldG;
+        src.K = K;
+        src.z0 = z0;
+        src.nsl = (L.kp8 + kMixKS - 1) / kMixKS;
+        src.ah = smem + L.ah;
+        src.al = smem + L.al;
+        src.abytes = L.abytes;
+        tc_pipeline<N, kMixKS, kMixStages>(L, smem, sbase, tmem, ncb, jm, zrow, P.M, src, &abort_flag);
+    }
     tc_end<N>(tmem);
 }
 

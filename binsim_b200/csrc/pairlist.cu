@@ -489,9 +489,9 @@ int pair_list_launch(const DevBasis<Ti> *B, const DevNet<Ti> *N, i64 gidx, PairA
     }
     ListArgs A{B->nb[0], d.y, d.w, G.rank, G.nza, G.nzb, d.x >= 0 ? P->d_alist + d.x : nullptr,
                d.z >= 0 ? P->d_blist + d.z : nullptr, G.za_off, G.zb_off, G.wa_off, G.wb_off};
-    // 16 alpha entries per tile (per pair of barriers), the loads of each group
+    // 32 alpha entries per tile (per pair of barriers), the loads of each group
     // of 4 pairs issued before their stores, 3 CTAs per SM
-    constexpr int kRT = 16;
+    constexpr int kRT = 32;
     const i64 cap = OP == kPairExpm ? (i64)148 * 64 : std::max<i64>(1, max_slots);
     const i64 tiles = (i64)((d.y + kRT - 1) / kRT) * ((d.w + kListCols - 1) / kListCols);
     const unsigned grid = (unsigned)std::min<i64>(tiles, cap);

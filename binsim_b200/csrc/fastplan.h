@@ -132,7 +132,7 @@ inline size_t ri_ls(size_t elem) { return gemm_ls(elem) + 8; }
 constexpr int kRiStagesHost = 3;   // X slices in the cp.async ring of the intermediate-string GEMM
 inline size_t ri_smem_bytes(int nU, size_t elem)
 {
-    return (((size_t)nU + 3) & ~size_t(3)) * ri_ls(elem) * elem + kRiStagesHost * 32 * gemm_xs(elem) * elem +
+    return (((size_t)nU + 7) & ~size_t(7)) * ri_ls(elem) * elem + kRiStagesHost * 32 * gemm_xs(elem) * elem +
            kRiMaxU * 8;
 }
 
@@ -146,7 +146,7 @@ constexpr size_t kSmemMax = 227 * 1024;
 // whose Lam_conn rows are 80 elements long)
 inline size_t mixed_smem_bytes(int nB, int nF, size_t elem, bool stream, bool grow, int rows = 64)
 {
-    const size_t lam_rows = stream ? 32 : (((size_t)nF + 3) & ~size_t(3));
+    const size_t lam_rows = stream ? 32 : (((size_t)nF + 7) & ~size_t(7));
     const size_t ls = rows > 64 ? (size_t)rows : gemm_ls(elem);
     return (grow ? 0 : (((size_t)nB + 7) & ~size_t(7)) * elem) + lam_rows * ls * elem +
            32 * gemm_xs(elem) * elem + 2 * kMaxConn * 4;

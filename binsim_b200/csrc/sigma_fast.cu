@@ -319,7 +319,7 @@ struct GemmCore {
 template <int EPT>
 struct GemmCore<double, EPT> {
     // warp w computes rows 16 (w / 4) .. + 15 and columns 32 (w % 4) .. + 31 of the
-    // 64 x kMixCols output chunk as four 16x8 tiles of mma.sync m16n8k4
+    // 64 x kMixCols output chunk as four 16x8 tiles of mma.sync m16n8k8
     static_assert(EPT == 4, "16 warps: 4 row groups x 4 column quarters");
     double c[4][4];
     __device__ __forceinline__ void zero()
@@ -336,13 +336,14 @@ struct GemmCore<double, EPT> {
         const int g = lane >> 2, t = lane & 3, rg = wid >> 2, cq = wid & 3;
         const double *la = lam + (size_t)(f0 + t) * LS + rg * 16 + g;
         const double *xb = xs + t * XS + cq * 32 + g;
-        for (int kk = 0; kk < nf; kk += 4) {   // slice rows past nf are zero in X and in Lam
-            const double2 a = make_double2(la[(size_t)kk * LS], la[(size_t)kk * LS + 8]);
-            double b[4];
+        for (int kk = 0; kk < nf; kk += 8) {   // slice rows past nf are zero in X and in Lam
+            const double2 a01 = make_double2(la[(size_t)kk * LS], la[(size_t)kk * LS + 8]);
+            const double2 a23 = make_double2(la[(size_t)(kk + 4) * LS], la[(size_t)(kk + 4) * LS + 8]);
+            double2 b[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) b[k] = xb[kk * XS + 8 * k];
+            for (int k = 0; k < 4; ++k) b[k] = make_double2(xb[kk * XS + 8 * k], xb[(kk + 4) * XS + 8 * k]);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) dmma_16x8x4(c[k], a, b[k]);
+            for (int k = 0; k < 4; ++k) dmma_16x8x8(c[k], a01, a23, b[k]);
         }
     }
     __device__ __forceinline__ void store(double *zbase, int W, int rows) const
@@ -386,7 +387,7 @@ mixed_gemm_kernel(const MixedArgs P, const Ti *__restrict__ astr, const T *__res
     const int K = P.nF, M = P.M;
     T *srow = reinterpret_cast<T *>(smem_raw);                    // [ldA] unless GROW
     constexpr int LS = ROWS > 64 ? ROWS : GemmLayout<T>::LS, XS = GemmLayout<T>::XS;
-    const int Kp = (K + 3) & ~3;
+    const int Kp = (K + 7) & ~7;   // whole K steps of 8 (FP64 m16n8k8), rows past K zero
     T *lam = srow + (GROW ? 0 : P.ldA);                            // [Kp or 32][LS], rows past K zero
     T *xs = lam + (size_t)(STREAM ? 32 : Kp) * LS;                 // [32][XS]
     int *conn = reinterpret_cast<int *>(xs + 32 * XS);             // [kMaxConn]
@@ -683,7 +684,7 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.nU;
     constexpr int LS = GemmLayout<T>::LS + 8, XS = GemmLayout<T>::XS;
-    const int Kp = (K + 3) & ~3;
+    const int Kp = (K + 7) & ~7;   // whole K steps of 8 (FP64 m16n8k8), rows past K zero
     T *wm = reinterpret_cast<T *>(smem_raw);                          // [Kp][LS], rows >= K zero
     T *xs = wm + (size_t)Kp * LS;                                      // [kRiStages][32][XS]
     long long *soff = reinterpret_cast<long long *>(xs + kRiStages * 32 * XS);   // [kRiMaxU]

@@ -331,8 +331,9 @@ def sigma_roofline(net, pairs, cfg, dim, stages, hbm, fp64_peak, world, ms, dmma
             if dense_total and dmma_peak else None,
             "note": "dominant kernel of the structured sigma, timed live per launch with CUDA events; achieved = "
                     "its compulsory HBM bytes per launch / launch time, of the measured HBM copy peak; the kernel "
-                    "is bound by FP64 issue and shared-memory gathers, see fp64_frac_of_measured_fma_peak; traffic "
-                    "= ncu dram bytes of a 15-orbital launch scaled by determinants per launch"}
+                    "is bound by the tensor cores' FP64 (DMMA) pipe, see dense_frac_of_measured_dmma_peak (the dense "
+                    "GEMM as executed against the measured DMMA peak); traffic = ncu dram bytes of a 15-orbital "
+                    "launch scaled by determinants per launch"}
     return roof, launches
 
 

@@ -773,7 +773,7 @@ ri_gemm_kernel(const RIArgs P, const T *__restrict__ in, T *__restrict__ Z, int 
 
 // FP64 intermediate-string GEMM with per-warp B fragments (as mixed_dmma_kernel):
 // warp w owns columns 8w..8w+7 of each 128-column chunk and all K output rows
-// (ceil(K / 16) <= 5 m16n8k4 tiles); lane (g, t) loads its B fragment elements
+// (ceil(K / 16) <= 5 m16n8k8 row tiles); lane (g, t) loads its B fragment elements
 // X[f0 + 4i + t][8w + g] = c~[row][col] straight from global memory (L2), a
 // 32-row K slice ahead, so the main loop has no block barrier; W_m (the A
 // fragments, k-major rows of kRiLS elements, zero past K) is staged once.
@@ -831,13 +831,25 @@ ri_dmma_kernel(const RIArgs P, const double *__restrict__ in, double *__restrict
         if (step + 1 < nsteps) load(step + 1);
         const double *la = wm + (size_t)(f0 + t) * kRiLS + g;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            if (i < nk) {
+        for (int i = 0; i < 4; ++i) {
+            // K steps of 8 (rows f0 + 8i + t and f0 + 8i + 4 + t); an odd last
+            // group of 4 rows takes one step of 4
+            if (2 * i + 1 < nk) {
 #pragma unroll
                 for (int rb = 0; rb < MAXRB; ++rb)
                     if (rb < nrb)
-                        dmma_16x8x4(c_[rb], make_double2(la[(size_t)(4 * i) * kRiLS + rb * 16],
-                                                         la[(size_t)(4 * i) * kRiLS + rb * 16 + 8]), x[i]);
+                        dmma_16x8x8(c_[rb],
+                                    make_double2(la[(size_t)(8 * i) * kRiLS + rb * 16],
+                                                 la[(size_t)(8 * i) * kRiLS + rb * 16 + 8]),
+                                    make_double2(la[(size_t)(8 * i + 4) * kRiLS + rb * 16],
+                                                 la[(size_t)(8 * i + 4) * kRiLS + rb * 16 + 8]),
+                                    make_double2(x[2 * i], x[2 * i + 1]));
+            } else if (2 * i < nk) {
+#pragma unroll
+                for (int rb = 0; rb < MAXRB; ++rb)
+                    if (rb < nrb)
+                        dmma_16x8x4(c_[rb], make_double2(la[(size_t)(8 * i) * kRiLS + rb * 16],
+                                                         la[(size_t)(8 * i) * kRiLS + rb * 16 + 8]), x[2 * i]);
             }
         }
         if (fci == nfc - 1) {
@@ -1168,15 +1180,13 @@ static int launch_mixed(const DevBasis<Ti> *B, FastPlan<Ti> &P, FastScratch<Ti> 
                      : launch_mixed_shape<Ti, T, EPT, false, false>(B, P, ma, ct, Z, dst, c0, c1, z.w, sh.smem, s, tm);
 }
 
-// BSIM_RI_DMMA selects the FP64 intermediate-string GEMM (read on every call:
-// tests compare the two): "0" always the shared-slice kernel, "1" always the
-// per-warp-fragment kernel, unset the automatic choice (2 = forced, 0 = off,
-// 1 = automatic in the return value)
-static int ri_dmma_mode()
+// BSIM_RI_DMMA=0 sends the FP64 intermediate-string GEMM to the shared-slice
+// kernel instead of the per-warp-fragment one (read on every call: tests
+// compare the two)
+static bool ri_dmma_on()
 {
     const char *e = getenv("BSIM_RI_DMMA");
-    if (!e || !e[0]) return 1;
-    return e[0] == '0' ? 0 : 2;
+    return !(e && e[0] == '0');
 }
 
 // BSIM_RI_TC=0 sends the FP32-bulk intermediate-string GEMM to the CUDA-core
@@ -1206,12 +1216,10 @@ static int launch_ri(const RISide &R, const T *in, int ld_in, double *out, int l
     BSIM_CUDA(cudaFuncSetAttribute(ri_gemm_kernel<T, EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     T *Z = static_cast<T *>(z.p);
     if constexpr (sizeof(T) == 8) {
-        // FP64 with more than 64 pairs outside an intermediate (18 orbitals, 8
-        // electrons: 66): per-warp B fragments, all rows on the DMMA path
-        // (measured: 676 against 742 ms per sigma at 18o; with <= 64 pairs the
-        // shared-slice kernel is faster, 50 against 56 ms at 16o)
-        if (ri_dmma_mode() != 0 && (R.nU > 64 || ri_dmma_mode() == 2) && R.nU <= kRiMaxU &&
-            ri_dmma_smem(R.nU) <= kSmemMax) {
+        // FP64: per-warp B fragments, all rows on the DMMA path (measured per
+        // sigma: 45.5 against 49.7 ms at 16o, 712 against 772 ms at 18o for
+        // the shared-slice kernel)
+        if (ri_dmma_on() && R.nU <= kRiMaxU && ri_dmma_smem(R.nU) <= kSmemMax) {
             const size_t sm = ri_dmma_smem(R.nU);
             BSIM_CUDA(cudaFuncSetAttribute(ri_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             for (int z0 = c0; z0 < c1; z0 += (int)Wz) {

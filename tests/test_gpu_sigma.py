@@ -249,12 +249,12 @@ def test_fp64_mixed_gemm_kernels_agree(cuda, oracle, monkeypatch, norb, na, nb, 
 
 @pytest.mark.parametrize("norb,na,nb", [(11, 5, 5), (12, 6, 5), (12, 2, 4)])
 def test_fp64_intermediate_gemm_kernels_agree(cuda, oracle, monkeypatch, norb, na, nb):
-    """The FP64 intermediate-string GEMM with per-warp B fragments (forced with
-    BSIM_RI_DMMA=1; by default it runs only above 64 pairs outside an intermediate)
+    """The FP64 intermediate-string GEMM with per-warp B fragments (the default)
     against the shared-slice kernel (BSIM_RI_DMMA=0), both against the oracle at
-    1e-12 x max|sigma|.  Pairs outside an intermediate 28 / 28, 28 / 36 and 66 / 45;
-    both run m16n8k4 DMMA tiles over the same K order (the shared-slice kernel
-    computes rows 64.. with scalar FMAs)."""
+    1e-12 x max|sigma|.  Pairs outside an intermediate 28 / 28, 28 / 36 and 66 / 45:
+    the per-warp kernel's m16n8k8 steps with an m16n8k4 step for an odd last group
+    of 4 rows (28, 36, 66) and without one (45); both kernels add over the same K
+    order (the shared-slice kernel computes rows 64.. with scalar FMAs)."""
     from binsim_b200 import cuotf, network as nw
     net = nw.hamiltonian_network(norb, seed=11)
     B = cuotf.CuBasis(norb, na, nb)
@@ -264,7 +264,7 @@ def test_fp64_intermediate_gemm_kernels_agree(cuda, oracle, monkeypatch, norb, n
     xh = np.random.default_rng(norb + 1).normal(size=B.dim)
     x = dev(cuda, xh)
     y_new, y_old = cuda.empty_like(x), cuda.empty_like(x)
-    monkeypatch.setenv("BSIM_RI_DMMA", "1")
+    monkeypatch.delenv("BSIM_RI_DMMA", raising=False)
     f.hvec(x, y_new)
     monkeypatch.setenv("BSIM_RI_DMMA", "0")
     f.hvec(x, y_old)

@@ -144,14 +144,32 @@ pure_rows_kernel(int row_begin, int col_begin, int ncols, int ld_in, const SideC
         const int R = (int)(t.toff_rank & 7);
         const T *tab = ctab + (t.toff_rank & ~7ll) + c;
         double f[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int r = 0; r < R; ++r) {
-            T cr[4];
-            load4(tab + (i64)r * ld_in, cr);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) f[k] += t.pa[r] * (double)cr[k];
-        }
         T v[4];
-        load4(in_c + t.off, v);
+        if constexpr (std::is_same<T, float>::value) {
+            // FP32: the rank loop unrolled to its bound, every table row of the
+            // entry and the source row loaded before the first use (measured per
+            // sigma: 0.143 -> 0.126 ms at 12o, 26.5 -> 26.3 ms at 16o; the FP64
+            // kernel, bound by L1 throughput, went 38.9 -> 43.9 ms at 16o with it)
+            T cr[kSideMaxRank][4];
+#pragma unroll
+            for (int r = 0; r < kSideMaxRank; ++r)
+                if (r < R) load4(tab + (i64)r * ld_in, cr[r]);
+            load4(in_c + t.off, v);
+#pragma unroll
+            for (int r = 0; r < kSideMaxRank; ++r)
+                if (r < R) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) f[k] += t.pa[r] * (double)cr[r][k];
+                }
+        } else {
+            for (int r = 0; r < R; ++r) {
+                T cr[4];
+                load4(tab + (i64)r * ld_in, cr);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) f[k] += t.pa[r] * (double)cr[k];
+            }
+            load4(in_c + t.off, v);
+        }
 #pragma unroll
         for (int k = 0; k < 4; ++k) acc[k] += f[k] * (double)v[k];
     }
